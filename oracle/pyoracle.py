@@ -1,0 +1,469 @@
+"""Test infrastructure: ctypes front-end of the CPU oracle and of the reference.
+
+Two CPU implementations of the YRT-PET projection hot path are reachable from
+here, both used only as checkers (tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py``):
+
+* ``liboracle.so``   -- the restatement in ``oracle/oracle.cpp`` (float mirror
+  of the reference's FP32 order, and an FP64 oracle);
+* ``_ref/libyrtref_harness.so`` -- the YRT-PET 2.0.7 reference library itself,
+  compiled from its own sources by ``oracle/ref.mk`` (present only where that
+  recipe ran).
+
+The product package never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libyrtref_harness.so")
+
+
+class ScannerDesc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in
+                ("axialFOV", "crystalSize_z", "crystalSize_trans",
+                 "crystalDepth", "scannerRadius")] + \
+               [(n, ctypes.c_uint64) for n in
+                ("detsPerRing", "numRings", "numDOI", "maxRingDiff",
+                 "minAngDiff", "detsPerBlock")]
+
+
+class ImageDesc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("nx", "ny", "nz", "nt")] + \
+               [(n, ctypes.c_float) for n in
+                ("length_x", "length_y", "length_z", "off_x", "off_y",
+                 "off_z")]
+
+
+class ProjDesc(ctypes.Structure):
+    _fields_ = [("projector", ctypes.c_int), ("incremental", ctypes.c_int),
+                ("tof_fwhm_ps", ctypes.c_float), ("tof_n_std", ctypes.c_int),
+                ("num_rays", ctypes.c_int), ("crystal_z", ctypes.c_float),
+                ("crystal_trans", ctypes.c_float),
+                ("psf_num_s", ctypes.c_int), ("psf_size", ctypes.c_int),
+                ("psf_s_step", ctypes.c_float),
+                ("psf_k_spacing", ctypes.c_float),
+                ("psf_taps", ctypes.c_void_p), ("threads", ctypes.c_int)]
+
+
+class OsemDesc(ctypes.Structure):
+    _fields_ = [("projector", ctypes.c_int), ("num_rays", ctypes.c_int),
+                ("tof_fwhm_ps", ctypes.c_float), ("tof_n_std", ctypes.c_int),
+                ("iterations", ctypes.c_int), ("subsets", ctypes.c_int),
+                ("threads", ctypes.c_int), ("global_scale", ctypes.c_float),
+                ("hard_threshold", ctypes.c_float), ("listmode", ctypes.c_int)]
+
+
+@dataclass
+class Scanner:
+    """Arguments of the reference ``Scanner`` constructor (Scanner.cpp:102)."""
+    axialFOV: float
+    crystalSize_z: float
+    crystalSize_trans: float
+    crystalDepth: float
+    scannerRadius: float
+    detsPerRing: int
+    numRings: int
+    numDOI: int = 1
+    maxRingDiff: int = 0
+    minAngDiff: int = 1
+    detsPerBlock: int = 1
+
+    def desc(self) -> ScannerDesc:
+        return ScannerDesc(self.axialFOV, self.crystalSize_z,
+                           self.crystalSize_trans, self.crystalDepth,
+                           self.scannerRadius, self.detsPerRing, self.numRings,
+                           self.numDOI, self.maxRingDiff, self.minAngDiff,
+                           self.detsPerBlock)
+
+    @property
+    def num_dets(self) -> int:
+        return self.detsPerRing * self.numRings * self.numDOI
+
+
+@dataclass
+class ImageParams:
+    nx: int
+    ny: int
+    nz: int
+    length_x: float
+    length_y: float
+    length_z: float
+    off_x: float = 0.0
+    off_y: float = 0.0
+    off_z: float = 0.0
+    nt: int = 1
+
+    def desc(self) -> ImageDesc:
+        return ImageDesc(self.nx, self.ny, self.nz, self.nt, self.length_x,
+                         self.length_y, self.length_z, self.off_x, self.off_y,
+                         self.off_z)
+
+    @property
+    def shape(self):
+        return (self.nt, self.nz, self.ny, self.nx)
+
+    @property
+    def num_voxels(self) -> int:
+        return self.nx * self.ny * self.nz
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c(a, dtype):
+    return None if a is None else np.ascontiguousarray(a, dtype=dtype)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        _oracle = ctypes.CDLL(ORACLE_SO)
+        _oracle.orc_siddon_trace_f32.restype = ctypes.c_int64
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_SO)
+        _ref.ref_dd_overlap.restype = ctypes.c_float
+        _ref.ref_dd_overlap.argtypes = [ctypes.c_float] * 4
+        _ref.ref_last_error.restype = ctypes.c_char_p
+        _ref.ref_tof.argtypes = [ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                                 ctypes.c_float, ctypes.c_float,
+                                 ctypes.c_float, ctypes.c_void_p]
+    return _ref
+
+
+def _ref_check(rc):
+    if rc != 0:
+        raise RuntimeError(ref_lib().ref_last_error().decode())
+
+
+@dataclass
+class Proj:
+    """Projector options (reference ProjectorParams subset)."""
+    projector: str = "S"          # "S" Siddon, "DD"
+    incremental: bool = True
+    tof_fwhm_ps: float = 0.0
+    tof_n_std: int = 0
+    num_rays: int = 1
+    crystal_z: float = 0.0
+    crystal_trans: float = 0.0
+    psf_taps: np.ndarray | None = None   # (num_s, size)
+    psf_s_step: float = 0.0
+    psf_k_spacing: float = 0.0
+    threads: int = 8
+
+    def desc(self) -> ProjDesc:
+        taps = self.psf_taps
+        if taps is not None:
+            taps = np.ascontiguousarray(taps, dtype=np.float32)
+            self._taps_keep = taps
+        return ProjDesc(0 if self.projector == "S" else 1,
+                        int(self.incremental), self.tof_fwhm_ps,
+                        self.tof_n_std, self.num_rays, self.crystal_z,
+                        self.crystal_trans,
+                        0 if taps is None else taps.shape[0],
+                        0 if taps is None else taps.shape[1],
+                        self.psf_s_step, self.psf_k_spacing,
+                        None if taps is None else taps.ctypes.data,
+                        self.threads)
+
+
+# ------------------------------------------------------------ oracle calls --
+def scanner_lut(sc: Scanner) -> np.ndarray:
+    out = np.zeros((sc.num_dets, 6), np.float32)
+    oracle_lib().orc_scanner_lut(ctypes.byref(sc.desc()), _p(out))
+    return out
+
+
+def histo3d_dims(sc: Scanner):
+    dims = np.zeros(3, np.uint64)
+    oracle_lib().orc_histo3d_dims(ctypes.byref(sc.desc()), _p(dims))
+    return tuple(int(x) for x in dims)
+
+
+def histo3d_bins(sc: Scanner, d1, d2) -> np.ndarray:
+    d1 = _c(d1, np.uint32)
+    d2 = _c(d2, np.uint32)
+    out = np.zeros(len(d1), np.uint64)
+    oracle_lib().orc_histo3d_bins(ctypes.byref(sc.desc()),
+                                  ctypes.c_uint64(len(d1)), _p(d1), _p(d2),
+                                  _p(out))
+    return out
+
+
+def histo3d_detpairs(sc: Scanner, bins):
+    bins = _c(bins, np.uint64)
+    d1 = np.zeros(len(bins), np.uint32)
+    d2 = np.zeros(len(bins), np.uint32)
+    oracle_lib().orc_histo3d_detpairs(ctypes.byref(sc.desc()),
+                                      ctypes.c_uint64(len(bins)), _p(bins),
+                                      _p(d1), _p(d2))
+    return d1, d2
+
+
+def lm_to_histo3d(sc: Scanner, d1, d2, values=None):
+    d1 = _c(d1, np.uint32)
+    d2 = _c(d2, np.uint32)
+    values = _c(values, np.float32)
+    histo = np.zeros(int(np.prod(histo3d_dims(sc))), np.float32)
+    bad = ctypes.c_uint64()
+    oracle_lib().orc_lm_to_histo3d(ctypes.byref(sc.desc()),
+                                   ctypes.c_uint64(len(d1)), _p(d1), _p(d2),
+                                   _p(values), _p(histo), ctypes.byref(bad))
+    return histo, int(bad.value)
+
+
+def tof_f32(fwhm, nstd, lor_norm, tof, lo, hi):
+    out = np.zeros(6, np.float32)
+    f = ctypes.c_float
+    oracle_lib().orc_tof_f32(f(fwhm), ctypes.c_int(nstd), f(lor_norm), f(tof),
+                             f(lo), f(hi), _p(out))
+    return out
+
+
+def project(ip: ImageParams, pr: Proj, lors, *, image=None, values=None,
+            orients=None, tof=None, frames=None, ray_offsets=None,
+            forward=True, precision="f32"):
+    """Oracle projection. forward: returns values; else returns the image."""
+    lib = oracle_lib()
+    lors = _c(lors, np.float32)
+    n = len(lors)
+    orients = _c(orients, np.float32)
+    tof = _c(tof, np.float32)
+    frames = _c(frames, np.int32)
+    ray_offsets = _c(ray_offsets, np.float32)
+    dt = np.float32 if precision == "f32" else np.float64
+    fn = lib.orc_project_f32 if precision == "f32" else lib.orc_project_f64
+    pd = pr.desc()
+    if forward:
+        img = _c(image, np.float32)
+        out = np.zeros(n, dt)
+        fn(ctypes.byref(ip.desc()), ctypes.byref(pd), ctypes.c_uint64(n),
+           _p(lors), _p(orients), _p(tof), _p(frames), _p(ray_offsets),
+           _p(img), 1, _p(out), None)
+        return out
+    vals = _c(values, dt)
+    out = np.zeros(ip.shape, dt)
+    fn(ctypes.byref(ip.desc()), ctypes.byref(pd), ctypes.c_uint64(n),
+       _p(lors), _p(orients), _p(tof), _p(frames), _p(ray_offsets), None, 0,
+       _p(vals), _p(out))
+    return out
+
+
+def siddon_trace(ip: ImageParams, pr: Proj, lor, tof=0.0, cap=1 << 16):
+    lor = _c(lor, np.float32)
+    idx = np.zeros(cap, np.int64)
+    w = np.zeros(cap, np.float32)
+    k = oracle_lib().orc_siddon_trace_f32(
+        ctypes.byref(ip.desc()), ctypes.byref(pr.desc()), _p(lor),
+        ctypes.c_float(tof), _p(idx), _p(w), ctypes.c_int64(cap))
+    return idx[:k], w[:k]
+
+
+def em_step_f64(ip: ImageParams, pr: Proj, lors, image, *, orients=None,
+                tof=None, frames=None, ray_offsets=None, measurement=None,
+                sens=None, att=None, additive=None, global_scale=1.0,
+                denom_thr=1e-35):
+    lib = oracle_lib()
+    lors = _c(lors, np.float32)
+    args = [_c(a, np.float32) for a in
+            (orients, tof)] + [_c(frames, np.int32), _c(ray_offsets,
+                                                          np.float32)]
+    extra = [_c(a, np.float32) for a in (measurement, sens, att, additive)]
+    img = _c(image, np.float32)
+    out = np.zeros(ip.shape, np.float64)
+    lib.orc_em_step_f64(ctypes.byref(ip.desc()), ctypes.byref(pr.desc()),
+                        ctypes.c_uint64(len(lors)), _p(lors),
+                        *[_p(a) for a in args], *[_p(a) for a in extra],
+                        ctypes.c_float(global_scale), ctypes.c_float(denom_thr),
+                        _p(img), _p(out))
+    return out
+
+
+def lors_from_detpairs(lut: np.ndarray, d1, d2):
+    """LOR endpoints (ProjectionData::getLOR without motion) and orientations."""
+    d1 = np.asarray(d1, np.int64)
+    d2 = np.asarray(d2, np.int64)
+    lors = np.concatenate([lut[d1, :3], lut[d2, :3]], axis=1)
+    ori = np.concatenate([lut[d1, 3:], lut[d2, 3:]], axis=1)
+    return np.ascontiguousarray(lors), np.ascontiguousarray(ori)
+
+
+# --------------------------------------------------------- reference calls --
+def ref_scanner_lut(sc: Scanner) -> np.ndarray:
+    out = np.zeros((sc.num_dets, 6), np.float32)
+    _ref_check(ref_lib().ref_scanner_lut(ctypes.byref(sc.desc()), _p(out)))
+    return out
+
+
+def ref_histo3d_dims(sc: Scanner):
+    dims = np.zeros(3, np.uint64)
+    _ref_check(ref_lib().ref_histo3d_dims(ctypes.byref(sc.desc()), _p(dims)))
+    return tuple(int(x) for x in dims)
+
+
+def ref_histo3d_bins(sc: Scanner, d1, d2):
+    d1 = _c(d1, np.uint32)
+    d2 = _c(d2, np.uint32)
+    out = np.zeros(len(d1), np.uint64)
+    _ref_check(ref_lib().ref_histo3d_bins(ctypes.byref(sc.desc()),
+                                          ctypes.c_uint64(len(d1)), _p(d1),
+                                          _p(d2), _p(out)))
+    return out
+
+
+def ref_histo3d_detpairs(sc: Scanner, bins):
+    bins = _c(bins, np.uint64)
+    d1 = np.zeros(len(bins), np.uint32)
+    d2 = np.zeros(len(bins), np.uint32)
+    _ref_check(ref_lib().ref_histo3d_detpairs(ctypes.byref(sc.desc()),
+                                              ctypes.c_uint64(len(bins)),
+                                              _p(bins), _p(d1), _p(d2)))
+    return d1, d2
+
+
+def ref_tof(fwhm, nstd, lor_norm, tof, lo, hi):
+    out = np.zeros(6, np.float32)
+    ref_lib().ref_tof(fwhm, nstd, lor_norm, tof, lo, hi, _p(out))
+    return out
+
+
+def ref_siddon(sc: Scanner, ip: ImageParams, lors, *, image=None, values=None,
+               orients=None, tof=None, tof_fwhm_ps=0.0, tof_n_std=0,
+               frames=None, num_rays=1, forward=True, incremental=True,
+               threads=8):
+    lors = _c(lors, np.float32)
+    n = len(lors)
+    orients = _c(orients, np.float32)
+    tof = _c(tof, np.float32)
+    frames = _c(frames, np.int32)
+    if forward:
+        img = np.ascontiguousarray(image, np.float32).copy()
+        vals = np.zeros(n, np.float32)
+    else:
+        img = np.zeros(ip.shape, np.float32)
+        vals = np.ascontiguousarray(values, np.float32).copy()
+    _ref_check(ref_lib().ref_siddon(
+        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), _p(img),
+        ctypes.c_uint64(n), _p(lors), _p(orients), _p(tof),
+        ctypes.c_float(tof_fwhm_ps), ctypes.c_int(tof_n_std), _p(frames),
+        ctypes.c_int(num_rays), ctypes.c_int(int(forward)),
+        ctypes.c_int(int(incremental)), ctypes.c_int(threads), _p(vals)))
+    return vals if forward else img
+
+
+def ref_dd(sc: Scanner, ip: ImageParams, lors, orients, *, image=None,
+           values=None, tof=None, tof_fwhm_ps=0.0, tof_n_std=0, psf_csv=None,
+           forward=True, threads=8):
+    lors = _c(lors, np.float32)
+    n = len(lors)
+    orients = _c(orients, np.float32)
+    tof = _c(tof, np.float32)
+    if forward:
+        img = np.ascontiguousarray(image, np.float32).copy()
+        vals = np.zeros(n, np.float32)
+    else:
+        img = np.zeros(ip.shape, np.float32)
+        vals = np.ascontiguousarray(values, np.float32).copy()
+    psf = None if psf_csv is None else psf_csv.encode()
+    _ref_check(ref_lib().ref_dd(
+        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), _p(img),
+        ctypes.c_uint64(n), _p(lors), _p(orients), _p(tof),
+        ctypes.c_float(tof_fwhm_ps), ctypes.c_int(tof_n_std), psf,
+        ctypes.c_int(int(forward)), ctypes.c_int(threads), _p(vals)))
+    return vals if forward else img
+
+
+def ref_dd_overlap(p0, p1, d0, d1) -> float:
+    return ref_lib().ref_dd_overlap(p0, p1, d0, d1)
+
+
+def ref_lm_to_histo3d(sc: Scanner, d1, d2, threads=8):
+    d1 = _c(d1, np.uint32)
+    d2 = _c(d2, np.uint32)
+    histo = np.zeros(int(np.prod(ref_histo3d_dims(sc))), np.float32)
+    sec = ctypes.c_double()
+    _ref_check(ref_lib().ref_lm_to_histo3d(
+        ctypes.byref(sc.desc()), ctypes.c_uint64(len(d1)), _p(d1), _p(d2),
+        ctypes.c_int(threads), _p(histo), ctypes.byref(sec)))
+    return histo, sec.value
+
+
+def _osem_desc(projector="S", num_rays=1, tof_fwhm_ps=0.0, tof_n_std=0,
+               iterations=1, subsets=1, threads=8, global_scale=1.0,
+               hard_threshold=1.0, listmode=True):
+    return OsemDesc(0 if projector == "S" else 1, num_rays, tof_fwhm_ps,
+                    tof_n_std, iterations, subsets, threads, global_scale,
+                    hard_threshold, int(listmode))
+
+
+def ref_sensitivity(sc: Scanner, ip: ImageParams, *, sens_histo=None,
+                    att_params: ImageParams | None = None, att_image=None,
+                    psf_csv=None, **kw):
+    o = _osem_desc(**kw)
+    nsub = 1 if o.listmode else o.subsets
+    out = np.zeros((nsub, ip.nz, ip.ny, ip.nx), np.float32)
+    sec = ctypes.c_double()
+    sh = _c(sens_histo, np.float32)
+    att = _c(att_image, np.float32)
+    _ref_check(ref_lib().ref_sensitivity(
+        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
+        _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
+        _p(att), None if psf_csv is None else psf_csv.encode(), _p(out),
+        ctypes.byref(sec)))
+    return out, sec.value
+
+
+def ref_osem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, *, tof=None,
+                      randoms=None, sens_histo=None,
+                      att_params: ImageParams | None = None, att_image=None,
+                      **kw):
+    o = _osem_desc(**kw)
+    out = np.zeros(ip.shape, np.float32)
+    sec = ctypes.c_double()
+    d1 = _c(d1, np.uint32)
+    d2 = _c(d2, np.uint32)
+    tof = _c(tof, np.float32)
+    randoms = _c(randoms, np.float32)
+    sh = _c(sens_histo, np.float32)
+    att = _c(att_image, np.float32)
+    s = _c(sens, np.float32)
+    _ref_check(ref_lib().ref_osem_listmode(
+        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
+        _p(s), ctypes.c_uint64(len(d1)), _p(d1), _p(d2), _p(tof), _p(randoms),
+        _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
+        _p(att), _p(out), ctypes.byref(sec)))
+    return out, sec.value
+
+
+def ref_osem_histo3d(sc: Scanner, ip: ImageParams, sens_images, histo, *,
+                     psf_csv=None, **kw):
+    o = _osem_desc(listmode=False, **kw)
+    out = np.zeros((ip.nz, ip.ny, ip.nx), np.float32)
+    sec = ctypes.c_double()
+    s = _c(sens_images, np.float32)
+    h = _c(histo, np.float32)
+    _ref_check(ref_lib().ref_osem_histo3d(
+        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
+        _p(s), _p(h), None if psf_csv is None else psf_csv.encode(), _p(out),
+        ctypes.byref(sec)))
+    return out, sec.value

@@ -1,0 +1,587 @@
+// Test infrastructure, not product code.
+//
+// C-ABI harness over the YRT-PET 2.0.7 reference library compiled from its own
+// sources by oracle/ref.mk.  Every entry point drives the reference's public
+// C++ API on plain arrays so that tests and the CPU-baseline leg of bench.py
+// can run the reference itself on the same inputs as the CUDA path.  Nothing
+// here is linked into or called by the product library.
+//
+// Reference interfaces exercised (paths inside the yrt-pet project):
+//   Scanner ctor + DetRegular LUT   src/datastruct/scanner/Scanner.cpp:102-127,
+//                                   src/datastruct/scanner/DetRegular.cpp:113-183
+//   Histogram3D maps                src/datastruct/projection/Histogram3D.cpp:165-450
+//   ProjectorSiddon                 src/operators/ProjectorSiddon.cpp:239-767
+//   ProjectorDD                     src/operators/ProjectorDD.cpp:185-578
+//   TimeOfFlightHelper              include/yrt-pet/operators/TimeOfFlight.hpp:19-85
+//   convertToHistogram3D            src/utils/ReconstructionUtils.cpp:659-800
+//   OSEM (CPU)                      src/recon/OSEM.cpp:315-365, OSEM_CPU.cpp:127-403
+
+#include "yrt-pet/datastruct/image/Image.hpp"
+#include "yrt-pet/datastruct/projection/Histogram3D.hpp"
+#include "yrt-pet/datastruct/projection/ListModeLUT.hpp"
+#include "yrt-pet/datastruct/projection/UniformHistogram.hpp"
+#include "yrt-pet/datastruct/scanner/Scanner.hpp"
+#include "yrt-pet/operators/ProjectionPsfManager.hpp"
+#include "yrt-pet/operators/ProjectorDD.hpp"
+#include "yrt-pet/operators/ProjectorParams.hpp"
+#include "yrt-pet/operators/ProjectorSiddon.hpp"
+#include "yrt-pet/operators/TimeOfFlight.hpp"
+#include "yrt-pet/recon/OSEM.hpp"
+#include "yrt-pet/utils/Globals.hpp"
+#include "yrt-pet/utils/ReconstructionUtils.hpp"
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace yrt;
+
+extern "C" {
+
+struct ref_scanner_desc
+{
+	float axialFOV, crystalSize_z, crystalSize_trans, crystalDepth,
+	    scannerRadius;
+	uint64_t detsPerRing, numRings, numDOI, maxRingDiff, minAngDiff,
+	    detsPerBlock;
+};
+
+struct ref_image_desc
+{
+	int64_t nx, ny, nz, nt;
+	float length_x, length_y, length_z, off_x, off_y, off_z;
+};
+
+static char g_err[512];
+const char* ref_last_error() { return g_err; }
+}
+
+namespace
+{
+std::unique_ptr<Scanner> makeScanner(const ref_scanner_desc* s)
+{
+	return std::make_unique<Scanner>(
+	    "ref", s->axialFOV, s->crystalSize_z, s->crystalSize_trans,
+	    s->crystalDepth, s->scannerRadius, s->detsPerRing, s->numRings,
+	    s->numDOI, s->maxRingDiff, s->minAngDiff, s->detsPerBlock);
+}
+
+ImageParams makeParams(const ref_image_desc* d)
+{
+	return ImageParams(d->nx, d->ny, d->nz, d->length_x, d->length_y,
+	                   d->length_z, d->off_x, d->off_y, d->off_z, d->nt);
+}
+
+std::unique_ptr<ImageOwned> makeImage(const ref_image_desc* d,
+                                      const float* data)
+{
+	auto img = std::make_unique<ImageOwned>(makeParams(d));
+	img->allocate();
+	const size_t n = d->nx * d->ny * d->nz * d->nt;
+	if (data)
+		std::memcpy(img->getRawPointer(), data, n * sizeof(float));
+	else
+		img->fill(0.0f);
+	return img;
+}
+
+template <typename F>
+int guarded(F&& f)
+{
+	try
+	{
+		f();
+		return 0;
+	}
+	catch (const std::exception& e)
+	{
+		std::snprintf(g_err, sizeof(g_err), "%s", e.what());
+		return 1;
+	}
+}
+
+template <typename F>
+void parallelFor(size_t n, int threads, F&& f)
+{
+	if (threads <= 1 || n < 1024)
+	{
+		for (size_t i = 0; i < n; i++)
+			f(i, 0);
+		return;
+	}
+	std::vector<std::thread> pool;
+	const size_t chunk = (n + threads - 1) / threads;
+	for (int t = 0; t < threads; t++)
+	{
+		pool.emplace_back(
+		    [&, t]()
+		    {
+			    const size_t b = t * chunk, e = std::min(n, b + chunk);
+			    for (size_t i = b; i < e; i++)
+				    f(i, t);
+		    });
+	}
+	for (auto& th : pool)
+		th.join();
+}
+}  // namespace
+
+extern "C" {
+
+int ref_set_threads(int n)
+{
+	globals::setNumThreads(n);
+	return 0;
+}
+
+// Crystal centres and orientations: out[d*6 + {0..5}] = x,y,z,nx,ny,nz.
+int ref_scanner_lut(const ref_scanner_desc* s, float* out)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    for (size_t d = 0; d < sc->getNumDets(); d++)
+		    {
+			    const Vector3D p = sc->getDetectorPos(d);
+			    const Vector3D n = sc->getDetectorOrient(d);
+			    out[d * 6 + 0] = p.x;
+			    out[d * 6 + 1] = p.y;
+			    out[d * 6 + 2] = p.z;
+			    out[d * 6 + 3] = n.x;
+			    out[d * 6 + 4] = n.y;
+			    out[d * 6 + 5] = n.z;
+		    }
+	    });
+}
+
+int ref_histo3d_dims(const ref_scanner_desc* s, uint64_t* dims)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    Histogram3DOwned h(*sc);
+		    dims[0] = h.numZBin;
+		    dims[1] = h.numPhi;
+		    dims[2] = h.numR;
+	    });
+}
+
+// bin id per detector pair; UINT64_MAX where the reference throws.
+int ref_histo3d_bins(const ref_scanner_desc* s, uint64_t n, const uint32_t* d1,
+                     const uint32_t* d2, uint64_t* bins)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    Histogram3DOwned h(*sc);
+		    for (uint64_t i = 0; i < n; i++)
+		    {
+			    try
+			    {
+				    bins[i] = h.getBinIdFromDetPair(d1[i], d2[i]);
+			    }
+			    catch (const std::exception&)
+			    {
+				    bins[i] = UINT64_MAX;
+			    }
+		    }
+	    });
+}
+
+int ref_histo3d_detpairs(const ref_scanner_desc* s, uint64_t n,
+                         const uint64_t* bins, uint32_t* d1, uint32_t* d2)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    Histogram3DOwned h(*sc);
+		    for (uint64_t i = 0; i < n; i++)
+		    {
+			    const det_pair_t p = h.getDetPairFromBinId(bins[i]);
+			    d1[i] = p.d1;
+			    d2[i] = p.d2;
+		    }
+	    });
+}
+
+int ref_tof(float fwhm_ps, int n_std, float lorNorm, float tof_ps, float lo,
+            float hi, float* out /* weight, amin, amax, sigma, trunc, norm */)
+{
+	TimeOfFlightHelper h(fwhm_ps, n_std);
+	out[0] = h.getWeight(lorNorm, tof_ps, lo, hi);
+	h.getAlphaRange(out[1], out[2], lorNorm, tof_ps);
+	out[3] = h.getSigma();
+	out[4] = h.getTruncWidth();
+	out[5] = h.getNorm();
+	return 0;
+}
+
+// Siddon forward (fwd=1: values[i] = A_i x) or back projection (fwd=0:
+// image += A_i^T values[i]) of n arbitrary LORs (6 floats each).
+// incr=1 uses the projector member path (offset subtracted, multi-ray
+// capable); incr=0 uses the slow explicit instantiation on offset-subtracted
+// LORs (single ray only).
+int ref_siddon(const ref_scanner_desc* s, const ref_image_desc* d, float* image,
+               uint64_t n, const float* lors, const float* orients,
+               const float* tof, float tof_fwhm_ps, int tof_n_std,
+               const int32_t* frames, int num_rays, int fwd, int incr,
+               int threads, float* values)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    auto img = makeImage(d, image);
+		    ProjectorParams pp(*sc);
+		    pp.numRays = num_rays;
+		    globals::setNumThreads(threads);
+		    ProjectorSiddon proj(pp);
+		    std::unique_ptr<TimeOfFlightHelper> tofh;
+		    if (tof)
+			    tofh = std::make_unique<TimeOfFlightHelper>(tof_fwhm_ps,
+			                                                tof_n_std);
+		    const Vector3D off{img->getParams().off_x, img->getParams().off_y,
+		                       img->getParams().off_z};
+		    parallelFor(
+		        n, threads,
+		        [&](size_t i, int tid)
+		        {
+			        Line3D lor{{lors[i * 6 + 0], lors[i * 6 + 1], lors[i * 6 + 2]},
+			                   {lors[i * 6 + 3], lors[i * 6 + 4], lors[i * 6 + 5]}};
+			        Vector3D n1{}, n2{};
+			        if (orients)
+			        {
+				        n1 = {orients[i * 6 + 0], orients[i * 6 + 1],
+				              orients[i * 6 + 2]};
+				        n2 = {orients[i * 6 + 3], orients[i * 6 + 4],
+				              orients[i * 6 + 5]};
+			        }
+			        const frame_t fr = frames ? frames[i] : 0;
+			        const float tv = tof ? tof[i] : 0.f;
+			        if (fr < 0)
+			        {
+				        if (fwd)
+					        values[i] = 0.f;
+				        return;
+			        }
+			        if (incr)
+			        {
+				        if (fwd)
+					        values[i] = proj.forwardProjection(
+					            img.get(), lor, n1, n2, tid, fr, tofh.get(), tv);
+				        else
+					        proj.backProjection(img.get(), lor, n1, n2, values[i],
+					                            tid, fr, tofh.get(), tv);
+			        }
+			        else
+			        {
+				        lor.point1 = lor.point1 - off;
+				        lor.point2 = lor.point2 - off;
+				        float v = fwd ? 0.f : values[i];
+				        if (tofh)
+				        {
+					        if (fwd)
+						        ProjectorSiddon::project_helper<true, false, true,
+						                                        false>(
+						            img.get(), lor, v, nullptr, fr, tid,
+						            tofh.get(), tv);
+					        else
+						        ProjectorSiddon::project_helper<false, false, true,
+						                                        false>(
+						            img.get(), lor, v, nullptr, fr, tid,
+						            tofh.get(), tv);
+				        }
+				        else
+				        {
+					        if (fwd)
+						        ProjectorSiddon::project_helper<true, false,
+						                                        false, false>(
+						            img.get(), lor, v, nullptr, fr, tid);
+					        else
+						        ProjectorSiddon::project_helper<false, false,
+						                                        false, false>(
+						            img.get(), lor, v, nullptr, fr, tid);
+				        }
+				        if (fwd)
+					        values[i] = v;
+			        }
+		        });
+		    if (!fwd)
+		    {
+			    const size_t nv = d->nx * d->ny * d->nz * d->nt;
+			    std::memcpy(image, img->getRawPointer(), nv * sizeof(float));
+		    }
+	    });
+}
+
+// Distance-driven forward/back projection (optionally TOF and with a
+// projection-space PSF read from a CSV file).
+int ref_dd(const ref_scanner_desc* s, const ref_image_desc* d, float* image,
+           uint64_t n, const float* lors, const float* orients, const float* tof,
+           float tof_fwhm_ps, int tof_n_std, const char* psf_csv, int fwd,
+           int threads, float* values)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    auto img = makeImage(d, image);
+		    ProjectorParams pp(*sc);
+		    globals::setNumThreads(threads);
+		    ProjectorDD proj(pp);
+		    std::unique_ptr<TimeOfFlightHelper> tofh;
+		    if (tof)
+			    tofh = std::make_unique<TimeOfFlightHelper>(tof_fwhm_ps,
+			                                                tof_n_std);
+		    std::unique_ptr<ProjectionPsfManager> psf;
+		    if (psf_csv && psf_csv[0])
+			    psf = std::make_unique<ProjectionPsfManager>(psf_csv);
+		    parallelFor(
+		        n, threads,
+		        [&](size_t i, int tid)
+		        {
+			        Line3D lor{{lors[i * 6 + 0], lors[i * 6 + 1], lors[i * 6 + 2]},
+			                   {lors[i * 6 + 3], lors[i * 6 + 4], lors[i * 6 + 5]}};
+			        Vector3D n1{orients[i * 6 + 0], orients[i * 6 + 1],
+			                    orients[i * 6 + 2]};
+			        Vector3D n2{orients[i * 6 + 3], orients[i * 6 + 4],
+			                    orients[i * 6 + 5]};
+			        const float tv = tof ? tof[i] : 0.f;
+			        if (fwd)
+				        values[i] = proj.forwardProjection(img.get(), lor, n1, n2,
+				                                           tid, 0, tofh.get(), tv,
+				                                           psf.get());
+			        else
+				        proj.backProjection(img.get(), lor, n1, n2, values[i], tid,
+				                            0, tofh.get(), tv, psf.get());
+		        });
+		    if (!fwd)
+		    {
+			    const size_t nv = d->nx * d->ny * d->nz * d->nt;
+			    std::memcpy(image, img->getRawPointer(), nv * sizeof(float));
+		    }
+	    });
+}
+
+float ref_dd_overlap(float p0, float p1, float d0, float d1)
+{
+	return ProjectorDD::getOverlap(p0, p1, d0, d1, nullptr, nullptr);
+}
+
+// List-mode -> Histogram3D binning (reference convertToHistogram3D with
+// atomic accumulation).  histo must hold numZBin*numPhi*numR floats.
+int ref_lm_to_histo3d(const ref_scanner_desc* s, uint64_t n, const uint32_t* d1,
+                      const uint32_t* d2, int threads, float* histo,
+                      double* seconds)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    globals::setNumThreads(threads);
+		    ListModeLUTOwned lm(*sc);
+		    lm.allocate(n);
+		    for (uint64_t i = 0; i < n; i++)
+			    lm.setDetectorIdsOfEvent(i, d1[i], d2[i]);
+		    Histogram3DOwned h(*sc);
+		    h.allocate();
+		    h.clearProjections(0.0f);
+		    const auto t0 = std::chrono::steady_clock::now();
+		    util::convertToHistogram3D<true, false>(lm, h);
+		    const auto t1 = std::chrono::steady_clock::now();
+		    if (seconds)
+			    *seconds = std::chrono::duration<double>(t1 - t0).count();
+		    std::memcpy(histo, h.getData().getRawPointer(),
+		                h.count() * sizeof(float));
+	    });
+}
+
+struct ref_osem_desc
+{
+	int projector;  // 0 = Siddon, 1 = DD
+	int num_rays;
+	float tof_fwhm_ps;  // <= 0: no TOF
+	int tof_n_std;
+	int iterations;
+	int subsets;
+	int threads;
+	float global_scale;
+	float hard_threshold;
+	int listmode;  // 1: list-mode events, 0: histogram input
+};
+
+// Sensitivity image (reference OSEM::generateSensitivityImages).  sens_histo
+// (nullable) is a Histogram3D of LOR sensitivities; att_image (nullable) is a
+// hardware attenuation image on att_desc's grid.  Output: one image per subset
+// (list-mode forces a single image), written back to back into out.
+int ref_sensitivity(const ref_scanner_desc* s, const ref_image_desc* d,
+                    const ref_osem_desc* o, const float* sens_histo,
+                    const ref_image_desc* att_desc, const float* att_image,
+                    const char* psf_csv, float* out, double* seconds)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    globals::setNumThreads(o->threads);
+		    auto osem = util::createOSEM(*sc, false);
+		    osem->setImageParams(makeParams(d));
+		    osem->num_OSEM_subsets = o->subsets;
+		    osem->num_MLEM_iterations = o->iterations;
+		    osem->hardThreshold = o->hard_threshold;
+		    osem->setListModeEnabled(o->listmode != 0);
+		    osem->setProjector(o->projector == 0 ? ProjectorType::SIDDON :
+		                                           ProjectorType::DD);
+		    osem->setNumRays(o->num_rays);
+		    if (psf_csv && psf_csv[0])
+			    osem->addProjPSF(psf_csv);
+		    osem->setGlobalScalingFactor(o->global_scale);
+		    std::unique_ptr<Histogram3DOwned> sh;
+		    if (sens_histo)
+		    {
+			    sh = std::make_unique<Histogram3DOwned>(*sc);
+			    sh->allocate();
+			    std::memcpy(sh->getData().getRawPointer(), sens_histo,
+			                sh->count() * sizeof(float));
+			    osem->setSensitivityHistogram(sh.get());
+		    }
+		    std::unique_ptr<ImageOwned> att;
+		    if (att_image)
+		    {
+			    att = makeImage(att_desc, att_image);
+			    osem->setAttenuationImage(att.get());
+		    }
+		    std::vector<std::unique_ptr<Image>> sens;
+		    const auto t0 = std::chrono::steady_clock::now();
+		    osem->generateSensitivityImages(sens, "");
+		    const auto t1 = std::chrono::steady_clock::now();
+		    if (seconds)
+			    *seconds = std::chrono::duration<double>(t1 - t0).count();
+		    const size_t nv = d->nx * d->ny * d->nz;
+		    for (size_t i = 0; i < sens.size(); i++)
+			    std::memcpy(out + i * nv, sens[i]->getRawPointer(),
+			                nv * sizeof(float));
+	    });
+}
+
+// List-mode OSEM with the reference CPU path.  sens: one sensitivity image
+// (list-mode).  Events: detector pairs, optional TOF (ps) and optional
+// per-event additive (randoms) estimates.  Optional sensitivity histogram and
+// attenuation image act as in the reference corrector.  out: nt images.
+int ref_osem_listmode(const ref_scanner_desc* s, const ref_image_desc* d,
+                      const ref_osem_desc* o, const float* sens, uint64_t n,
+                      const uint32_t* d1, const uint32_t* d2, const float* tof,
+                      const float* randoms, const float* sens_histo,
+                      const ref_image_desc* att_desc, const float* att_image,
+                      float* out, double* seconds)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    globals::setNumThreads(o->threads);
+		    ListModeLUTOwned lm(*sc, tof != nullptr, randoms != nullptr);
+		    lm.allocate(n);
+		    for (uint64_t i = 0; i < n; i++)
+		    {
+			    lm.setDetectorIdsOfEvent(i, d1[i], d2[i]);
+			    if (tof)
+				    lm.setTOFValueOfEvent(i, tof[i]);
+			    if (randoms)
+				    lm.setRandomsEstimateOfEvent(i, randoms[i]);
+		    }
+		    auto osem = util::createOSEM(*sc, false);
+		    ImageParams ip = makeParams(d);
+		    osem->setImageParams(ip);
+		    osem->num_OSEM_subsets = o->subsets;
+		    osem->num_MLEM_iterations = o->iterations;
+		    osem->setListModeEnabled(true);
+		    osem->setProjector(o->projector == 0 ? ProjectorType::SIDDON :
+		                                           ProjectorType::DD);
+		    osem->setNumRays(o->num_rays);
+		    if (o->tof_fwhm_ps > 0)
+			    osem->addTOF(o->tof_fwhm_ps, o->tof_n_std);
+		    osem->setGlobalScalingFactor(o->global_scale);
+		    std::unique_ptr<Histogram3DOwned> sh;
+		    if (sens_histo)
+		    {
+			    sh = std::make_unique<Histogram3DOwned>(*sc);
+			    sh->allocate();
+			    std::memcpy(sh->getData().getRawPointer(), sens_histo,
+			                sh->count() * sizeof(float));
+			    osem->setSensitivityHistogram(sh.get());
+		    }
+		    std::unique_ptr<ImageOwned> att;
+		    if (att_image)
+		    {
+			    att = makeImage(att_desc, att_image);
+			    osem->setAttenuationImage(att.get());
+		    }
+		    ref_image_desc sd = *d;
+		    sd.nt = 1;
+		    auto sensImg = makeImage(&sd, sens);
+		    osem->setSensitivityImage(sensImg.get(), 0);
+		    osem->setDataInput(&lm);
+		    const auto t0 = std::chrono::steady_clock::now();
+		    auto res = osem->reconstruct("");
+		    const auto t1 = std::chrono::steady_clock::now();
+		    if (seconds)
+			    *seconds = std::chrono::duration<double>(t1 - t0).count();
+		    const size_t nv = d->nx * d->ny * d->nz * d->nt;
+		    std::memcpy(out, res->getRawPointer(), nv * sizeof(float));
+	    });
+}
+
+// Histogram-mode OSEM (measurements in a Histogram3D).
+int ref_osem_histo3d(const ref_scanner_desc* s, const ref_image_desc* d,
+                     const ref_osem_desc* o, const float* sens_images,
+                     const float* histo, const char* psf_csv, float* out,
+                     double* seconds)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    globals::setNumThreads(o->threads);
+		    Histogram3DOwned h(*sc);
+		    h.allocate();
+		    std::memcpy(h.getData().getRawPointer(), histo,
+		                h.count() * sizeof(float));
+		    auto osem = util::createOSEM(*sc, false);
+		    osem->setImageParams(makeParams(d));
+		    osem->num_OSEM_subsets = o->subsets;
+		    osem->num_MLEM_iterations = o->iterations;
+		    osem->setListModeEnabled(false);
+		    osem->setProjector(o->projector == 0 ? ProjectorType::SIDDON :
+		                                           ProjectorType::DD);
+		    osem->setNumRays(o->num_rays);
+		    if (psf_csv && psf_csv[0])
+			    osem->addProjPSF(psf_csv);
+		    if (o->tof_fwhm_ps > 0)
+			    osem->addTOF(o->tof_fwhm_ps, o->tof_n_std);
+		    const size_t nv = d->nx * d->ny * d->nz;
+		    std::vector<std::unique_ptr<ImageOwned>> sensImgs;
+		    for (int i = 0; i < o->subsets; i++)
+		    {
+			    sensImgs.push_back(makeImage(d, sens_images + i * nv));
+			    osem->setSensitivityImage(sensImgs.back().get(), i);
+		    }
+		    osem->setDataInput(&h);
+		    const auto t0 = std::chrono::steady_clock::now();
+		    auto res = osem->reconstruct("");
+		    const auto t1 = std::chrono::steady_clock::now();
+		    if (seconds)
+			    *seconds = std::chrono::duration<double>(t1 - t0).count();
+		    std::memcpy(out, res->getRawPointer(), nv * sizeof(float));
+	    });
+}
+
+}  // extern "C"
