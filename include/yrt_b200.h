@@ -1,0 +1,326 @@
+/*
+ * yrt_b200.h -- C ABI of the B200 (sm_100a) projection library libyrtb.so.
+ *
+ * Drop-in boundary for YRT-PET's projection hot path: list-mode and
+ * histogram forward/back projectors (Siddon, multi-ray Siddon, distance-driven
+ * with TOF and projection-space PSF), the sensitivity image and the OSEM
+ * multiplicative update.  Plain pointers and sizes only; no C++ or torch types
+ * cross this boundary and no exception escapes it.
+ *
+ * Conventions
+ *  - Pointers named d_* are device pointers owned by the caller (ImageDevice
+ *    buffers, torch tensors, cudaMalloc'd arrays).  Handles own only their
+ *    internal tables (detector LUT, PSF taps, histogram maps).
+ *  - Images are float32, frame-major [t][z][y][x] (the reference Image
+ *    layout, include/yrt-pet/datastruct/image/Image.hpp).
+ *  - Every call enqueues work on the given stream and returns without
+ *    synchronising, except where stated.
+ *  - Return value: YRTB_OK or an error code; yrtb_last_error() gives the
+ *    message of the last failing call on the calling thread.
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the yrt-pet project).
+ */
+#ifndef YRT_B200_H
+#define YRT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int yrtb_status;
+#define YRTB_OK 0
+#define YRTB_ERR_ARGUMENT 1     /* invalid argument (reference: ASSERT_MSG -> std::runtime_error) */
+#define YRTB_ERR_CUDA 2         /* CUDA runtime error */
+#define YRTB_ERR_RANGE 3        /* detector pair outside the histogram (reference: std::range_error) */
+#define YRTB_ERR_EVENT 4        /* events with detector ids >= number of detectors were skipped */
+
+typedef struct CUstream_st* yrtb_stream; /* cudaStream_t; NULL = legacy default stream */
+
+/* Scanner description: the arguments of the reference Scanner constructor
+ * (src/datastruct/scanner/Scanner.cpp:102-127). */
+typedef struct
+{
+	float axial_fov, crystal_size_z, crystal_size_trans, crystal_depth,
+	    scanner_radius;
+	uint64_t dets_per_ring, num_rings, num_doi, max_ring_diff, min_ang_diff,
+	    dets_per_block;
+} yrtb_scanner;
+
+/* Image grid: the reference ImageParams(nx, ny, nz, length_x, length_y,
+ * length_z, off_x, off_y, off_z, nt) (src/datastruct/image/ImageParams.cpp:136-218).
+ * Voxel size = length / n; FOV radius = max(lx, ly)/2 - max(vx, vy)/1000. */
+typedef struct
+{
+	int64_t nx, ny, nz, nt;
+	float length_x, length_y, length_z, off_x, off_y, off_z;
+} yrtb_image_params;
+
+#define YRTB_SIDDON 0
+#define YRTB_DD 1
+
+/* Arithmetic of the traversal. */
+#define YRTB_MIRROR 0       /* FP32 in the reference's operation order (bit-exact voxel sequence) */
+#define YRTB_COMPENSATED 1  /* FP64 entry/exit (alpha) setup, Kahan-compensated FP32 forward sums */
+
+/* Projector options: the reference ProjectorParams
+ * (include/yrt-pet/operators/ProjectorParams.hpp:27-71) plus the PSF table
+ * that ProjectionPsfManager reads from its CSV
+ * (src/operators/ProjectionPsfManager.cpp:27-50). */
+typedef struct
+{
+	int projector;          /* YRTB_SIDDON or YRTB_DD */
+	int num_rays;           /* Siddon multi-ray count (>= 1) */
+	float tof_fwhm_ps;      /* <= 0: no TOF */
+	int tof_n_std;          /* truncation in sigmas (<= 0: none) */
+	int psf_num_s;          /* projection-space PSF kernels (DD only); 0: no PSF */
+	int psf_size;           /* taps per kernel (odd) */
+	float psf_s_step, psf_k_spacing;
+	const float* psf_taps;  /* host, psf_num_s * psf_size */
+	int precision;          /* YRTB_MIRROR or YRTB_COMPENSATED */
+} yrtb_projector_params;
+
+/* Events (list-mode) in structure-of-arrays form, device pointers.  Either
+ * (d1, d2) detector ids or lor (6 floats per event: p1 xyz, p2 xyz) must be
+ * given.  All other arrays are optional (NULL):
+ *   tof_ps        TOF value in ps (needs a TOF projector)
+ *   frame         dynamic frame; events with frame < 0 are skipped, frames
+ *                 >= nt are counted as invalid and skipped
+ *   motion_frame  rigid-motion frame per event; motion: 12 floats per motion
+ *                 frame (r00 r01 r02 r10 r11 r12 r20 r21 r22 tx ty tz), applied
+ *                 to both endpoints as in ProjectionData::getLOR
+ *                 (src/datastruct/projection/ProjectionData.cpp:275-321);
+ *                 a negative motion frame leaves the LOR unmoved;
+ *                 num_motion_frames bounds the motion-frame index
+ *   measurement   per-event measurement (histogram bins); 1 when NULL
+ *   sens, att     multiplicative correction factors per event
+ *   additive      randoms + scatter estimate per event */
+typedef struct
+{
+	const uint32_t* d1;
+	const uint32_t* d2;
+	const float* lor;
+	const float* tof_ps;
+	const int32_t* frame;
+	const int32_t* motion_frame;
+	const float* motion;
+	uint64_t num_motion_frames;
+	const float* measurement;
+	const float* sens;
+	const float* att;
+	const float* additive;
+	uint64_t count;
+} yrtb_events;
+
+/* Events start + k*stride for k < count: one OSEM subset of the reference
+ * BinIteratorChronologicalInterleaved (BinIterator.cpp:261-265) when
+ * start = subset, stride = numSubsets.  count = 0 selects every event of the
+ * subset. */
+typedef struct
+{
+	uint64_t start, stride, count;
+} yrtb_range;
+
+typedef struct yrtb_projector yrtb_projector;
+
+/* ---------------------------------------------------------------- misc --- */
+const char* yrtb_last_error(void);
+int yrtb_version(void);
+/* Number of events skipped because of invalid detector ids since the last
+ * call (synchronises the handle's error counter). */
+yrtb_status yrtb_projector_take_event_errors(yrtb_projector* h,
+                                             uint64_t* count);
+
+/* ---------------------------------------------------- scanner geometry --- */
+/* Regular detector LUT, out[d*6 + 0..5] = x, y, z, orient x, y, z.
+ * Replaces DetRegular::generateLUT (src/datastruct/scanner/DetRegular.cpp:113-183);
+ * host call, bit-identical to the reference. */
+yrtb_status yrtb_scanner_regular_lut(const yrtb_scanner* scanner,
+                                     float* out_host);
+
+/* Histogram3D dimensions {numZBin, numPhi, numR}
+ * (src/datastruct/projection/Histogram3D.cpp:165-203). */
+yrtb_status yrtb_histo3d_dims(const yrtb_scanner* scanner, uint64_t* dims3);
+
+/* ---------------------------------------------------------- projector --- */
+/* Creates a projector for one scanner and image grid.  det_lut_host:
+ * numDets*6 floats (positions, orientations) or NULL for the regular LUT.
+ * Replaces OperatorProjectorDevice::create / util::createOperatorProjectorDevice
+ * (include/yrt-pet/operators/OperatorProjectorDevice.cuh:27-31,
+ * src/utils/ReconstructionUtilsDevice.cu:313). */
+yrtb_status yrtb_projector_create(const yrtb_scanner* scanner,
+                                  const float* det_lut_host,
+                                  const yrtb_image_params* image,
+                                  const yrtb_projector_params* params,
+                                  yrtb_projector** out);
+void yrtb_projector_destroy(yrtb_projector* h);
+
+/* Offsets drawn by the multi-ray Siddon projector for events k = 0..count-1
+ * of a range: d_out[k*4*(num_rays-1) + 4*(ray-1) + {0..3}] = (i1, j1, i2, j2),
+ * uniforms in [-0.5, 0.5) along z and across the crystal at each endpoint.
+ * Same stream as the reference device path (curand XORWOW, seed 13,
+ * subsequence = index in the batch; SiddonKernels.cuh:27-84).  For
+ * validation against CPU re-computations of the same rays. */
+yrtb_status yrtb_multiray_offsets(yrtb_projector* h, uint64_t count,
+                                  float* d_out, yrtb_stream stream);
+
+/* d_out[e] = (A x)_e for every event e of the range (entries of other events
+ * untouched).  Replaces OperatorProjectorDevice::applyA
+ * (src/operators/OperatorProjectorDevice.cu:442-544) with the kernels of
+ * OperatorProjectorSiddon_GPU / _DD_GPU. */
+yrtb_status yrtb_forward(yrtb_projector* h, const float* d_image,
+                         const yrtb_events* ev, yrtb_range range,
+                         float* d_out, yrtb_stream stream);
+
+/* d_image += A^T v over the range (v = d_values[e]).  Replaces
+ * OperatorProjectorDevice::applyAH (src/operators/OperatorProjectorDevice.cu:546-706). */
+yrtb_status yrtb_backward(yrtb_projector* h, const float* d_values,
+                          const yrtb_events* ev, yrtb_range range,
+                          float* d_image, yrtb_stream stream);
+
+/* One fused EM pass over the range: per event u = A x, corrections, ratio,
+ * d_em += A^T u.  Replaces computeEMUpdateImage_kernel
+ * (src/recon/OSEM_GPU.cu:1159-1341) and OSEM_CPU::computeEMUpdateImage
+ * (src/recon/OSEM_CPU.cpp:284-393); corrections are applied in the CPU
+ * order: *sens, *att, *global, +additive, |u| > denom_threshold. */
+yrtb_status yrtb_em_step(yrtb_projector* h, const float* d_image,
+                         float* d_em, const yrtb_events* ev,
+                         yrtb_range range, float global_scale,
+                         float denom_threshold, yrtb_stream stream);
+
+/* Number of voxel crossings (Siddon) or footprint voxels (DD) of every event
+ * of the range, summed over rays: d_out[e] (uint32).  Used to count the
+ * algorithmic traffic of a projection; no counterpart in the reference. */
+yrtb_status yrtb_count_crossings(yrtb_projector* h, const yrtb_events* ev,
+                                 yrtb_range range, uint32_t* d_out,
+                                 yrtb_stream stream);
+
+/* Per-event attenuation factors exp(-0.1 * Siddon(mu-image)).  Replaces the
+ * Corrector's ACF precompute (src/recon/Corrector.cpp:601-612,
+ * include/yrt-pet/utils/Tools.hpp:98-102). */
+yrtb_status yrtb_attenuation_factors(yrtb_projector* h, const float* d_mu,
+                                     const yrtb_image_params* mu_params,
+                                     const yrtb_events* ev, yrtb_range range,
+                                     float* d_out, yrtb_stream stream);
+
+/* Per-event gather of a Histogram3D through the detector pair (sensitivity,
+ * randoms, scatter histograms).  invert != 0 replaces nonzero v by 1/v
+ * (Corrector::getSensitivity, src/recon/Corrector.cpp:294-306).  Pairs that
+ * map to no bin give 0 and are counted in the error counter. */
+yrtb_status yrtb_gather_histo3d(yrtb_projector* h, const float* d_histo,
+                                const yrtb_events* ev, yrtb_range range,
+                                int invert, float* d_out, yrtb_stream stream);
+
+/* ----------------------------------------------------- histogram mode --- */
+/* Sensitivity image over one subset of Histogram3D bins (phi = subset mod
+ * num_subsets), non-TOF: d_sens += A^T (sens_bin * acf_bin).  d_sens_histo /
+ * d_acf_histo may be NULL (1); d_mu (with mu_params) gives ACFs from an
+ * attenuation image when d_acf_histo is NULL.  Replaces
+ * generateSensImage_kernel (src/recon/OSEM_GPU.cu:1048-1157) and
+ * OSEM_CPU::generateSensitivityImageForCurrentSubset (src/recon/OSEM_CPU.cpp:127-188)
+ * without the final threshold (see yrtb_apply_threshold). */
+yrtb_status yrtb_sensitivity_histo3d(yrtb_projector* h, float* d_sens,
+                                     const float* d_sens_histo,
+                                     const float* d_acf_histo,
+                                     const float* d_mu,
+                                     const yrtb_image_params* mu_params,
+                                     int num_subsets, int subset,
+                                     yrtb_stream stream);
+
+/* Histogram-mode EM pass over one subset of bins: bins with zero measurement
+ * are skipped (OSEM_GPU.cu:1224-1225).  Optional per-bin histograms: sens,
+ * acf (multiplicative), additive. */
+yrtb_status yrtb_em_step_histo3d(yrtb_projector* h, const float* d_image,
+                                 float* d_em, const float* d_measurements,
+                                 const float* d_sens_histo,
+                                 const float* d_acf_histo,
+                                 const float* d_additive_histo,
+                                 int num_subsets, int subset,
+                                 float global_scale, float denom_threshold,
+                                 yrtb_stream stream);
+
+/* List-mode -> Histogram3D: d_histo[bin(d1,d2)] += value for value > 0 and
+ * d1 != d2 (values NULL: 1).  Pairs outside the histogram (ring difference,
+ * minimum angle) are skipped and counted in *n_invalid (the reference
+ * throws; this call returns YRTB_ERR_RANGE when any are found).  Synchronises
+ * the stream.  Replaces util::convertToHistogram3D
+ * (src/utils/ReconstructionUtils.cpp:659-800). */
+yrtb_status yrtb_listmode_to_histo3d(yrtb_projector* h, const uint32_t* d_d1,
+                                     const uint32_t* d_d2,
+                                     const float* d_values, uint64_t n,
+                                     float* d_histo, uint64_t* n_invalid,
+                                     yrtb_stream stream);
+
+/* Histogram3D maps on the device: bin ids of detector pairs (UINT64_MAX for
+ * pairs outside the histogram) and detector pairs of bin ids.  Replace
+ * Histogram3D::getBinIdFromDetPair / getDetPairFromBinId
+ * (src/datastruct/projection/Histogram3D.cpp:366-426). */
+yrtb_status yrtb_histo3d_bins(yrtb_projector* h, const uint32_t* d_d1,
+                              const uint32_t* d_d2, uint64_t n,
+                              uint64_t* d_bins, yrtb_stream stream);
+yrtb_status yrtb_histo3d_detpairs(yrtb_projector* h, const uint64_t* d_bins,
+                                  uint64_t n, uint32_t* d_d1, uint32_t* d_d2,
+                                  yrtb_stream stream);
+
+/* -------------------------------------------------------- image space --- */
+/* x *= u / s where s > threshold.  sens_nt == 1 broadcasts one sensitivity
+ * image over nt frames; d_frame_scale (nullable, nt floats) divides u and
+ * the threshold per frame.  Replaces Image::updateEMThreshold{Static,
+ * DynamicWithScaling,DynamicWith4DSens} (src/datastruct/image/Image.cpp:651-833)
+ * and updateEM_kernel / updateEMDynamic_kernel
+ * (src/datastruct/image/ImageSpaceKernels.cu:13-76). */
+yrtb_status yrtb_em_update(float* d_image, const float* d_em,
+                           const float* d_sens, uint64_t voxels_per_frame,
+                           int64_t nt, int64_t sens_nt, float threshold,
+                           const float* d_frame_scale, yrtb_stream stream);
+
+/* x = x*le_scale + le_off where mask <= threshold, else x*gt_scale + gt_off.
+ * broadcast != 0 applies a one-frame mask to every frame.  Replaces
+ * Image::applyThreshold / applyThresholdBroadcast
+ * (src/datastruct/image/Image.cpp:594-649). */
+yrtb_status yrtb_apply_threshold(float* d_image, const float* d_mask,
+                                 uint64_t voxels_per_frame, int64_t nt,
+                                 int broadcast, float threshold,
+                                 float le_scale, float le_off, float gt_scale,
+                                 float gt_off, yrtb_stream stream);
+
+/* d_x[i] = value (ImageDevice::fill). */
+yrtb_status yrtb_fill(float* d_x, uint64_t n, float value, yrtb_stream stream);
+
+/* d_x[i] *= scale (ImageDevice::multWithScalar). */
+yrtb_status yrtb_scale(float* d_x, uint64_t n, float scale,
+                       yrtb_stream stream);
+
+/* ------------------------------------------------------ OSEM (driver) --- */
+/* List-mode OSEM over device-resident events.  Mirrors OSEM::reconstruct
+ * (src/recon/OSEM.cpp:315-365) with the GPU hooks of OSEM_GPU
+ * (src/recon/OSEM_GPU.cu:311-537): x0 = 0.125 (or the given estimate),
+ * masked by sens > 0, sensitivity divided by the number of subsets,
+ * subsets = chronologically interleaved events.  d_image holds nt frames and
+ * is both the initial estimate (when init_from_image != 0) and the result.
+ * d_sens: one image (voxels_per_frame floats).  d_work: scratch of
+ * nt*voxels_per_frame floats + voxels_per_frame floats.  use_graph != 0
+ * captures each subset (reset, EM pass, update) into a CUDA graph and
+ * replays it. */
+typedef struct
+{
+	int iterations, subsets;
+	float global_scale, denom_threshold, em_threshold;
+	int init_from_image;
+	int use_graph;
+	const float* d_frame_scale; /* nullable, nt floats */
+} yrtb_osem_params;
+
+yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
+                               const float* d_sens, float* d_image,
+                               float* d_work, const yrtb_osem_params* p,
+                               yrtb_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YRT_B200_H */

@@ -151,6 +151,33 @@ def ref_lib():
     return _ref
 
 
+class _StdoutToStderr:
+    """Sends the reference's progress prints (std::cout) to stderr so that
+    stdout carries only the caller's own output."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self._saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        import sys
+        try:
+            ctypes.CDLL(None).fflush(None)
+        except Exception:
+            pass
+        sys.stdout.flush()
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        return False
+
+
+def quiet():
+    return _StdoutToStderr()
+
+
 def _ref_check(rc):
     if rc != 0:
         raise RuntimeError(ref_lib().ref_last_error().decode())
@@ -362,12 +389,14 @@ def ref_siddon(sc: Scanner, ip: ImageParams, lors, *, image=None, values=None,
     else:
         img = np.zeros(ip.shape, np.float32)
         vals = np.ascontiguousarray(values, np.float32).copy()
-    _ref_check(ref_lib().ref_siddon(
-        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), _p(img),
-        ctypes.c_uint64(n), _p(lors), _p(orients), _p(tof),
-        ctypes.c_float(tof_fwhm_ps), ctypes.c_int(tof_n_std), _p(frames),
-        ctypes.c_int(num_rays), ctypes.c_int(int(forward)),
-        ctypes.c_int(int(incremental)), ctypes.c_int(threads), _p(vals)))
+    with quiet():
+        rc = ref_lib().ref_siddon(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), _p(img),
+            ctypes.c_uint64(n), _p(lors), _p(orients), _p(tof),
+            ctypes.c_float(tof_fwhm_ps), ctypes.c_int(tof_n_std), _p(frames),
+            ctypes.c_int(num_rays), ctypes.c_int(int(forward)),
+            ctypes.c_int(int(incremental)), ctypes.c_int(threads), _p(vals))
+    _ref_check(rc)
     return vals if forward else img
 
 
@@ -385,11 +414,13 @@ def ref_dd(sc: Scanner, ip: ImageParams, lors, orients, *, image=None,
         img = np.zeros(ip.shape, np.float32)
         vals = np.ascontiguousarray(values, np.float32).copy()
     psf = None if psf_csv is None else psf_csv.encode()
-    _ref_check(ref_lib().ref_dd(
-        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), _p(img),
-        ctypes.c_uint64(n), _p(lors), _p(orients), _p(tof),
-        ctypes.c_float(tof_fwhm_ps), ctypes.c_int(tof_n_std), psf,
-        ctypes.c_int(int(forward)), ctypes.c_int(threads), _p(vals)))
+    with quiet():
+        rc = ref_lib().ref_dd(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), _p(img),
+            ctypes.c_uint64(n), _p(lors), _p(orients), _p(tof),
+            ctypes.c_float(tof_fwhm_ps), ctypes.c_int(tof_n_std), psf,
+            ctypes.c_int(int(forward)), ctypes.c_int(threads), _p(vals))
+    _ref_check(rc)
     return vals if forward else img
 
 
@@ -402,9 +433,11 @@ def ref_lm_to_histo3d(sc: Scanner, d1, d2, threads=8):
     d2 = _c(d2, np.uint32)
     histo = np.zeros(int(np.prod(ref_histo3d_dims(sc))), np.float32)
     sec = ctypes.c_double()
-    _ref_check(ref_lib().ref_lm_to_histo3d(
-        ctypes.byref(sc.desc()), ctypes.c_uint64(len(d1)), _p(d1), _p(d2),
-        ctypes.c_int(threads), _p(histo), ctypes.byref(sec)))
+    with quiet():
+        rc = ref_lib().ref_lm_to_histo3d(
+            ctypes.byref(sc.desc()), ctypes.c_uint64(len(d1)), _p(d1), _p(d2),
+            ctypes.c_int(threads), _p(histo), ctypes.byref(sec))
+    _ref_check(rc)
     return histo, sec.value
 
 
@@ -425,11 +458,13 @@ def ref_sensitivity(sc: Scanner, ip: ImageParams, *, sens_histo=None,
     sec = ctypes.c_double()
     sh = _c(sens_histo, np.float32)
     att = _c(att_image, np.float32)
-    _ref_check(ref_lib().ref_sensitivity(
-        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
-        _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
-        _p(att), None if psf_csv is None else psf_csv.encode(), _p(out),
-        ctypes.byref(sec)))
+    with quiet():
+        rc = ref_lib().ref_sensitivity(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
+            _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
+            _p(att), None if psf_csv is None else psf_csv.encode(), _p(out),
+            ctypes.byref(sec))
+    _ref_check(rc)
     return out, sec.value
 
 
@@ -447,11 +482,13 @@ def ref_osem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, *, tof=None,
     sh = _c(sens_histo, np.float32)
     att = _c(att_image, np.float32)
     s = _c(sens, np.float32)
-    _ref_check(ref_lib().ref_osem_listmode(
-        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
-        _p(s), ctypes.c_uint64(len(d1)), _p(d1), _p(d2), _p(tof), _p(randoms),
-        _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
-        _p(att), _p(out), ctypes.byref(sec)))
+    with quiet():
+        rc = ref_lib().ref_osem_listmode(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
+            _p(s), ctypes.c_uint64(len(d1)), _p(d1), _p(d2), _p(tof), _p(randoms),
+            _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
+            _p(att), _p(out), ctypes.byref(sec))
+    _ref_check(rc)
     return out, sec.value
 
 
@@ -462,8 +499,10 @@ def ref_osem_histo3d(sc: Scanner, ip: ImageParams, sens_images, histo, *,
     sec = ctypes.c_double()
     s = _c(sens_images, np.float32)
     h = _c(histo, np.float32)
-    _ref_check(ref_lib().ref_osem_histo3d(
-        ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
-        _p(s), _p(h), None if psf_csv is None else psf_csv.encode(), _p(out),
-        ctypes.byref(sec)))
+    with quiet():
+        rc = ref_lib().ref_osem_histo3d(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
+            _p(s), _p(h), None if psf_csv is None else psf_csv.encode(), _p(out),
+            ctypes.byref(sec))
+    _ref_check(rc)
     return out, sec.value

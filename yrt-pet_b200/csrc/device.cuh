@@ -1,0 +1,639 @@
+// Device-side projection math for libyrtb (sm_100a).
+//
+// This translation unit is compiled with -fmad=false: in YRTB_MIRROR mode
+// every expression below is evaluated in FP32 with the operation order of the
+// reference CPU projector, so the voxel index sequence of each ray (and, for
+// non-TOF rays, every weight) is bit-identical to it.  The traversal itself
+// is written from the published incremental Siddon method: parametric entry
+// into the image slabs, then stepping to the nearest of the next x/y/z plane
+// crossings.  Reference behaviour followed (paths inside yrt-pet):
+//   FOV-cylinder clip, slab alphas, entry step, tie rule (<=), early exit
+//                                 src/operators/ProjectorSiddon.cpp:495-766
+//   TOF window and midpoint weight include/yrt-pet/operators/TimeOfFlight.hpp:53-84
+//   multi-ray offsets (curand)    include/yrt-pet/operators/SiddonKernels.cuh:27-84
+//   distance-driven footprint     src/operators/ProjectorDD.cpp:260-578
+//   projection-space PSF integral include/yrt-pet/operators/ProjectorUtils.hpp:43-98
+#pragma once
+
+#include <cuda_runtime.h>
+#include <curand_kernel.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+namespace yrtb
+{
+
+constexpr double kSpeedOfLightMmPs = 0.299792458;
+// The reference stores c as a double holding the float value 0.299792458f.
+constexpr double kSpeedOfLightMmPsFlt = 0.299792458f;
+
+struct Geom
+{
+	int nx, ny, nz, nt;
+	int64_t nxy, nvox;
+	float lx, ly, lz;
+	float vx, vy, vz;
+	float fovRadius;
+	float offx, offy, offz;
+};
+
+struct TofP
+{
+	float sigma, trunc, norm;
+};
+
+struct Psf
+{
+	const float* taps;     // num_s * size
+	const float* flipped;  // adjoint taps
+	int num_s, size;
+	float sStep, kSpacing;
+};
+
+struct Scan
+{
+	const float4* pos;  // crystal centres
+	const float4* ori;  // crystal orientations
+	uint32_t numDets;
+	float crystalZ, crystalTrans;
+};
+
+// Device copy of the event arrays (see yrtb_events in include/yrt_b200.h).
+struct Events
+{
+	const uint32_t* d1;
+	const uint32_t* d2;
+	const float* lor;
+	const float* tof;
+	const int32_t* frame;
+	const int32_t* mframe;
+	const float* motion;
+	uint64_t numMotion;
+	const float* meas;
+	const float* sens;
+	const float* att;
+	const float* add;
+};
+
+struct Range
+{
+	uint64_t start, stride, count;
+};
+
+__device__ __forceinline__ float3 f3sub(float3 a, float3 b)
+{
+	return make_float3(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+
+// ---------------------------------------------------------------- TOF ----
+// Alpha window of the TOF kernel: 0.5 + (c*t/2 -/+ trunc)/L clamped to [0,1],
+// with the reference's float/double mix.
+__device__ __forceinline__ void tofAlphaRange(const TofP& t, float lorNorm,
+                                              float tof_ps, float& amin,
+                                              float& amax)
+{
+	if (t.trunc <= 0.f)
+	{
+		amin = 0.f;
+		amax = 1.f;
+		return;
+	}
+	const float tof_mm =
+	    static_cast<float>(static_cast<double>(tof_ps) * kSpeedOfLightMmPsFlt * 0.5);
+	amin = static_cast<float>(fmax(0.0, 0.5 + static_cast<double>((tof_mm - t.trunc) / lorNorm)));
+	amax = static_cast<float>(fmin(1.0, 0.5 + static_cast<double>((tof_mm + t.trunc) / lorNorm)));
+}
+
+// Gaussian TOF weight evaluated at the centre of [lo, hi] (mm along the LOR).
+__device__ __forceinline__ float tofWeight(const TofP& t, float lorNorm,
+                                           float tof_ps, float lo, float hi)
+{
+	const float tof_mm =
+	    static_cast<float>(static_cast<double>(tof_ps) * kSpeedOfLightMmPsFlt * 0.5);
+	const float pc = static_cast<float>(0.5 * static_cast<double>(lorNorm) +
+	                                    static_cast<double>(tof_mm));
+	const float xc = (0.5f * (lo + hi) - pc) / t.sigma;
+	return expf(-0.5f * xc * xc) * t.norm;
+}
+
+// Parametric interval of a ray inside the slab [r0, r1] along one axis.
+template <typename R>
+__device__ __forceinline__ void slabAlpha(R r0, R r1, R p1, R p2, R inv,
+                                          R& amin, R& amax)
+{
+	amin = R(0);
+	amax = R(1);
+	if (p1 != p2)
+	{
+		const R a0 = (r0 - p1) * inv;
+		const R a1 = (r1 - p1) * inv;
+		if (a0 < a1)
+		{
+			amin = a0;
+			amax = a1;
+		}
+		else
+		{
+			amin = a1;
+			amax = a0;
+		}
+	}
+	else if (p1 < r0 || p1 > r1)
+	{
+		amax = R(0);
+		amin = R(1);
+	}
+}
+
+// ------------------------------------------------------------ Siddon ----
+// Walks one ray through the image grid and calls visit(offset, weight) for
+// each voxel crossing, in order.  p1, p2: endpoints relative to the image
+// centre.  COMP selects the FP64 entry/exit setup.
+template <bool TOF, bool COMP, typename Visit>
+__device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
+                                           const float3 p2, const TofP& tp,
+                                           float tofValue, Visit& visit)
+{
+	using R = typename std::conditional<COMP, double, float>::type;
+	// 1. Clip to the FOV cylinder.
+	float t0, t1;
+	{
+		const R dxr = R(p2.x) - R(p1.x), dyr = R(p2.y) - R(p1.y);
+		const R A = dxr * dxr + dyr * dyr;
+		const R B = R(2) * (dxr * R(p1.x) + dyr * R(p1.y));
+		const R C = R(p1.x) * R(p1.x) + R(p1.y) * R(p1.y) -
+		            R(g.fovRadius) * R(g.fovRadius);
+		const R Delta = B * B - R(4) * A * C;
+		if (A != R(0))
+		{
+			if (Delta <= R(0))
+				return;
+			const R sq = sqrt(Delta);
+			t0 = static_cast<float>((-B - sq) / (R(2) * A));
+			t1 = static_cast<float>((-B + sq) / (R(2) * A));
+		}
+		else
+		{
+			t0 = 0.f;
+			t1 = 1.f;
+		}
+	}
+	const float3 d12 = f3sub(p1, p2);
+	const float d_norm = sqrtf(d12.x * d12.x + d12.y * d12.y + d12.z * d12.z);
+	const bool flat_x = (p1.x == p2.x);
+	const bool flat_y = (p1.y == p2.y);
+	const bool flat_z = (p1.z == p2.z);
+	const float inv_x = flat_x ? 0.0f : 1.0f / (p2.x - p1.x);
+	const float inv_y = flat_y ? 0.0f : 1.0f / (p2.y - p1.y);
+	const float inv_z = flat_z ? 0.0f : 1.0f / (p2.z - p1.z);
+	const int dir_x = (inv_x >= 0.0f) ? 1 : -1;
+	const int dir_y = (inv_y >= 0.0f) ? 1 : -1;
+	const int dir_z = (inv_z >= 0.0f) ? 1 : -1;
+
+	// 2. Intersection with the volume.
+	const float dx = g.vx, dy = g.vy, dz = g.vz;
+	const float inv_dx = 1.0f / dx, inv_dy = 1.0f / dy, inv_dz = 1.0f / dz;
+	const float x0 = -g.lx * 0.5f, x1 = g.lx * 0.5f;
+	const float y0 = -g.ly * 0.5f, y1 = g.ly * 0.5f;
+	const float z0 = -g.lz * 0.5f, z1 = g.lz * 0.5f;
+	float amin, amax;
+	float ax_min, ay_min, az_min;
+	{
+		R axmin, axmax, aymin, aymax, azmin, azmax;
+		const R ix = COMP ? (flat_x ? R(0) : R(1) / (R(p2.x) - R(p1.x))) : R(inv_x);
+		const R iy = COMP ? (flat_y ? R(0) : R(1) / (R(p2.y) - R(p1.y))) : R(inv_y);
+		const R iz = COMP ? (flat_z ? R(0) : R(1) / (R(p2.z) - R(p1.z))) : R(inv_z);
+		slabAlpha<R>(R(-0.5f * g.lx), R(0.5f * g.lx), R(p1.x), R(p2.x), ix, axmin, axmax);
+		slabAlpha<R>(R(-0.5f * g.ly), R(0.5f * g.ly), R(p1.y), R(p2.y), iy, aymin, aymax);
+		slabAlpha<R>(R(-0.5f * g.lz), R(0.5f * g.lz), R(p1.z), R(p2.z), iz, azmin, azmax);
+		ax_min = static_cast<float>(axmin);
+		ay_min = static_cast<float>(aymin);
+		az_min = static_cast<float>(azmin);
+		// max/min over {0|1, t, ax, ay, az} in the reference's order.
+		amin = fmaxf(fmaxf(fmaxf(fmaxf(0.0f, t0), ax_min), ay_min), az_min);
+		amax = fminf(fminf(fminf(fminf(1.0f, t1), static_cast<float>(axmax)),
+		                   static_cast<float>(aymax)),
+		             static_cast<float>(azmax));
+	}
+	if constexpr (TOF)
+	{
+		float a0, a1;
+		tofAlphaRange(tp, d_norm, tofValue, a0, a1);
+		amin = fmaxf(amin, a0);
+		amax = fminf(amax, a1);
+	}
+
+	float a_cur = amin;
+	float a_next = -1.0f;
+	float x_cur = (inv_x > 0.0f) ? x0 : x1;
+	float y_cur = (inv_y > 0.0f) ? y0 : y1;
+	float z_cur = (inv_z > 0.0f) ? z0 : z1;
+	if ((inv_x >= 0.0f && p1.x > x1) || (inv_x < 0.0f && p1.x < x0) ||
+	    (inv_y >= 0.0f && p1.y > y1) || (inv_y < 0.0f && p1.y < y0) ||
+	    (inv_z >= 0.0f && p1.z > z1) || (inv_z < 0.0f && p1.z < z0))
+		return;
+
+	// First plane crossing at or beyond the entry point, per axis.
+	float ax_next = flat_x ? 3.402823466e+38f : ax_min;
+	if (!flat_x)
+	{
+		const long long kx = static_cast<long long>(
+		    ceilf(static_cast<float>(dir_x) * (a_cur * (p2.x - p1.x) - x_cur + p1.x) / dx));
+		x_cur += static_cast<float>(kx * dir_x) * dx;
+		ax_next = (x_cur - p1.x) * inv_x;
+	}
+	float ay_next = flat_y ? 3.402823466e+38f : ay_min;
+	if (!flat_y)
+	{
+		const long long ky = static_cast<long long>(
+		    ceilf(static_cast<float>(dir_y) * (a_cur * (p2.y - p1.y) - y_cur + p1.y) / dy));
+		y_cur += static_cast<float>(ky * dir_y) * dy;
+		ay_next = (y_cur - p1.y) * inv_y;
+	}
+	float az_next = flat_z ? 3.402823466e+38f : az_min;
+	if (!flat_z)
+	{
+		const long long kz = static_cast<long long>(
+		    ceilf(static_cast<float>(dir_z) * (a_cur * (p2.z - p1.z) - z_cur + p1.z) / dz));
+		z_cur += static_cast<float>(kz * dir_z) * dz;
+		az_next = (z_cur - p1.z) * inv_z;
+	}
+
+	bool first = true;
+	int vx = -1, vy = -1, vz = -1;
+	int dir_prev = 0;
+	const int nx = g.nx, ny = g.ny, nz = g.nz;
+	const int nxy = nx * ny;
+	int off = 0;
+	float axp = ax_next, ayp = ay_next, azp = az_next;
+	const float fdx = static_cast<float>(dir_x) * dx;
+	const float fdy = static_cast<float>(dir_y) * dy;
+	const float fdz = static_cast<float>(dir_z) * dz;
+
+	// 3. Incremental walk: step to the nearest crossing (ties step together).
+	// A ray crosses at most nx+ny+nz+3 planes inside the grid; the cap only
+	// guards against non-finite input and never binds for finite rays.
+	const int maxSteps = 2 * (nx + ny + nz) + 16;
+	for (int step = 0; a_cur < amax && step < maxSteps; step++)
+	{
+		int dir_next = 0;
+		if (axp <= ayp && axp <= azp)
+		{
+			a_next = ax_next;
+			x_cur += fdx;
+			ax_next = (x_cur - p1.x) * inv_x;
+			dir_next |= 1;
+		}
+		if (ayp <= axp && ayp <= azp)
+		{
+			a_next = ay_next;
+			y_cur += fdy;
+			ay_next = (y_cur - p1.y) * inv_y;
+			dir_next |= 2;
+		}
+		if (azp <= axp && azp <= ayp)
+		{
+			a_next = az_next;
+			z_cur += fdz;
+			az_next = (z_cur - p1.z) * inv_z;
+			dir_next |= 4;
+		}
+		if (a_next > amax)
+			a_next = amax;
+		if (a_cur >= a_next)
+		{
+			axp = ax_next;
+			ayp = ay_next;
+			azp = az_next;
+			continue;
+		}
+		if (first)
+		{
+			const float a_mid = 0.5f * (a_cur + a_next);
+			vx = static_cast<int>((p1.x + a_mid * (p2.x - p1.x) + g.lx / 2.0f) * inv_dx);
+			vy = static_cast<int>((p1.y + a_mid * (p2.y - p1.y) + g.ly / 2.0f) * inv_dy);
+			vz = static_cast<int>((p1.z + a_mid * (p2.z - p1.z) + g.lz / 2.0f) * inv_dz);
+			off = vz * nxy + vy * nx;
+			first = false;
+			if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
+				break;
+		}
+		else
+		{
+			bool out = false;
+			if (dir_prev & 1)
+			{
+				vx += dir_x;
+				out |= (vx < 0 || vx >= nx);
+			}
+			if (dir_prev & 2)
+			{
+				vy += dir_y;
+				if (vy < 0 || vy >= ny)
+					out = true;
+				else
+					off += dir_y * nx;
+			}
+			if (dir_prev & 4)
+			{
+				vz += dir_z;
+				if (vz < 0 || vz >= nz)
+					out = true;
+				else
+					off += dir_z * nxy;
+			}
+			if (out)
+				break;
+		}
+		dir_prev = dir_next;
+		float w = (a_next - a_cur) * d_norm;
+		if constexpr (TOF)
+			w *= tofWeight(tp, d_norm, tofValue, a_cur * d_norm, a_next * d_norm);
+		visit(vx + off, w);
+		a_cur = a_next;
+		axp = ax_next;
+		ayp = ay_next;
+		azp = az_next;
+	}
+}
+
+// ----------------------------------------------------------- multi-ray ----
+// Random offsets of the extra rays, as the reference device path draws them:
+// curand XORWOW seeded with 13, subsequence = event index in the batch, four
+// uniforms per extra ray (i1, j1, i2, j2), each shifted by -0.5.
+struct MultiRay
+{
+	curandState state;
+	float3 t1, t2;
+	__device__ __forceinline__ void init(unsigned long long id, float3 n1,
+	                                     float3 n2)
+	{
+		curand_init(13ULL, id, 0ULL, &state);
+		// cross(n, z) normalised with norm3df, as the reference device code.
+		t1 = make_float3(n1.y * 1.f - n1.z * 0.f, n1.z * 0.f - n1.x * 1.f,
+		                 n1.x * 0.f - n1.y * 0.f);
+		t2 = make_float3(n2.y * 1.f - n2.z * 0.f, n2.z * 0.f - n2.x * 1.f,
+		                 n2.x * 0.f - n2.y * 0.f);
+		const float l1 = norm3df(t1.x, t1.y, t1.z);
+		const float l2 = norm3df(t2.x, t2.y, t2.z);
+		t1 = make_float3(t1.x / l1, t1.y / l1, t1.z / l1);
+		t2 = make_float3(t2.x / l2, t2.y / l2, t2.z / l2);
+	}
+	__device__ __forceinline__ void next(float u[4])
+	{
+		u[0] = curand_uniform(&state) - 0.5f;
+		u[1] = curand_uniform(&state) - 0.5f;
+		u[2] = curand_uniform(&state) - 0.5f;
+		u[3] = curand_uniform(&state) - 0.5f;
+	}
+	__device__ __forceinline__ void offset(const float u[4], float csz,
+	                                       float cst, float3& p1, float3& p2) const
+	{
+		const float zi1 = u[0] * csz, tj1 = u[1] * cst;
+		const float zi2 = u[2] * csz, tj2 = u[3] * cst;
+		p1 = make_float3(p1.x + 0.f * zi1 + t1.x * tj1, p1.y + 0.f * zi1 + t1.y * tj1,
+		                 p1.z + 1.f * zi1 + t1.z * tj1);
+		p2 = make_float3(p2.x + 0.f * zi2 - t2.x * tj2, p2.y + 0.f * zi2 - t2.y * tj2,
+		                 p2.z + 1.f * zi2 - t2.z * tj2);
+	}
+};
+
+// ---------------------------------------------------------------- DD -----
+__device__ __forceinline__ float psfIntegral(const float* kernel,
+                                             int kernelSize, float kernelStep,
+                                             float x0, float x1)
+{
+	const int halfSize = (kernelSize - 1) / 2;
+	if (x0 > (halfSize + 1) * kernelStep || x1 < -(halfSize + 1) * kernelStep ||
+	    x0 >= x1)
+		return 0.f;
+	const float x0_s = x0 / kernelStep;
+	const int x0_i = static_cast<int>(floorf(x0_s + halfSize));
+	const float tau_0 = x0_s + -(-halfSize + x0_i);
+	const float v0_lo = (x0_i < 0 || x0_i >= kernelSize) ? 0.f : __ldg(kernel + x0_i);
+	const float v0_hi = (x0_i < -1 || x0_i >= kernelSize - 1) ? 0.f : __ldg(kernel + x0_i + 1);
+	const float v0 = v0_lo * (1 - tau_0) + v0_hi * tau_0;
+	const float x1_s = x1 / kernelStep;
+	const int x1_i = static_cast<int>(floorf(x1_s + halfSize));
+	const float tau_1 = x1_s - (-halfSize + x1_i);
+	const float v1_lo = (x1_i < 0 || x1_i >= kernelSize) ? 0.f : __ldg(kernel + x1_i);
+	const float v1_hi = (x1_i < -1 || x1_i >= kernelSize - 1) ? 0.f : __ldg(kernel + x1_i + 1);
+	const float v1 = v1_lo * (1 - tau_1) + v1_hi * tau_1;
+	float out = 0.f;
+	if (x0_i == x1_i)
+	{
+		out = 0.5f * (v0 + v1) * (x1 - x0);
+	}
+	else
+	{
+		out += 0.5f * (v0 + v0_hi) * kernelStep * (1 - tau_0);
+		out += 0.5f * (v1_lo + v1) * kernelStep * tau_1;
+		// Bins entirely outside [-1, kernelSize] contribute exactly zero.
+		const int xi_lo = max(x0_i + 1, -1);
+		const int xi_hi = min(x1_i, kernelSize + 1);
+		for (int xi = xi_lo; xi < xi_hi; xi++)
+		{
+			const float v_lo = (xi < 0 || xi >= kernelSize) ? 0.f : __ldg(kernel + xi);
+			const float v_hi = (xi + 1 < 0 || xi + 1 >= kernelSize) ? 0.f : __ldg(kernel + xi + 1);
+			out += kernelStep * 0.5f * (v_lo + v_hi);
+		}
+	}
+	return out;
+}
+
+// Distance-driven footprint of one LOR.  d1, d2: crystal centres relative to
+// the image centre; n1, n2: crystal orientations.  visit(offset, weight).
+template <bool TOF, bool PSF, typename Visit>
+__device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
+                                       const float3 d2, const float3 n1,
+                                       const float3 n2, float thickness_trans,
+                                       float thickness_z, const TofP& tp,
+                                       float tofValue, const Psf& psf,
+                                       bool forward, Visit& visit)
+{
+	const float3 d12 = f3sub(d1, d2);
+	const bool flag_y = fabsf(d12.y) > fabsf(d12.x);
+	const float d_norm = sqrtf(d12.x * d12.x + d12.y * d12.y + d12.z * d12.z);
+	const float* kern = nullptr;
+	float ext = 0.f;
+	if constexpr (PSF)
+	{
+		float npx = d2.y - d1.y;
+		float npy = d1.x - d2.x;
+		const float nn = sqrtf(npx * npx + npy * npy);
+		int s_idx = 0;
+		if (nn != 0.f)
+		{
+			npx /= nn;
+			npy /= nn;
+			const float s = fabsf(d1.x * npx + d1.y * npy);
+			const float si = floorf(s / psf.sStep);
+			s_idx = (si >= static_cast<float>(psf.num_s - 1)) ? psf.num_s - 1 :
+			                                                    static_cast<int>(si);
+		}
+		kern = (forward ? psf.taps : psf.flipped) + s_idx * psf.size;
+		ext = static_cast<float>((psf.size + 1) / 2) * psf.kSpacing;
+	}
+	const float dx = g.vx, dy = g.vy, dz = g.vz;
+	const float inv_x = (d1.x == d2.x) ? 0.0f : 1.0f / (d2.x - d1.x);
+	const float inv_y = (d1.y == d2.y) ? 0.0f : 1.0f / (d2.y - d1.y);
+	const float inv_z = (d1.z == d2.z) ? 0.0f : 1.0f / (d2.z - d1.z);
+	float ax_min, ax_max, ay_min, ay_max, az_min, az_max;
+	slabAlpha<float>(-0.5f * (g.lx - dx), 0.5f * (g.lx - dx), d1.x, d2.x, inv_x, ax_min, ax_max);
+	slabAlpha<float>(-0.5f * (g.ly - dy), 0.5f * (g.ly - dy), d1.y, d2.y, inv_y, ay_min, ay_max);
+	slabAlpha<float>(-0.5f * (g.lz - dz), 0.5f * (g.lz - dz), d1.z, d2.z, inv_z, az_min, az_max);
+	float amin = fmaxf(fmaxf(fmaxf(0.0f, ax_min), ay_min), az_min);
+	float amax = fminf(fminf(fminf(1.0f, ax_max), ay_max), az_max);
+	if constexpr (TOF)
+	{
+		float a0, a1;
+		tofAlphaRange(tp, d_norm, tofValue, a0, a1);
+		amin = fmaxf(amin, a0);
+		amax = fminf(amax, a1);
+	}
+	const float x_0 = d1.x + amin * (d2.x - d1.x);
+	const float y_0 = d1.y + amin * (d2.y - d1.y);
+	const float x_1 = d1.x + amax * (d2.x - d1.x);
+	const float y_1 = d1.y + amax * (d2.y - d1.y);
+	const int x_i_0 = static_cast<int>(floorf(x_0 / dx + 0.5f * (g.nx - 1) + 0.5f));
+	const int y_i_0 = static_cast<int>(floorf(y_0 / dy + 0.5f * (g.ny - 1) + 0.5f));
+	const int x_i_1 = static_cast<int>(floorf(x_1 / dx + 0.5f * (g.nx - 1) + 0.5f));
+	const int y_i_1 = static_cast<int>(floorf(y_1 / dy + 0.5f * (g.ny - 1) + 0.5f));
+	const float d1_i = flag_y ? d1.y : d1.x;
+	const float d2_i = flag_y ? d2.y : d2.x;
+	const float n1_i = flag_y ? n1.y : n1.x;
+	const float n2_i = flag_y ? n2.y : n2.x;
+	const float n1_xy_norm2 = n1.x * n1.x + n1.y * n1.y;
+	const float n1_xy_norm = sqrtf(n1_xy_norm2);
+	const float n1_p_x = n1.y / n1_xy_norm;
+	const float n1_p_y = -n1.x / n1_xy_norm;
+	const float n1_z_norm = sqrtf((n1.x * n1.z) * (n1.x * n1.z) + (n1.y * n1.z) * (n1.y * n1.z) + n1_xy_norm2);
+	const float n1_p_i = (n1_i * n1.z) / n1_z_norm;
+	const float n1_p_z = -n1_xy_norm2 / n1_z_norm;
+	const float n2_xy_norm2 = n2.x * n2.x + n2.y * n2.y;
+	const float n2_xy_norm = sqrtf(n2_xy_norm2);
+	const float n2_p_x = n2.y / n2_xy_norm;
+	const float n2_p_y = -n2.x / n2_xy_norm;
+	const float n2_z_norm = sqrtf((n2.x * n2.z) * (n2.x * n2.z) + (n2.y * n2.z) * (n2.y * n2.z) + n2_xy_norm2);
+	const float n2_p_i = (n2_i * n2.z) / n2_z_norm;
+	const float n2_p_z = -n2_xy_norm2 / n2_z_norm;
+	const float htt = thickness_trans * 0.5f;
+	const float d1_xy_lo_x = d1.x - htt * n1_p_x, d1_xy_lo_y = d1.y - htt * n1_p_y;
+	const float d1_xy_hi_x = d1.x + htt * n1_p_x, d1_xy_hi_y = d1.y + htt * n1_p_y;
+	const float d2_xy_lo_x = d2.x - htt * n2_p_x, d2_xy_lo_y = d2.y - htt * n2_p_y;
+	const float d2_xy_hi_x = d2.x + htt * n2_p_x, d2_xy_hi_y = d2.y + htt * n2_p_y;
+	const float htz = thickness_z * 0.5f;
+	const float d1_z_lo_i = d1_i - htz * n1_p_i, d1_z_lo_z = d1.z - htz * n1_p_z;
+	const float d1_z_hi_i = d1_i + htz * n1_p_i, d1_z_hi_z = d1.z + htz * n1_p_z;
+	const float d2_z_lo_i = d2_i - htz * n2_p_i, d2_z_lo_z = d2.z - htz * n2_p_z;
+	const float d2_z_hi_i = d2_i + htz * n2_p_i, d2_z_hi_z = d2.z + htz * n2_p_z;
+
+	int xy_i_0, xy_i_1, nyx;
+	float lxy, lyx, dxy, dyx;
+	float d1_xy_lo, d1_xy_hi, d2_xy_lo, d2_xy_hi, d1_yx_lo, d1_yx_hi, d2_yx_lo, d2_yx_hi;
+	if (flag_y)
+	{
+		xy_i_0 = max(0, min(y_i_0, y_i_1));
+		xy_i_1 = min(g.ny - 1, max(y_i_0, y_i_1));
+		lxy = g.ly; dxy = g.vy; lyx = g.lx; dyx = g.vx; nyx = g.nx;
+		d1_xy_lo = d1_xy_lo_y; d1_xy_hi = d1_xy_hi_y; d2_xy_lo = d2_xy_lo_y; d2_xy_hi = d2_xy_hi_y;
+		d1_yx_lo = d1_xy_lo_x; d1_yx_hi = d1_xy_hi_x; d2_yx_lo = d2_xy_lo_x; d2_yx_hi = d2_xy_hi_x;
+	}
+	else
+	{
+		xy_i_0 = max(0, min(x_i_0, x_i_1));
+		xy_i_1 = min(g.nx - 1, max(x_i_0, x_i_1));
+		lxy = g.lx; dxy = g.vx; lyx = g.ly; dyx = g.vy; nyx = g.ny;
+		d1_xy_lo = d1_xy_lo_x; d1_xy_hi = d1_xy_hi_x; d2_xy_lo = d2_xy_lo_x; d2_xy_hi = d2_xy_hi_x;
+		d1_yx_lo = d1_xy_lo_y; d1_yx_hi = d1_xy_hi_y; d2_yx_lo = d2_xy_lo_y; d2_yx_hi = d2_xy_hi_y;
+	}
+	const float dxy_cos_theta =
+	    (d1_i != d2_i) ? dxy / (fabsf(d1_i - d2_i) / d_norm) : dxy;
+	const int nxy = g.nx * g.ny;
+	const float yx_off = static_cast<float>(nyx - 1) / 2.f;
+	const float inv_dyx = 1.0f / dyx;
+	const float z_off = static_cast<float>(g.nz - 1) * 0.5f;
+	const float inv_dz = 1.0f / dz;
+	const float half_dyx = dyx * 0.5f;
+
+	for (int xyi = xy_i_0; xyi <= xy_i_1; xyi++)
+	{
+		const float pix_xy = -0.5f * lxy + (static_cast<float>(xyi) + 0.5f) * dxy;
+		const float a_xy_lo = (pix_xy - d1_xy_lo) / (d2_xy_hi - d1_xy_lo);
+		const float a_xy_hi = (pix_xy - d1_xy_hi) / (d2_xy_lo - d1_xy_hi);
+		const float a_z_lo = (pix_xy - d1_z_lo_i) / (d2_z_lo_i - d1_z_lo_i);
+		const float a_z_hi = (pix_xy - d1_z_hi_i) / (d2_z_hi_i - d1_z_hi_i);
+		float r0 = d1_yx_lo + a_xy_lo * (d2_yx_hi - d1_yx_lo);
+		float r1 = d1_yx_hi + a_xy_hi * (d2_yx_lo - d1_yx_hi);
+		if (r0 > r1)
+		{
+			const float t = r0;
+			r0 = r1;
+			r1 = t;
+		}
+		const float widthFrac_yx = r1 - r0;
+		const float r0_ov = r0, r1_ov = r1;
+		r0 -= ext;
+		r1 += ext;
+		const int i0 = max(0, static_cast<int>(rintf(r0 * inv_dyx + yx_off)));
+		const int i1 = min(nyx - 1, static_cast<int>(rintf(r1 * inv_dyx + yx_off)));
+		float zr0 = d1_z_lo_z + a_z_lo * (d2_z_lo_z - d1_z_lo_z);
+		float zr1 = d1_z_hi_z + a_z_hi * (d2_z_hi_z - d1_z_hi_z);
+		if (zr0 > zr1)
+		{
+			const float t = zr0;
+			zr0 = zr1;
+			zr1 = t;
+		}
+		const float widthFrac_z = zr1 - zr0;
+		const int zi0 = max(0, static_cast<int>(rintf(zr0 * inv_dz + z_off)));
+		const int zi1 = min(g.nz - 1, static_cast<int>(rintf(zr1 * inv_dz + z_off)));
+		float tw = 1.f;
+		if constexpr (TOF)
+		{
+			const float a_lo = (pix_xy - d1_i - 0.5f * dxy) / (d2_i - d1_i);
+			const float a_hi = (pix_xy - d1_i + 0.5f * dxy) / (d2_i - d1_i);
+			tw = tofWeight(tp, d_norm, tofValue, a_lo * d_norm, a_hi * d_norm);
+		}
+		for (int yxi = i0; yxi <= i1; yxi++)
+		{
+			const float pix_yx = -0.5f * lyx + (static_cast<float>(yxi) + 0.5f) * dyx;
+			const float p0 = pix_yx - half_dyx, p1 = pix_yx + half_dyx;
+			if (!(r1 >= p0 && r0 < p1))
+				continue;
+			float wxy;
+			if constexpr (PSF)
+			{
+				const int halfWidth = (psf.size + 1) / 2;
+				const float xa = p0 - r1_ov, xb = p1 - r0_ov;
+				if (xa > halfWidth * psf.kSpacing || xb < -halfWidth * psf.kSpacing || xa >= xb)
+					wxy = 0.f;
+				else
+					wxy = psfIntegral(kern, psf.size, psf.kSpacing, xa, xb);
+			}
+			else
+			{
+				wxy = fminf(p1, r1_ov) - fmaxf(p0, r0_ov);
+			}
+			const float wxy_s = wxy / widthFrac_yx;
+			for (int zi = zi0; zi <= zi1; zi++)
+			{
+				const float pix_z = -0.5f * g.lz + (static_cast<float>(zi) + 0.5f) * g.vz;
+				const float zp0 = pix_z - g.vz * 0.5f, zp1 = pix_z + g.vz * 0.5f;
+				if (zr1 >= zp0 && zr0 < zp1)
+				{
+					const float wz = fminf(zp1, zr1) - fmaxf(zp0, zr0);
+					const float wz_s = wz / widthFrac_z;
+					const int o = zi * nxy + (flag_y ? g.nx * xyi + yxi : g.nx * yxi + xyi);
+					float w = wxy_s * wz_s * dxy_cos_theta;
+					if constexpr (TOF)
+						w *= tw;
+					visit(o, w);
+				}
+			}
+		}
+	}
+}
+
+}  // namespace yrtb

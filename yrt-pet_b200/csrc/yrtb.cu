@@ -1,0 +1,1567 @@
+// libyrtb: B200 (sm_100a) kernels and C ABI for YRT-PET's projection path.
+//
+// Layout in HBM
+//   events   structure-of-arrays, one entry per event (detector ids u32 x2,
+//            TOF f32, frame i32, correction factors f32), device resident
+//            across OSEM iterations; subsets are index ranges.
+//   LUT      crystal centres and orientations as float4 pairs (32 B per
+//            crystal, L2 resident: 1.7 MB for 53,760 crystals).
+//   images   float32 [t][z][y][x]; forward projection gathers from them,
+//            back projection scatters with fire-and-forget float reductions
+//            (red.global.add.f32) that resolve in L2 (the 4-42 MB images of
+//            the target workloads stay L2 resident on B200's 126 MB L2).
+//
+// Kernels are grid-stride loops sized to a multiple of the SM count; one
+// thread walks one LOR (or one histogram bin) so that every voxel crossing is
+// an independent L2 transaction and no inter-thread synchronisation is needed.
+
+#include "yrt_b200.h"
+#include "device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace yrtb;
+
+namespace
+{
+thread_local std::string g_lastError;
+
+yrtb_status fail(yrtb_status code, const std::string& msg)
+{
+	g_lastError = msg;
+	return code;
+}
+
+#define YRTB_CUDA(call)                                                      \
+	do                                                                       \
+	{                                                                        \
+		cudaError_t e_ = (call);                                             \
+		if (e_ != cudaSuccess)                                               \
+			return fail(YRTB_ERR_CUDA, std::string(#call) + ": " +           \
+			                               cudaGetErrorString(e_));          \
+	} while (0)
+
+#define YRTB_LAUNCHED()                                                      \
+	do                                                                       \
+	{                                                                        \
+		cudaError_t e_ = cudaGetLastError();                                 \
+		if (e_ != cudaSuccess)                                               \
+			return fail(YRTB_ERR_CUDA,                                       \
+			            std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+	} while (0)
+
+constexpr int kBlock = 256;
+
+// ------------------------------------------------------ Histogram3D maps --
+// Integer maps of the reference Histogram3D (Histogram3D.cpp:165-450) in a
+// form a kernel can evaluate: the in-ring pair <-> (r, phi) map becomes a
+// dense dpr x dpr table, the z-bin decode loop becomes a table of (z1, z2).
+struct H3Host
+{
+	uint64_t numR, numPhi, numZBin, numZBinDiff, numDOIPoss, rCut;
+	uint64_t dpr, rings, ndoi, mrd;
+	std::vector<int32_t> ringMap;  // d1_ring*dpr + d2_ring -> r_ring*dpr + phi | -1
+	std::vector<int2> zPairs;      // z_bin -> (z1, z2)
+
+	void pairInRing(uint64_t r_ring, uint64_t phi, uint32_t& a, uint32_t& b) const
+	{
+		const int n = static_cast<int>(dpr);
+		const int r = static_cast<int>(r_ring);
+		const int d02 = (phi % 2 != 0) ? n / 2 + 1 : n / 2;
+		int dr1 = r - n / 4 + static_cast<int>(rCut);
+		int dr2 = d02 - (r - n / 4 + static_cast<int>(rCut));
+		if (dr1 < 0)
+			dr1 += n;
+		if (dr2 < 0)
+			dr2 += n;
+		a = static_cast<uint32_t>((dr1 + static_cast<int>(phi) / 2) % n);
+		b = static_cast<uint32_t>((dr2 + static_cast<int>(phi) / 2) % n);
+		if (a > b)
+			std::swap(a, b);
+	}
+
+	explicit H3Host(const yrtb_scanner& s)
+	{
+		dpr = s.dets_per_ring;
+		rings = s.num_rings;
+		ndoi = s.num_doi;
+		mrd = s.max_ring_diff;
+		rCut = s.min_ang_diff / 2;
+		if (s.min_ang_diff % 2 != 0 && dpr % 4 == 0)
+			rCut++;
+		numDOIPoss = ndoi * ndoi;
+		numR = numDOIPoss * (dpr / 2 + 1 - s.min_ang_diff);
+		numPhi = dpr;
+		const uint64_t nz = (mrd + 1) * rings - (mrd * (mrd + 1)) / 2;
+		numZBinDiff = nz - rings;
+		numZBin = nz + numZBinDiff;
+		ringMap.assign(dpr * dpr, -1);
+		for (uint64_t phi = 0; phi < numPhi; phi++)
+			for (uint64_t r = 0; r < numR / numDOIPoss; r++)
+			{
+				uint32_t a, b;
+				pairInRing(r, phi, a, b);
+				ringMap[a * dpr + b] = static_cast<int32_t>(r * dpr + phi);
+			}
+		zPairs.resize(numZBin);
+		for (uint64_t zb = 0; zb < numZBin; zb++)
+		{
+			int z1, z2;
+			if (zb < rings)
+			{
+				z1 = z2 = static_cast<int>(zb);
+			}
+			else
+			{
+				int cur = (static_cast<int>(zb) - static_cast<int>(rings)) %
+				              static_cast<int>(numZBinDiff) +
+				          static_cast<int>(rings);
+				int planes = static_cast<int>(rings);
+				int dz = 0;
+				while (cur - planes >= 0)
+				{
+					cur -= planes;
+					planes -= 1;
+					dz++;
+				}
+				z1 = cur;
+				z2 = z1 + dz;
+				if (zb - rings >= numZBinDiff)
+					std::swap(z1, z2);
+			}
+			zPairs[zb] = make_int2(z1, z2);
+		}
+	}
+};
+
+struct H3Dev
+{
+	uint32_t numDets;
+	const int32_t* ringMap;
+	const int2* zPairs;
+	uint32_t dpr, rings, ndoi, numDOIPoss, rCut;
+	uint32_t mrd;
+	uint64_t numR, numPhi, numZBin, numZBinDiff;
+};
+
+__device__ __forceinline__ bool h3Bin(const H3Dev& h, uint32_t d1, uint32_t d2,
+                                      uint64_t& out)
+{
+	if ((d1 == 0 && d2 == 0) || d1 >= h.numDets || d2 >= h.numDets)
+		return false;
+	if (d1 > d2)
+	{
+		const uint32_t t = d1;
+		d1 = d2;
+		d2 = t;
+	}
+	uint32_t r1 = d1 % h.dpr, r2 = d2 % h.dpr;
+	if (r1 > r2)
+	{
+		uint32_t t = d1;
+		d1 = d2;
+		d2 = t;
+		t = r1;
+		r1 = r2;
+		r2 = t;
+	}
+	const int32_t m = __ldg(h.ringMap + static_cast<uint64_t>(r1) * h.dpr + r2);
+	if (m < 0)
+		return false;
+	const uint64_t r_ring = static_cast<uint32_t>(m) / h.dpr;
+	const uint64_t phi = static_cast<uint32_t>(m) % h.dpr;
+	const uint64_t ringDets = static_cast<uint64_t>(h.rings) * h.dpr;
+	const uint64_t doi1 = d1 / ringDets, doi2 = d2 / ringDets;
+	const uint64_t r = r_ring * h.numDOIPoss + (doi1 + doi2 * h.ndoi);
+	const int z1 = static_cast<int>((d1 / h.dpr) % h.rings);
+	const int z2 = static_cast<int>((d2 / h.dpr) % h.rings);
+	const uint32_t dz = static_cast<uint32_t>(abs(z2 - z1));
+	if (dz > h.mrd)
+		return false;
+	const uint64_t removed = static_cast<uint64_t>(dz) * (dz - 1) / 2;
+	uint64_t zb = static_cast<uint64_t>(dz) * h.rings + min(z1, z2) - removed;
+	if (dz > 0 && z1 > z2)
+		zb += h.numZBinDiff;
+	out = zb * h.numPhi * h.numR + phi * h.numR + r;
+	return true;
+}
+
+__device__ __forceinline__ void h3Pair(const H3Dev& h, uint64_t bin,
+                                       uint32_t& d1, uint32_t& d2)
+{
+	const uint64_t z_bin = bin / (h.numPhi * h.numR);
+	const uint64_t rem = bin % (h.numPhi * h.numR);
+	const uint32_t phi = static_cast<uint32_t>(rem / h.numR);
+	const uint32_t r = static_cast<uint32_t>(rem % h.numR);
+	const int n = static_cast<int>(h.dpr);
+	const int rr = static_cast<int>(r / h.numDOIPoss);
+	const int d02 = (phi % 2 != 0) ? n / 2 + 1 : n / 2;
+	int dr1 = rr - n / 4 + static_cast<int>(h.rCut);
+	int dr2 = d02 - (rr - n / 4 + static_cast<int>(h.rCut));
+	if (dr1 < 0)
+		dr1 += n;
+	if (dr2 < 0)
+		dr2 += n;
+	uint32_t a = static_cast<uint32_t>((dr1 + static_cast<int>(phi) / 2) % n);
+	uint32_t b = static_cast<uint32_t>((dr2 + static_cast<int>(phi) / 2) % n);
+	if (a > b)
+	{
+		const uint32_t t = a;
+		a = b;
+		b = t;
+	}
+	if (a == b)
+	{
+		d1 = d2 = 0;
+		return;
+	}
+	const uint32_t doi_case = r % h.numDOIPoss;
+	const uint32_t doi1 = doi_case % h.ndoi, doi2 = doi_case / h.ndoi;
+	const int2 zz = __ldg(h.zPairs + z_bin);
+	d1 = a + static_cast<uint32_t>(zz.x) * h.dpr + doi1 * (h.dpr * h.rings);
+	d2 = b + static_cast<uint32_t>(zz.y) * h.dpr + doi2 * (h.dpr * h.rings);
+}
+
+// Bin of the idx-th element of histogram subset `subset` (phi = subset mod
+// numSubsets): BinIteratorRangeHistogram3D::getSafe (BinIterator.cpp:185-193).
+__device__ __forceinline__ uint64_t h3SubsetBin(const H3Dev& h, uint64_t idx,
+                                                uint64_t numPhiSubset,
+                                                uint64_t numSubsets,
+                                                uint64_t subset)
+{
+	const uint64_t per = numPhiSubset * h.numR;
+	const uint64_t z_bin = idx / per;
+	const uint64_t rem = idx % per;
+	const uint64_t phi = (rem / h.numR) * numSubsets + subset;
+	const uint64_t r = rem % h.numR;
+	return z_bin * h.numPhi * h.numR + phi * h.numR + r;
+}
+
+uint64_t h3SubsetSize(const H3Host& h, uint64_t numSubsets, uint64_t subset,
+                      uint64_t& numPhiSubset)
+{
+	numPhiSubset = h.numPhi / numSubsets;
+	if (subset + numPhiSubset * numSubsets < h.numPhi)
+		numPhiSubset += 1;
+	return h.numR * numPhiSubset * h.numZBin;
+}
+
+// ------------------------------------------------------------ kernels ----
+enum Kind
+{
+	K_SIDDON = 0,
+	K_SIDDON_MR = 1,
+	K_DD = 2,
+	K_DD_PSF = 3
+};
+
+struct KParams
+{
+	Geom g;
+	TofP tof;
+	Psf psf;
+	Scan scan;
+	int numRays;
+};
+
+// Endpoints (relative to the image centre) and orientations of event e.
+__device__ __forceinline__ bool fetchEvent(const KParams& P, const Events& E,
+                                           uint64_t e, float3& p1, float3& p2,
+                                           float3& n1, float3& n2)
+{
+	if (E.d1 != nullptr)
+	{
+		const uint32_t a = __ldg(E.d1 + e), b = __ldg(E.d2 + e);
+		// Invalid ids are counted by the caller and never dereferenced.
+		if (a >= P.scan.numDets || b >= P.scan.numDets)
+			return false;
+		const float4 pa = __ldg(P.scan.pos + a), pb = __ldg(P.scan.pos + b);
+		const float4 oa = __ldg(P.scan.ori + a), ob = __ldg(P.scan.ori + b);
+		p1 = make_float3(pa.x, pa.y, pa.z);
+		p2 = make_float3(pb.x, pb.y, pb.z);
+		n1 = make_float3(oa.x, oa.y, oa.z);
+		n2 = make_float3(ob.x, ob.y, ob.z);
+	}
+	else
+	{
+		const float* l = E.lor + e * 6;
+		p1 = make_float3(__ldg(l + 0), __ldg(l + 1), __ldg(l + 2));
+		p2 = make_float3(__ldg(l + 3), __ldg(l + 4), __ldg(l + 5));
+		n1 = make_float3(0.f, 0.f, 0.f);
+		n2 = n1;
+	}
+	if (E.mframe != nullptr)
+	{
+		const int mf = __ldg(E.mframe + e);
+		if (mf >= 0 && static_cast<uint64_t>(mf) >= E.numMotion)
+			return false;
+		if (mf >= 0)
+		{
+			const float* m = E.motion + static_cast<int64_t>(mf) * 12;
+			const float r00 = __ldg(m + 0), r01 = __ldg(m + 1), r02 = __ldg(m + 2);
+			const float r10 = __ldg(m + 3), r11 = __ldg(m + 4), r12 = __ldg(m + 5);
+			const float r20 = __ldg(m + 6), r21 = __ldg(m + 7), r22 = __ldg(m + 8);
+			const float tx = __ldg(m + 9), ty = __ldg(m + 10), tz = __ldg(m + 11);
+			// Matrix::operator*(Vector3D) then + translation (Matrix.cpp:177-186).
+			float3 q1 = make_float3(r00 * p1.x + r01 * p1.y + r02 * p1.z,
+			                        r10 * p1.x + r11 * p1.y + r12 * p1.z,
+			                        r20 * p1.x + r21 * p1.y + r22 * p1.z);
+			float3 q2 = make_float3(r00 * p2.x + r01 * p2.y + r02 * p2.z,
+			                        r10 * p2.x + r11 * p2.y + r12 * p2.z,
+			                        r20 * p2.x + r21 * p2.y + r22 * p2.z);
+			p1 = make_float3(q1.x + tx, q1.y + ty, q1.z + tz);
+			p2 = make_float3(q2.x + tx, q2.y + ty, q2.z + tz);
+		}
+	}
+	const float3 off = make_float3(P.g.offx, P.g.offy, P.g.offz);
+	p1 = f3sub(p1, off);
+	p2 = f3sub(p2, off);
+	return isfinite(p1.x) && isfinite(p1.y) && isfinite(p1.z) &&
+	       isfinite(p2.x) && isfinite(p2.y) && isfinite(p2.z);
+}
+
+// Runs the configured projector over one event; endRay() after each ray.
+template <int KIND, bool TOF, bool COMP, typename Visit, typename EndRay>
+__device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
+                                             float3 p2, float3 n1, float3 n2,
+                                             float tofv, uint64_t rid,
+                                             bool forward, Visit& visit,
+                                             EndRay& endRay)
+{
+	if constexpr (KIND == K_SIDDON)
+	{
+		siddonWalk<TOF, COMP>(P.g, p1, p2, P.tof, tofv, visit);
+		endRay();
+	}
+	else if constexpr (KIND == K_SIDDON_MR)
+	{
+		MultiRay mr;
+		mr.init(rid, n1, n2);
+		for (int k = 0; k < P.numRays; k++)
+		{
+			float3 a = p1, b = p2;
+			if (k > 0)
+			{
+				float u[4];
+				mr.next(u);
+				mr.offset(u, P.scan.crystalZ, P.scan.crystalTrans, a, b);
+			}
+			siddonWalk<TOF, COMP>(P.g, a, b, P.tof, tofv, visit);
+			endRay();
+		}
+	}
+	else
+	{
+		ddWalk<TOF, KIND == K_DD_PSF>(P.g, p1, p2, n1, n2, P.scan.crystalTrans,
+		                              P.scan.crystalZ, P.tof, tofv, P.psf,
+		                              forward, visit);
+		endRay();
+	}
+}
+
+// Forward sum of one event: per-ray partial sums added ray by ray; mirror
+// mode sums in traversal order, compensated mode uses Kahan summation.
+template <int KIND, bool TOF, bool COMP>
+__device__ __forceinline__ float forwardEvent(const KParams& P,
+                                              const float* __restrict__ img,
+                                              float3 p1, float3 p2, float3 n1,
+                                              float3 n2, float tofv,
+                                              uint64_t rid)
+{
+	float acc = 0.f, ray = 0.f, comp = 0.f;
+	auto visit = [&](int o, float w)
+	{
+		const float term = w * __ldg(img + o);
+		if constexpr (COMP)
+		{
+			const float y = term - comp;
+			const float t = ray + y;
+			comp = (t - ray) - y;
+			ray = t;
+		}
+		else
+		{
+			ray += term;
+		}
+	};
+	auto endRay = [&]
+	{
+		acc += ray;
+		ray = 0.f;
+		comp = 0.f;
+	};
+	projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, true, visit,
+	                              endRay);
+	if constexpr (KIND == K_SIDDON_MR)
+		acc = acc / static_cast<float>(P.numRays);
+	return acc;
+}
+
+template <int KIND, bool TOF, bool COMP>
+__device__ __forceinline__ void backwardEvent(const KParams& P,
+                                              float* __restrict__ img,
+                                              float v, float3 p1, float3 p2,
+                                              float3 n1, float3 n2, float tofv,
+                                              uint64_t rid)
+{
+	if constexpr (KIND == K_SIDDON_MR)
+		v = v / static_cast<float>(P.numRays);
+	auto visit = [&](int o, float w) { atomicAdd(img + o, v * w); };
+	auto endRay = [] {};
+	projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+	                              endRay);
+}
+
+enum Op
+{
+	OP_FWD = 0,
+	OP_BWD = 1,
+	OP_EM = 2,
+	OP_COUNT = 3
+};
+
+template <int OP, int KIND, bool TOF, bool COMP>
+__global__ void __launch_bounds__(kBlock)
+    k_events(KParams P, Events E, Range R, const float* __restrict__ in,
+             float* __restrict__ out, float globalScale, float denomThr,
+             unsigned long long* err)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     k < R.count; k += nthreads)
+	{
+		const uint64_t e = R.start + k * R.stride;
+		const int frame = E.frame ? __ldg(E.frame + e) : 0;
+		float3 p1, p2, n1, n2;
+		if (frame < 0 || frame >= P.g.nt || !fetchEvent(P, E, e, p1, p2, n1, n2))
+		{
+			if (frame >= 0)
+				atomicAdd(err, 1ULL);
+			if constexpr (OP == OP_FWD)
+				out[e] = 0.f;
+			if constexpr (OP == OP_COUNT)
+				reinterpret_cast<uint32_t*>(out)[e] = 0u;
+			continue;
+		}
+		const float tofv = TOF ? __ldg(E.tof + e) : 0.f;
+		const int64_t fo = static_cast<int64_t>(frame) * P.g.nvox;
+		if constexpr (OP == OP_COUNT)
+		{
+			unsigned c = 0;
+			auto visit = [&](int, float) { c++; };
+			auto endRay = [] {};
+			projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, k, true, visit,
+			                              endRay);
+			reinterpret_cast<uint32_t*>(out)[e] = c;
+		}
+		else if constexpr (OP == OP_FWD)
+		{
+			out[e] = forwardEvent<KIND, TOF, COMP>(P, in + fo, p1, p2, n1, n2,
+			                                       tofv, k);
+		}
+		else if constexpr (OP == OP_BWD)
+		{
+			backwardEvent<KIND, TOF, COMP>(P, out + fo, __ldg(in + e), p1, p2,
+			                               n1, n2, tofv, k);
+		}
+		else
+		{
+			const float m = E.meas ? __ldg(E.meas + e) : 1.0f;
+			const float s = E.sens ? __ldg(E.sens + e) : 1.0f;
+			const float a = E.att ? __ldg(E.att + e) : 1.0f;
+			if (m == 0.f || s == 0.f || a == 0.f)
+				continue;
+			float u = forwardEvent<KIND, TOF, COMP>(P, in + fo, p1, p2, n1, n2,
+			                                        tofv, k);
+			u *= s;
+			u *= a;
+			u *= globalScale;
+			if (E.add)
+				u += __ldg(E.add + e);
+			if (fabsf(u) > denomThr)
+			{
+				u = m / u;
+				u *= s;
+				u *= a;
+				u *= globalScale;
+				backwardEvent<KIND, TOF, COMP>(P, out + fo, u, p1, p2, n1, n2,
+				                               tofv, k);
+			}
+		}
+	}
+}
+
+// Attenuation factor per event: exp(-0.1 * line integral of mu).
+__global__ void __launch_bounds__(kBlock)
+    k_attenuation(KParams P, Geom mu, Events E, Range R,
+                  const float* __restrict__ muImg, float* __restrict__ out,
+                  unsigned long long* err)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     k < R.count; k += nthreads)
+	{
+		const uint64_t e = R.start + k * R.stride;
+		float3 p1, p2, n1, n2;
+		if (!fetchEvent(P, E, e, p1, p2, n1, n2))
+		{
+			atomicAdd(err, 1ULL);
+			out[e] = 0.f;
+			continue;
+		}
+		// fetchEvent subtracted the reconstruction grid offset; move to the
+		// attenuation grid instead.
+		const float3 fix = make_float3(P.g.offx - mu.offx, P.g.offy - mu.offy,
+		                               P.g.offz - mu.offz);
+		p1 = make_float3(p1.x + fix.x, p1.y + fix.y, p1.z + fix.z);
+		p2 = make_float3(p2.x + fix.x, p2.y + fix.y, p2.z + fix.z);
+		float acc = 0.f;
+		auto visit = [&](int o, float w) { acc += w * __ldg(muImg + o); };
+		siddonWalk<false, false>(mu, p1, p2, P.tof, 0.f, visit);
+		out[e] = expf(-acc * 0.1f);
+	}
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_gather_histo(KParams P, H3Dev H, Events E, Range R,
+                   const float* __restrict__ histo, int invert,
+                   float* __restrict__ out, unsigned long long* err)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     k < R.count; k += nthreads)
+	{
+		const uint64_t e = R.start + k * R.stride;
+		uint64_t b;
+		float v = 0.f;
+		if (h3Bin(H, __ldg(E.d1 + e), __ldg(E.d2 + e), b))
+		{
+			v = __ldg(histo + b);
+			if (invert && v != 0.f)
+				v = 1.0f / v;
+		}
+		else
+		{
+			atomicAdd(err, 1ULL);
+		}
+		out[e] = v;
+	}
+}
+
+// Histogram-bin kernels: sensitivity back projection and histogram EM.
+template <int KIND, bool EM>
+__global__ void __launch_bounds__(kBlock)
+    k_histo(KParams P, H3Dev H, uint64_t count, uint64_t numPhiSubset,
+            uint64_t numSubsets, uint64_t subset, const float* __restrict__ img,
+            float* __restrict__ out, const float* __restrict__ meas,
+            const float* __restrict__ sensH, const float* __restrict__ acfH,
+            const float* __restrict__ addH, Geom mu,
+            const float* __restrict__ muImg, float globalScale, float denomThr)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     k < count; k += nthreads)
+	{
+		const uint64_t bin = h3SubsetBin(H, k, numPhiSubset, numSubsets, subset);
+		uint32_t d1, d2;
+		h3Pair(H, bin, d1, d2);
+		if (d1 == 0 && d2 == 0)
+			continue;
+		const float m = EM ? __ldg(meas + bin) : 1.0f;
+		if (EM && m == 0.f)
+			continue;
+		const float s = sensH ? __ldg(sensH + bin) : 1.0f;
+		const float4 pa = __ldg(P.scan.pos + d1), pb = __ldg(P.scan.pos + d2);
+		const float4 oa = __ldg(P.scan.ori + d1), ob = __ldg(P.scan.ori + d2);
+		float3 p1 = make_float3(pa.x, pa.y, pa.z), p2 = make_float3(pb.x, pb.y, pb.z);
+		const float3 n1 = make_float3(oa.x, oa.y, oa.z), n2 = make_float3(ob.x, ob.y, ob.z);
+		float a = 1.0f;
+		if (acfH)
+		{
+			a = __ldg(acfH + bin);
+		}
+		else if (muImg)
+		{
+			float acc = 0.f;
+			auto visit = [&](int o, float w) { acc += w * __ldg(muImg + o); };
+			const float3 mo = make_float3(mu.offx, mu.offy, mu.offz);
+			siddonWalk<false, false>(mu, f3sub(p1, mo), f3sub(p2, mo), P.tof, 0.f, visit);
+			a = expf(-acc * 0.1f);
+		}
+		const float3 off = make_float3(P.g.offx, P.g.offy, P.g.offz);
+		p1 = f3sub(p1, off);
+		p2 = f3sub(p2, off);
+		if constexpr (!EM)
+		{
+			backwardEvent<KIND, false, false>(P, out, a * s, p1, p2, n1, n2, 0.f, k);
+		}
+		else
+		{
+			float u = forwardEvent<KIND, false, false>(P, img, p1, p2, n1, n2, 0.f, k);
+			u *= s;
+			u *= a;
+			u *= globalScale;
+			if (addH)
+				u += __ldg(addH + bin);
+			if (fabsf(u) > denomThr)
+			{
+				u = m / u;
+				u *= s;
+				u *= a;
+				u *= globalScale;
+				backwardEvent<KIND, false, false>(P, out, u, p1, p2, n1, n2, 0.f, k);
+			}
+		}
+	}
+}
+
+__global__ void k_multiray_offsets(uint64_t count, int numRays,
+                                   float* __restrict__ out)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	const int per = 4 * (numRays - 1);
+	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     k < count; k += nthreads)
+	{
+		MultiRay mr;
+		mr.init(k, make_float3(1.f, 0.f, 0.f), make_float3(1.f, 0.f, 0.f));
+		for (int r = 1; r < numRays; r++)
+		{
+			float u[4];
+			mr.next(u);
+			for (int i = 0; i < 4; i++)
+				out[k * per + 4 * (r - 1) + i] = u[i];
+		}
+	}
+}
+
+__global__ void k_lm_to_histo(H3Dev H, const uint32_t* __restrict__ d1,
+                              const uint32_t* __restrict__ d2,
+                              const float* __restrict__ vals, uint64_t n,
+                              float* __restrict__ histo,
+                              unsigned long long* invalid)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+	{
+		const float v = vals ? __ldg(vals + i) : 1.0f;
+		if (!(v > 0.f))
+			continue;
+		const uint32_t a = __ldg(d1 + i), b = __ldg(d2 + i);
+		if (a == b)
+			continue;
+		uint64_t bin;
+		if (!h3Bin(H, a, b, bin))
+		{
+			atomicAdd(invalid, 1ULL);
+			continue;
+		}
+		atomicAdd(histo + bin, v);
+	}
+}
+
+__global__ void k_bins(H3Dev H, const uint32_t* __restrict__ d1,
+                       const uint32_t* __restrict__ d2, uint64_t n,
+                       uint64_t* __restrict__ bins)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+	{
+		uint64_t b;
+		bins[i] = h3Bin(H, __ldg(d1 + i), __ldg(d2 + i), b) ? b : ~0ULL;
+	}
+}
+
+__global__ void k_pairs(H3Dev H, const uint64_t* __restrict__ bins, uint64_t n,
+                        uint32_t* __restrict__ d1, uint32_t* __restrict__ d2)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	const uint64_t total = H.numZBin * H.numPhi * H.numR;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+	{
+		const uint64_t b = __ldg(bins + i);
+		uint32_t a = 0, c = 0;
+		if (b < total)
+			h3Pair(H, b, a, c);
+		d1[i] = a;
+		d2[i] = c;
+	}
+}
+
+// ---------------------------------------------------- image-space ops ----
+__global__ void k_em_update(float* __restrict__ x, const float* __restrict__ u,
+                            const float* __restrict__ s, uint64_t J, int64_t nt,
+                            int64_t sens_nt, float thr,
+                            const float* __restrict__ scale)
+{
+	const uint64_t total = J * static_cast<uint64_t>(nt);
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < total; i += nthreads)
+	{
+		const uint64_t j = i % J;
+		const uint64_t r = i / J;
+		if (sens_nt == nt && nt > 1)
+		{
+			const float sv = __ldg(s + i);
+			if (sv > thr)
+				x[i] *= __ldg(u + i) / sv;
+		}
+		else if (nt == 1)
+		{
+			const float sv = __ldg(s + j);
+			if (sv > thr)
+				x[i] *= __ldg(u + i) / sv;
+		}
+		else
+		{
+			// updateEMThresholdDynamicWithScaling (Image.cpp:760-800).
+			const float inv_c = scale ? 1.0f / __ldg(scale + r) : 1.0f;
+			const float thr_r = thr * inv_c;
+			const float sv = __ldg(s + j);
+			if (sv > thr_r)
+				x[i] *= (__ldg(u + i) * inv_c) / sv;
+		}
+	}
+}
+
+__global__ void k_threshold(float* __restrict__ x, const float* __restrict__ m,
+                            uint64_t J, int64_t nt, int broadcast, float thr,
+                            float les, float leo, float gts, float gto)
+{
+	const uint64_t total = J * static_cast<uint64_t>(nt);
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < total; i += nthreads)
+	{
+		const float mv = __ldg(m + (broadcast ? i % J : i));
+		x[i] = (mv <= thr) ? x[i] * les + leo : x[i] * gts + gto;
+	}
+}
+
+__global__ void k_fill(float* __restrict__ x, uint64_t n, float v)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+		x[i] = v;
+}
+
+__global__ void k_scale(float* __restrict__ x, uint64_t n, float v)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+		x[i] *= v;
+}
+
+int g_numSMs = 0;
+
+unsigned gridFor(uint64_t n, int perSM = 8)
+{
+	if (g_numSMs == 0)
+	{
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&g_numSMs, cudaDevAttrMultiProcessorCount, dev);
+		if (g_numSMs <= 0)
+			g_numSMs = 148;
+	}
+	const uint64_t need = (n + kBlock - 1) / kBlock;
+	const uint64_t cap = static_cast<uint64_t>(g_numSMs) * perSM;
+	return static_cast<unsigned>(std::max<uint64_t>(1, std::min(need, cap)));
+}
+
+Geom makeGeom(const yrtb_image_params& ip)
+{
+	Geom g{};
+	g.nt = static_cast<int>(ip.nt);
+	g.nx = static_cast<int>(ip.nx);
+	g.ny = static_cast<int>(ip.ny);
+	g.nz = static_cast<int>(ip.nz);
+	g.nxy = ip.nx * ip.ny;
+	g.nvox = ip.nx * ip.ny * ip.nz;
+	g.lx = ip.length_x;
+	g.ly = ip.length_y;
+	g.lz = ip.length_z;
+	// ImageParams::completeDimInfo / setup (ImageParams.cpp:205-270).
+	g.vx = ip.length_x / static_cast<float>(ip.nx);
+	g.vy = ip.length_y / static_cast<float>(ip.ny);
+	g.vz = ip.length_z / static_cast<float>(ip.nz);
+	float fr = std::max(ip.length_x / 2.0f, ip.length_y / 2.0f);
+	fr -= std::max(g.vx, g.vy) / 1000.0f;
+	g.fovRadius = fr;
+	auto snap = [](float o) { return std::fabs(o) < 1e-4f ? 0.0f : o; };
+	g.offx = snap(ip.off_x);
+	g.offy = snap(ip.off_y);
+	g.offz = snap(ip.off_z);
+	return g;
+}
+
+bool validImage(const yrtb_image_params* ip)
+{
+	return ip && ip->nx > 0 && ip->ny > 0 && ip->nz > 0 && ip->nt > 0 &&
+	       ip->length_x > 0 && ip->length_y > 0 && ip->length_z > 0 &&
+	       ip->nx * ip->ny * ip->nz < (int64_t(1) << 31);
+}
+
+}  // namespace
+
+struct yrtb_projector
+{
+	yrtb_scanner sc;
+	yrtb_image_params ip;
+	yrtb_projector_params pp;
+	KParams P;
+	int kind;
+	bool hasTof;
+	bool comp;
+	std::unique_ptr<H3Host> h3;
+	H3Dev h3d;
+	float4* d_pos = nullptr;
+	float4* d_ori = nullptr;
+	float* d_taps = nullptr;
+	float* d_flipped = nullptr;
+	int32_t* d_ring = nullptr;
+	int2* d_z = nullptr;
+	unsigned long long* d_err = nullptr;
+	int device = 0;
+
+	~yrtb_projector()
+	{
+		cudaFree(d_pos);
+		cudaFree(d_ori);
+		cudaFree(d_taps);
+		cudaFree(d_flipped);
+		cudaFree(d_ring);
+		cudaFree(d_z);
+		cudaFree(d_err);
+	}
+};
+
+namespace
+{
+Events toDev(const yrtb_events* ev)
+{
+	Events E{};
+	E.d1 = ev->d1;
+	E.d2 = ev->d2;
+	E.lor = ev->lor;
+	E.tof = ev->tof_ps;
+	E.frame = ev->frame;
+	E.mframe = ev->motion_frame;
+	E.motion = ev->motion;
+	E.numMotion = ev->num_motion_frames;
+	E.meas = ev->measurement;
+	E.sens = ev->sens;
+	E.att = ev->att;
+	E.add = ev->additive;
+	return E;
+}
+
+yrtb_status checkEvents(const yrtb_projector* h, const yrtb_events* ev,
+                        yrtb_range& r, bool needTof)
+{
+	if (!h || !ev)
+		return fail(YRTB_ERR_ARGUMENT, "null projector or events");
+	if (!ev->d1 && !ev->lor)
+		return fail(YRTB_ERR_ARGUMENT, "events need detector ids or LORs");
+	if ((ev->d1 == nullptr) != (ev->d2 == nullptr))
+		return fail(YRTB_ERR_ARGUMENT, "d1 and d2 must both be given");
+	if (ev->motion_frame && (!ev->motion || ev->num_motion_frames == 0))
+		return fail(YRTB_ERR_ARGUMENT, "motion frames given without transforms");
+	if (h->kind != K_SIDDON && h->kind != K_SIDDON_MR && !ev->d1)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "distance-driven and multi-ray projection need detector ids "
+		            "(crystal orientations)");
+	if (h->kind == K_SIDDON_MR && !ev->d1)
+		return fail(YRTB_ERR_ARGUMENT, "multi-ray projection needs detector ids");
+	if (needTof && h->hasTof && !ev->tof_ps)
+		return fail(YRTB_ERR_ARGUMENT, "TOF projector requires per-event TOF values");
+	if (r.stride == 0)
+		r.stride = 1;
+	if (r.start >= ev->count && ev->count > 0)
+		return fail(YRTB_ERR_ARGUMENT, "range start beyond the event count");
+	const uint64_t avail = ev->count == 0 ? 0 : (ev->count - r.start + r.stride - 1) / r.stride;
+	if (r.count == 0 || r.count > avail)
+		r.count = avail;
+	return YRTB_OK;
+}
+
+template <int OP, int KIND, bool TOF, bool COMP>
+void launchEvents(yrtb_projector* h, const Events& E, Range R, const float* in,
+                  float* out, float gs, float thr, cudaStream_t st)
+{
+	k_events<OP, KIND, TOF, COMP><<<gridFor(R.count), kBlock, 0, st>>>(
+	    h->P, E, R, in, out, gs, thr, h->d_err);
+}
+
+template <int OP>
+yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
+                           yrtb_range range, const float* in, float* out,
+                           float gs, float thr, yrtb_stream stream)
+{
+	yrtb_status s = checkEvents(h, ev, range, true);
+	if (s != YRTB_OK)
+		return s;
+	if (range.count == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	const Events E = toDev(ev);
+	const Range R{range.start, range.stride, range.count};
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	const bool tof = h->hasTof;
+	const bool comp = h->comp;
+#define YRTB_DISPATCH(KIND)                                                    \
+	do                                                                         \
+	{                                                                          \
+		if (tof)                                                               \
+		{                                                                      \
+			if (comp)                                                          \
+				launchEvents<OP, KIND, true, true>(h, E, R, in, out, gs, thr, st); \
+			else                                                               \
+				launchEvents<OP, KIND, true, false>(h, E, R, in, out, gs, thr, st); \
+		}                                                                      \
+		else                                                                   \
+		{                                                                      \
+			if (comp)                                                          \
+				launchEvents<OP, KIND, false, true>(h, E, R, in, out, gs, thr, st); \
+			else                                                               \
+				launchEvents<OP, KIND, false, false>(h, E, R, in, out, gs, thr, st); \
+		}                                                                      \
+	} while (0)
+	switch (h->kind)
+	{
+	case K_SIDDON: YRTB_DISPATCH(K_SIDDON); break;
+	case K_SIDDON_MR: YRTB_DISPATCH(K_SIDDON_MR); break;
+	case K_DD:
+		if (tof)
+			launchEvents<OP, K_DD, true, false>(h, E, R, in, out, gs, thr, st);
+		else
+			launchEvents<OP, K_DD, false, false>(h, E, R, in, out, gs, thr, st);
+		break;
+	default:
+		if (tof)
+			launchEvents<OP, K_DD_PSF, true, false>(h, E, R, in, out, gs, thr, st);
+		else
+			launchEvents<OP, K_DD_PSF, false, false>(h, E, R, in, out, gs, thr, st);
+		break;
+	}
+#undef YRTB_DISPATCH
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+template <bool EM>
+yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
+                          const float* img, float* out, const float* meas,
+                          const float* sensH, const float* acfH,
+                          const float* addH, const float* mu,
+                          const yrtb_image_params* muParams, float gs,
+                          float thr, yrtb_stream stream)
+{
+	if (!h || !out || numSubsets <= 0 || subset < 0 || subset >= numSubsets)
+		return fail(YRTB_ERR_ARGUMENT, "invalid histogram subset or buffers");
+	if (EM && (!img || !meas))
+		return fail(YRTB_ERR_ARGUMENT, "histogram EM needs image and measurements");
+	if (mu && !validImage(muParams))
+		return fail(YRTB_ERR_ARGUMENT, "attenuation image needs valid parameters");
+	if (h->ip.nt != 1)
+		return fail(YRTB_ERR_ARGUMENT, "histogram-mode projection is single-frame");
+	YRTB_CUDA(cudaSetDevice(h->device));
+	uint64_t nps = 0;
+	const uint64_t count = h3SubsetSize(*h->h3, numSubsets, subset, nps);
+	const Geom mg = mu ? makeGeom(*muParams) : Geom{};
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	const unsigned grid = gridFor(count);
+#define YRTB_HISTO(KIND)                                                       \
+	k_histo<KIND, EM><<<grid, kBlock, 0, st>>>(h->P, h->h3d, count, nps,       \
+	                                           numSubsets, subset, img, out,  \
+	                                           meas, sensH, acfH, addH, mg, mu, \
+	                                           gs, thr)
+	switch (h->kind)
+	{
+	case K_SIDDON: YRTB_HISTO(K_SIDDON); break;
+	case K_SIDDON_MR: YRTB_HISTO(K_SIDDON_MR); break;
+	case K_DD: YRTB_HISTO(K_DD); break;
+	default: YRTB_HISTO(K_DD_PSF); break;
+	}
+#undef YRTB_HISTO
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status scannerCheck(const yrtb_scanner* s)
+{
+	if (!s)
+		return fail(YRTB_ERR_ARGUMENT, "null scanner");
+	if (s->dets_per_ring == 0 || s->num_rings == 0 || s->num_doi == 0 ||
+	    s->dets_per_block == 0 || s->dets_per_ring % s->dets_per_block != 0)
+		return fail(YRTB_ERR_ARGUMENT, "invalid scanner detector counts");
+	if (s->max_ring_diff >= s->num_rings)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "Maximum Ring difference has to be lower than the number of rings");
+	if (s->min_ang_diff == 0)
+		return fail(YRTB_ERR_ARGUMENT, "Minimum angle difference has to be non-zero");
+	const uint64_t nd = s->dets_per_ring * s->num_rings * s->num_doi;
+	if (nd >= (uint64_t(1) << 32))
+		return fail(YRTB_ERR_ARGUMENT, "too many detectors for 32-bit ids");
+	return YRTB_OK;
+}
+
+}  // namespace
+
+// ================================================================ C ABI ===
+extern "C" {
+
+const char* yrtb_last_error(void)
+{
+	return g_lastError.c_str();
+}
+
+int yrtb_version(void)
+{
+	return 1;
+}
+
+yrtb_status yrtb_scanner_regular_lut(const yrtb_scanner* s, float* out)
+{
+	yrtb_status st = scannerCheck(s);
+	if (st != YRTB_OK)
+		return st;
+	if (!out)
+		return fail(YRTB_ERR_ARGUMENT, "null output");
+	// DetRegular::generateLUT (DetRegular.cpp:113-183), float arithmetic with
+	// the reference's double constants.
+	const double PI_ = 3.14159265358979;
+	const double TWOPI_ = 6.28318530717959;
+	const size_t numBlocks = s->dets_per_ring / s->dets_per_block;
+	const float blockLength = s->crystal_size_trans * s->dets_per_block;
+	for (size_t doi = 0; doi < s->num_doi; doi++)
+	{
+		const float blockDistance = s->scanner_radius + s->crystal_depth * doi;
+		for (size_t ring = 0; ring < s->num_rings; ring++)
+		{
+			const float zGap = s->axial_fov / static_cast<float>(s->num_rings);
+			const float zPos = -s->axial_fov / 2.0 + (ring + 0.5f) * zGap;
+			for (size_t block = 0; block < numBlocks; block++)
+			{
+				const float angle = block * TWOPI_ / numBlocks;
+				const float xb = (blockDistance + 0.5f * s->crystal_depth) * std::cos(angle);
+				const float yb = (blockDistance + 0.5f * s->crystal_depth) * std::sin(angle);
+				for (size_t det = 0; det < s->dets_per_block; det++)
+				{
+					float rel = 0.0f;
+					if (s->dets_per_block != 1)
+						rel = -0.5 + (det + 0.5) / static_cast<float>(s->dets_per_block);
+					const float rx = rel * std::cos(angle + PI_ / 2.0);
+					const float ry = rel * std::sin(angle + PI_ / 2.0);
+					const size_t idx = det + block * s->dets_per_block +
+					                   ring * s->dets_per_ring +
+					                   doi * (s->num_rings * s->dets_per_ring);
+					out[idx * 6 + 0] = xb + blockLength * rx;
+					out[idx * 6 + 1] = yb + blockLength * ry;
+					out[idx * 6 + 2] = zPos;
+					out[idx * 6 + 3] = std::cos(angle);
+					out[idx * 6 + 4] = std::sin(angle);
+					out[idx * 6 + 5] = 0.0f;
+				}
+			}
+		}
+	}
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_histo3d_dims(const yrtb_scanner* s, uint64_t* dims)
+{
+	yrtb_status st = scannerCheck(s);
+	if (st != YRTB_OK)
+		return st;
+	if (s->dets_per_ring % 2 != 0)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "The number of detectors per ring has to be even");
+	H3Host h(*s);
+	dims[0] = h.numZBin;
+	dims[1] = h.numPhi;
+	dims[2] = h.numR;
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_projector_create(const yrtb_scanner* s, const float* lut,
+                                  const yrtb_image_params* ip,
+                                  const yrtb_projector_params* pp,
+                                  yrtb_projector** out)
+{
+	if (!out)
+		return fail(YRTB_ERR_ARGUMENT, "null output handle");
+	*out = nullptr;
+	yrtb_status st = scannerCheck(s);
+	if (st != YRTB_OK)
+		return st;
+	if (!validImage(ip))
+		return fail(YRTB_ERR_ARGUMENT, "invalid image parameters");
+	if (!pp || (pp->projector != YRTB_SIDDON && pp->projector != YRTB_DD))
+		return fail(YRTB_ERR_ARGUMENT, "unknown projector type");
+	if (pp->num_rays < 1)
+		return fail(YRTB_ERR_ARGUMENT, "num_rays must be >= 1");
+	if (pp->psf_num_s > 0 && (!pp->psf_taps || pp->psf_size <= 0 ||
+	                          pp->psf_size % 2 == 0 || pp->psf_k_spacing <= 0 ||
+	                          pp->psf_s_step <= 0))
+		return fail(YRTB_ERR_ARGUMENT, "Kernels must be of odd length (invalid PSF table)");
+	if (pp->precision != YRTB_MIRROR && pp->precision != YRTB_COMPENSATED)
+		return fail(YRTB_ERR_ARGUMENT, "unknown precision mode");
+
+	auto h = std::make_unique<yrtb_projector>();
+	h->sc = *s;
+	h->ip = *ip;
+	h->pp = *pp;
+	h->pp.psf_taps = nullptr;
+	cudaGetDevice(&h->device);
+	const uint64_t nd = s->dets_per_ring * s->num_rings * s->num_doi;
+	std::vector<float> hl(nd * 6);
+	if (lut)
+		std::memcpy(hl.data(), lut, nd * 6 * sizeof(float));
+	else
+		yrtb_scanner_regular_lut(s, hl.data());
+	std::vector<float4> pos(nd), ori(nd);
+	for (uint64_t d = 0; d < nd; d++)
+	{
+		pos[d] = make_float4(hl[d * 6 + 0], hl[d * 6 + 1], hl[d * 6 + 2], 0.f);
+		ori[d] = make_float4(hl[d * 6 + 3], hl[d * 6 + 4], hl[d * 6 + 5], 0.f);
+	}
+	YRTB_CUDA(cudaMalloc(&h->d_pos, nd * sizeof(float4)));
+	YRTB_CUDA(cudaMalloc(&h->d_ori, nd * sizeof(float4)));
+	YRTB_CUDA(cudaMemcpy(h->d_pos, pos.data(), nd * sizeof(float4), cudaMemcpyHostToDevice));
+	YRTB_CUDA(cudaMemcpy(h->d_ori, ori.data(), nd * sizeof(float4), cudaMemcpyHostToDevice));
+	YRTB_CUDA(cudaMalloc(&h->d_err, sizeof(unsigned long long)));
+	YRTB_CUDA(cudaMemset(h->d_err, 0, sizeof(unsigned long long)));
+
+	KParams& P = h->P;
+	P.g = makeGeom(*ip);
+	P.scan.pos = h->d_pos;
+	P.scan.ori = h->d_ori;
+	P.scan.numDets = static_cast<uint32_t>(nd);
+	P.scan.crystalZ = s->crystal_size_z;
+	P.scan.crystalTrans = s->crystal_size_trans;
+	P.numRays = pp->num_rays;
+	h->hasTof = pp->tof_fwhm_ps > 0.f;
+	if (h->hasTof)
+	{
+		// TimeOfFlightHelper constructor (TimeOfFlight.hpp:20-34).
+		const double w_mm = pp->tof_fwhm_ps * kSpeedOfLightMmPs * 0.5;
+		P.tof.sigma = static_cast<float>(w_mm / (2 * sqrtf(2 * logf(2))));
+		P.tof.trunc = (pp->tof_n_std <= 0) ? -1.f : pp->tof_n_std * P.tof.sigma;
+		P.tof.norm = static_cast<float>(1 / (std::sqrt(2 * 3.14159265358979) * P.tof.sigma));
+	}
+	h->comp = pp->precision == YRTB_COMPENSATED;
+	if (pp->projector == YRTB_SIDDON)
+		h->kind = pp->num_rays > 1 ? K_SIDDON_MR : K_SIDDON;
+	else
+		h->kind = pp->psf_num_s > 0 ? K_DD_PSF : K_DD;
+	if (pp->psf_num_s > 0)
+	{
+		const size_t n = static_cast<size_t>(pp->psf_num_s) * pp->psf_size;
+		std::vector<float> flipped(n);
+		for (int i = 0; i < pp->psf_num_s; i++)
+			for (int j = 0; j < pp->psf_size; j++)
+				flipped[i * pp->psf_size + pp->psf_size - 1 - j] =
+				    pp->psf_taps[i * pp->psf_size + j];
+		YRTB_CUDA(cudaMalloc(&h->d_taps, n * sizeof(float)));
+		YRTB_CUDA(cudaMalloc(&h->d_flipped, n * sizeof(float)));
+		YRTB_CUDA(cudaMemcpy(h->d_taps, pp->psf_taps, n * sizeof(float), cudaMemcpyHostToDevice));
+		YRTB_CUDA(cudaMemcpy(h->d_flipped, flipped.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+		P.psf = Psf{h->d_taps, h->d_flipped, pp->psf_num_s, pp->psf_size,
+		            pp->psf_s_step, pp->psf_k_spacing};
+	}
+	if (s->dets_per_ring % 2 == 0)
+	{
+		h->h3 = std::make_unique<H3Host>(*s);
+		const H3Host& H = *h->h3;
+		YRTB_CUDA(cudaMalloc(&h->d_ring, H.ringMap.size() * sizeof(int32_t)));
+		YRTB_CUDA(cudaMalloc(&h->d_z, H.zPairs.size() * sizeof(int2)));
+		YRTB_CUDA(cudaMemcpy(h->d_ring, H.ringMap.data(), H.ringMap.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+		YRTB_CUDA(cudaMemcpy(h->d_z, H.zPairs.data(), H.zPairs.size() * sizeof(int2), cudaMemcpyHostToDevice));
+		h->h3d = H3Dev{static_cast<uint32_t>(nd), h->d_ring, h->d_z, static_cast<uint32_t>(H.dpr),
+		               static_cast<uint32_t>(H.rings), static_cast<uint32_t>(H.ndoi),
+		               static_cast<uint32_t>(H.numDOIPoss), static_cast<uint32_t>(H.rCut),
+		               static_cast<uint32_t>(H.mrd), H.numR, H.numPhi, H.numZBin,
+		               H.numZBinDiff};
+	}
+	*out = h.release();
+	return YRTB_OK;
+}
+
+void yrtb_projector_destroy(yrtb_projector* h)
+{
+	delete h;
+}
+
+yrtb_status yrtb_multiray_offsets(yrtb_projector* h, uint64_t count,
+                                  float* d_out, yrtb_stream stream)
+{
+	if (!h || !d_out)
+		return fail(YRTB_ERR_ARGUMENT, "null argument");
+	if (h->P.numRays < 2 || count == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	k_multiray_offsets<<<gridFor(count), kBlock, 0,
+	                     reinterpret_cast<cudaStream_t>(stream)>>>(
+	    count, h->P.numRays, d_out);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_projector_take_event_errors(yrtb_projector* h, uint64_t* count)
+{
+	if (!h || !count)
+		return fail(YRTB_ERR_ARGUMENT, "null argument");
+	unsigned long long v = 0;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	YRTB_CUDA(cudaMemcpy(&v, h->d_err, sizeof(v), cudaMemcpyDeviceToHost));
+	YRTB_CUDA(cudaMemset(h->d_err, 0, sizeof(v)));
+	*count = v;
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_forward(yrtb_projector* h, const float* d_image,
+                         const yrtb_events* ev, yrtb_range range, float* d_out,
+                         yrtb_stream stream)
+{
+	if (!d_image || !d_out)
+		return fail(YRTB_ERR_ARGUMENT, "null image or output");
+	return dispatchEvents<OP_FWD>(h, ev, range, d_image, d_out, 1.f, 0.f, stream);
+}
+
+yrtb_status yrtb_backward(yrtb_projector* h, const float* d_values,
+                          const yrtb_events* ev, yrtb_range range,
+                          float* d_image, yrtb_stream stream)
+{
+	if (!d_image || !d_values)
+		return fail(YRTB_ERR_ARGUMENT, "null image or values");
+	return dispatchEvents<OP_BWD>(h, ev, range, d_values, d_image, 1.f, 0.f, stream);
+}
+
+yrtb_status yrtb_em_step(yrtb_projector* h, const float* d_image, float* d_em,
+                         const yrtb_events* ev, yrtb_range range,
+                         float global_scale, float denom_threshold,
+                         yrtb_stream stream)
+{
+	if (!d_image || !d_em)
+		return fail(YRTB_ERR_ARGUMENT, "null image or EM buffer");
+	return dispatchEvents<OP_EM>(h, ev, range, d_image, d_em, global_scale,
+	                             denom_threshold, stream);
+}
+
+yrtb_status yrtb_count_crossings(yrtb_projector* h, const yrtb_events* ev,
+                                 yrtb_range range, uint32_t* d_out,
+                                 yrtb_stream stream)
+{
+	if (!d_out)
+		return fail(YRTB_ERR_ARGUMENT, "null output");
+	return dispatchEvents<OP_COUNT>(h, ev, range, nullptr,
+	                                reinterpret_cast<float*>(d_out), 1.f, 0.f,
+	                                stream);
+}
+
+yrtb_status yrtb_attenuation_factors(yrtb_projector* h, const float* d_mu,
+                                     const yrtb_image_params* mu_params,
+                                     const yrtb_events* ev, yrtb_range range,
+                                     float* d_out, yrtb_stream stream)
+{
+	if (!d_mu || !d_out || !validImage(mu_params))
+		return fail(YRTB_ERR_ARGUMENT, "invalid attenuation image or output");
+	yrtb_status s = checkEvents(h, ev, range, false);
+	if (s != YRTB_OK)
+		return s;
+	if (range.count == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	k_attenuation<<<gridFor(range.count), kBlock, 0,
+	                reinterpret_cast<cudaStream_t>(stream)>>>(
+	    h->P, makeGeom(*mu_params), toDev(ev),
+	    Range{range.start, range.stride, range.count}, d_mu, d_out, h->d_err);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_gather_histo3d(yrtb_projector* h, const float* d_histo,
+                                const yrtb_events* ev, yrtb_range range,
+                                int invert, float* d_out, yrtb_stream stream)
+{
+	if (!d_histo || !d_out)
+		return fail(YRTB_ERR_ARGUMENT, "null histogram or output");
+	yrtb_status s = checkEvents(h, ev, range, false);
+	if (s != YRTB_OK)
+		return s;
+	if (!ev->d1 || !h->h3)
+		return fail(YRTB_ERR_ARGUMENT, "histogram gather needs detector ids and an even ring");
+	if (range.count == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	k_gather_histo<<<gridFor(range.count), kBlock, 0,
+	                 reinterpret_cast<cudaStream_t>(stream)>>>(
+	    h->P, h->h3d, toDev(ev), Range{range.start, range.stride, range.count},
+	    d_histo, invert, d_out, h->d_err);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_sensitivity_histo3d(yrtb_projector* h, float* d_sens,
+                                     const float* d_sens_histo,
+                                     const float* d_acf_histo,
+                                     const float* d_mu,
+                                     const yrtb_image_params* mu_params,
+                                     int num_subsets, int subset,
+                                     yrtb_stream stream)
+{
+	if (!h || !h->h3)
+		return fail(YRTB_ERR_ARGUMENT, "projector has no Histogram3D (odd ring)");
+	return dispatchHisto<false>(h, num_subsets, subset, nullptr, d_sens, nullptr,
+	                            d_sens_histo, d_acf_histo, nullptr, d_mu,
+	                            mu_params, 1.f, 0.f, stream);
+}
+
+yrtb_status yrtb_em_step_histo3d(yrtb_projector* h, const float* d_image,
+                                 float* d_em, const float* d_meas,
+                                 const float* d_sens_histo,
+                                 const float* d_acf_histo,
+                                 const float* d_add_histo, int num_subsets,
+                                 int subset, float global_scale,
+                                 float denom_threshold, yrtb_stream stream)
+{
+	if (!h || !h->h3)
+		return fail(YRTB_ERR_ARGUMENT, "projector has no Histogram3D (odd ring)");
+	return dispatchHisto<true>(h, num_subsets, subset, d_image, d_em, d_meas,
+	                           d_sens_histo, d_acf_histo, d_add_histo, nullptr,
+	                           nullptr, global_scale, denom_threshold, stream);
+}
+
+yrtb_status yrtb_listmode_to_histo3d(yrtb_projector* h, const uint32_t* d1,
+                                     const uint32_t* d2, const float* vals,
+                                     uint64_t n, float* histo,
+                                     uint64_t* n_invalid, yrtb_stream stream)
+{
+	if (!h || !h->h3 || !d1 || !d2 || !histo)
+		return fail(YRTB_ERR_ARGUMENT, "invalid list-mode to histogram arguments");
+	YRTB_CUDA(cudaSetDevice(h->device));
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	unsigned long long* d_bad = nullptr;
+	YRTB_CUDA(cudaMallocAsync(&d_bad, sizeof(unsigned long long), st));
+	YRTB_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), st));
+	if (n > 0)
+	{
+		k_lm_to_histo<<<gridFor(n, 16), kBlock, 0, st>>>(h->h3d, d1, d2, vals, n,
+		                                                 histo, d_bad);
+		YRTB_LAUNCHED();
+	}
+	unsigned long long bad = 0;
+	YRTB_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, st));
+	YRTB_CUDA(cudaFreeAsync(d_bad, st));
+	YRTB_CUDA(cudaStreamSynchronize(st));
+	if (n_invalid)
+		*n_invalid = bad;
+	if (bad > 0)
+		return fail(YRTB_ERR_RANGE,
+		            std::to_string(bad) +
+		                " detector pairs do not respect the maximum ring difference "
+		                "or minimum angle difference of the histogram");
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_histo3d_bins(yrtb_projector* h, const uint32_t* d1,
+                              const uint32_t* d2, uint64_t n, uint64_t* bins,
+                              yrtb_stream stream)
+{
+	if (!h || !h->h3 || !d1 || !d2 || !bins)
+		return fail(YRTB_ERR_ARGUMENT, "invalid histogram map arguments");
+	if (n == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	k_bins<<<gridFor(n, 16), kBlock, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+	    h->h3d, d1, d2, n, bins);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_histo3d_detpairs(yrtb_projector* h, const uint64_t* bins,
+                                  uint64_t n, uint32_t* d1, uint32_t* d2,
+                                  yrtb_stream stream)
+{
+	if (!h || !h->h3 || !d1 || !d2 || !bins)
+		return fail(YRTB_ERR_ARGUMENT, "invalid histogram map arguments");
+	if (n == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	k_pairs<<<gridFor(n, 16), kBlock, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+	    h->h3d, bins, n, d1, d2);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_em_update(float* x, const float* u, const float* s,
+                           uint64_t J, int64_t nt, int64_t sens_nt, float thr,
+                           const float* scale, yrtb_stream stream)
+{
+	if (!x || !u || !s || J == 0 || nt <= 0 || (sens_nt != 1 && sens_nt != nt))
+		return fail(YRTB_ERR_ARGUMENT, "invalid EM update arguments");
+	k_em_update<<<gridFor(J * nt, 16), kBlock, 0,
+	              reinterpret_cast<cudaStream_t>(stream)>>>(x, u, s, J, nt, sens_nt,
+	                                                        thr, scale);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_apply_threshold(float* x, const float* m, uint64_t J,
+                                 int64_t nt, int broadcast, float thr,
+                                 float les, float leo, float gts, float gto,
+                                 yrtb_stream stream)
+{
+	if (!x || !m || J == 0 || nt <= 0)
+		return fail(YRTB_ERR_ARGUMENT, "invalid threshold arguments");
+	k_threshold<<<gridFor(J * nt, 16), kBlock, 0,
+	              reinterpret_cast<cudaStream_t>(stream)>>>(x, m, J, nt, broadcast,
+	                                                        thr, les, leo, gts, gto);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_fill(float* x, uint64_t n, float v, yrtb_stream stream)
+{
+	if (!x)
+		return fail(YRTB_ERR_ARGUMENT, "null buffer");
+	if (n == 0)
+		return YRTB_OK;
+	k_fill<<<gridFor(n, 16), kBlock, 0, reinterpret_cast<cudaStream_t>(stream)>>>(x, n, v);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_scale(float* x, uint64_t n, float v, yrtb_stream stream)
+{
+	if (!x)
+		return fail(YRTB_ERR_ARGUMENT, "null buffer");
+	if (n == 0)
+		return YRTB_OK;
+	k_scale<<<gridFor(n, 16), kBlock, 0, reinterpret_cast<cudaStream_t>(stream)>>>(x, n, v);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
+                               const float* d_sens, float* d_image,
+                               float* d_work, const yrtb_osem_params* p,
+                               yrtb_stream stream)
+{
+	if (!h || !ev || !d_sens || !d_image || !d_work || !p)
+		return fail(YRTB_ERR_ARGUMENT, "null OSEM argument");
+	if (p->iterations <= 0 || p->subsets <= 0)
+		return fail(YRTB_ERR_ARGUMENT, "Not enough OSEM subsets / MLEM iterations");
+	YRTB_CUDA(cudaSetDevice(h->device));
+	const uint64_t J = static_cast<uint64_t>(h->P.g.nvox);
+	const int64_t nt = h->ip.nt;
+	float* em = d_work;
+	float* sens = d_work + J * nt;
+	// List-mode sensitivity is shared by all subsets and divided by their
+	// number (OSEM::initializeSensImageBuffer, OSEM.cpp:1007-1035).
+	YRTB_CUDA(cudaMemcpyAsync(sens, d_sens, J * sizeof(float),
+	                          cudaMemcpyDeviceToDevice,
+	                          reinterpret_cast<cudaStream_t>(stream)));
+	yrtb_status s = YRTB_OK;
+	if (p->subsets != 1)
+		s = yrtb_scale(sens, J, 1.0f / static_cast<float>(p->subsets), stream);
+	if (s != YRTB_OK)
+		return s;
+	// x0 = 0.125 (OSEM::INITIAL_VALUE_MLEM), masked where sens <= 0
+	// (OSEM_GPU::prepareBuffersForRecon, OSEM_GPU.cu:311-360).
+	if (!p->init_from_image)
+		if ((s = yrtb_fill(d_image, J * nt, 0.125f, stream)) != YRTB_OK)
+			return s;
+	if ((s = yrtb_apply_threshold(d_image, d_sens, J, nt, 1, 0.f, 0.f, 0.f, 1.f,
+	                              0.f, stream)) != YRTB_OK)
+		return s;
+
+	auto subsetOps = [&](int sub) -> yrtb_status
+	{
+		yrtb_status r;
+		if ((r = yrtb_fill(em, J * nt, 0.f, stream)) != YRTB_OK)
+			return r;
+		yrtb_range range{static_cast<uint64_t>(sub),
+		                 static_cast<uint64_t>(p->subsets), 0};
+		if ((r = yrtb_em_step(h, d_image, em, ev, range, p->global_scale,
+		                      p->denom_threshold, stream)) != YRTB_OK)
+			return r;
+		return yrtb_em_update(d_image, em, sens, J, nt, 1, p->em_threshold,
+		                      p->d_frame_scale, stream);
+	};
+
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	if (!p->use_graph)
+	{
+		for (int it = 0; it < p->iterations; it++)
+			for (int sub = 0; sub < p->subsets; sub++)
+				if ((s = subsetOps(sub)) != YRTB_OK)
+					return s;
+		return YRTB_OK;
+	}
+	// One graph per subset, captured once and replayed every iteration.
+	if (st == nullptr)
+		return fail(YRTB_ERR_ARGUMENT, "CUDA-graph OSEM needs a non-default stream");
+	std::vector<cudaGraphExec_t> execs(p->subsets, nullptr);
+	auto cleanup = [&]
+	{
+		for (auto& e : execs)
+			if (e)
+				cudaGraphExecDestroy(e);
+	};
+	for (int sub = 0; sub < p->subsets; sub++)
+	{
+		cudaGraph_t g = nullptr;
+		cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+		if (ce != cudaSuccess)
+		{
+			cleanup();
+			return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+		}
+		const yrtb_status r = subsetOps(sub);
+		ce = cudaStreamEndCapture(st, &g);
+		if (r != YRTB_OK || ce != cudaSuccess)
+		{
+			if (g)
+				cudaGraphDestroy(g);
+			cleanup();
+			return r != YRTB_OK ? r : fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+		}
+		ce = cudaGraphInstantiate(&execs[sub], g, 0);
+		cudaGraphDestroy(g);
+		if (ce != cudaSuccess)
+		{
+			cleanup();
+			return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+		}
+	}
+	for (int it = 0; it < p->iterations; it++)
+		for (int sub = 0; sub < p->subsets; sub++)
+		{
+			const cudaError_t ce = cudaGraphLaunch(execs[sub], st);
+			if (ce != cudaSuccess)
+			{
+				cleanup();
+				return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+			}
+		}
+	cleanup();
+	return YRTB_OK;
+}
+
+}  // extern "C"

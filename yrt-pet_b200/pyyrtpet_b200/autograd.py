@@ -1,0 +1,61 @@
+"""Differentiable TOF Siddon projection as a torch.autograd.Function.
+
+forward(x) = A x for a fixed set of list-mode events; backward(g) = A^T g,
+computed by the hand-written back-projection kernel (the ray traversal is
+recomputed, no system matrix is stored).  A batch of images (B, nt, nz, ny,
+nx) may share one event set or use one event set per batch element.
+"""
+from __future__ import annotations
+
+from typing import Sequence, Union
+
+import torch
+
+from .core import DeviceEvents, DeviceProjector
+
+
+class SiddonProjectFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x: torch.Tensor, projector: DeviceProjector,
+                events: Union[DeviceEvents, Sequence[DeviceEvents]]):
+        batched = x.dim() == 5
+        xs = x if batched else x[None]
+        evs = events if isinstance(events, (list, tuple)) else [events] * xs.shape[0]
+        if len(evs) != xs.shape[0]:
+            raise RuntimeError("one event set per batch element expected")
+        outs = []
+        for b in range(xs.shape[0]):
+            xb = xs[b].detach().contiguous().float()
+            outs.append(projector.forward(xb, evs[b]))
+        ctx.projector = projector
+        ctx.events = evs
+        ctx.batched = batched
+        ctx.shape = xs.shape
+        y = torch.stack(outs) if batched else outs[0]
+        return y
+
+    @staticmethod
+    def backward(ctx, g: torch.Tensor):
+        gs = g if ctx.batched else g[None]
+        grads = []
+        for b in range(gs.shape[0]):
+            img = torch.zeros(ctx.shape[1:], dtype=torch.float32, device=g.device)
+            ctx.projector.backward(gs[b].contiguous().float(), ctx.events[b],
+                                   img=img)
+            grads.append(img)
+        gx = torch.stack(grads) if ctx.batched else grads[0]
+        return gx, None, None
+
+
+def project(x, projector, events):
+    return SiddonProjectFn.apply(x, projector, events)
+
+
+def poisson_nll(x, projector, events, sens_image, eps: float = 1e-12):
+    """List-mode Poisson negative log-likelihood:
+    sum_j s_j x_j - sum_e log(y_e) with y = A x."""
+    y = project(x, projector, events)
+    if x.dim() == 5:
+        lin = (sens_image[None] * x).sum(dim=tuple(range(1, x.dim())))
+        return lin - torch.log(y.clamp_min(eps)).sum(dim=-1)
+    return (sens_image * x).sum() - torch.log(y.clamp_min(eps)).sum()
