@@ -238,6 +238,12 @@ def main():
     img.mul_((sens > 0).float())
     em = torch.zeros(J, device="cuda")
 
+    # Plain form: events in file order, subset = interleaved stride (the
+    # reference's batching).  Ordered form: subset-major, LOR-sorted copy.
+    ev_plain = ev
+    ev, offsets = proj.order_events(ev_plain, SUBSETS)
+    torch.cuda.synchronize()
+
     # Algorithmic traffic of the fused EM kernel: per event 24 B of event data
     # (d1, d2, tof, sens, att, additive) + 4 B per crossing for the forward
     # gather + 8 B per crossing for the back-projection read-modify-write.
@@ -252,15 +258,22 @@ def main():
     evc = ev.c()
     launches = [0]
 
-    def step(record=None):
+    evc_plain = ev_plain.c()
+
+    def step(record=None, plain=False):
         for s in range(SUBSETS):
             L.check(lib.yrtb_fill(em.data_ptr(), J, 0.0, s_ptr))
-            r = L.yrtb_range(s, SUBSETS, 0)
+            if plain:
+                r = L.yrtb_range(s, SUBSETS, 0)
+            else:
+                r = L.yrtb_range(int(offsets[s]), 1,
+                                 int(offsets[s + 1] - offsets[s]))
             if record is not None:
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(st)
             L.check(lib.yrtb_em_step(proj.h, img.data_ptr(), em.data_ptr(),
-                                     ctypes.byref(evc), r, 1.0, 1e-35, s_ptr))
+                                     ctypes.byref(evc_plain if plain else evc),
+                                     r, 1.0, 1e-35, s_ptr))
             if record is not None:
                 b.record(st)
                 record.append((a, b))
@@ -304,6 +317,23 @@ def main():
         ms, em_ms = tt.tolist()
     total_events = ev.count * world
     value = total_events / (ms * 1e-3)
+    timed_launches = launches[0]
+
+    # Plain (file-order) form on the same GPU, for the batched-vs-plain ratio.
+    for _ in range(1):
+        step(plain=True)
+    pa = torch.cuda.Event(enable_timing=True)
+    pb = torch.cuda.Event(enable_timing=True)
+    pa.record(st)
+    for _ in range(args.steps):
+        step(plain=True)
+    pb.record(st)
+    torch.cuda.synchronize()
+    plain_ms = pa.elapsed_time(pb) / args.steps
+    if dist is not None:
+        tt = torch.tensor([plain_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        plain_ms = tt.item()
 
     # ---- e2e: public OSEM API from pinned host buffers (1 iteration/step).
     e2e = None
@@ -325,10 +355,12 @@ def main():
             e = yrt.DeviceEvents(int(d_d1.numel()), d_d1, d_d2, tof=d_tof)
             e.sens = (eff_d[d_d1.long()] * eff_d[d_d2.long()]).contiguous()
             e.att = proj.attenuation_factors(mu_flat, ip, e)
-            e.additive = ev.additive
+            e.additive = ev_plain.additive
+            e, offs = proj.order_events(e, SUBSETS)
             x = torch.full((J,), 0.125, device="cuda")
             work = torch.empty(2 * J, device="cuda")
-            p = L.yrtb_osem_params(1, SUBSETS, 1.0, 1e-35, 1.19209e-07, 0, 0, None)
+            p = L.yrtb_osem_params(1, SUBSETS, 1.0, 1e-35, 1.19209e-07, 0, 0,
+                                   None, offs.ctypes.data)
             L.check(lib.yrtb_osem_listmode(proj.h, ctypes.byref(e.c()),
                                            sens.data_ptr(), x.data_ptr(),
                                            work.data_ptr(), ctypes.byref(p),
@@ -354,8 +386,8 @@ def main():
                "h2d_bytes_per_step": int(h_d1.numel() * 12),
                "d2h_bytes_per_step": int(J * 4), "ms_per_step": e2e_ms,
                "path": "yrtb_osem_listmode (C ABI) from pinned host events; "
-                       "per step: H2D events, device corrections, 1 OSEM "
-                       "iteration x 10 subsets, D2H image"}
+                       "per step: H2D events, device corrections, event "
+                       "ordering, 1 OSEM iteration x 10 subsets, D2H image"}
 
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes_iter / SUBSETS / (em_ms * 1e-3) / 1e9
@@ -404,7 +436,12 @@ def main():
                                  "image (42 MB) L2-resident by design",
                            "parallelism": f"dp{world} (events sharded, EM image "
                                           "all-reduced per subset)"},
-                "gpu_launches": launches[0],
+                "gpu_launches": timed_launches,
+                "plain": {"value": total_events / (plain_ms * 1e-3),
+                          "ms_per_step": plain_ms,
+                          "what": "same kernels, events in file order with "
+                                  "interleaved subsets (the reference's "
+                                  "single-frame batching)"},
                 "osem_s_per_iteration": ms * 1e-3,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clocks}

@@ -214,6 +214,26 @@ yrtb_status yrtb_gather_histo3d(yrtb_projector* h, const float* d_histo,
                                 const yrtb_events* ev, yrtb_range range,
                                 int invert, float* d_out, yrtb_stream stream);
 
+/* ------------------------------------------------------- event ordering --- */
+/* Permutation that groups events by OSEM subset (event index mod
+ * num_subsets, the reference's chronological interleaving) and, inside a
+ * subset, by LOR (Histogram3D bin or detector pair) and TOF, so that
+ * neighbouring GPU threads trace neighbouring rays of similar length.
+ * d_perm[i] = source index of output position i (n uint64); subset_offsets
+ * (host, num_subsets+1) delimits the subsets in the reordered arrays.  The
+ * result of an OSEM subset does not depend on the order of its events
+ * beyond floating-point summation order.  No counterpart in the reference
+ * (its batches keep file order). */
+yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
+                                     int num_subsets, uint64_t* d_perm,
+                                     uint64_t* subset_offsets,
+                                     yrtb_stream stream);
+
+/* out->X[i] = in->X[d_perm[i]] for every array present in `in` (output
+ * buffers allocated by the caller; out->count == in->count). */
+yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
+                               const yrtb_events* out, yrtb_stream stream);
+
 /* ----------------------------------------------------- histogram mode --- */
 /* Sensitivity image over one subset of Histogram3D bins (phi = subset mod
  * num_subsets), non-TOF: d_sens += A^T (sens_bin * acf_bin).  d_sens_histo /
@@ -312,6 +332,10 @@ typedef struct
 	int init_from_image;
 	int use_graph;
 	const float* d_frame_scale; /* nullable, nt floats */
+	const uint64_t* subset_offsets; /* host, subsets+1; NULL: interleaved
+	                                   events (stride = subsets); else subset s
+	                                   = events [off[s], off[s+1]) as produced
+	                                   by yrtb_events_subset_order */
 } yrtb_osem_params;
 
 yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,

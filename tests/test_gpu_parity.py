@@ -26,8 +26,8 @@ needs_ref = pytest.mark.skipif(not po.ref_available(),
 
 
 def rel_l2(a, b):
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
@@ -170,7 +170,10 @@ def test_siddon_random_vs_oracle(tof):
     b = p.backward(torch.from_numpy(y).cuda(), ev).cpu().numpy()
     b64 = po.project(oip, pr, lors, values=y.astype(np.float64), tof=tv,
                      forward=False, precision="f64")
-    assert rel_l2(b, b64) < 1e-5
+    # Image budget (1e-4); FP32 scatter of many small TOF-weighted terms.
+    assert rel_l2(b, b64) < 1e-4
+    b32 = po.project(oip, pr, lors, values=y, tof=tv, forward=False)
+    assert rel_l2(b, b64) < 2 * rel_l2(b32, b64) + 1e-6
     # Adjoint identity of the device operator pair.
     lhs = float(np.dot(v.astype(np.float64), y))
     rhs = float(np.sum(b.astype(np.float64) * img))
@@ -294,7 +297,7 @@ def test_em_step_vs_oracle_f64():
     ref = po.em_step_f64(po.ImageParams(*IP_ARGS), po.Proj(tof_fwhm_ps=214.0, tof_n_std=5),
                          lors, img, tof=tv, sens=sens, att=att, additive=add,
                          global_scale=1.3)
-    assert rel_l2(em.cpu().numpy(), ref) < 1e-5
+    assert rel_l2(em.cpu().numpy(), ref) < 1e-4
 
 
 def _small_c1_problem(n=60000, seed=18, tof=False):
@@ -434,10 +437,10 @@ def test_em_update_variants_vs_numpy():
     s = rng.uniform(-0.1, 2, J).astype(np.float32)
     c = np.array([0.5, 1.0, 2.0], np.float32)
     xt = torch.from_numpy(x.copy()).cuda()
-    L.check(L.lib().yrtb_em_update(xt.data_ptr(), torch.from_numpy(u).cuda().data_ptr(),
-                                   torch.from_numpy(s).cuda().data_ptr(), J, nt, 1,
-                                   1.19209e-07, torch.from_numpy(c).cuda().data_ptr(),
-                                   None))
+    ut, st, ct = (torch.from_numpy(a).cuda() for a in (u, s, c))
+    L.check(L.lib().yrtb_em_update(xt.data_ptr(), ut.data_ptr(), st.data_ptr(),
+                                   J, nt, 1, 1.19209e-07, ct.data_ptr(), None))
+    torch.cuda.synchronize()
     ref = x.copy()
     for r in range(nt):
         inv_c = np.float32(1) / c[r]
@@ -461,3 +464,28 @@ def test_tof_projector_requires_tof_values():
     ev = yrt.DeviceEvents.from_arrays(GOLD["d1"], GOLD["d2"])
     with pytest.raises(yrt.YrtbError, match="TOF"):
         p.forward(torch.ones(ip.shape, device="cuda"), ev)
+
+
+def test_event_ordering_is_subset_major_permutation():
+    sc, ip, p = make(tof=(214.0, 5))
+    d1, d2 = random_events(SC_ARGS, 50001, 25)
+    rng = np.random.default_rng(26)
+    tv = rng.normal(0, 300, len(d1)).astype(np.float32)
+    ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv)
+    out, offs = p.order_events(ev, 7)
+    perm = out.perm.cpu().numpy()
+    n = len(d1)
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    for s in range(7):
+        src = perm[offs[s]:offs[s + 1]]
+        assert np.all(src % 7 == s)
+        assert len(src) == len(range(s, n, 7))
+    assert np.array_equal(out.d1.cpu().numpy().view(np.uint32), d1[perm])
+    assert np.array_equal(out.tof.cpu().numpy(), tv[perm])
+    # Same EM image for the subset whatever the event order.
+    img = torch.from_numpy(rng.uniform(0.5, 1.5, ip.shape).astype(np.float32)).cuda()
+    em_a = torch.zeros(ip.shape, device="cuda")
+    em_b = torch.zeros(ip.shape, device="cuda")
+    p.em_step(img, em_a, ev, rng=L.yrtb_range(3, 7, 0))
+    p.em_step(img, em_b, out, rng=L.yrtb_range(int(offs[3]), 1, int(offs[4] - offs[3])))
+    assert rel_l2(em_b.cpu().numpy(), em_a.cpu().numpy()) < 1e-5

@@ -18,6 +18,7 @@
 #include "yrt_b200.h"
 #include "device.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -623,6 +624,51 @@ __global__ void __launch_bounds__(kBlock)
 	}
 }
 
+// Sort key of event e: subset (e mod S) in bits 48..63, LOR (Histogram3D
+// bin, or the ordered detector pair) in bits 8..47, TOF in 16 ps steps in
+// bits 0..7.
+__global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
+                             uint64_t numSubsets, unsigned long long* __restrict__ keys,
+                             unsigned long long* __restrict__ vals)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t e = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     e < n; e += nthreads)
+	{
+		uint64_t lorKey = 0;
+		if (E.d1 != nullptr)
+		{
+			const uint32_t a = __ldg(E.d1 + e), b = __ldg(E.d2 + e);
+			uint64_t bin;
+			if (hasH3 && h3Bin(H, a, b, bin))
+				lorKey = bin;
+			else
+				lorKey = (static_cast<uint64_t>(min(a, b)) << 20) ^ max(a, b);
+		}
+		uint64_t q = 128;
+		if (E.tof != nullptr)
+		{
+			const float t = __ldg(E.tof + e) / 16.0f + 128.0f;
+			q = t <= 0.f ? 0 : (t >= 255.f ? 255 : static_cast<uint64_t>(t));
+		}
+		keys[e] = ((e % numSubsets) << 48) | ((lorKey & 0xFFFFFFFFFFULL) << 8) | q;
+		vals[e] = e;
+	}
+}
+
+template <typename T>
+__global__ void k_gather(const T* __restrict__ in, const unsigned long long* __restrict__ perm,
+                         uint64_t n, int width, T* __restrict__ out)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n * width; i += nthreads)
+	{
+		const uint64_t r = i / width, c = i % width;
+		out[i] = __ldg(in + perm[r] * width + c);
+	}
+}
+
 __global__ void k_multiray_offsets(uint64_t count, int numRays,
                                    float* __restrict__ out)
 {
@@ -1222,6 +1268,95 @@ yrtb_status yrtb_multiray_offsets(yrtb_projector* h, uint64_t count,
 	return YRTB_OK;
 }
 
+yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
+                                     int num_subsets, uint64_t* d_perm,
+                                     uint64_t* subset_offsets,
+                                     yrtb_stream stream)
+{
+	if (!h || !ev || !d_perm || !subset_offsets || num_subsets <= 0 ||
+	    num_subsets > 65535)
+		return fail(YRTB_ERR_ARGUMENT, "invalid subset-order arguments");
+	const uint64_t n = ev->count;
+	const uint64_t S = static_cast<uint64_t>(num_subsets);
+	subset_offsets[0] = 0;
+	for (uint64_t s = 0; s < S; s++)
+		subset_offsets[s + 1] = subset_offsets[s] + (n > s ? (n - s + S - 1) / S : 0);
+	if (n == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	unsigned long long *keys = nullptr, *keys2 = nullptr, *vals = nullptr;
+	void* temp = nullptr;
+	size_t tempBytes = 0;
+	auto release = [&]
+	{
+		cudaFreeAsync(keys, st);
+		cudaFreeAsync(keys2, st);
+		cudaFreeAsync(vals, st);
+		cudaFreeAsync(temp, st);
+	};
+	cudaError_t ce = cudaMallocAsync(&keys, n * 8, st);
+	if (ce == cudaSuccess)
+		ce = cudaMallocAsync(&keys2, n * 8, st);
+	if (ce == cudaSuccess)
+		ce = cudaMallocAsync(&vals, n * 8, st);
+	if (ce != cudaSuccess)
+	{
+		release();
+		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+	}
+	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(h->h3d, h->h3 != nullptr,
+	                                                toDev(ev), n, S, keys, vals);
+	ce = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals,
+	                                     reinterpret_cast<unsigned long long*>(d_perm),
+	                                     n, 0, 64, st);
+	if (ce == cudaSuccess)
+		ce = cudaMallocAsync(&temp, tempBytes, st);
+	if (ce == cudaSuccess)
+		ce = cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals,
+		                                     reinterpret_cast<unsigned long long*>(d_perm),
+		                                     n, 0, 64, st);
+	release();
+	if (ce != cudaSuccess)
+		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
+                               const yrtb_events* out, yrtb_stream stream)
+{
+	if (!in || !out || !d_perm)
+		return fail(YRTB_ERR_ARGUMENT, "invalid gather arguments");
+	const uint64_t n = in->count;
+	if (out->count != n)
+		return fail(YRTB_ERR_ARGUMENT, "gather needs equal event counts");
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	const unsigned long long* perm = reinterpret_cast<const unsigned long long*>(d_perm);
+	auto g32 = [&](const void* a, const void* b, int w) -> yrtb_status
+	{
+		if (a == nullptr)
+			return YRTB_OK;
+		if (b == nullptr)
+			return fail(YRTB_ERR_ARGUMENT, "gather output array missing");
+		k_gather<uint32_t><<<gridFor(n * w, 16), kBlock, 0, st>>>(
+		    static_cast<const uint32_t*>(a), perm, n, w,
+		    const_cast<uint32_t*>(static_cast<const uint32_t*>(b)));
+		return YRTB_OK;
+	};
+	yrtb_status r;
+	if ((r = g32(in->d1, out->d1, 1)) || (r = g32(in->d2, out->d2, 1)) ||
+	    (r = g32(in->lor, out->lor, 6)) || (r = g32(in->tof_ps, out->tof_ps, 1)) ||
+	    (r = g32(in->frame, out->frame, 1)) ||
+	    (r = g32(in->motion_frame, out->motion_frame, 1)) ||
+	    (r = g32(in->measurement, out->measurement, 1)) ||
+	    (r = g32(in->sens, out->sens, 1)) || (r = g32(in->att, out->att, 1)) ||
+	    (r = g32(in->additive, out->additive, 1)))
+		return r;
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
 yrtb_status yrtb_projector_take_event_errors(yrtb_projector* h, uint64_t* count)
 {
 	if (!h || !count)
@@ -1498,6 +1633,15 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 			return r;
 		yrtb_range range{static_cast<uint64_t>(sub),
 		                 static_cast<uint64_t>(p->subsets), 0};
+		if (p->subset_offsets)
+		{
+			range.start = p->subset_offsets[sub];
+			range.stride = 1;
+			range.count = p->subset_offsets[sub + 1] - p->subset_offsets[sub];
+			if (range.count == 0)
+				return yrtb_em_update(d_image, em, sens, J, nt, 1, p->em_threshold,
+				                      p->d_frame_scale, stream);
+		}
 		if ((r = yrtb_em_step(h, d_image, em, ev, range, p->global_scale,
 		                      p->denom_threshold, stream)) != YRTB_OK)
 			return r;

@@ -66,7 +66,8 @@ class yrtb_osem_params(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("subsets", ctypes.c_int),
                 ("global_scale", c_f), ("denom_threshold", c_f),
                 ("em_threshold", c_f), ("init_from_image", ctypes.c_int),
-                ("use_graph", ctypes.c_int), ("d_frame_scale", c_vp)]
+                ("use_graph", ctypes.c_int), ("d_frame_scale", c_vp),
+                ("subset_offsets", c_vp)]
 
 
 # (name, argtypes) of every entry point of include/yrt_b200.h.
@@ -103,6 +104,10 @@ SIGNATURES = {
                              ctypes.c_int),
     "yrtb_listmode_to_histo3d": ([c_vp, c_vp, c_vp, c_vp, c_u64, c_vp,
                                   _P(c_u64), c_vp], ctypes.c_int),
+    "yrtb_events_subset_order": ([c_vp, _P(yrtb_events), ctypes.c_int, c_vp,
+                                  c_vp, c_vp], ctypes.c_int),
+    "yrtb_events_gather": ([_P(yrtb_events), c_vp, _P(yrtb_events), c_vp],
+                           ctypes.c_int),
     "yrtb_histo3d_bins": ([c_vp, c_vp, c_vp, c_u64, c_vp, c_vp], ctypes.c_int),
     "yrtb_histo3d_detpairs": ([c_vp, c_vp, c_u64, c_vp, c_vp, c_vp],
                               ctypes.c_int),

@@ -541,6 +541,7 @@ class DeviceEvents:
     sens: Optional[torch.Tensor] = None
     att: Optional[torch.Tensor] = None
     additive: Optional[torch.Tensor] = None
+    perm: Optional[torch.Tensor] = None
     _c_cache: object = field(default=None, repr=False)
 
     @staticmethod
@@ -657,6 +658,25 @@ class DeviceProjector:
                                      float(global_scale),
                                      float(denom_threshold), _stream()))
         return em
+
+    def order_events(self, ev: DeviceEvents, num_subsets: int):
+        """Subset-major, LOR-sorted copy of the events (yrtb_events_subset_order
+        + yrtb_events_gather).  Returns (events, subset offsets)."""
+        n = ev.count
+        perm = torch.empty(n, dtype=torch.int64, device="cuda")
+        offs = np.zeros(num_subsets + 1, np.uint64)
+        L.check(L.lib().yrtb_events_subset_order(
+            self.h, ctypes.byref(ev.c()), int(num_subsets), perm.data_ptr(),
+            offs.ctypes.data, _stream()))
+        like = lambda t: None if t is None else torch.empty_like(t)
+        out = DeviceEvents(n, like(ev.d1), like(ev.d2), like(ev.lor),
+                           like(ev.tof), like(ev.frame), like(ev.motion_frame),
+                           ev.motion, like(ev.measurement), like(ev.sens),
+                           like(ev.att), like(ev.additive))
+        L.check(L.lib().yrtb_events_gather(ctypes.byref(ev.c()), perm.data_ptr(),
+                                           ctypes.byref(out.c()), _stream()))
+        out.perm = perm
+        return out, offs
 
     def count_crossings(self, ev: DeviceEvents, rng=None) -> torch.Tensor:
         out = torch.zeros(ev.count, dtype=torch.int32, device="cuda")

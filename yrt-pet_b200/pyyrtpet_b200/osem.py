@@ -40,6 +40,10 @@ class OSEM_GPU:
         self.imageParams: Optional[ImageParams] = None
         self.usingListModeInput = False
         self.useGraphs = True
+        # Reorder events subset-major and by LOR before iterating (GPU
+        # coherence); results differ from file order only by FP summation
+        # order.
+        self.orderEvents = True
         self._data = None
         self._sens_images: List[torch.Tensor] = []
         self._sens_histo = None
@@ -234,6 +238,9 @@ class OSEM_GPU:
         ip = self.imageParams.withFrames(nt)
         proj = DeviceProjector(self.scanner, ip, self.projectorParams)
         ev = self._listmode_events(proj, lm)
+        offsets = None
+        if self.orderEvents:
+            ev, offsets = proj.order_events(ev, self.num_OSEM_subsets)
         J = ip.numVoxels
         img = torch.empty(nt * J, dtype=torch.float32, device="cuda")
         init = 0
@@ -251,7 +258,8 @@ class OSEM_GPU:
         p = L.yrtb_osem_params(self.num_MLEM_iterations, self.num_OSEM_subsets,
                                self._global, self.denomThreshold, self.EPS_FLT,
                                init, int(self.useGraphs),
-                               _ptr(self._frame_scale))
+                               _ptr(self._frame_scale),
+                               None if offsets is None else offsets.ctypes.data)
         stream = torch.cuda.current_stream()
         use_side = self.useGraphs and stream.cuda_stream == 0
         s = torch.cuda.Stream() if use_side else stream
