@@ -266,48 +266,38 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	const int nx = g.nx, ny = g.ny, nz = g.nz;
 	const int nxy = nx * ny;
 	int off = 0;
-	float axp = ax_next, ayp = ay_next, azp = az_next;
 	const float fdx = static_cast<float>(dir_x) * dx;
 	const float fdy = static_cast<float>(dir_y) * dy;
 	const float fdz = static_cast<float>(dir_z) * dz;
 
-	// 3. Incremental walk: step to the nearest crossing (ties step together).
-	// A ray crosses at most nx+ny+nz+3 planes inside the grid; the cap only
-	// guards against non-finite input and never binds for finite rays.
+	// 3. Incremental walk: step to the nearest crossing; ties step together
+	// (<= on the crossing values from the start of the step).  Written with
+	// selects instead of branches so that the threads of a warp, whose rays
+	// step along different axes, stay converged; every value is the one the
+	// branchy formulation computes.  A ray crosses at most nx+ny+nz+3 planes
+	// inside the grid; the step cap only guards against non-finite input.
 	const int maxSteps = 2 * (nx + ny + nz) + 16;
 	for (int step = 0; a_cur < amax && step < maxSteps; step++)
 	{
-		int dir_next = 0;
-		if (axp <= ayp && axp <= azp)
-		{
-			a_next = ax_next;
-			x_cur += fdx;
-			ax_next = (x_cur - p1.x) * inv_x;
-			dir_next |= 1;
-		}
-		if (ayp <= axp && ayp <= azp)
-		{
-			a_next = ay_next;
-			y_cur += fdy;
-			ay_next = (y_cur - p1.y) * inv_y;
-			dir_next |= 2;
-		}
-		if (azp <= axp && azp <= ayp)
-		{
-			a_next = az_next;
-			z_cur += fdz;
-			az_next = (z_cur - p1.z) * inv_z;
-			dir_next |= 4;
-		}
-		if (a_next > amax)
-			a_next = amax;
+		const float ax = ax_next, ay = ay_next, az = az_next;
+		const bool sx = (ax <= ay) && (ax <= az);
+		const bool sy = (ay <= ax) && (ay <= az);
+		const bool sz = (az <= ax) && (az <= ay);
+		a_next = sz ? az : (sy ? ay : (sx ? ax : a_next));
+		const float xn = x_cur + fdx, yn = y_cur + fdy, zn = z_cur + fdz;
+		const float axn = (xn - p1.x) * inv_x;
+		const float ayn = (yn - p1.y) * inv_y;
+		const float azn = (zn - p1.z) * inv_z;
+		x_cur = sx ? xn : x_cur;
+		y_cur = sy ? yn : y_cur;
+		z_cur = sz ? zn : z_cur;
+		ax_next = sx ? axn : ax_next;
+		ay_next = sy ? ayn : ay_next;
+		az_next = sz ? azn : az_next;
+		const int dir_next = (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
+		a_next = (a_next > amax) ? amax : a_next;
 		if (a_cur >= a_next)
-		{
-			axp = ax_next;
-			ayp = ay_next;
-			azp = az_next;
 			continue;
-		}
 		if (first)
 		{
 			const float a_mid = 0.5f * (a_cur + a_next);
@@ -316,45 +306,23 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 			vz = static_cast<int>((p1.z + a_mid * (p2.z - p1.z) + g.lz / 2.0f) * inv_dz);
 			off = vz * nxy + vy * nx;
 			first = false;
-			if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
-				break;
 		}
 		else
 		{
-			bool out = false;
-			if (dir_prev & 1)
-			{
-				vx += dir_x;
-				out |= (vx < 0 || vx >= nx);
-			}
-			if (dir_prev & 2)
-			{
-				vy += dir_y;
-				if (vy < 0 || vy >= ny)
-					out = true;
-				else
-					off += dir_y * nx;
-			}
-			if (dir_prev & 4)
-			{
-				vz += dir_z;
-				if (vz < 0 || vz >= nz)
-					out = true;
-				else
-					off += dir_z * nxy;
-			}
-			if (out)
-				break;
+			const int mx = dir_prev & 1, my = (dir_prev >> 1) & 1, mz = (dir_prev >> 2) & 1;
+			vx += mx * dir_x;
+			vy += my * dir_y;
+			vz += mz * dir_z;
+			off += my * dir_y * nx + mz * dir_z * nxy;
 		}
+		if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
+			break;
 		dir_prev = dir_next;
 		float w = (a_next - a_cur) * d_norm;
 		if constexpr (TOF)
 			w *= tofWeight(tp, d_norm, tofValue, a_cur * d_norm, a_next * d_norm);
 		visit(vx + off, w);
 		a_cur = a_next;
-		axp = ax_next;
-		ayp = ay_next;
-		azp = az_next;
 	}
 }
 
