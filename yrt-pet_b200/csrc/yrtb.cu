@@ -435,9 +435,10 @@ __global__ void __launch_bounds__(kBlock)
              float* __restrict__ out, float globalScale, float denomThr,
              unsigned long long* err)
 {
-	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-	     k < R.count; k += nthreads)
+	// One item per thread: a warp's threads stay converged across items
+	// (a grid-stride loop lets them drift apart between items).
+	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (k < R.count)
 	{
 		const uint64_t e = R.start + k * R.stride;
 		const int frame = E.frame ? __ldg(E.frame + e) : 0;
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(kBlock)
 				out[e] = 0.f;
 			if constexpr (OP == OP_COUNT)
 				reinterpret_cast<uint32_t*>(out)[e] = 0u;
-			continue;
+			return;
 		}
 		const float tofv = TOF ? __ldg(E.tof + e) : 0.f;
 		const int64_t fo = static_cast<int64_t>(frame) * P.g.nvox;
@@ -479,7 +480,7 @@ __global__ void __launch_bounds__(kBlock)
 			const float s = E.sens ? __ldg(E.sens + e) : 1.0f;
 			const float a = E.att ? __ldg(E.att + e) : 1.0f;
 			if (m == 0.f || s == 0.f || a == 0.f)
-				continue;
+				return;
 			float u = forwardEvent<KIND, TOF, COMP>(P, in + fo, p1, p2, n1, n2,
 			                                        tofv, k);
 			u *= s;
@@ -506,9 +507,10 @@ __global__ void __launch_bounds__(kBlock)
                   const float* __restrict__ muImg, float* __restrict__ out,
                   unsigned long long* err)
 {
-	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-	     k < R.count; k += nthreads)
+	// One item per thread: a warp's threads stay converged across items
+	// (a grid-stride loop lets them drift apart between items).
+	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (k < R.count)
 	{
 		const uint64_t e = R.start + k * R.stride;
 		float3 p1, p2, n1, n2;
@@ -516,7 +518,7 @@ __global__ void __launch_bounds__(kBlock)
 		{
 			atomicAdd(err, 1ULL);
 			out[e] = 0.f;
-			continue;
+			return;
 		}
 		// fetchEvent subtracted the reconstruction grid offset; move to the
 		// attenuation grid instead.
@@ -536,9 +538,10 @@ __global__ void __launch_bounds__(kBlock)
                    const float* __restrict__ histo, int invert,
                    float* __restrict__ out, unsigned long long* err)
 {
-	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-	     k < R.count; k += nthreads)
+	// One item per thread: a warp's threads stay converged across items
+	// (a grid-stride loop lets them drift apart between items).
+	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (k < R.count)
 	{
 		const uint64_t e = R.start + k * R.stride;
 		uint64_t b;
@@ -567,18 +570,19 @@ __global__ void __launch_bounds__(kBlock)
             const float* __restrict__ addH, Geom mu,
             const float* __restrict__ muImg, float globalScale, float denomThr)
 {
-	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-	     k < count; k += nthreads)
+	// One item per thread: a warp's threads stay converged across items
+	// (a grid-stride loop lets them drift apart between items).
+	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (k < count)
 	{
 		const uint64_t bin = h3SubsetBin(H, k, numPhiSubset, numSubsets, subset);
 		uint32_t d1, d2;
 		h3Pair(H, bin, d1, d2);
 		if (d1 == 0 && d2 == 0)
-			continue;
+			return;
 		const float m = EM ? __ldg(meas + bin) : 1.0f;
 		if (EM && m == 0.f)
-			continue;
+			return;
 		const float s = sensH ? __ldg(sensH + bin) : 1.0f;
 		const float4 pa = __ldg(P.scan.pos + d1), pb = __ldg(P.scan.pos + d2);
 		const float4 oa = __ldg(P.scan.ori + d1), ob = __ldg(P.scan.ori + d2);
@@ -672,10 +676,11 @@ __global__ void k_gather(const T* __restrict__ in, const unsigned long long* __r
 __global__ void k_multiray_offsets(uint64_t count, int numRays,
                                    float* __restrict__ out)
 {
-	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	// One item per thread: a warp's threads stay converged across items
+	// (a grid-stride loop lets them drift apart between items).
+	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
 	const int per = 4 * (numRays - 1);
-	for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-	     k < count; k += nthreads)
+	if (k < count)
 	{
 		MultiRay mr;
 		mr.init(k, make_float3(1.f, 0.f, 0.f), make_float3(1.f, 0.f, 0.f));
@@ -814,6 +819,12 @@ __global__ void k_scale(float* __restrict__ x, uint64_t n, float v)
 
 int g_numSMs = 0;
 
+// Blocks for one item per thread.
+unsigned gridAll(uint64_t n)
+{
+	return static_cast<unsigned>(std::max<uint64_t>(1, (n + kBlock - 1) / kBlock));
+}
+
 unsigned gridFor(uint64_t n, int perSM = 8)
 {
 	if (g_numSMs == 0)
@@ -949,7 +960,7 @@ template <int OP, int KIND, bool TOF, bool COMP>
 void launchEvents(yrtb_projector* h, const Events& E, Range R, const float* in,
                   float* out, float gs, float thr, cudaStream_t st)
 {
-	k_events<OP, KIND, TOF, COMP><<<gridFor(R.count), kBlock, 0, st>>>(
+	k_events<OP, KIND, TOF, COMP><<<gridAll(R.count), kBlock, 0, st>>>(
 	    h->P, E, R, in, out, gs, thr, h->d_err);
 }
 
@@ -1030,7 +1041,7 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 	const uint64_t count = h3SubsetSize(*h->h3, numSubsets, subset, nps);
 	const Geom mg = mu ? makeGeom(*muParams) : Geom{};
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-	const unsigned grid = gridFor(count);
+	const unsigned grid = gridAll(count);
 #define YRTB_HISTO(KIND)                                                       \
 	k_histo<KIND, EM><<<grid, kBlock, 0, st>>>(h->P, h->h3d, count, nps,       \
 	                                           numSubsets, subset, img, out,  \
@@ -1261,7 +1272,7 @@ yrtb_status yrtb_multiray_offsets(yrtb_projector* h, uint64_t count,
 	if (h->P.numRays < 2 || count == 0)
 		return YRTB_OK;
 	YRTB_CUDA(cudaSetDevice(h->device));
-	k_multiray_offsets<<<gridFor(count), kBlock, 0,
+	k_multiray_offsets<<<gridAll(count), kBlock, 0,
 	                     reinterpret_cast<cudaStream_t>(stream)>>>(
 	    count, h->P.numRays, d_out);
 	YRTB_LAUNCHED();
@@ -1422,7 +1433,7 @@ yrtb_status yrtb_attenuation_factors(yrtb_projector* h, const float* d_mu,
 	if (range.count == 0)
 		return YRTB_OK;
 	YRTB_CUDA(cudaSetDevice(h->device));
-	k_attenuation<<<gridFor(range.count), kBlock, 0,
+	k_attenuation<<<gridAll(range.count), kBlock, 0,
 	                reinterpret_cast<cudaStream_t>(stream)>>>(
 	    h->P, makeGeom(*mu_params), toDev(ev),
 	    Range{range.start, range.stride, range.count}, d_mu, d_out, h->d_err);
@@ -1444,7 +1455,7 @@ yrtb_status yrtb_gather_histo3d(yrtb_projector* h, const float* d_histo,
 	if (range.count == 0)
 		return YRTB_OK;
 	YRTB_CUDA(cudaSetDevice(h->device));
-	k_gather_histo<<<gridFor(range.count), kBlock, 0,
+	k_gather_histo<<<gridAll(range.count), kBlock, 0,
 	                 reinterpret_cast<cudaStream_t>(stream)>>>(
 	    h->P, h->h3d, toDev(ev), Range{range.start, range.stride, range.count},
 	    d_histo, invert, d_out, h->d_err);
