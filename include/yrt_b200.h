@@ -343,6 +343,26 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
                                float* d_work, const yrtb_osem_params* p,
                                yrtb_stream stream);
 
+/* Same as yrtb_osem_listmode, for callers that cannot allocate device
+ * memory: it takes no work buffer and calls no allocating routine.  Some
+ * hosts own every byte of device memory through their own pool, or run
+ * inside a real-time loop where cudaMalloc / cudaFree (which synchronise the
+ * device) are not allowed after start-up; they still have to reconstruct.
+ * The scratch (EM image and scaled sensitivity, (nt + 1) x voxels floats)
+ * lives in one static device array of YRTB_OSEM_STATIC_MAX_FLOATS floats
+ * (16 MiB) that every GPU loading the library holds until exit; larger images
+ * are rejected with YRTB_ERR_ARGUMENT.  use_graph must be 0.  The first call
+ * on a device looks up the array's device address (with that device
+ * current); make that first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (other streams, other host
+ * threads, same device) race and must be serialised by the caller.  No
+ * counterpart in the reference. */
+#define YRTB_OSEM_STATIC_MAX_FLOATS (4u * 1024u * 1024u)
+yrtb_status yrtb_osem_listmode_static(yrtb_projector* h, const yrtb_events* ev,
+                                      const float* d_sens, float* d_image,
+                                      const yrtb_osem_params* p,
+                                      yrtb_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

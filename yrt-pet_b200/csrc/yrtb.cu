@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1720,3 +1721,71 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 }
 
 }  // extern "C"
+
+// ------------------------------------------- OSEM without any allocation --
+// Scratch of yrtb_osem_listmode_static: the EM image (nt frames) followed by
+// the 1/numSubsets-scaled sensitivity image.  A file-scope device array, so
+// the entry point never allocates; every GPU that loads the library holds it
+// (16 MiB) until the process exits.
+static __device__ __align__(256) float g_osemStaticScratch[YRTB_OSEM_STATIC_MAX_FLOATS];
+
+namespace
+{
+// Device address of g_osemStaticScratch per device.  In host code the array's
+// name is only a host-side stand-in, so the address is looked up once per
+// device with that device current.
+yrtb_status osemStaticScratch(int device, float** out)
+{
+	constexpr int kMaxDevices = 64;
+	static std::mutex lock;
+	static float* addr[kMaxDevices] = {};
+	if (device < 0 || device >= kMaxDevices)
+		return fail(YRTB_ERR_ARGUMENT, "device index out of range");
+	std::lock_guard<std::mutex> guard(lock);
+	if (addr[device] == nullptr)
+	{
+		void* p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_osemStaticScratch);
+		if (e != cudaSuccess || p == nullptr)
+			return fail(YRTB_ERR_CUDA,
+			            std::string("cudaGetSymbolAddress(osem static scratch): ") +
+			                cudaGetErrorString(e));
+		addr[device] = static_cast<float*>(p);
+	}
+	*out = addr[device];
+	return YRTB_OK;
+}
+}  // namespace
+
+extern "C" yrtb_status yrtb_osem_listmode_static(yrtb_projector* h,
+                                                 const yrtb_events* ev,
+                                                 const float* d_sens,
+                                                 float* d_image,
+                                                 const yrtb_osem_params* p,
+                                                 yrtb_stream stream)
+{
+	if (!h || !ev || !d_sens || !d_image || !p)
+		return fail(YRTB_ERR_ARGUMENT, "null OSEM argument");
+	if (p->use_graph)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "yrtb_osem_listmode_static does not build CUDA graphs "
+		            "(instantiating one allocates); set use_graph = 0");
+	const uint64_t J = static_cast<uint64_t>(h->P.g.nvox);
+	const uint64_t need = J * static_cast<uint64_t>(h->ip.nt) + J;
+	if (need > YRTB_OSEM_STATIC_MAX_FLOATS)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "image too large for yrtb_osem_listmode_static: needs " +
+		                std::to_string(need) + " floats of scratch ((nt+1) x voxels), "
+		                "the static buffer holds " +
+		                std::to_string(static_cast<uint64_t>(YRTB_OSEM_STATIC_MAX_FLOATS)) +
+		                "; use yrtb_osem_listmode with a caller-provided work buffer");
+	YRTB_CUDA(cudaSetDevice(h->device));
+	float* scratch = nullptr;
+	const yrtb_status st = osemStaticScratch(h->device, &scratch);
+	if (st != YRTB_OK)
+		return st;
+	// The shared driver overwrites the sensitivity part and clears the EM
+	// image before every subset, so stale contents of earlier calls are never
+	// read.
+	return yrtb_osem_listmode(h, ev, d_sens, d_image, scratch, p, stream);
+}

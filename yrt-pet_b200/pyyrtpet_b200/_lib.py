@@ -19,6 +19,7 @@ YRTB_ERR_EVENT = 4
 
 YRTB_SIDDON = 0
 YRTB_DD = 1
+YRTB_OSEM_STATIC_MAX_FLOATS = 4 * 1024 * 1024
 YRTB_MIRROR = 0
 YRTB_COMPENSATED = 1
 
@@ -119,6 +120,8 @@ SIGNATURES = {
     "yrtb_scale": ([c_vp, c_u64, c_f, c_vp], ctypes.c_int),
     "yrtb_osem_listmode": ([c_vp, _P(yrtb_events), c_vp, c_vp, c_vp,
                             _P(yrtb_osem_params), c_vp], ctypes.c_int),
+    "yrtb_osem_listmode_static": ([c_vp, _P(yrtb_events), c_vp, c_vp,
+                                   _P(yrtb_osem_params), c_vp], ctypes.c_int),
 }
 
 _lib = None
