@@ -90,7 +90,9 @@ typedef struct
  *   frame         dynamic frame; events with frame < 0 are skipped, frames
  *                 >= nt are counted as invalid and skipped
  *   motion_frame  rigid-motion frame per event; motion: 12 floats per motion
- *                 frame (r00 r01 r02 r10 r11 r12 r20 r21 r22 tx ty tz), applied
+ *                 frame in the reference's transform_t order (r00 r01 r02 tx
+ *                 r10 r11 r12 ty r20 r21 r22 tz, include/yrt-pet/utils/Types.hpp:57),
+ *                 applied
  *                 to both endpoints as in ProjectionData::getLOR
  *                 (src/datastruct/projection/ProjectionData.cpp:275-321);
  *                 a negative motion frame leaves the LOR unmoved;
@@ -273,6 +275,22 @@ yrtb_status yrtb_listmode_to_histo3d(yrtb_projector* h, const uint32_t* d_d1,
                                      const float* d_values, uint64_t n,
                                      float* d_histo, uint64_t* n_invalid,
                                      yrtb_stream stream);
+
+/* List-mode file records on the device (after one H2D copy of the raw file
+ * bytes) -> structure of arrays.  Record layout of ListModeLUT files
+ * (src/datastruct/projection/ListModeLUT.cpp:224-307): u32 timestamp, u32 d1,
+ * u32 d2, then f32 TOF if has_tof, then f32 randoms if has_randoms.  d_ts,
+ * d_tof, d_randoms may be NULL to drop a field.  Records with a detector id
+ * >= num_dets make the call return YRTB_ERR_EVENT naming the first such
+ * event (the reference throws "Detectors invalid in list-mode event N").
+ * Synchronises the stream.  Replaces the host-side ListModeLUTOwned::
+ * readFromFile unpacking and the per-batch host gather of
+ * OSEM_GPU::precomputeBatchPropsForRecon (src/recon/OSEM_GPU.cu:698-805). */
+yrtb_status yrtb_unpack_listmode(const void* d_raw, uint64_t n, int has_tof,
+                                 int has_randoms, uint32_t num_dets,
+                                 uint32_t* d_ts, uint32_t* d_d1, uint32_t* d_d2,
+                                 float* d_tof, float* d_randoms,
+                                 yrtb_stream stream);
 
 /* Histogram3D maps on the device: bin ids of detector pairs (UINT64_MAX for
  * pairs outside the histogram) and detector pairs of bin ids.  Replace

@@ -52,6 +52,12 @@ class ProjDesc(ctypes.Structure):
                 ("psf_taps", ctypes.c_void_p), ("threads", ctypes.c_int)]
 
 
+class LmExtra(ctypes.Structure):
+    _fields_ = [("timestamps", ctypes.c_void_p), ("num_frame_ts", ctypes.c_uint64),
+                ("frame_ts", ctypes.c_void_p), ("num_motion", ctypes.c_uint64),
+                ("motion_starts", ctypes.c_void_p), ("motion", ctypes.c_void_p)]
+
+
 class OsemDesc(ctypes.Structure):
     _fields_ = [("projector", ctypes.c_int), ("num_rays", ctypes.c_int),
                 ("tof_fwhm_ps", ctypes.c_float), ("tof_n_std", ctypes.c_int),
@@ -424,6 +430,25 @@ def ref_dd(sc: Scanner, ip: ImageParams, lors, orients, *, image=None,
     return vals if forward else img
 
 
+def ref_read_listmode(sc: Scanner, fname: str, tof: bool, randoms: bool,
+                      cap: int):
+    L = ref_lib()
+    L.ref_read_listmode.restype = ctypes.c_int64
+    ts = np.zeros(cap, np.uint32)
+    d1 = np.zeros(cap, np.uint32)
+    d2 = np.zeros(cap, np.uint32)
+    tv = np.zeros(cap, np.float32)
+    rv = np.zeros(cap, np.float32)
+    with quiet():
+        n = L.ref_read_listmode(ctypes.byref(sc.desc()), fname.encode(),
+                                int(tof), int(randoms), ctypes.c_uint64(cap),
+                                _p(ts), _p(d1), _p(d2), _p(tv), _p(rv))
+    if n < 0:
+        raise RuntimeError(ref_lib().ref_last_error().decode())
+    n = min(n, cap)
+    return ts[:n], d1[:n], d2[:n], tv[:n], rv[:n]
+
+
 def ref_dd_overlap(p0, p1, d0, d1) -> float:
     return ref_lib().ref_dd_overlap(p0, p1, d0, d1)
 
@@ -488,6 +513,36 @@ def ref_osem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, *, tof=None,
             _p(s), ctypes.c_uint64(len(d1)), _p(d1), _p(d2), _p(tof), _p(randoms),
             _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
             _p(att), _p(out), ctypes.byref(sec))
+    _ref_check(rc)
+    return out, sec.value
+
+
+def ref_osem_listmode_dynamic(sc: Scanner, ip: ImageParams, sens, d1, d2,
+                              timestamps, *, frame_ts=None, motion_starts=None,
+                              motion=None, tof=None, **kw):
+    """Reference OSEM with DynamicFraming and/or LORMotion; ip.nt must equal
+    the number of dynamic frames (len(frame_ts) - 1)."""
+    o = _osem_desc(**kw)
+    out = np.zeros(ip.shape, np.float32)
+    sec = ctypes.c_double()
+    d1 = _c(d1, np.uint32)
+    d2 = _c(d2, np.uint32)
+    ts = _c(timestamps, np.uint32)
+    fts = _c(frame_ts, np.uint32)
+    ms = _c(motion_starts, np.uint32)
+    mo = _c(motion, np.float32)
+    tof = _c(tof, np.float32)
+    s = _c(sens, np.float32)
+    ex = LmExtra(ts.ctypes.data, 0 if fts is None else len(fts),
+                 None if fts is None else fts.ctypes.data,
+                 0 if ms is None else len(ms),
+                 None if ms is None else ms.ctypes.data,
+                 None if mo is None else mo.ctypes.data)
+    with quiet():
+        rc = ref_lib().ref_osem_listmode_ex(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
+            _p(s), ctypes.c_uint64(len(d1)), _p(d1), _p(d2), _p(tof), None,
+            None, None, None, ctypes.byref(ex), _p(out), ctypes.byref(sec))
     _ref_check(rc)
     return out, sec.value
 

@@ -17,6 +17,8 @@
 //   OSEM (CPU)                      src/recon/OSEM.cpp:315-365, OSEM_CPU.cpp:127-403
 
 #include "yrt-pet/datastruct/image/Image.hpp"
+#include "yrt-pet/datastruct/projection/DynamicFraming.hpp"
+#include "yrt-pet/datastruct/projection/LORMotion.hpp"
 #include "yrt-pet/datastruct/projection/Histogram3D.hpp"
 #include "yrt-pet/datastruct/projection/ListModeLUT.hpp"
 #include "yrt-pet/datastruct/projection/UniformHistogram.hpp"
@@ -371,6 +373,33 @@ int ref_dd(const ref_scanner_desc* s, const ref_image_desc* d, float* image,
 	    });
 }
 
+// Reads a ListModeLUT file with the reference reader; returns the number of
+// events (or -1 on error) and fills the arrays when they are large enough.
+int64_t ref_read_listmode(const ref_scanner_desc* s, const char* fname,
+                          int tof, int randoms, uint64_t cap, uint32_t* ts,
+                          uint32_t* d1, uint32_t* d2, float* tofv, float* rnd)
+{
+	int64_t n = -1;
+	const int rc = guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    ListModeLUTOwned lm(*sc, fname, tof != 0, randoms != 0);
+		    n = static_cast<int64_t>(lm.count());
+		    for (uint64_t i = 0; i < std::min<uint64_t>(cap, lm.count()); i++)
+		    {
+			    ts[i] = lm.getTimestamp(i);
+			    d1[i] = lm.getDetector1(i);
+			    d2[i] = lm.getDetector2(i);
+			    if (tof)
+				    tofv[i] = lm.getTOFValue(i);
+			    if (randoms)
+				    rnd[i] = lm.getRandomsEstimate(i);
+		    }
+	    });
+	return rc == 0 ? n : -1;
+}
+
 float ref_dd_overlap(float p0, float p1, float d0, float d1)
 {
 	return ProjectorDD::getOverlap(p0, p1, d0, d1, nullptr, nullptr);
@@ -472,16 +501,30 @@ int ref_sensitivity(const ref_scanner_desc* s, const ref_image_desc* d,
 	    });
 }
 
+// Optional list-mode extras: event timestamps, dynamic framing
+// (numFrames+1 timestamps, DynamicFraming) and rigid LOR motion (LORMotion:
+// starting timestamp + transform_t per motion frame).
+struct ref_lm_extra
+{
+	const uint32_t* timestamps;
+	uint64_t num_frame_ts;
+	const uint32_t* frame_ts;
+	uint64_t num_motion;
+	const uint32_t* motion_starts;
+	const float* motion;  // 12 floats per motion frame, transform_t order
+};
+
 // List-mode OSEM with the reference CPU path.  sens: one sensitivity image
 // (list-mode).  Events: detector pairs, optional TOF (ps) and optional
 // per-event additive (randoms) estimates.  Optional sensitivity histogram and
 // attenuation image act as in the reference corrector.  out: nt images.
-int ref_osem_listmode(const ref_scanner_desc* s, const ref_image_desc* d,
-                      const ref_osem_desc* o, const float* sens, uint64_t n,
-                      const uint32_t* d1, const uint32_t* d2, const float* tof,
-                      const float* randoms, const float* sens_histo,
-                      const ref_image_desc* att_desc, const float* att_image,
-                      float* out, double* seconds)
+int ref_osem_listmode_ex(const ref_scanner_desc* s, const ref_image_desc* d,
+                         const ref_osem_desc* o, const float* sens, uint64_t n,
+                         const uint32_t* d1, const uint32_t* d2,
+                         const float* tof, const float* randoms,
+                         const float* sens_histo, const ref_image_desc* att_desc,
+                         const float* att_image, const ref_lm_extra* ex,
+                         float* out, double* seconds)
 {
 	return guarded(
 	    [&]
@@ -497,6 +540,28 @@ int ref_osem_listmode(const ref_scanner_desc* s, const ref_image_desc* d,
 				    lm.setTOFValueOfEvent(i, tof[i]);
 			    if (randoms)
 				    lm.setRandomsEstimateOfEvent(i, randoms[i]);
+			    if (ex && ex->timestamps)
+				    lm.setTimestampOfEvent(i, ex->timestamps[i]);
+		    }
+		    if (ex && ex->num_frame_ts > 1)
+		    {
+			    std::vector<timestamp_t> v(ex->frame_ts,
+			                               ex->frame_ts + ex->num_frame_ts);
+			    lm.addDynamicFraming(v);
+		    }
+		    if (ex && ex->num_motion > 0)
+		    {
+			    auto mot = std::make_shared<LORMotion>(ex->num_motion);
+			    for (uint64_t f = 0; f < ex->num_motion; f++)
+			    {
+				    const float* m = ex->motion + f * 12;
+				    transform_t t{m[0], m[1], m[2],  m[3],  m[4],  m[5],
+				                  m[6], m[7], m[8], m[9], m[10], m[11]};
+				    mot->setTransform(static_cast<frame_t>(f), t);
+				    mot->setStartingTimestamp(static_cast<frame_t>(f),
+				                              ex->motion_starts[f]);
+			    }
+			    lm.addLORMotion(mot);
 		    }
 		    auto osem = util::createOSEM(*sc, false);
 		    ImageParams ip = makeParams(d);
@@ -535,9 +600,22 @@ int ref_osem_listmode(const ref_scanner_desc* s, const ref_image_desc* d,
 		    const auto t1 = std::chrono::steady_clock::now();
 		    if (seconds)
 			    *seconds = std::chrono::duration<double>(t1 - t0).count();
-		    const size_t nv = d->nx * d->ny * d->nz * d->nt;
+		    const ImageParams& rp = res->getParams();
+		    const size_t nv = rp.nx * rp.ny * rp.nz * rp.nt;
 		    std::memcpy(out, res->getRawPointer(), nv * sizeof(float));
 	    });
+}
+
+int ref_osem_listmode(const ref_scanner_desc* s, const ref_image_desc* d,
+                      const ref_osem_desc* o, const float* sens, uint64_t n,
+                      const uint32_t* d1, const uint32_t* d2, const float* tof,
+                      const float* randoms, const float* sens_histo,
+                      const ref_image_desc* att_desc, const float* att_image,
+                      float* out, double* seconds)
+{
+	return ref_osem_listmode_ex(s, d, o, sens, n, d1, d2, tof, randoms,
+	                            sens_histo, att_desc, att_image, nullptr, out,
+	                            seconds);
 }
 
 // Histogram-mode OSEM (measurements in a Histogram3D).

@@ -203,8 +203,8 @@ def test_siddon_image_offset_and_motion_and_frames():
     f32 = np.float32
     moved = lors.copy()
     for i in np.nonzero(mframe >= 0)[0]:
-        R = xf[mframe[i], :9].reshape(3, 3)
-        t = xf[mframe[i], 9:]
+        M = xf[mframe[i]].reshape(3, 4)
+        R, t = M[:, :3], M[:, 3]
         for e in (0, 3):
             p_ = lors[i, e:e + 3]
             q = [f32(f32(f32(R[r, 0] * p_[0]) + f32(R[r, 1] * p_[1])) + f32(R[r, 2] * p_[2]))

@@ -308,10 +308,13 @@ __device__ __forceinline__ bool fetchEvent(const KParams& P, const Events& E,
 		if (mf >= 0)
 		{
 			const float* m = E.motion + static_cast<int64_t>(mf) * 12;
+			// transform_t layout: r00 r01 r02 tx r10 r11 r12 ty r20 r21 r22 tz.
 			const float r00 = __ldg(m + 0), r01 = __ldg(m + 1), r02 = __ldg(m + 2);
-			const float r10 = __ldg(m + 3), r11 = __ldg(m + 4), r12 = __ldg(m + 5);
-			const float r20 = __ldg(m + 6), r21 = __ldg(m + 7), r22 = __ldg(m + 8);
-			const float tx = __ldg(m + 9), ty = __ldg(m + 10), tz = __ldg(m + 11);
+			const float tx = __ldg(m + 3);
+			const float r10 = __ldg(m + 4), r11 = __ldg(m + 5), r12 = __ldg(m + 6);
+			const float ty = __ldg(m + 7);
+			const float r20 = __ldg(m + 8), r21 = __ldg(m + 9), r22 = __ldg(m + 10);
+			const float tz = __ldg(m + 11);
 			// Matrix::operator*(Vector3D) then + translation (Matrix.cpp:177-186).
 			float3 q1 = make_float3(r00 * p1.x + r01 * p1.y + r02 * p1.z,
 			                        r10 * p1.x + r11 * p1.y + r12 * p1.z,
@@ -692,6 +695,43 @@ __global__ void k_multiray_offsets(uint64_t count, int numRays,
 			for (int i = 0; i < 4; i++)
 				out[k * per + 4 * (r - 1) + i] = u[i];
 		}
+	}
+}
+
+// List-mode records (ListModeLUT file layout: u32 timestamp, u32 d1, u32 d2,
+// [f32 TOF], [f32 randoms]) -> structure of arrays.  The lowest index of an
+// event with an invalid detector id is recorded in *firstBad.
+__global__ void k_unpack_listmode(const uint32_t* __restrict__ raw, uint64_t n,
+                                  int fields, int hasTof, int hasRandoms,
+                                  uint32_t numDets, uint32_t* __restrict__ ts,
+                                  uint32_t* __restrict__ d1,
+                                  uint32_t* __restrict__ d2,
+                                  float* __restrict__ tof,
+                                  float* __restrict__ randoms,
+                                  unsigned long long* firstBad)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+	{
+		const uint32_t* r = raw + i * fields;
+		const uint32_t a = __ldg(r + 1), b = __ldg(r + 2);
+		if (a >= numDets || b >= numDets)
+			atomicMin(firstBad, static_cast<unsigned long long>(i));
+		if (ts)
+			ts[i] = __ldg(r);
+		d1[i] = a;
+		d2[i] = b;
+		int f = 3;
+		if (hasTof)
+		{
+			const float v = __uint_as_float(__ldg(r + f));
+			if (tof)
+				tof[i] = v;
+			f++;
+		}
+		if (hasRandoms && randoms)
+			randoms[i] = __uint_as_float(__ldg(r + f));
 	}
 }
 
@@ -1523,6 +1563,37 @@ yrtb_status yrtb_listmode_to_histo3d(yrtb_projector* h, const uint32_t* d1,
 		            std::to_string(bad) +
 		                " detector pairs do not respect the maximum ring difference "
 		                "or minimum angle difference of the histogram");
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_unpack_listmode(const void* d_raw, uint64_t n, int has_tof,
+                                 int has_randoms, uint32_t num_dets,
+                                 uint32_t* d_ts, uint32_t* d_d1, uint32_t* d_d2,
+                                 float* d_tof, float* d_randoms,
+                                 yrtb_stream stream)
+{
+	if (!d_raw || !d_d1 || !d_d2)
+		return fail(YRTB_ERR_ARGUMENT, "null list-mode buffer");
+	if (reinterpret_cast<uintptr_t>(d_raw) % 4 != 0)
+		return fail(YRTB_ERR_ARGUMENT, "list-mode records must be 4-byte aligned");
+	if (n == 0)
+		return YRTB_OK;
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	unsigned long long* d_bad = nullptr;
+	YRTB_CUDA(cudaMallocAsync(&d_bad, sizeof(unsigned long long), st));
+	YRTB_CUDA(cudaMemsetAsync(d_bad, 0xFF, sizeof(unsigned long long), st));
+	const int fields = 3 + (has_tof ? 1 : 0) + (has_randoms ? 1 : 0);
+	k_unpack_listmode<<<gridFor(n, 16), kBlock, 0, st>>>(
+	    static_cast<const uint32_t*>(d_raw), n, fields, has_tof, has_randoms,
+	    num_dets, d_ts, d_d1, d_d2, d_tof, d_randoms, d_bad);
+	YRTB_LAUNCHED();
+	unsigned long long bad = 0;
+	YRTB_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, st));
+	YRTB_CUDA(cudaFreeAsync(d_bad, st));
+	YRTB_CUDA(cudaStreamSynchronize(st));
+	if (bad != ~0ULL)
+		return fail(YRTB_ERR_EVENT,
+		            "Detectors invalid in list-mode event " + std::to_string(bad));
 	return YRTB_OK;
 }
 

@@ -109,6 +109,9 @@ SIGNATURES = {
                                   c_vp, c_vp], ctypes.c_int),
     "yrtb_events_gather": ([_P(yrtb_events), c_vp, _P(yrtb_events), c_vp],
                            ctypes.c_int),
+    "yrtb_unpack_listmode": ([c_vp, c_u64, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_uint32, c_vp, c_vp, c_vp, c_vp, c_vp,
+                              c_vp], ctypes.c_int),
     "yrtb_histo3d_bins": ([c_vp, c_vp, c_vp, c_u64, c_vp, c_vp], ctypes.c_int),
     "yrtb_histo3d_detpairs": ([c_vp, c_vp, c_u64, c_vp, c_vp, c_vp],
                               ctypes.c_int),

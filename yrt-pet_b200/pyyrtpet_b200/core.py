@@ -385,6 +385,67 @@ class ListModeLUT(ProjectionData):
         self.randoms[i] = v
         self._dev = None
 
+    # -- file I/O (ListModeLUT format: u32 ts, u32 d1, u32 d2, [f32 tof],
+    #    [f32 randoms] per event; ListModeLUT.cpp:224-307)
+    def _fields(self):
+        return 3 + int(self.flagTOF) + int(self.flagRandoms)
+
+    def readFromFile(self, fname: str, device: bool = True):
+        """Loads a list-mode file.  device=True: the raw bytes go to the GPU
+        in one copy and are unpacked there (yrtb_unpack_listmode); the host
+        arrays are filled from the device result."""
+        raw = np.fromfile(fname, dtype=np.uint32)
+        f = self._fields()
+        if raw.size == 0 or raw.size % f != 0:
+            raise RuntimeError("Error: Input file has incorrect size in "
+                               "ListModeLUTOwned::readFromFile.")
+        n = raw.size // f
+        if device:
+            d_raw = torch.from_numpy(raw.view(np.int32)).cuda()
+            ts = torch.empty(n, dtype=torch.int32, device="cuda")
+            d1 = torch.empty_like(ts)
+            d2 = torch.empty_like(ts)
+            tof = torch.empty(n, dtype=torch.float32, device="cuda") if self.flagTOF else None
+            rnd = torch.empty(n, dtype=torch.float32, device="cuda") if self.flagRandoms else None
+            L.check(L.lib().yrtb_unpack_listmode(
+                d_raw.data_ptr(), n, int(self.flagTOF), int(self.flagRandoms),
+                self.scanner.getNumDets(), ts.data_ptr(), d1.data_ptr(),
+                d2.data_ptr(), _ptr(tof), _ptr(rnd), _stream()))
+            self.d1 = d1.cpu().numpy().view(np.uint32)
+            self.d2 = d2.cpu().numpy().view(np.uint32)
+            self.timestamps = ts.cpu().numpy().view(np.uint32)
+            self.tof = None if tof is None else tof.cpu().numpy()
+            self.randoms = None if rnd is None else rnd.cpu().numpy()
+            self._dev = DeviceEvents(n, d1, d2, tof=tof, additive=rnd)
+            return self
+        rec = raw.reshape(n, f)
+        if np.any(rec[:, 1:3] >= self.scanner.getNumDets()):
+            bad = int(np.nonzero(np.any(rec[:, 1:3] >= self.scanner.getNumDets(), axis=1))[0][0])
+            raise RuntimeError(f"Detectors invalid in list-mode event {bad}")
+        self.timestamps = rec[:, 0].copy()
+        self.d1 = rec[:, 1].copy()
+        self.d2 = rec[:, 2].copy()
+        k = 3
+        self.tof = None
+        self.randoms = None
+        if self.flagTOF:
+            self.tof = rec[:, k].copy().view(np.float32)
+            k += 1
+        if self.flagRandoms:
+            self.randoms = rec[:, k].copy().view(np.float32)
+        self._dev = None
+        return self
+
+    def writeToFile(self, fname: str):
+        n = self.count()
+        cols = [self.timestamps if self.timestamps is not None else
+                np.zeros(n, np.uint32), self.d1, self.d2]
+        if self.flagTOF:
+            cols.append(np.asarray(self.tof, np.float32).view(np.uint32))
+        if self.flagRandoms:
+            cols.append(np.asarray(self.randoms, np.float32).view(np.uint32))
+        np.stack([np.asarray(c, np.uint32) for c in cols], 1).tofile(fname)
+
     # -- queries
     def count(self) -> int:
         return len(self.d1)
@@ -415,27 +476,29 @@ class ListModeLUT(ProjectionData):
                                                    idxSubset)
 
     # -- dynamic framing and motion (ListMode.cpp:89-182)
-    def addDynamicFraming(self, frame_starts, frame_stops):
-        """Frames [start_i, stop_i) in timestamp units; events outside every
-        frame get frame -1 (skipped)."""
+    def addDynamicFraming(self, frame_timestamps):
+        """Contiguous frames given by numFrames+1 timestamps (the reference's
+        DynamicFraming vector): frame f = [ts_f, ts_{f+1}); events before the
+        first or at/after the last timestamp get frame -1 (skipped).  Events
+        are chronological, as ListMode::addDynamicFraming assumes
+        (ListMode.cpp:137-182)."""
         if self.timestamps is None:
             raise RuntimeError("dynamic framing needs event timestamps")
-        starts = np.asarray(frame_starts, np.int64)
-        stops = np.asarray(frame_stops, np.int64)
-        if len(starts) == 0:
+        b = np.asarray(frame_timestamps, np.int64)
+        if len(b) < 2:
             raise RuntimeError("Number of frames cannot be zero.")
         ts = self.timestamps.astype(np.int64)
-        fr = np.full(len(ts), -1, np.int32)
-        # The reference walks the (chronological) events once.
-        ev = 0
         n = len(ts)
-        while ev < n and ts[ev] < starts[0]:
+        fr = np.full(n, -1, np.int32)
+        ev = 0
+        while ev < n and ts[ev] < b[0]:
             ev += 1
-        for f in range(len(starts)):
-            e1 = ev + np.searchsorted(ts[ev:], stops[f], side="left")
+        for f in range(len(b) - 1):
+            e1 = ev + int(np.searchsorted(ts[ev:], b[f + 1], side="left"))
             fr[ev:e1] = f
             ev = e1
         self.dynamicFrames = fr
+        self._numDynamicFrames = len(b) - 1
         self._dev = None
 
     def setDynamicFrames(self, frames):
@@ -445,11 +508,17 @@ class ListModeLUT(ProjectionData):
     def getNumDynamicFrames(self) -> int:
         if self.dynamicFrames is None:
             return 1
+        n = getattr(self, "_numDynamicFrames", None)
+        if n is not None:
+            return n
         return int(self.dynamicFrames.max()) + 1 if len(self.dynamicFrames) else 1
 
     def addLORMotion(self, frame_starts, transforms):
-        """Rigid motion: frame f covers timestamps [start_f, start_{f+1});
-        transforms (numFrames, 12) = r00..r22, tx, ty, tz."""
+        """Rigid motion (LORMotion): motion frame f starts at frame_starts[f]
+        and lasts until the next start (the last frame until the end);
+        events before the first start get frame -1 (unmoved).  transforms:
+        (numFrames, 12) in transform_t order (r00 r01 r02 tx r10 r11 r12 ty
+        r20 r21 r22 tz), ListMode::addLORMotion (ListMode.cpp:89-127)."""
         if self.timestamps is None:
             raise RuntimeError("LOR motion needs event timestamps")
         starts = np.asarray(frame_starts, np.int64)

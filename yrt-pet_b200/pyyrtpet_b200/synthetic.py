@@ -305,8 +305,9 @@ def frame_counts_loguniform(num_frames: int, lo: float, hi: float,
 
 def rigid_transforms(num_frames: int, seed: int, max_deg: float = 3.0,
                      max_mm: float = 5.0) -> np.ndarray:
-    """(num_frames, 12): rotation (<= max_deg about a random axis) row-major,
-    then translation (<= max_mm per axis)."""
+    """(num_frames, 12) in transform_t order (r00 r01 r02 tx r10 r11 r12 ty
+    r20 r21 r22 tz): rotation <= max_deg about a random axis, translation
+    <= max_mm per axis."""
     g = np.random.default_rng(seed)
     out = np.zeros((num_frames, 12), np.float32)
     for f in range(num_frames):
@@ -317,6 +318,5 @@ def rigid_transforms(num_frames: int, seed: int, max_deg: float = 3.0,
                       [-axis[1], axis[0], 0]])
         R = np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
         t = g.uniform(-max_mm, max_mm, 3)
-        out[f, :9] = R.ravel()
-        out[f, 9:] = t
+        out[f] = np.concatenate([R, t[:, None]], axis=1).ravel()
     return out
