@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--ref-sample", type=int, default=1_000_000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="compensated",
+                    choices=["mirror", "compensated"])
+    ap.add_argument("--parity-sample", type=int, default=200_000)
     return ap.parse_args()
 
 
@@ -151,6 +154,37 @@ def reference_rate(sc, ip, ev, mu, eff_np, n_sample, threads, iterations=1):
     return n / sec, "port", sec
 
 
+def fp64_parity(sc, ip, proj, ev, n_sample, precision):
+    """rel-L2 of this path's forward projections vs the FP64 oracle on the
+    first n_sample events (non-zero random image)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    import pyyrtpet_b200 as yrt
+    n = min(n_sample, ev.count)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    img = torch.rand(ip.shape, generator=g, device="cuda") + 0.5
+    sub = yrt.DeviceEvents(n, ev.d1[:n], ev.d2[:n], tof=ev.tof[:n])
+    got = proj.forward(img, sub).double().cpu().numpy()
+    osc = po.Scanner(sc.axialFOV, sc.crystalSize_z, sc.crystalSize_trans,
+                     sc.crystalDepth, sc.scannerRadius, sc.detsPerRing,
+                     sc.numRings, sc.numDOI, sc.maxRingDiff, sc.minAngDiff,
+                     sc.detsPerBlock)
+    lut = po.scanner_lut(osc)
+    d1 = sub.d1.cpu().numpy().view(np.uint32)
+    d2 = sub.d2.cpu().numpy().view(np.uint32)
+    lors, _ = po.lors_from_detpairs(lut, d1, d2)
+    oip = po.ImageParams(ip.nx, ip.ny, ip.nz, ip.length_x, ip.length_y,
+                         ip.length_z)
+    ref = po.project(oip, po.Proj(tof_fwhm_ps=TOF_FWHM, tof_n_std=TOF_NSTD,
+                                  threads=os.cpu_count() or 1),
+                     lors, image=img.cpu().numpy(), tof=sub.tof.cpu().numpy(),
+                     precision="f64")
+    err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    return {"fwd_rel_l2": err, "sample_events": n, "precision": precision,
+            "oracle": "FP64 restatement (oracle/oracle.cpp)"}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -211,6 +245,8 @@ def main():
                                               seed=SEED + 7919 * rank)
     pp = yrt.ProjectorParams(sc)
     pp.addTOF(TOF_FWHM, TOF_NSTD)
+    pp.precision = (L.YRTB_COMPENSATED if args.precision == "compensated"
+                    else L.YRTB_MIRROR)
     proj = yrt.DeviceProjector(sc, ip, pp)
     # Correction factors per event, on device (sens = eff1*eff2 histogram
     # gather is equivalent to the direct product here; ACF via Siddon
@@ -406,7 +442,16 @@ def main():
             pass
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # Checker (CPU baseline leg): forward projections of a sample of the
+        # workload's events in this run's precision mode against the FP64
+        # oracle.
+        try:
+            parity = fp64_parity(sc, ip, proj, ev_plain, args.parity_sample,
+                                 args.precision)
+        except Exception as exc:
+            parity = {"error": str(exc)[:200]}
         try:
             r, kind, sec = reference_rate(sc, ip, evs, mu, None,
                                           min(args.ref_sample, ev.count),
@@ -431,7 +476,7 @@ def main():
                                        "256x256x160 @2mm, 214 ps TOF 5 sigma, "
                                        "10 subsets",
                            "events_per_gpu": ev.count, "subsets": SUBSETS,
-                           "precision": "mirror (reference FP32 order)",
+                           "precision": args.precision,
                            "l2": "event arrays (1.2 GB) larger than L2; "
                                  "image (42 MB) L2-resident by design",
                            "parallelism": f"dp{world} (events sharded, EM image "
@@ -444,6 +489,7 @@ def main():
                                   "single-frame batching)"},
                 "osem_s_per_iteration": ms * 1e-3,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "parity_vs_fp64": parity,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
     if dist is not None:

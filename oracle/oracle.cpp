@@ -1183,6 +1183,26 @@ int64_t orc_siddon_trace_f32(const Image* im, const orc_proj* p,
 	return k;
 }
 
+int64_t orc_siddon_trace_f64(const Image* im, const orc_proj* p,
+                             const float* lor, float tof, int64_t* idx,
+                             double* w, int64_t cap)
+{
+	ProjCtx<double> c(im, p);
+	int64_t k = 0;
+	c.visitEvent(lor, nullptr, p->tof_fwhm_ps > 0 ? &tof : nullptr, nullptr,
+	             true,
+	             [&](int64_t o, double ww)
+	             {
+		             if (k < cap)
+		             {
+			             idx[k] = o;
+			             w[k] = ww;
+		             }
+		             k++;
+	             });
+	return k;
+}
+
 // One EM subset pass in the order of OSEM_CPU::computeEMUpdateImage
 // (OSEM_CPU.cpp:329-374), per event: u = A x; u *= sens; u *= att;
 // u *= global; u += additive; if |u| > thr: u = m/u * sens * att * global and

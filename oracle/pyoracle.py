@@ -312,6 +312,18 @@ def siddon_trace(ip: ImageParams, pr: Proj, lor, tof=0.0, cap=1 << 16):
     return idx[:k], w[:k]
 
 
+def siddon_trace_f64(ip: ImageParams, pr: Proj, lor, tof=0.0, cap=1 << 16):
+    lib = oracle_lib()
+    lib.orc_siddon_trace_f64.restype = ctypes.c_int64
+    lor = _c(lor, np.float32)
+    idx = np.zeros(cap, np.int64)
+    w = np.zeros(cap, np.float64)
+    k = lib.orc_siddon_trace_f64(
+        ctypes.byref(ip.desc()), ctypes.byref(pr.desc()), _p(lor),
+        ctypes.c_float(tof), _p(idx), _p(w), ctypes.c_int64(cap))
+    return idx[:k], w[:k]
+
+
 def em_step_f64(ip: ImageParams, pr: Proj, lors, image, *, orients=None,
                 tof=None, frames=None, ray_offsets=None, measurement=None,
                 sens=None, att=None, additive=None, global_scale=1.0,

@@ -147,7 +147,7 @@ def test_autograd_batched_and_adjoint():
     gy = torch.from_numpy(rng.uniform(0, 1, (2, ev.count)).astype(np.float32)).cuda()
     (y * gy).sum().backward()
     for b in range(2):
-        lhs = float((y[b].double() * gy[b].double()).sum())
+        lhs = float((y[b].detach().double() * gy[b].double()).sum())
         rhs = float((xb[b].detach().double() * xb.grad[b].double()).sum())
         assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
     # torch.autograd.gradcheck-style check of linearity: A(a x) = a A(x).
@@ -172,13 +172,22 @@ def test_compensated_mode_error_vs_fp64():
         outs[prec] = p.forward(torch.from_numpy(img).cuda(), ev).cpu().numpy()
     lut = po.scanner_lut(po.Scanner(*C1))
     lors, _ = po.lors_from_detpairs(lut, e["d1"], e["d2"])
-    f64 = po.project(po.ImageParams(64, 64, 32, 256, 256, 128),
-                     po.Proj(tof_fwhm_ps=214.0, tof_n_std=5), lors, image=img,
-                     tof=e["tof"], precision="f64")
-    err_m = rel_l2(outs[L.YRTB_MIRROR], f64)
+    oip = po.ImageParams(64, 64, 32, 256, 256, 128)
+    pr = po.Proj(tof_fwhm_ps=214.0, tof_n_std=5)
+    f32 = po.project(oip, pr, lors, image=img, tof=e["tof"])
+    f64 = po.project(oip, pr, lors, image=img, tof=e["tof"], precision="f64")
+    # Mirror mode reproduces the reference's FP32 arithmetic (only the TOF
+    # exponential differs, <= 2 ulp) ...
+    assert rel_l2(outs[L.YRTB_MIRROR], f32) < 1e-6
+    # ... including its error on rays that run within float rounding of a
+    # voxel boundary (LORs between crystals on the x or y axis through the
+    # centre of this 4 mm grid), where FP32 puts the entry voxel on the other
+    # side of the plane: the reference's own error vs FP64 here is ~1e-3.
+    err_ref = rel_l2(f32, f64)
+    # Compensated mode takes the entry set-up in FP64 and meets the budget.
     err_c = rel_l2(outs[L.YRTB_COMPENSATED], f64)
-    assert err_m < 1e-5 and err_c < 1e-5
-    assert err_c <= err_m * 1.05
+    assert err_c < 1e-5
+    assert err_c < err_ref
 
 
 @pytest.mark.parametrize("tof,randoms", [(False, False), (True, False), (True, True)])

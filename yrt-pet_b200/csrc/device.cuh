@@ -300,10 +300,24 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 			continue;
 		if (first)
 		{
-			const float a_mid = 0.5f * (a_cur + a_next);
-			vx = static_cast<int>((p1.x + a_mid * (p2.x - p1.x) + g.lx / 2.0f) * inv_dx);
-			vy = static_cast<int>((p1.y + a_mid * (p2.y - p1.y) + g.ly / 2.0f) * inv_dy);
-			vz = static_cast<int>((p1.z + a_mid * (p2.z - p1.z) + g.lz / 2.0f) * inv_dz);
+			if constexpr (COMP)
+			{
+				// Entry voxel from the segment midpoint in FP64: a ray lying
+				// within float rounding of a voxel boundary (e.g. an LOR between
+				// opposite crystals on an axis) is placed on the side the exact
+				// geometry gives, not where the FP32 sum with l/2 rounds it.
+				const double am = 0.5 * (static_cast<double>(a_cur) + static_cast<double>(a_next));
+				vx = static_cast<int>((double(p1.x) + am * (double(p2.x) - double(p1.x)) + 0.5 * double(g.lx)) / double(dx));
+				vy = static_cast<int>((double(p1.y) + am * (double(p2.y) - double(p1.y)) + 0.5 * double(g.ly)) / double(dy));
+				vz = static_cast<int>((double(p1.z) + am * (double(p2.z) - double(p1.z)) + 0.5 * double(g.lz)) / double(dz));
+			}
+			else
+			{
+				const float a_mid = 0.5f * (a_cur + a_next);
+				vx = static_cast<int>((p1.x + a_mid * (p2.x - p1.x) + g.lx / 2.0f) * inv_dx);
+				vy = static_cast<int>((p1.y + a_mid * (p2.y - p1.y) + g.ly / 2.0f) * inv_dy);
+				vz = static_cast<int>((p1.z + a_mid * (p2.z - p1.z) + g.lz / 2.0f) * inv_dz);
+			}
 			off = vz * nxy + vy * nx;
 			first = false;
 		}
