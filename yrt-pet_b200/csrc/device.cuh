@@ -149,29 +149,27 @@ __device__ __forceinline__ void slabAlpha(R r0, R r1, R p1, R p2, R inv,
 // ------------------------------------------------------------ Siddon ----
 // Walks one ray through the image grid and calls visit(offset, weight) for
 // each voxel crossing, in order.  p1, p2: endpoints relative to the image
-// centre.  COMP selects the FP64 entry/exit setup.
+// centre.  COMP places the entry voxel with FP64 arithmetic (see below); the
+// parametric set-up and the walk are FP32 in both modes.
 template <bool TOF, bool COMP, typename Visit>
 __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
                                            const float3 p2, const TofP& tp,
                                            float tofValue, Visit& visit)
 {
-	using R = typename std::conditional<COMP, double, float>::type;
 	// 1. Clip to the FOV cylinder.
 	float t0, t1;
 	{
-		const R dxr = R(p2.x) - R(p1.x), dyr = R(p2.y) - R(p1.y);
-		const R A = dxr * dxr + dyr * dyr;
-		const R B = R(2) * (dxr * R(p1.x) + dyr * R(p1.y));
-		const R C = R(p1.x) * R(p1.x) + R(p1.y) * R(p1.y) -
-		            R(g.fovRadius) * R(g.fovRadius);
-		const R Delta = B * B - R(4) * A * C;
-		if (A != R(0))
+		const float A = (p2.x - p1.x) * (p2.x - p1.x) + (p2.y - p1.y) * (p2.y - p1.y);
+		const float B = 2.0f * ((p2.x - p1.x) * p1.x + (p2.y - p1.y) * p1.y);
+		const float C = p1.x * p1.x + p1.y * p1.y - g.fovRadius * g.fovRadius;
+		const float Delta = B * B - 4.0f * A * C;
+		if (A != 0.0f)
 		{
-			if (Delta <= R(0))
+			if (Delta <= 0.0f)
 				return;
-			const R sq = sqrt(Delta);
-			t0 = static_cast<float>((-B - sq) / (R(2) * A));
-			t1 = static_cast<float>((-B + sq) / (R(2) * A));
+			const float sq = sqrtf(Delta);
+			t0 = (-B - sq) / (2.0f * A);
+			t1 = (-B + sq) / (2.0f * A);
 		}
 		else
 		{
@@ -200,21 +198,13 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	float amin, amax;
 	float ax_min, ay_min, az_min;
 	{
-		R axmin, axmax, aymin, aymax, azmin, azmax;
-		const R ix = COMP ? (flat_x ? R(0) : R(1) / (R(p2.x) - R(p1.x))) : R(inv_x);
-		const R iy = COMP ? (flat_y ? R(0) : R(1) / (R(p2.y) - R(p1.y))) : R(inv_y);
-		const R iz = COMP ? (flat_z ? R(0) : R(1) / (R(p2.z) - R(p1.z))) : R(inv_z);
-		slabAlpha<R>(R(-0.5f * g.lx), R(0.5f * g.lx), R(p1.x), R(p2.x), ix, axmin, axmax);
-		slabAlpha<R>(R(-0.5f * g.ly), R(0.5f * g.ly), R(p1.y), R(p2.y), iy, aymin, aymax);
-		slabAlpha<R>(R(-0.5f * g.lz), R(0.5f * g.lz), R(p1.z), R(p2.z), iz, azmin, azmax);
-		ax_min = static_cast<float>(axmin);
-		ay_min = static_cast<float>(aymin);
-		az_min = static_cast<float>(azmin);
+		float ax_max, ay_max, az_max;
+		slabAlpha<float>(-0.5f * g.lx, 0.5f * g.lx, p1.x, p2.x, inv_x, ax_min, ax_max);
+		slabAlpha<float>(-0.5f * g.ly, 0.5f * g.ly, p1.y, p2.y, inv_y, ay_min, ay_max);
+		slabAlpha<float>(-0.5f * g.lz, 0.5f * g.lz, p1.z, p2.z, inv_z, az_min, az_max);
 		// max/min over {0|1, t, ax, ay, az} in the reference's order.
 		amin = fmaxf(fmaxf(fmaxf(fmaxf(0.0f, t0), ax_min), ay_min), az_min);
-		amax = fminf(fminf(fminf(fminf(1.0f, t1), static_cast<float>(axmax)),
-		                   static_cast<float>(aymax)),
-		             static_cast<float>(azmax));
+		amax = fminf(fminf(fminf(fminf(1.0f, t1), ax_max), ay_max), az_max);
 	}
 	if constexpr (TOF)
 	{
@@ -260,12 +250,11 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		az_next = (z_cur - p1.z) * inv_z;
 	}
 
-	bool first = true;
-	int vx = -1, vy = -1, vz = -1;
+	int vx, vy, vz;
 	int dir_prev = 0;
 	const int nx = g.nx, ny = g.ny, nz = g.nz;
 	const int nxy = nx * ny;
-	int off = 0;
+	int off;
 	const float fdx = static_cast<float>(dir_x) * dx;
 	const float fdy = static_cast<float>(dir_y) * dy;
 	const float fdz = static_cast<float>(dir_z) * dz;
@@ -277,7 +266,7 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	// branchy formulation computes.  A ray crosses at most nx+ny+nz+3 planes
 	// inside the grid; the step cap only guards against non-finite input.
 	const int maxSteps = 2 * (nx + ny + nz) + 16;
-	for (int step = 0; a_cur < amax && step < maxSteps; step++)
+	auto advance = [&]() -> int
 	{
 		const float ax = ax_next, ay = ay_next, az = az_next;
 		const bool sx = (ax <= ay) && (ax <= az);
@@ -294,49 +283,69 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		ax_next = sx ? axn : ax_next;
 		ay_next = sy ? ayn : ay_next;
 		az_next = sz ? azn : az_next;
-		const int dir_next = (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
 		a_next = (a_next > amax) ? amax : a_next;
-		if (a_cur >= a_next)
-			continue;
-		if (first)
-		{
-			if constexpr (COMP)
-			{
-				// Entry voxel from the segment midpoint in FP64: a ray lying
-				// within float rounding of a voxel boundary (e.g. an LOR between
-				// opposite crystals on an axis) is placed on the side the exact
-				// geometry gives, not where the FP32 sum with l/2 rounds it.
-				const double am = 0.5 * (static_cast<double>(a_cur) + static_cast<double>(a_next));
-				vx = static_cast<int>((double(p1.x) + am * (double(p2.x) - double(p1.x)) + 0.5 * double(g.lx)) / double(dx));
-				vy = static_cast<int>((double(p1.y) + am * (double(p2.y) - double(p1.y)) + 0.5 * double(g.ly)) / double(dy));
-				vz = static_cast<int>((double(p1.z) + am * (double(p2.z) - double(p1.z)) + 0.5 * double(g.lz)) / double(dz));
-			}
-			else
-			{
-				const float a_mid = 0.5f * (a_cur + a_next);
-				vx = static_cast<int>((p1.x + a_mid * (p2.x - p1.x) + g.lx / 2.0f) * inv_dx);
-				vy = static_cast<int>((p1.y + a_mid * (p2.y - p1.y) + g.ly / 2.0f) * inv_dy);
-				vz = static_cast<int>((p1.z + a_mid * (p2.z - p1.z) + g.lz / 2.0f) * inv_dz);
-			}
-			off = vz * nxy + vy * nx;
-			first = false;
-		}
-		else
-		{
-			const int mx = dir_prev & 1, my = (dir_prev >> 1) & 1, mz = (dir_prev >> 2) & 1;
-			vx += mx * dir_x;
-			vy += my * dir_y;
-			vz += mz * dir_z;
-			off += my * dir_y * nx + mz * dir_z * nxy;
-		}
-		if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
-			break;
-		dir_prev = dir_next;
+		return (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
+	};
+	auto emit = [&]()
+	{
 		float w = (a_next - a_cur) * d_norm;
 		if constexpr (TOF)
 			w *= tofWeight(tp, d_norm, tofValue, a_cur * d_norm, a_next * d_norm);
 		visit(vx + off, w);
 		a_cur = a_next;
+	};
+
+	// First non-empty segment: its voxel comes from the segment midpoint.
+	int step = 0;
+	int dir_next = 0;
+	for (;; step++)
+	{
+		if (!(a_cur < amax) || step >= maxSteps)
+			return;
+		dir_next = advance();
+		if (a_cur < a_next)
+			break;
+	}
+	step++;
+	if constexpr (COMP)
+	{
+		// Entry voxel in FP64: a ray lying within float rounding of a voxel
+		// boundary (e.g. an LOR between opposite crystals on an image axis)
+		// is placed on the side the exact geometry gives, not where the FP32
+		// sum with l/2 rounds it.
+		const double am = 0.5 * (static_cast<double>(a_cur) + static_cast<double>(a_next));
+		vx = static_cast<int>((double(p1.x) + am * (double(p2.x) - double(p1.x)) + 0.5 * double(g.lx)) / double(dx));
+		vy = static_cast<int>((double(p1.y) + am * (double(p2.y) - double(p1.y)) + 0.5 * double(g.ly)) / double(dy));
+		vz = static_cast<int>((double(p1.z) + am * (double(p2.z) - double(p1.z)) + 0.5 * double(g.lz)) / double(dz));
+	}
+	else
+	{
+		const float a_mid = 0.5f * (a_cur + a_next);
+		vx = static_cast<int>((p1.x + a_mid * (p2.x - p1.x) + g.lx / 2.0f) * inv_dx);
+		vy = static_cast<int>((p1.y + a_mid * (p2.y - p1.y) + g.ly / 2.0f) * inv_dy);
+		vz = static_cast<int>((p1.z + a_mid * (p2.z - p1.z) + g.lz / 2.0f) * inv_dz);
+	}
+	if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
+		return;
+	off = vz * nxy + vy * nx;
+	dir_prev = dir_next;
+	emit();
+
+	// Following segments: move the voxel along the axes stepped last time.
+	for (; a_cur < amax && step < maxSteps; step++)
+	{
+		dir_next = advance();
+		if (a_cur >= a_next)
+			continue;
+		const int mx = dir_prev & 1, my = (dir_prev >> 1) & 1, mz = (dir_prev >> 2) & 1;
+		vx += mx * dir_x;
+		vy += my * dir_y;
+		vz += mz * dir_z;
+		off += my * dir_y * nx + mz * dir_z * nxy;
+		if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
+			break;
+		dir_prev = dir_next;
+		emit();
 	}
 }
 

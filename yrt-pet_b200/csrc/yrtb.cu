@@ -433,8 +433,10 @@ enum Op
 	OP_COUNT = 3
 };
 
+// Siddon: 4 blocks of 256 threads per SM (64 registers per thread, 32
+// warps); the other projectors keep the compiler's register choice.
 template <int OP, int KIND, bool TOF, bool COMP>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, KIND == K_SIDDON ? 4 : 1)
     k_events(KParams P, Events E, Range R, const float* __restrict__ in,
              float* __restrict__ out, float globalScale, float denomThr,
              unsigned long long* err)
