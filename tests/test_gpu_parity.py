@@ -489,3 +489,30 @@ def test_event_ordering_is_subset_major_permutation():
     p.em_step(img, em_a, ev, rng=L.yrtb_range(3, 7, 0))
     p.em_step(img, em_b, out, rng=L.yrtb_range(int(offs[3]), 1, int(offs[4] - offs[3])))
     assert rel_l2(em_b.cpu().numpy(), em_a.cpu().numpy()) < 1e-5
+
+
+@pytest.mark.parametrize("support", ["cylinder", "offcentre", "empty"])
+def test_attenuation_factors_vs_oracle(support):
+    from pyyrtpet_b200 import synthetic as S
+    sc = S.scanner_c1()
+    ip = yrt.ImageParams(64, 64, 32, 256, 256, 128)
+    p = yrt.DeviceProjector(sc, ip, yrt.ProjectorParams(sc))
+    evs = S.generate_events(sc, 30000, 91)
+    e = evs.numpy()
+    mu = S.Phantom(cyl_half_length=32).mu_image(ip).numpy()
+    if support == "offcentre":
+        mu = np.zeros_like(mu)
+        mu[0, 3:9, 40:52, 10:20] = 0.15
+    elif support == "empty":
+        mu = np.zeros_like(mu)
+    ev = yrt.DeviceEvents.from_arrays(e["d1"], e["d2"])
+    acf = p.attenuation_factors(torch.from_numpy(mu).cuda().reshape(-1), ip, ev).cpu().numpy()
+    lut = po.scanner_lut(po.Scanner(*SC_ARGS))
+    lors, _ = po.lors_from_detpairs(lut, e["d1"], e["d2"])
+    line = po.project(po.ImageParams(64, 64, 32, 256, 256, 128), po.Proj(), lors,
+                      image=mu, precision="f64")
+    ref = np.exp(-0.1 * line)
+    if support == "empty":
+        assert np.all(acf == 1.0)
+    assert rel_l2(acf, ref) < 1e-6
+    assert np.max(np.abs(acf - ref) / ref) < 1e-5

@@ -105,14 +105,21 @@ __device__ __forceinline__ void tofAlphaRange(const TofP& t, float lorNorm,
 	amax = static_cast<float>(fmin(1.0, 0.5 + static_cast<double>((tof_mm + t.trunc) / lorNorm)));
 }
 
+// Centre of the TOF kernel in mm from p1: L/2 + c*t/2, with the reference's
+// float/double mix.
+__device__ __forceinline__ float tofCenter(float lorNorm, float tof_ps)
+{
+	const float tof_mm =
+	    static_cast<float>(static_cast<double>(tof_ps) * kSpeedOfLightMmPsFlt * 0.5);
+	return static_cast<float>(0.5 * static_cast<double>(lorNorm) +
+	                          static_cast<double>(tof_mm));
+}
+
 // Gaussian TOF weight evaluated at the centre of [lo, hi] (mm along the LOR).
 __device__ __forceinline__ float tofWeight(const TofP& t, float lorNorm,
                                            float tof_ps, float lo, float hi)
 {
-	const float tof_mm =
-	    static_cast<float>(static_cast<double>(tof_ps) * kSpeedOfLightMmPsFlt * 0.5);
-	const float pc = static_cast<float>(0.5 * static_cast<double>(lorNorm) +
-	                                    static_cast<double>(tof_mm));
+	const float pc = tofCenter(lorNorm, tof_ps);
 	const float xc = (0.5f * (lo + hi) - pc) / t.sigma;
 	return expf(-0.5f * xc * xc) * t.norm;
 }
@@ -154,7 +161,8 @@ __device__ __forceinline__ void slabAlpha(R r0, R r1, R p1, R p2, R inv,
 template <bool TOF, bool COMP, typename Visit>
 __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
                                            const float3 p2, const TofP& tp,
-                                           float tofValue, Visit& visit)
+                                           float tofValue, Visit& visit,
+                                           float wlo = 0.f, float whi = 1.f)
 {
 	// 1. Clip to the FOV cylinder.
 	float t0, t1;
@@ -213,6 +221,9 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		amin = fmaxf(amin, a0);
 		amax = fminf(amax, a1);
 	}
+	// Optional extra window [wlo, whi] (defaults leave amin, amax unchanged).
+	amin = fmaxf(amin, wlo);
+	amax = fminf(amax, whi);
 
 	float a_cur = amin;
 	float a_next = -1.0f;
@@ -286,11 +297,29 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		a_next = (a_next > amax) ? amax : a_next;
 		return (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
 	};
+	// TOF kernel centre along the LOR (mm from p1), loop invariant.
+	const float pc = TOF ? tofCenter(d_norm, tofValue) : 0.f;
+	const float inv_sigma = TOF ? 1.0f / tp.sigma : 0.f;
 	auto emit = [&]()
 	{
 		float w = (a_next - a_cur) * d_norm;
 		if constexpr (TOF)
-			w *= tofWeight(tp, d_norm, tofValue, a_cur * d_norm, a_next * d_norm);
+		{
+			if constexpr (COMP)
+			{
+				// Gaussian at the segment midpoint with a multiply by 1/sigma
+				// and the fast exponential (<= 2 + 1.2|x| ulp); the error of
+				// the projection stays far below the FP64 budget.
+				const float xc = (0.5f * (a_cur + a_next) * d_norm - pc) * inv_sigma;
+				w *= __expf(-0.5f * xc * xc) * tp.norm;
+			}
+			else
+			{
+				const float lo = a_cur * d_norm, hi = a_next * d_norm;
+				const float xc = (0.5f * (lo + hi) - pc) / tp.sigma;
+				w *= expf(-0.5f * xc * xc) * tp.norm;
+			}
+		}
 		visit(vx + off, w);
 		a_cur = a_next;
 	};
@@ -342,10 +371,45 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		vy += my * dir_y;
 		vz += mz * dir_z;
 		off += my * dir_y * nx + mz * dir_z * nxy;
-		if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
+		if (static_cast<unsigned>(vx) >= static_cast<unsigned>(nx) ||
+		    static_cast<unsigned>(vy) >= static_cast<unsigned>(ny) ||
+		    static_cast<unsigned>(vz) >= static_cast<unsigned>(nz))
 			break;
 		dir_prev = dir_next;
 		emit();
+	}
+}
+
+// Parametric window of the ray p1 -> p2 inside the box of voxels
+// [b[0], b[3]] x [b[1], b[4]] x [b[2], b[5]] (inclusive) of grid g; an empty
+// box or a miss gives wlo > whi.
+__device__ __forceinline__ void boxWindow(const Geom& g, const int* b,
+                                          float3 p1, float3 p2, float& wlo,
+                                          float& whi)
+{
+	wlo = 0.f;
+	whi = 1.f;
+	if (b[3] < b[0])
+	{
+		wlo = 1.f;
+		whi = 0.f;
+		return;
+	}
+	const float lo[3] = {-0.5f * g.lx + b[0] * g.vx, -0.5f * g.ly + b[1] * g.vy,
+	                     -0.5f * g.lz + b[2] * g.vz};
+	const float hi[3] = {-0.5f * g.lx + (b[3] + 1) * g.vx,
+	                     -0.5f * g.ly + (b[4] + 1) * g.vy,
+	                     -0.5f * g.lz + (b[5] + 1) * g.vz};
+	const float a[3] = {p1.x, p1.y, p1.z};
+	const float c[3] = {p2.x, p2.y, p2.z};
+#pragma unroll
+	for (int k = 0; k < 3; k++)
+	{
+		float amn, amx;
+		const float inv = (a[k] == c[k]) ? 0.f : 1.0f / (c[k] - a[k]);
+		slabAlpha<float>(lo[k], hi[k], a[k], c[k], inv, amn, amx);
+		wlo = fmaxf(wlo, amn);
+		whi = fminf(whi, amx);
 	}
 }
 

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -507,11 +508,54 @@ __global__ void __launch_bounds__(kBlock, KIND == K_SIDDON ? 4 : 1)
 	}
 }
 
+__global__ void k_box_init(int* box)
+{
+	if (threadIdx.x < 6)
+		box[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : -1;
+}
+
+// Bounding box (voxel indices, inclusive) of the non-zero voxels of an image:
+// box = {min x, min y, min z, max x, max y, max z}; initialised to an empty
+// box by the caller.
+__global__ void k_support_box(const float* __restrict__ img, Geom g, int* box)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {-1, -1, -1};
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < static_cast<uint64_t>(g.nvox); i += nthreads)
+	{
+		if (__ldg(img + i) != 0.f)
+		{
+			const int x = static_cast<int>(i % g.nx);
+			const int y = static_cast<int>((i / g.nx) % g.ny);
+			const int z = static_cast<int>(i / g.nxy);
+			mn[0] = min(mn[0], x); mn[1] = min(mn[1], y); mn[2] = min(mn[2], z);
+			mx[0] = max(mx[0], x); mx[1] = max(mx[1], y); mx[2] = max(mx[2], z);
+		}
+	}
+	for (int k = 0; k < 3; k++)
+	{
+		for (int o = 16; o > 0; o >>= 1)
+		{
+			mn[k] = min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+			mx[k] = max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+		}
+	}
+	if ((threadIdx.x & 31) == 0 && mx[0] >= 0)
+	{
+		for (int k = 0; k < 3; k++)
+		{
+			atomicMin(box + k, mn[k]);
+			atomicMax(box + 3 + k, mx[k]);
+		}
+	}
+}
+
 // Attenuation factor per event: exp(-0.1 * line integral of mu).
 __global__ void __launch_bounds__(kBlock)
     k_attenuation(KParams P, Geom mu, Events E, Range R,
-                  const float* __restrict__ muImg, float* __restrict__ out,
-                  unsigned long long* err)
+                  const float* __restrict__ muImg, const int* __restrict__ box,
+                  float* __restrict__ out, unsigned long long* err)
 {
 	// One item per thread: a warp's threads stay converged across items
 	// (a grid-stride loop lets them drift apart between items).
@@ -532,9 +576,14 @@ __global__ void __launch_bounds__(kBlock)
 		                               P.g.offz - mu.offz);
 		p1 = make_float3(p1.x + fix.x, p1.y + fix.y, p1.z + fix.z);
 		p2 = make_float3(p2.x + fix.x, p2.y + fix.y, p2.z + fix.z);
+		// Only voxels of the mu-map's non-zero bounding box contribute, so
+		// the walk is limited to the ray's window inside that box.
+		float wlo, whi;
+		boxWindow(mu, box, p1, p2, wlo, whi);
 		float acc = 0.f;
 		auto visit = [&](int o, float w) { acc += w * __ldg(muImg + o); };
-		siddonWalk<false, false>(mu, p1, p2, P.tof, 0.f, visit);
+		if (wlo < whi)
+			siddonWalk<false, false>(mu, p1, p2, P.tof, 0.f, visit, wlo, whi);
 		out[e] = expf(-acc * 0.1f);
 	}
 }
@@ -1476,11 +1525,17 @@ yrtb_status yrtb_attenuation_factors(yrtb_projector* h, const float* d_mu,
 	if (range.count == 0)
 		return YRTB_OK;
 	YRTB_CUDA(cudaSetDevice(h->device));
-	k_attenuation<<<gridAll(range.count), kBlock, 0,
-	                reinterpret_cast<cudaStream_t>(stream)>>>(
-	    h->P, makeGeom(*mu_params), toDev(ev),
-	    Range{range.start, range.stride, range.count}, d_mu, d_out, h->d_err);
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	const Geom mg = makeGeom(*mu_params);
+	int* d_box = nullptr;
+	YRTB_CUDA(cudaMallocAsync(&d_box, 6 * sizeof(int), st));
+	k_box_init<<<1, 32, 0, st>>>(d_box);
+	k_support_box<<<gridFor(mg.nvox, 4), kBlock, 0, st>>>(d_mu, mg, d_box);
+	k_attenuation<<<gridAll(range.count), kBlock, 0, st>>>(
+	    h->P, mg, toDev(ev), Range{range.start, range.stride, range.count},
+	    d_mu, d_box, d_out, h->d_err);
 	YRTB_LAUNCHED();
+	YRTB_CUDA(cudaFreeAsync(d_box, st));
 	return YRTB_OK;
 }
 
