@@ -683,11 +683,14 @@ __global__ void __launch_bounds__(kBlock)
 	}
 }
 
-// Sort key of event e: subset (e mod S) in bits 48..63, LOR (Histogram3D
-// bin, or the ordered detector pair) in bits 8..47, TOF in 16 ps steps in
-// bits 0..7.
+// Sort key of event e: subset (e mod S) in bits 48..63, the ray's number of
+// voxel crossings in steps of 8 (when counts are given) in bits 43..47, LOR
+// (Histogram3D bin, or the ordered detector pair) in bits 8..42, TOF in 16 ps
+// steps in bits 0..7.  Grouping rays of similar length keeps the threads of
+// a warp iterating together; the LOR key keeps neighbouring rays together.
 __global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
-                             uint64_t numSubsets, unsigned long long* __restrict__ keys,
+                             uint64_t numSubsets, const uint32_t* __restrict__ counts,
+                             unsigned long long* __restrict__ keys,
                              unsigned long long* __restrict__ vals)
 {
 	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -710,7 +713,9 @@ __global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
 			const float t = __ldg(E.tof + e) / 16.0f + 128.0f;
 			q = t <= 0.f ? 0 : (t >= 255.f ? 255 : static_cast<uint64_t>(t));
 		}
-		keys[e] = ((e % numSubsets) << 48) | ((lorKey & 0xFFFFFFFFFFULL) << 8) | q;
+		const uint64_t bucket = counts ? min(__ldg(counts + e) / 8u, 31u) : 0u;
+		keys[e] = ((e % numSubsets) << 48) | (bucket << 43) |
+		          ((lorKey & 0x7FFFFFFFFULL) << 8) | q;
 		vals[e] = e;
 	}
 }
@@ -1408,8 +1413,23 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
 		release();
 		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
 	}
-	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(h->h3d, h->h3 != nullptr,
-	                                                toDev(ev), n, S, keys, vals);
+	// Crossing counts of the single-ray Siddon projector (into keys2, which
+	// the sort overwrites afterwards).
+	const uint32_t* counts = nullptr;
+	if (h->kind == K_SIDDON && (!h->hasTof || ev->tof_ps))
+	{
+		const yrtb_status cs = dispatchEvents<OP_COUNT>(
+		    h, ev, yrtb_range{0, 1, n}, nullptr, reinterpret_cast<float*>(keys2),
+		    1.f, 0.f, stream);
+		if (cs != YRTB_OK)
+		{
+			release();
+			return cs;
+		}
+		counts = reinterpret_cast<const uint32_t*>(keys2);
+	}
+	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(
+	    h->h3d, h->h3 != nullptr, toDev(ev), n, S, counts, keys, vals);
 	ce = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals,
 	                                     reinterpret_cast<unsigned long long*>(d_perm),
 	                                     n, 0, 64, st);
