@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--precision", default="compensated",
                     choices=["mirror", "compensated"])
     ap.add_argument("--parity-sample", type=int, default=200_000)
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2 (default) is the headline workload; the others "
+                         "run bench_configs.py")
+    ap.add_argument("--cfg-events", type=int, default=0,
+                    help="override the event count of --config c1/c3/c4/c5")
     return ap.parse_args()
 
 
@@ -223,6 +228,11 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.config != "c2":
+        import bench_configs
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps(bench_configs.RUNNERS[args.config](args)), flush=True)
         return
     import ctypes
     import pyyrtpet_b200 as yrt

@@ -1,0 +1,403 @@
+"""Per-configuration benchmark runs behind `bench.py --config c1|c3|c4|c5`.
+
+The default `bench.py` line is the C2 workload (50M TOF events).  These runs
+measure the other four configurations of the projection path on one GPU,
+each printing one JSON line:
+
+  c1  list-mode OSEM, Siddon without TOF, 16 rings x 256 crystals, 128x128x64
+      image, 1M events: sensitivity image (8.32M-bin uniform histogram) and
+      2 iterations x 5 subsets; reference CPU OSEM on the same events and the
+      image difference.
+  c3  list-mode -> Histogram3D binning of 200M events (bit-exact check on a
+      sample against the reference), then histogram-mode OSEM with the
+      distance-driven projector and a 4 mm FWHM projection-space PSF,
+      200x200x100 image at 2.5 mm, 3 iterations x 12 subsets.
+  c4  differentiable TOF Siddon: Poisson log-likelihood and its gradient for
+      8 phantoms x 5M TOF events (forward + adjoint per phantom).
+  c5  24 dynamic frames with per-frame rigid motion on the C2 scanner and
+      image (1.0 GB 4D image), frame sizes log-uniform in [2e5, 2e7]:
+      batched form (all frames in one EM launch per subset, CUDA-graph
+      subsets) against the plain form (one single-frame reconstruction per
+      frame).
+
+Inputs are seeded synthetic events (SURVEY: no datasets are available); the
+reference CPU measurements use oracle/_ref, the reference library built from
+its sources, where present.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import sys
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def _yrt():
+    sys.path.insert(0, os.path.join(ROOT, "yrt-pet_b200"))
+    import pyyrtpet_b200 as yrt
+    from pyyrtpet_b200 import _lib as L
+    from pyyrtpet_b200 import synthetic as S
+    from pyyrtpet_b200.core import _stream
+    return yrt, L, S, _stream
+
+
+def _po():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    return po
+
+
+class Timer:
+    """CUDA-event timer on the current stream."""
+
+    def __enter__(self):
+        torch.cuda.synchronize()
+        self.a = torch.cuda.Event(enable_timing=True)
+        self.b = torch.cuda.Event(enable_timing=True)
+        self.a.record()
+        return self
+
+    def __exit__(self, *exc):
+        self.b.record()
+        torch.cuda.synchronize()
+        self.ms = self.a.elapsed_time(self.b)
+        return False
+
+
+def _po_scanner(po, sc):
+    return po.Scanner(sc.axialFOV, sc.crystalSize_z, sc.crystalSize_trans,
+                      sc.crystalDepth, sc.scannerRadius, sc.detsPerRing,
+                      sc.numRings, sc.numDOI, sc.maxRingDiff, sc.minAngDiff,
+                      sc.detsPerBlock)
+
+
+def _po_image(po, ip, nt=1):
+    return po.ImageParams(ip.nx, ip.ny, ip.nz, ip.length_x, ip.length_y,
+                          ip.length_z, nt=nt)
+
+
+def _rel_l2(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _base(cfg, metric, value, unit, steps, warmup, ms, config):
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": 1,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded phantom events)",
+            "config": dict(workload=cfg, **config)}
+
+
+# ------------------------------------------------------------------- C1 ----
+def run_c1(args):
+    """List-mode OSEM, Siddon without TOF, C1 scanner/image, 1M events."""
+    yrt, L, S, _stream = _yrt()
+    sc = S.scanner_c1()
+    ip = S.image_c1()
+    ev = S.generate_events(sc, 1_000_000, 20261203 + 0, device="cuda",
+                           chunk=1 << 24)
+    e = {"d1": ev.d1.cpu().numpy().astype(np.uint32),
+         "d2": ev.d2.cpu().numpy().astype(np.uint32)}
+    osem = yrt.createOSEM(sc)
+    osem.setImageParams(ip)
+    osem.num_MLEM_iterations = 2
+    osem.num_OSEM_subsets = 5
+    osem.setListModeEnabled(True)
+    for _ in range(args.warmup):
+        osem.generateSensitivityImages()
+    with Timer() as ts:
+        sens = osem.generateSensitivityImages()
+    lm = yrt.ListModeLUT(sc)
+    lm.bind(e["d1"], e["d2"])
+    osem.setDataInput(lm)
+    for _ in range(args.warmup):
+        osem.reconstruct()
+    times = []
+    img = None
+    for _ in range(args.steps):
+        with Timer() as t:
+            img = osem.reconstruct()
+        times.append(t.ms)
+    ms = float(np.median(times))
+    out = _base("C1 list-mode OSEM 2x5, Siddon, no TOF, 16x256 scanner, "
+                "128x128x64 @2mm, 1M events",
+                "events/s (list-mode OSEM, Siddon, events x iterations / time)",
+                1e6 * 2 / (ms * 1e-3), "events/s", args.steps, args.warmup, ms,
+                {"events": 1_000_000, "iterations": 2, "subsets": 5})
+    out["sens_image_ms"] = ts.ms
+    out["sens_bins"] = int(yrt.Histogram3D(sc).count())
+    po = _po()
+    if po.ref_available() and not args.no_cpu_baseline:
+        osc = _po_scanner(po, sc)
+        oip = _po_image(po, ip)
+        rs, rsec = po.ref_sensitivity(osc, oip, listmode=True,
+                                      threads=os.cpu_count() or 1)
+        rimg, rosec = po.ref_osem_listmode(osc, oip, rs[0], e["d1"], e["d2"],
+                                           iterations=2, subsets=5,
+                                           threads=os.cpu_count() or 1)
+        out["cpu_baseline"] = {
+            "value": 1e6 * 2 / rosec, "unit": "events/s",
+            "cores": os.cpu_count(), "kind": "reference",
+            "sample": "the full workload (1M events, 2 x 5)",
+            "sens_image_s": rsec, "osem_s": rosec}
+        out["parity_vs_reference"] = {
+            "sens_rel_l2": _rel_l2(sens[0].cpu().numpy(), rs[0]),
+            "image_rel_l2": _rel_l2(img.cpu().numpy(), rimg)}
+    return out
+
+
+# ------------------------------------------------------------------- C5 ----
+def run_c5(args):
+    """24 dynamic frames with rigid motion: batched vs plain single-frame."""
+    yrt, L, S, _stream = _yrt()
+    sc = S.scanner_c2()
+    ip1 = S.image_c2()
+    nt = 24
+    subsets = 10
+    counts = S.frame_counts_loguniform(nt, 2e5, 2e7, 20261203 + 4)
+    if args.cfg_events:
+        counts = np.maximum(1, np.round(counts * (args.cfg_events / counts.sum()))).astype(np.int64)
+    n = int(counts.sum())
+    ev = S.generate_events(sc, n, 20261203 + 4, tof_fwhm_ps=214.0, device="cuda",
+                           chunk=1 << 24)
+    frames = torch.repeat_interleave(torch.arange(nt, device="cuda", dtype=torch.int32),
+                                     torch.from_numpy(counts).cuda())
+    motion = S.rigid_transforms(nt, 20261203 + 5)
+    ipT = ip1.withFrames(nt)
+    pp = yrt.ProjectorParams(sc)
+    pp.addTOF(214.0, 5)
+    pp.precision = L.YRTB_COMPENSATED
+    proj = yrt.DeviceProjector(sc, ipT, pp)
+    d1 = ev.d1.to(torch.int32)
+    d2 = ev.d2.to(torch.int32)
+    base = yrt.DeviceEvents.from_arrays(d1, d2, tof=ev.tof, frame=frames,
+                                        motion_frame=frames, motion=motion)
+    J = ip1.numVoxels
+    sens_proj = yrt.DeviceProjector(sc, ip1, yrt.ProjectorParams(sc))
+    sens = torch.zeros(J, device="cuda")
+    sens_proj.sensitivity_histo3d(sens, 20, 0)
+    sens.mul_(20.0)
+    s_ptr = _stream()
+    lib = L.lib()
+
+    # Batched: one event set for all frames, subset-major / frame ordering,
+    # one CUDA graph per subset replayed by yrtb_osem_listmode.
+    ordered, offs = proj.order_events(base, subsets)
+    evc = ordered.c()
+    img = torch.empty(nt * J, device="cuda")
+    work = torch.empty((nt + 1) * J, device="cuda")
+    stream = torch.cuda.Stream()
+
+    def batched(iters):
+        p = L.yrtb_osem_params(iters, subsets, 1.0, 1e-35, 1.19209e-07, 0, 1,
+                               None, offs.ctypes.data)
+        with torch.cuda.stream(stream):
+            L.check(lib.yrtb_osem_listmode(proj.h, ctypes.byref(evc),
+                                           sens.data_ptr(), img.data_ptr(),
+                                           work.data_ptr(), ctypes.byref(p),
+                                           _stream()))
+        torch.cuda.current_stream().wait_stream(stream)
+
+    # Plain: one single-frame reconstruction per frame (events in file order,
+    # interleaved subsets), as a frame-by-frame reference workflow runs it.
+    proj1 = yrt.DeviceProjector(sc, ip1, pp)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    per_frame = []
+    for f in range(nt):
+        a, b = int(starts[f]), int(starts[f + 1])
+        per_frame.append(yrt.DeviceEvents.from_arrays(
+            d1[a:b], d2[a:b], tof=ev.tof[a:b],
+            motion_frame=torch.full((b - a,), f, dtype=torch.int32, device="cuda"),
+            motion=motion))
+    img1 = torch.empty(J, device="cuda")
+    work1 = torch.empty(2 * J, device="cuda")
+
+    def plain(iters):
+        p = L.yrtb_osem_params(iters, subsets, 1.0, 1e-35, 1.19209e-07, 0, 0,
+                               None, None)
+        for f in range(nt):
+            L.check(lib.yrtb_osem_listmode(proj1.h, ctypes.byref(per_frame[f].c()),
+                                           sens.data_ptr(), img1.data_ptr(),
+                                           work1.data_ptr(), ctypes.byref(p),
+                                           s_ptr))
+
+    for _ in range(max(1, args.warmup)):
+        batched(1)
+        plain(1)
+    bt, pt = [], []
+    for _ in range(args.steps):
+        with Timer() as t:
+            batched(1)
+        bt.append(t.ms)
+        with Timer() as t:
+            plain(1)
+        pt.append(t.ms)
+    ms_b = float(np.median(bt))
+    ms_p = float(np.median(pt))
+    out = _base("C5 dynamic + motion list-mode TOF OSEM, 24 frames (log-uniform "
+                "2e5-2e7 events), C2 scanner/image, 10 subsets",
+                "events/s (one OSEM iteration over all frames, batched)",
+                n / (ms_b * 1e-3), "events/s", args.steps, args.warmup, ms_b,
+                {"events": n, "frames": nt, "subsets": subsets,
+                 "precision": "compensated"})
+    out["plain"] = {"value": n / (ms_p * 1e-3), "ms_per_step": ms_p,
+                    "what": "24 separate single-frame reconstructions (one per "
+                            "frame, file order, interleaved subsets)"}
+    out["batched_over_plain"] = ms_p / ms_b
+    out["frame_events"] = [int(c) for c in counts]
+    return out
+
+
+def _gaussian_psf(fwhm=4.0, ks=0.5):
+    sig = fwhm / 2.3548
+    half = int(np.ceil(3 * sig / ks))
+    x = (np.arange(2 * half + 1) - half) * ks
+    k = np.exp(-0.5 * (x / sig) ** 2)
+    k /= k.sum() * ks
+    return 1e9, ks, k[None].astype(np.float32)
+
+
+# ------------------------------------------------------------------- C3 ----
+def run_c3(args):
+    """200M events -> Histogram3D; DD + projection PSF histogram OSEM."""
+    import tempfile
+    yrt, L, S, _stream = _yrt()
+    sc = S.scanner_c1(15)
+    ip = S.image_c3()
+    total = args.cfg_events or 200_000_000
+    chunk = 20_000_000
+    h = yrt.Histogram3D(sc)
+    hist = torch.zeros(h.histoSize, dtype=torch.float32, device="cuda")
+    p0 = yrt.core._scratch_projector(sc)
+    bin_ms = 0.0
+    sample = None
+    done = 0
+    seed = 20261203 + 3
+    while done < total:
+        m = min(chunk, total - done)
+        ev = S.generate_events(sc, m, seed + done, device="cuda", chunk=1 << 24)
+        a = ev.d1.to(torch.int32).contiguous()
+        b = ev.d2.to(torch.int32).contiguous()
+        if sample is None:
+            sample = (a[:2_000_000].cpu().numpy().view(np.uint32),
+                      b[:2_000_000].cpu().numpy().view(np.uint32))
+        bad = ctypes.c_uint64()
+        with Timer() as t:
+            L.check(L.lib().yrtb_listmode_to_histo3d(
+                p0.h, a.data_ptr(), b.data_ptr(), None, m, hist.data_ptr(),
+                ctypes.byref(bad), _stream()))
+        bin_ms += t.ms
+        done += m
+        del ev, a, b
+    h.data = hist.cpu().numpy()
+    s_step, ks, taps = _gaussian_psf()
+    csv = os.path.join(tempfile.mkdtemp(), "psf.csv")
+    yrt.write_psf_csv(csv, s_step, ks, taps)
+    osem = yrt.createOSEM(sc)
+    osem.setImageParams(ip)
+    osem.num_MLEM_iterations = 3
+    osem.num_OSEM_subsets = 12
+    osem.setProjector("DD")
+    osem.addProjPSF(csv)
+    osem.setDataInput(h)
+    with Timer() as ts:
+        sens = osem.generateSensitivityImages()
+    osem.num_MLEM_iterations = 1
+    for _ in range(args.warmup):
+        osem.reconstruct()
+    times = []
+    for _ in range(args.steps):
+        with Timer() as t:
+            img = osem.reconstruct()
+        times.append(t.ms)
+    ms = float(np.median(times))
+    nz = int((hist > 0).sum().item())
+    out = _base("C3 histogram OSEM, distance-driven + projection PSF (4 mm FWHM), "
+                "C1 scanner mrd 15 (8.32M bins) from 200M events, 200x200x100 "
+                "@2.5mm, 12 subsets",
+                "histogram bins/s (DD+PSF OSEM iteration over all bins)",
+                h.count() / (ms * 1e-3), "bins/s", args.steps, args.warmup, ms,
+                {"events_binned": total, "bins": h.count(), "nonzero_bins": nz,
+                 "subsets": 12})
+    out["binning"] = {"events_per_s": total / (bin_ms * 1e-3), "ms": bin_ms}
+    out["sens_images_ms"] = ts.ms
+    out["osem_s_per_iteration"] = ms * 1e-3
+    po = _po()
+    if po.ref_available() and not args.no_cpu_baseline:
+        osc = _po_scanner(po, sc)
+        ours = yrt.ListModeLUT(sc)
+        ours.bind(*sample)
+        mine = yrt.convertToHistogram3D(ours).data
+        ref_h, ref_s = po.ref_lm_to_histo3d(osc, *sample, threads=os.cpu_count() or 1)
+        out["binning"]["bitexact_vs_reference_2M_sample"] = bool(
+            np.array_equal(mine.view(np.uint32), ref_h.view(np.uint32)))
+        out["binning"]["reference_events_per_s"] = len(sample[0]) / ref_s
+        oip = _po_image(po, ip)
+        rimg, rsec = po.ref_osem_histo3d(osc, oip,
+                                         np.stack([x.cpu().numpy() for x in sens]),
+                                         h.data, psf_csv=csv, projector="DD",
+                                         iterations=1, subsets=12,
+                                         threads=os.cpu_count() or 1)
+        out["cpu_baseline"] = {"value": h.count() / rsec, "unit": "bins/s",
+                               "cores": os.cpu_count(), "kind": "reference",
+                               "sample": "1 OSEM iteration x 12 subsets of the "
+                                         "same histogram"}
+        out["parity_vs_reference"] = {"image_rel_l2_1_iteration": _rel_l2(
+            img.cpu().numpy(), rimg)}
+    return out
+
+
+# ------------------------------------------------------------------- C4 ----
+def run_c4(args):
+    """Poisson NLL + gradient through the autograd projector, 8 phantoms."""
+    yrt, L, S, _stream = _yrt()
+    from pyyrtpet_b200.autograd import poisson_nll
+    sc = S.scanner_c1()
+    ip = S.image_c1()
+    pp = yrt.ProjectorParams(sc)
+    pp.addTOF(214.0, 5)
+    pp.precision = L.YRTB_COMPENSATED
+    proj = yrt.DeviceProjector(sc, ip, pp)
+    per = (args.cfg_events or 40_000_000) // 8
+    evs, imgs = [], []
+    for b in range(8):
+        ph = S.random_phantom(20261203 + 40 + b, sc.axialFOV / 2)
+        e = S.generate_events(sc, per, 20261203 + 40 + b, phantom=ph,
+                              tof_fwhm_ps=214.0, device="cuda", chunk=1 << 24)
+        evs.append(yrt.DeviceEvents.from_arrays(e.d1.to(torch.int32),
+                                                e.d2.to(torch.int32), tof=e.tof))
+        imgs.append(ph.image(ip, device="cuda") + 0.1)
+    x = torch.stack(imgs).contiguous().requires_grad_(True)
+    sens = torch.ones(ip.shape, device="cuda")
+
+    def step():
+        x.grad = None
+        loss = poisson_nll(x, proj, evs, sens).sum()
+        loss.backward()
+        return loss
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        with Timer() as t:
+            step()
+        times.append(t.ms)
+    ms = float(np.median(times))
+    return _base("C4 differentiable TOF Siddon: Poisson NLL + gradient, 8 "
+                 "phantoms x 5M TOF events, C1 scanner, 128x128x64 @2mm",
+                 "events/s (forward + adjoint per event, autograd)",
+                 per * 8 / (ms * 1e-3), "events/s", args.steps, args.warmup, ms,
+                 {"phantoms": 8, "events_per_phantom": per,
+                  "precision": "compensated"})
+
+
+RUNNERS = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}

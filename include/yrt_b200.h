@@ -219,10 +219,11 @@ yrtb_status yrtb_gather_histo3d(yrtb_projector* h, const float* d_histo,
 /* ------------------------------------------------------- event ordering --- */
 /* Permutation that groups events by OSEM subset (event index mod
  * num_subsets, the reference's chronological interleaving) and, inside a
- * subset, by ray length (voxel crossings of the single-ray Siddon
- * projector, in steps of 8), then LOR (Histogram3D bin or detector pair) and
- * TOF, so that neighbouring GPU threads trace neighbouring rays of similar
- * length.
+ * subset, by dynamic frame (when given), ray length (voxel crossings of the
+ * single-ray Siddon projector, in steps of 8), then LOR (Histogram3D bin or
+ * detector pair) and TOF, so that neighbouring GPU threads trace
+ * neighbouring rays of similar length in one frame's image.  num_subsets <=
+ * 65535 (4095 with dynamic frames).
  * d_perm[i] = source index of output position i (n uint64); subset_offsets
  * (host, num_subsets+1) delimits the subsets in the reordered arrays.  The
  * result of an OSEM subset does not depend on the order of its events

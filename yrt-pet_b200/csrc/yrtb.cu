@@ -686,7 +686,8 @@ __global__ void __launch_bounds__(kBlock)
 // Sort key of event e: subset (e mod S) in bits 48..63, the ray's number of
 // voxel crossings in steps of 8 (when counts are given) in bits 43..47, LOR
 // (Histogram3D bin, or the ordered detector pair) in bits 8..42, TOF in 16 ps
-// steps in bits 0..7.  Grouping rays of similar length keeps the threads of
+// steps in bits 0..7.  With dynamic frames: subset in bits 52..63, frame in
+// 44..51, crossings in 39..43, LOR in 8..38.  Grouping rays of similar length keeps the threads of
 // a warp iterating together; the LOR key keeps neighbouring rays together.
 __global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
                              uint64_t numSubsets, const uint32_t* __restrict__ counts,
@@ -714,8 +715,20 @@ __global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
 			q = t <= 0.f ? 0 : (t >= 255.f ? 255 : static_cast<uint64_t>(t));
 		}
 		const uint64_t bucket = counts ? min(__ldg(counts + e) / 8u, 31u) : 0u;
-		keys[e] = ((e % numSubsets) << 48) | (bucket << 43) |
-		          ((lorKey & 0x7FFFFFFFFULL) << 8) | q;
+		if (E.frame != nullptr)
+		{
+			// Dynamic data: frame after subset, so that one frame's image
+			// is traced at a time and stays L2 resident.
+			const int f = __ldg(E.frame + e);
+			const uint64_t fk = f < 0 ? 255u : static_cast<uint64_t>(min(f, 254));
+			keys[e] = ((e % numSubsets) << 52) | (fk << 44) | (bucket << 39) |
+			          ((lorKey & 0x7FFFFFFFULL) << 8) | q;
+		}
+		else
+		{
+			keys[e] = ((e % numSubsets) << 48) | (bucket << 43) |
+			          ((lorKey & 0x7FFFFFFFFULL) << 8) | q;
+		}
 		vals[e] = e;
 	}
 }
@@ -1382,7 +1395,7 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
                                      yrtb_stream stream)
 {
 	if (!h || !ev || !d_perm || !subset_offsets || num_subsets <= 0 ||
-	    num_subsets > 65535)
+	    num_subsets > (ev && ev->frame ? 4095 : 65535))
 		return fail(YRTB_ERR_ARGUMENT, "invalid subset-order arguments");
 	const uint64_t n = ev->count;
 	const uint64_t S = static_cast<uint64_t>(num_subsets);
