@@ -64,7 +64,8 @@ typedef struct
 
 /* Arithmetic of the traversal. */
 #define YRTB_MIRROR 0       /* FP32 in the reference's operation order (bit-exact voxel sequence) */
-#define YRTB_COMPENSATED 1  /* FP64 entry/exit (alpha) setup, Kahan-compensated FP32 forward sums */
+#define YRTB_COMPENSATED 1  /* FP64 entry-voxel placement, Kahan-compensated FP32 forward sums,
+                               TOF Gaussian as a multiply by 1/sigma and the fast exponential */
 
 /* Projector options: the reference ProjectorParams
  * (include/yrt-pet/operators/ProjectorParams.hpp:27-71) plus the PSF table
@@ -81,6 +82,14 @@ typedef struct
 	float psf_s_step, psf_k_spacing;
 	const float* psf_taps;  /* host, psf_num_s * psf_size */
 	int precision;          /* YRTB_MIRROR or YRTB_COMPENSATED */
+	int deterministic;      /* 1: back projections (yrtb_backward, yrtb_em_step, the histogram
+	                           kernels and everything built on them) run in two passes and
+	                           accumulate in 64-bit fixed point, so their images are bit-identical
+	                           whatever the order of events and atomics (the exact sum to within
+	                           n * 2^-61 of n * max|v w| for n events); the projector then holds
+	                           an 8-byte-per-voxel image (nx*ny*nz*nt).  No reference counterpart:
+	                           the reference accumulates with float atomics (CPU atomic_ref,
+	                           GPU atomicAdd) and is order dependent. */
 } yrtb_projector_params;
 
 /* Events (list-mode) in structure-of-arrays form, device pointers.  Either
@@ -160,6 +169,54 @@ yrtb_status yrtb_projector_create(const yrtb_scanner* scanner,
                                   yrtb_projector** out);
 void yrtb_projector_destroy(yrtb_projector* h);
 
+/* Launch configuration of the single-ray Siddon event kernels (yrtb_forward,
+ * yrtb_backward, yrtb_em_step and the OSEM driver) and of the event ordering.
+ * No reference counterpart: the reference launches one thread per event in
+ * 256-thread blocks (GPUBatchSetup, include/yrt-pet/utils/GPUTypes.cuh:17-55)
+ * on events in file order.  Default: {256, 1, 3}. */
+typedef struct
+{
+	int block;            /* threads per block: 128, 256 or 512 */
+	int threads_per_lor;  /* 1, 2 or 4 threads walk one LOR, each a piece cut
+	                         at voxel planes, the forward sum reduced over the
+	                         group; > 1 needs YRTB_COMPENSATED precision (the
+	                         pieces' sums round differently from one walk) and
+	                         is not used by deterministic back projections */
+	int bucket_shift;     /* yrtb_events_subset_order groups rays by
+	                         (voxel crossings >> bucket_shift), 0..6 */
+} yrtb_launch_config;
+
+yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
+                                      const yrtb_launch_config* cfg);
+yrtb_status yrtb_projector_get_launch(const yrtb_projector* h,
+                                      yrtb_launch_config* cfg);
+
+#define YRTB_TUNE_MAX 64
+
+typedef struct
+{
+	yrtb_launch_config best;
+	int num_tried;
+	uint64_t sample_events;
+	yrtb_launch_config tried[YRTB_TUNE_MAX];
+	float ms[YRTB_TUNE_MAX];  /* best of 3 timed EM steps over the sample */
+} yrtb_tune_report;
+
+/* Autotuner (no reference counterpart).  Times the fused EM step of this
+ * projector over a sample of the events -- subset 0 of num_subsets
+ * interleaved subsets, at most max_sample events -- for every launch
+ * configuration the projector admits (block x threads_per_lor x bucket_shift,
+ * each bucket_shift on the sample ordered with it), keeps the fastest
+ * (yrtb_projector_set_launch) and reports all timings.  d_image: the image
+ * the EM steps read (nx*ny*nz*nt floats; its values do not change the work).
+ * Setup-time call: allocates temporaries and synchronises the stream, so it
+ * must not run under stream capture.  Projectors other than single-ray
+ * Siddon keep the default configuration (num_tried = 0). */
+yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
+                          const yrtb_events* ev, int num_subsets,
+                          uint64_t max_sample, yrtb_tune_report* report,
+                          yrtb_stream stream);
+
 /* Offsets drawn by the multi-ray Siddon projector for events k = 0..count-1
  * of a range: d_out[k*4*(num_rays-1) + 4*(ray-1) + {0..3}] = (i1, j1, i2, j2),
  * uniforms in [-0.5, 0.5) along z and across the crystal at each endpoint.
@@ -220,7 +277,8 @@ yrtb_status yrtb_gather_histo3d(yrtb_projector* h, const float* d_histo,
 /* Permutation that groups events by OSEM subset (event index mod
  * num_subsets, the reference's chronological interleaving) and, inside a
  * subset, by dynamic frame (when given), ray length (voxel crossings of the
- * single-ray Siddon projector, in steps of 8), then LOR (Histogram3D bin or
+ * single-ray Siddon projector, in steps of 2^bucket_shift of the projector's
+ * launch configuration), then LOR (Histogram3D bin or
  * detector pair) and TOF, so that neighbouring GPU threads trace
  * neighbouring rays of similar length in one frame's image.  num_subsets <=
  * 65535 (4095 with dynamic frames).

@@ -162,7 +162,8 @@ template <bool TOF, bool COMP, typename Visit>
 __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
                                            const float3 p2, const TofP& tp,
                                            float tofValue, Visit& visit,
-                                           float wlo = 0.f, float whi = 1.f)
+                                           float wlo = 0.f, float whi = 1.f,
+                                           int part = 0, int parts = 1)
 {
 	// 1. Clip to the FOV cylinder.
 	float t0, t1;
@@ -224,6 +225,32 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	// Optional extra window [wlo, whi] (defaults leave amin, amax unchanged).
 	amin = fmaxf(amin, wlo);
 	amax = fminf(amax, whi);
+	if (parts > 1)
+	{
+		// Piece `part` of `parts` (several threads per LOR).  The cuts sit on
+		// voxel planes of the axis the ray crosses most often, so every
+		// segment of the walk stays whole and keeps the TOF weight of its
+		// midpoint; neighbouring pieces compute the same cut bit for bit.
+		const float cx = flat_x ? -1.f : fabsf(p2.x - p1.x) * inv_dx;
+		const float cy = flat_y ? -1.f : fabsf(p2.y - p1.y) * inv_dy;
+		const float cz = flat_z ? -1.f : fabsf(p2.z - p1.z) * inv_dz;
+		const int ax = (cx >= cy && cx >= cz) ? 0 : (cy >= cz ? 1 : 2);
+		const float q1 = ax == 0 ? p1.x : (ax == 1 ? p1.y : p1.z);
+		const float q2 = ax == 0 ? p2.x : (ax == 1 ? p2.y : p2.z);
+		const float qi = ax == 0 ? inv_x : (ax == 1 ? inv_y : inv_z);
+		const float q0 = ax == 0 ? x0 : (ax == 1 ? y0 : z0);
+		const float dq = ax == 0 ? dx : (ax == 1 ? dy : dz);
+		const float lo = amin, span = amax - amin;
+		auto cut = [&](int j) -> float
+		{
+			const float at = lo + (static_cast<float>(j) / static_cast<float>(parts)) * span;
+			const float plane = q0 + rintf((q1 + at * (q2 - q1) - q0) / dq) * dq;
+			return fminf(fmaxf((plane - q1) * qi, lo), lo + span);
+		};
+		const float hi = amax;
+		amin = part == 0 ? lo : cut(part);
+		amax = part == parts - 1 ? hi : cut(part + 1);
+	}
 
 	float a_cur = amin;
 	float a_next = -1.0f;
@@ -346,6 +373,28 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		vx = static_cast<int>((double(p1.x) + am * (double(p2.x) - double(p1.x)) + 0.5 * double(g.lx)) / double(dx));
 		vy = static_cast<int>((double(p1.y) + am * (double(p2.y) - double(p1.y)) + 0.5 * double(g.ly)) / double(dy));
 		vz = static_cast<int>((double(p1.z) + am * (double(p2.z) - double(p1.z)) + 0.5 * double(g.lz)) / double(dz));
+		if (part > 0)
+		{
+			// A piece that starts at a cut inside the ray: its first segment
+			// can be arbitrarily short (a plane of another axis right after
+			// the cut, e.g. at a voxel corner), and an exact midpoint may then
+			// fall on the other side of a plane than the FP32 crossings the
+			// walk steps by.  Take the voxel from the walk's own crossings:
+			// the segment lies just before the next plane of each stepping
+			// axis (the plane at a_next for the axes stepped last).
+			auto fromPlanes = [](bool flat, bool stepped, float cur, float fd,
+			                     float q0, float d, int dir, int& v)
+			{
+				if (flat)
+					return;
+				const float pre = stepped ? cur - fd : cur;
+				const int ip = static_cast<int>(rintf((pre - q0) / d));
+				v = dir > 0 ? ip - 1 : ip;
+			};
+			fromPlanes(flat_x, dir_next & 1, x_cur, fdx, x0, dx, dir_x, vx);
+			fromPlanes(flat_y, dir_next & 2, y_cur, fdy, y0, dy, dir_y, vy);
+			fromPlanes(flat_z, dir_next & 4, z_cur, fdz, z0, dz, dir_z, vz);
+		}
 	}
 	else
 	{

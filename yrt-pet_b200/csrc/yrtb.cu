@@ -10,10 +10,16 @@
 //            back projection scatters with fire-and-forget float reductions
 //            (red.global.add.f32) that resolve in L2 (the 4-42 MB images of
 //            the target workloads stay L2 resident on B200's 126 MB L2).
+//            Deterministic projectors scatter into a 64-bit fixed-point
+//            image instead (integer addition is associative, so the result
+//            does not depend on the order in which the reductions land).
 //
-// Kernels are grid-stride loops sized to a multiple of the SM count; one
-// thread walks one LOR (or one histogram bin) so that every voxel crossing is
-// an independent L2 transaction and no inter-thread synchronisation is needed.
+// Projection kernels run one event (or histogram bin) per thread, or per
+// group of 2-4 threads that split the ray: every voxel crossing is an
+// independent L2 transaction, no inter-thread synchronisation is needed, and
+// the threads of a warp stay converged (events are ordered by ray length
+// beforehand).  Image-space kernels are grid-stride loops sized to a multiple
+// of the SM count.
 
 #include "yrt_b200.h"
 #include "device.cuh"
@@ -29,6 +35,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using namespace yrtb;
@@ -340,11 +347,13 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
                                              float3 p2, float3 n1, float3 n2,
                                              float tofv, uint64_t rid,
                                              bool forward, Visit& visit,
-                                             EndRay& endRay)
+                                             EndRay& endRay, int part = 0,
+                                             int parts = 1)
 {
 	if constexpr (KIND == K_SIDDON)
 	{
-		siddonWalk<TOF, COMP>(P.g, p1, p2, P.tof, tofv, visit);
+		siddonWalk<TOF, COMP>(P.g, p1, p2, P.tof, tofv, visit, 0.f, 1.f, part,
+		                      parts);
 		endRay();
 	}
 	else if constexpr (KIND == K_SIDDON_MR)
@@ -373,18 +382,25 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
 	}
 }
 
-// Forward sum of one event: per-ray partial sums added ray by ray; mirror
-// mode sums in traversal order, compensated mode uses Kahan summation.
-template <int KIND, bool TOF, bool COMP>
+// Forward sum of one event (or of piece `part` of `parts` of a single-ray
+// Siddon walk): per-ray partial sums added ray by ray; mirror mode sums in
+// traversal order, compensated mode uses Kahan summation.  With TRACK, maxw
+// receives the largest |weight| of the event's rays (the sum itself is
+// computed exactly as without TRACK).
+template <int KIND, bool TOF, bool COMP, bool TRACK = false>
 __device__ __forceinline__ float forwardEvent(const KParams& P,
                                               const float* __restrict__ img,
                                               float3 p1, float3 p2, float3 n1,
                                               float3 n2, float tofv,
-                                              uint64_t rid)
+                                              uint64_t rid,
+                                              float* maxw = nullptr,
+                                              int part = 0, int parts = 1)
 {
-	float acc = 0.f, ray = 0.f, comp = 0.f;
+	float acc = 0.f, ray = 0.f, comp = 0.f, mw = 0.f;
 	auto visit = [&](int o, float w)
 	{
+		if constexpr (TRACK)
+			mw = fmaxf(mw, fabsf(w));
 		const float term = w * __ldg(img + o);
 		if constexpr (COMP)
 		{
@@ -405,25 +421,102 @@ __device__ __forceinline__ float forwardEvent(const KParams& P,
 		comp = 0.f;
 	};
 	projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, true, visit,
-	                              endRay);
+	                              endRay, part, parts);
 	if constexpr (KIND == K_SIDDON_MR)
 		acc = acc / static_cast<float>(P.numRays);
+	if constexpr (TRACK)
+		*maxw = mw;
 	return acc;
 }
 
+// Largest |weight| along the event's rays (a walk without image reads).
 template <int KIND, bool TOF, bool COMP>
+__device__ __forceinline__ float maxWeightEvent(const KParams& P, float3 p1,
+                                                float3 p2, float3 n1, float3 n2,
+                                                float tofv, uint64_t rid)
+{
+	float mw = 0.f;
+	auto visit = [&](int, float w) { mw = fmaxf(mw, fabsf(w)); };
+	auto endRay = [] {};
+	projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+	                              endRay);
+	return mw;
+}
+
+// ------------------------------------------- deterministic back projection --
+// Two passes.  Pass 1 reduces M = max over events of |v_e| * max_k |w_ek|
+// (v_e the value back-projected along event e, w_ek its voxel weights; for
+// multi-ray, the rays of one event add at most |v_e| max|w| to a voxel).  Any
+// voxel then receives at most n * M in magnitude from the n events of the
+// call.  Pass 2 scatters round(v_e * w_ek * 2^s) into 64-bit integers with
+// 2^s the largest power of two for which n * M * 2^s <= 2^61, so the integer
+// sums cannot overflow (the roundings add at most numRays * n / 2 < 2^62).
+// Integer addition is associative: the image is the same whatever order the
+// atomics land in, and equal to the exact sum to within n/2 units of 2^-s.
+struct Fixed
+{
+	unsigned long long* acc;  // nvox * nt fixed-point image (zeroed by the caller)
+	const unsigned* maxBits;  // M as float bits (pass 1 result)
+	uint64_t n;               // events (bins) of the call
+};
+
+// Exponent k with n * M < 2^k; 0x7fffffff when M is zero or not finite.
+__device__ __forceinline__ int fixedExponent(unsigned maxBits, uint64_t n)
+{
+	const double b = static_cast<double>(n) * static_cast<double>(__uint_as_float(maxBits));
+	if (!(b > 0.0) || !isfinite(b))
+		return 0x7fffffff;
+	int k;
+	frexp(b, &k);
+	return k;
+}
+
+// 2^(61 - k): exact scale of the fixed-point contributions (0 if none).
+__device__ __forceinline__ double fixedScale(const Fixed& F)
+{
+	const int k = fixedExponent(*F.maxBits, F.n);
+	return k == 0x7fffffff ? 0.0 : ldexp(1.0, 61 - k);
+}
+
+// Warp max of a non-negative float (as bits) folded into *out by lane 0.  All
+// 32 lanes of the warp must call it.
+__device__ __forceinline__ void warpMaxInto(unsigned* out, float b)
+{
+	const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(b));
+	if ((threadIdx.x & 31) == 0 && bits != 0u)
+		atomicMax(out, bits);
+}
+
+template <int KIND, bool TOF, bool COMP, bool FIX = false>
 __device__ __forceinline__ void backwardEvent(const KParams& P,
                                               float* __restrict__ img,
                                               float v, float3 p1, float3 p2,
                                               float3 n1, float3 n2, float tofv,
-                                              uint64_t rid)
+                                              uint64_t rid,
+                                              unsigned long long* fix = nullptr,
+                                              double scale = 0.0, int part = 0,
+                                              int parts = 1)
 {
 	if constexpr (KIND == K_SIDDON_MR)
 		v = v / static_cast<float>(P.numRays);
-	auto visit = [&](int o, float w) { atomicAdd(img + o, v * w); };
 	auto endRay = [] {};
-	projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
-	                              endRay);
+	if constexpr (FIX)
+	{
+		const double vs = static_cast<double>(v) * scale;
+		auto visit = [&](int o, float w)
+		{
+			const long long q = __double2ll_rn(vs * static_cast<double>(w));
+			atomicAdd(fix + o, static_cast<unsigned long long>(q));
+		};
+		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+		                              endRay, part, parts);
+	}
+	else
+	{
+		auto visit = [&](int o, float w) { atomicAdd(img + o, v * w); };
+		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+		                              endRay, part, parts);
+	}
 }
 
 enum Op
@@ -434,17 +527,42 @@ enum Op
 	OP_COUNT = 3
 };
 
-// Siddon: 4 blocks of 256 threads per SM (64 registers per thread, 32
-// warps); the other projectors keep the compiler's register choice.
-template <int OP, int KIND, bool TOF, bool COMP>
-__global__ void __launch_bounds__(kBlock, KIND == K_SIDDON ? 4 : 1)
+// Sum over the TPL lanes that share one event (all of them active).
+template <int TPL>
+__device__ __forceinline__ float groupSum(float v)
+{
+	if constexpr (TPL > 1)
+	{
+		const unsigned lane = threadIdx.x & 31u;
+		const unsigned mask = ((1u << TPL) - 1u) << (lane & ~static_cast<unsigned>(TPL - 1));
+		// xor butterfly: every lane adds the same pairs, so all TPL lanes end
+		// with the same bits.
+		for (int o = TPL / 2; o > 0; o >>= 1)
+			v += __shfl_xor_sync(mask, v, o);
+	}
+	return v;
+}
+
+// One event per TPL threads (TPL > 1: single-ray Siddon, compensated
+// arithmetic; lane j of the group walks piece j of the ray and the forward
+// sum is reduced over the group).  Siddon: 1024 threads per SM (64 registers
+// per thread, 32 warps) whatever the block size; the other projectors keep
+// the compiler's register choice.  FIX (OP_BWD, OP_EM): pass 2 of the
+// deterministic back projection.
+template <int OP, int KIND, bool TOF, bool COMP, bool FIX = false,
+          int BLOCK = kBlock, int TPL = 1>
+__global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
     k_events(KParams P, Events E, Range R, const float* __restrict__ in,
              float* __restrict__ out, float globalScale, float denomThr,
-             unsigned long long* err)
+             unsigned long long* err, Fixed F)
 {
-	// One item per thread: a warp's threads stay converged across items
+	static_assert(TPL == 1 || (KIND == K_SIDDON && COMP && !FIX && OP != OP_COUNT),
+	              "several threads per LOR: single-ray Siddon, compensated");
+	// One item per thread group: a warp's threads stay converged across items
 	// (a grid-stride loop lets them drift apart between items).
-	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	const uint64_t gt = static_cast<uint64_t>(blockIdx.x) * BLOCK + threadIdx.x;
+	const uint64_t k = gt / TPL;
+	const int part = static_cast<int>(gt % TPL);
 	if (k < R.count)
 	{
 		const uint64_t e = R.start + k * R.stride;
@@ -452,12 +570,15 @@ __global__ void __launch_bounds__(kBlock, KIND == K_SIDDON ? 4 : 1)
 		float3 p1, p2, n1, n2;
 		if (frame < 0 || frame >= P.g.nt || !fetchEvent(P, E, e, p1, p2, n1, n2))
 		{
-			if (frame >= 0)
-				atomicAdd(err, 1ULL);
-			if constexpr (OP == OP_FWD)
-				out[e] = 0.f;
-			if constexpr (OP == OP_COUNT)
-				reinterpret_cast<uint32_t*>(out)[e] = 0u;
+			if (part == 0)
+			{
+				if (frame >= 0)
+					atomicAdd(err, 1ULL);
+				if constexpr (OP == OP_FWD)
+					out[e] = 0.f;
+				if constexpr (OP == OP_COUNT)
+					reinterpret_cast<uint32_t*>(out)[e] = 0u;
+			}
 			return;
 		}
 		const float tofv = TOF ? __ldg(E.tof + e) : 0.f;
@@ -473,13 +594,21 @@ __global__ void __launch_bounds__(kBlock, KIND == K_SIDDON ? 4 : 1)
 		}
 		else if constexpr (OP == OP_FWD)
 		{
-			out[e] = forwardEvent<KIND, TOF, COMP>(P, in + fo, p1, p2, n1, n2,
-			                                       tofv, k);
+			const float v = groupSum<TPL>(forwardEvent<KIND, TOF, COMP>(
+			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
+			if (part == 0)
+				out[e] = v;
 		}
 		else if constexpr (OP == OP_BWD)
 		{
-			backwardEvent<KIND, TOF, COMP>(P, out + fo, __ldg(in + e), p1, p2,
-			                               n1, n2, tofv, k);
+			if constexpr (FIX)
+				backwardEvent<KIND, TOF, COMP, true>(P, nullptr, __ldg(in + e), p1,
+				                                     p2, n1, n2, tofv, k,
+				                                     F.acc + fo, fixedScale(F));
+			else
+				backwardEvent<KIND, TOF, COMP>(P, out + fo, __ldg(in + e), p1, p2,
+				                               n1, n2, tofv, k, nullptr, 0.0, part,
+				                               TPL);
 		}
 		else
 		{
@@ -488,8 +617,8 @@ __global__ void __launch_bounds__(kBlock, KIND == K_SIDDON ? 4 : 1)
 			const float a = E.att ? __ldg(E.att + e) : 1.0f;
 			if (m == 0.f || s == 0.f || a == 0.f)
 				return;
-			float u = forwardEvent<KIND, TOF, COMP>(P, in + fo, p1, p2, n1, n2,
-			                                        tofv, k);
+			float u = groupSum<TPL>(forwardEvent<KIND, TOF, COMP>(
+			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			u *= s;
 			u *= a;
 			u *= globalScale;
@@ -501,10 +630,96 @@ __global__ void __launch_bounds__(kBlock, KIND == K_SIDDON ? 4 : 1)
 				u *= s;
 				u *= a;
 				u *= globalScale;
-				backwardEvent<KIND, TOF, COMP>(P, out + fo, u, p1, p2, n1, n2,
-				                               tofv, k);
+				if constexpr (FIX)
+					backwardEvent<KIND, TOF, COMP, true>(P, nullptr, u, p1, p2, n1,
+					                                     n2, tofv, k, F.acc + fo,
+					                                     fixedScale(F));
+				else
+					backwardEvent<KIND, TOF, COMP>(P, out + fo, u, p1, p2, n1, n2,
+					                               tofv, k, nullptr, 0.0, part, TPL);
 			}
 		}
+	}
+}
+
+// Pass 1 of the deterministic back projection of k_events<OP_BWD / OP_EM>:
+// folds |v_e| * max|w| of every event that pass 2 back-projects into
+// *maxBits.  The EM value v_e is computed exactly as in k_events (same
+// forward sum, same correction order).  Invalid events are left to pass 2,
+// which counts them.
+template <bool EM, int KIND, bool TOF, bool COMP>
+__global__ void __launch_bounds__(kBlock, KIND == K_SIDDON ? 4 : 1)
+    k_events_bound(KParams P, Events E, Range R, const float* __restrict__ in,
+                   float globalScale, float denomThr, unsigned* maxBits)
+{
+	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	float b = 0.f;
+	if (k < R.count)
+	{
+		const uint64_t e = R.start + k * R.stride;
+		const int frame = E.frame ? __ldg(E.frame + e) : 0;
+		float3 p1, p2, n1, n2;
+		if (frame >= 0 && frame < P.g.nt && fetchEvent(P, E, e, p1, p2, n1, n2))
+		{
+			const float tofv = TOF ? __ldg(E.tof + e) : 0.f;
+			if constexpr (!EM)
+			{
+				const float v = __ldg(in + e);
+				if (v != 0.f)
+					b = fabsf(v) * maxWeightEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2,
+					                                                tofv, k);
+			}
+			else
+			{
+				const int64_t fo = static_cast<int64_t>(frame) * P.g.nvox;
+				const float m = E.meas ? __ldg(E.meas + e) : 1.0f;
+				const float s = E.sens ? __ldg(E.sens + e) : 1.0f;
+				const float a = E.att ? __ldg(E.att + e) : 1.0f;
+				if (m != 0.f && s != 0.f && a != 0.f)
+				{
+					float mw = 0.f;
+					float u = forwardEvent<KIND, TOF, COMP, true>(
+					    P, in + fo, p1, p2, n1, n2, tofv, k, &mw);
+					u *= s;
+					u *= a;
+					u *= globalScale;
+					if (E.add)
+						u += __ldg(E.add + e);
+					if (fabsf(u) > denomThr)
+					{
+						u = m / u;
+						u *= s;
+						u *= a;
+						u *= globalScale;
+						b = fabsf(u) * mw;
+					}
+				}
+			}
+		}
+	}
+	// NaN bits order above every finite value, so a NaN bound is kept.
+	warpMaxInto(maxBits, b != b ? __uint_as_float(0x7fffffffu) : b);
+}
+
+// out[i] += fixed-point image / 2^s (NaN everywhere if the bound was not
+// finite: a value back-projected was NaN or infinite).
+__global__ void k_fixed_finish(const unsigned long long* __restrict__ acc,
+                               uint64_t n, Fixed F, float* __restrict__ out)
+{
+	const int k = fixedExponent(*F.maxBits, F.n);
+	const bool bad = k == 0x7fffffff && *F.maxBits != 0u;
+	if (k == 0x7fffffff && !bad)
+		return;  // nothing was back-projected
+	const double inv = bad ? 0.0 : ldexp(1.0, k - 61);
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+	{
+		if (bad)
+			out[i] = __int_as_float(0x7fffffff);
+		else
+			out[i] += static_cast<float>(
+			    static_cast<double>(static_cast<long long>(acc[i])) * inv);
 	}
 }
 
@@ -616,28 +831,41 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // Histogram-bin kernels: sensitivity back projection and histogram EM.
-template <int KIND, bool EM>
+// MODE H_BOUND is pass 1 and H_FIX pass 2 of the deterministic back
+// projection (see Fixed); H_PLAIN scatters floats.
+enum HistoMode
+{
+	H_PLAIN = 0,
+	H_BOUND = 1,
+	H_FIX = 2
+};
+
+template <int KIND, bool EM, int MODE = H_PLAIN>
 __global__ void __launch_bounds__(kBlock)
     k_histo(KParams P, H3Dev H, uint64_t count, uint64_t numPhiSubset,
             uint64_t numSubsets, uint64_t subset, const float* __restrict__ img,
             float* __restrict__ out, const float* __restrict__ meas,
             const float* __restrict__ sensH, const float* __restrict__ acfH,
             const float* __restrict__ addH, Geom mu,
-            const float* __restrict__ muImg, float globalScale, float denomThr)
+            const float* __restrict__ muImg, float globalScale, float denomThr,
+            Fixed F, unsigned* maxBits)
 {
 	// One item per thread: a warp's threads stay converged across items
 	// (a grid-stride loop lets them drift apart between items).
 	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-	if (k < count)
+	float bound = 0.f;  // H_BOUND: |v| * max|w| of this bin
+	do
 	{
+		if (k >= count)
+			break;
 		const uint64_t bin = h3SubsetBin(H, k, numPhiSubset, numSubsets, subset);
 		uint32_t d1, d2;
 		h3Pair(H, bin, d1, d2);
 		if (d1 == 0 && d2 == 0)
-			return;
+			break;
 		const float m = EM ? __ldg(meas + bin) : 1.0f;
 		if (EM && m == 0.f)
-			return;
+			break;
 		const float s = sensH ? __ldg(sensH + bin) : 1.0f;
 		const float4 pa = __ldg(P.scan.pos + d1), pb = __ldg(P.scan.pos + d2);
 		const float4 oa = __ldg(P.scan.ori + d1), ob = __ldg(P.scan.ori + d2);
@@ -659,38 +887,56 @@ __global__ void __launch_bounds__(kBlock)
 		const float3 off = make_float3(P.g.offx, P.g.offy, P.g.offz);
 		p1 = f3sub(p1, off);
 		p2 = f3sub(p2, off);
-		if constexpr (!EM)
+		float v = a * s;
+		float mw = 0.f;
+		if constexpr (EM)
 		{
-			backwardEvent<KIND, false, false>(P, out, a * s, p1, p2, n1, n2, 0.f, k);
-		}
-		else
-		{
-			float u = forwardEvent<KIND, false, false>(P, img, p1, p2, n1, n2, 0.f, k);
+			float u;
+			if constexpr (MODE == H_BOUND)
+				u = forwardEvent<KIND, false, false, true>(P, img, p1, p2, n1, n2,
+				                                           0.f, k, &mw);
+			else
+				u = forwardEvent<KIND, false, false>(P, img, p1, p2, n1, n2, 0.f, k);
 			u *= s;
 			u *= a;
 			u *= globalScale;
 			if (addH)
 				u += __ldg(addH + bin);
-			if (fabsf(u) > denomThr)
-			{
-				u = m / u;
-				u *= s;
-				u *= a;
-				u *= globalScale;
-				backwardEvent<KIND, false, false>(P, out, u, p1, p2, n1, n2, 0.f, k);
-			}
+			if (!(fabsf(u) > denomThr))
+				break;
+			u = m / u;
+			u *= s;
+			u *= a;
+			u *= globalScale;
+			v = u;
 		}
-	}
+		else if constexpr (MODE == H_BOUND)
+		{
+			if (v != 0.f)
+				mw = maxWeightEvent<KIND, false, false>(P, p1, p2, n1, n2, 0.f, k);
+		}
+		if constexpr (MODE == H_BOUND)
+			bound = fabsf(v) * mw;
+		else if constexpr (MODE == H_FIX)
+			backwardEvent<KIND, false, false, true>(P, nullptr, v, p1, p2, n1, n2,
+			                                        0.f, k, F.acc, fixedScale(F));
+		else
+			backwardEvent<KIND, false, false>(P, out, v, p1, p2, n1, n2, 0.f, k);
+	} while (false);
+	if constexpr (MODE == H_BOUND)
+		warpMaxInto(maxBits, bound != bound ? __uint_as_float(0x7fffffffu) : bound);
 }
 
-// Sort key of event e: subset (e mod S) in bits 48..63, the ray's number of
-// voxel crossings in steps of 8 (when counts are given) in bits 43..47, LOR
-// (Histogram3D bin, or the ordered detector pair) in bits 8..42, TOF in 16 ps
-// steps in bits 0..7.  With dynamic frames: subset in bits 52..63, frame in
-// 44..51, crossings in 39..43, LOR in 8..38.  Grouping rays of similar length keeps the threads of
-// a warp iterating together; the LOR key keeps neighbouring rays together.
+// Sort key of event e.  Without dynamic frames: subset (e mod S) in bits
+// 48..63, ray length bucket (voxel crossings >> bucketShift, at most 127, when
+// counts are given) in bits 41..47, LOR (Histogram3D bin, or the ordered
+// detector pair, >> lorShift to fit) in bits 8..40, TOF in 16 ps steps in bits
+// 0..7.  With dynamic frames: subset in bits 52..63, frame in 44..51, bucket
+// in 37..43, LOR in 8..36.  Grouping rays of similar length keeps the threads
+// of a warp iterating together; the LOR key keeps neighbouring rays together.
 __global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
                              uint64_t numSubsets, const uint32_t* __restrict__ counts,
+                             int bucketShift, int lorShift,
                              unsigned long long* __restrict__ keys,
                              unsigned long long* __restrict__ vals)
 {
@@ -706,31 +952,42 @@ __global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
 			if (hasH3 && h3Bin(H, a, b, bin))
 				lorKey = bin;
 			else
-				lorKey = (static_cast<uint64_t>(min(a, b)) << 20) ^ max(a, b);
+				lorKey = static_cast<uint64_t>(min(a, b)) * H.numDets + max(a, b);
 		}
+		lorKey >>= lorShift;
 		uint64_t q = 128;
 		if (E.tof != nullptr)
 		{
 			const float t = __ldg(E.tof + e) / 16.0f + 128.0f;
 			q = t <= 0.f ? 0 : (t >= 255.f ? 255 : static_cast<uint64_t>(t));
 		}
-		const uint64_t bucket = counts ? min(__ldg(counts + e) / 8u, 31u) : 0u;
+		const uint64_t bucket = counts ? min(__ldg(counts + e) >> bucketShift, 127u) : 0u;
 		if (E.frame != nullptr)
 		{
 			// Dynamic data: frame after subset, so that one frame's image
 			// is traced at a time and stays L2 resident.
 			const int f = __ldg(E.frame + e);
 			const uint64_t fk = f < 0 ? 255u : static_cast<uint64_t>(min(f, 254));
-			keys[e] = ((e % numSubsets) << 52) | (fk << 44) | (bucket << 39) |
-			          ((lorKey & 0x7FFFFFFFULL) << 8) | q;
+			keys[e] = ((e % numSubsets) << 52) | (fk << 44) | (bucket << 37) |
+			          ((lorKey & 0x1FFFFFFFULL) << 8) | q;
 		}
 		else
 		{
-			keys[e] = ((e % numSubsets) << 48) | (bucket << 43) |
-			          ((lorKey & 0x7FFFFFFFFULL) << 8) | q;
+			keys[e] = ((e % numSubsets) << 48) | (bucket << 41) |
+			          ((lorKey & 0x1FFFFFFFFULL) << 8) | q;
 		}
 		vals[e] = e;
 	}
+}
+
+// perm[i] = i * stride (the events of one interleaved subset).
+__global__ void k_iota_stride(unsigned long long* __restrict__ perm, uint64_t n,
+                              uint64_t stride)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+		perm[i] = i * stride;
 }
 
 template <typename T>
@@ -1003,10 +1260,18 @@ struct yrtb_projector
 	int32_t* d_ring = nullptr;
 	int2* d_z = nullptr;
 	unsigned long long* d_err = nullptr;
+	// Launch configuration of the single-ray Siddon event kernels.
+	yrtb_launch_config launch{256, 1, 3};
+	// Deterministic back projection: fixed-point image (nvox * nt) and bound.
+	bool det = false;
+	unsigned long long* d_fix = nullptr;
+	unsigned* d_fixMax = nullptr;
 	int device = 0;
 
 	~yrtb_projector()
 	{
+		cudaFree(d_fix);
+		cudaFree(d_fixMax);
 		cudaFree(d_pos);
 		cudaFree(d_ori);
 		cudaFree(d_taps);
@@ -1066,12 +1331,90 @@ yrtb_status checkEvents(const yrtb_projector* h, const yrtb_events* ev,
 	return YRTB_OK;
 }
 
-template <int OP, int KIND, bool TOF, bool COMP>
-void launchEvents(yrtb_projector* h, const Events& E, Range R, const float* in,
-                  float* out, float gs, float thr, cudaStream_t st)
+// Calls fn(kind, tof, comp) with the projector's configuration as
+// std::integral_constant / bool_constant values (compensated arithmetic
+// exists for the Siddon projectors only).
+template <typename Fn>
+void withConfig(const yrtb_projector* h, Fn&& fn)
 {
-	k_events<OP, KIND, TOF, COMP><<<gridAll(R.count), kBlock, 0, st>>>(
-	    h->P, E, R, in, out, gs, thr, h->d_err);
+	const bool tof = h->hasTof, comp = h->comp;
+	auto go = [&](auto kind)
+	{
+		using K = decltype(kind);
+		if constexpr (K::value == K_SIDDON || K::value == K_SIDDON_MR)
+		{
+			if (tof && comp)
+				fn(kind, std::true_type{}, std::true_type{});
+			else if (tof)
+				fn(kind, std::true_type{}, std::false_type{});
+			else if (comp)
+				fn(kind, std::false_type{}, std::true_type{});
+			else
+				fn(kind, std::false_type{}, std::false_type{});
+		}
+		else
+		{
+			if (tof)
+				fn(kind, std::true_type{}, std::false_type{});
+			else
+				fn(kind, std::false_type{}, std::false_type{});
+		}
+	};
+	switch (h->kind)
+	{
+	case K_SIDDON: go(std::integral_constant<int, K_SIDDON>{}); break;
+	case K_SIDDON_MR: go(std::integral_constant<int, K_SIDDON_MR>{}); break;
+	case K_DD: go(std::integral_constant<int, K_DD>{}); break;
+	default: go(std::integral_constant<int, K_DD_PSF>{}); break;
+	}
+}
+
+// Clears the fixed-point image (frames 0..nt-1) and the bound of a
+// deterministic back projection over n items.
+yrtb_status fixedBegin(yrtb_projector* h, uint64_t n, cudaStream_t st, Fixed& F)
+{
+	const uint64_t J = static_cast<uint64_t>(h->P.g.nvox) * h->ip.nt;
+	YRTB_CUDA(cudaMemsetAsync(h->d_fix, 0, J * sizeof(unsigned long long), st));
+	YRTB_CUDA(cudaMemsetAsync(h->d_fixMax, 0, sizeof(unsigned), st));
+	F = Fixed{h->d_fix, h->d_fixMax, n};
+	return YRTB_OK;
+}
+
+void fixedEnd(yrtb_projector* h, const Fixed& F, float* out, cudaStream_t st)
+{
+	const uint64_t J = static_cast<uint64_t>(h->P.g.nvox) * h->ip.nt;
+	k_fixed_finish<<<gridFor(J, 8), kBlock, 0, st>>>(h->d_fix, J, F, out);
+}
+
+// Single-ray Siddon event kernel with block size B and the projector's
+// threads per LOR (compensated arithmetic only; 1 otherwise).
+template <int OP, int K, bool T, bool C, int B>
+void launchTuned(const yrtb_projector* h, const Events& E, Range R,
+                 const float* in, float* out, float gs, float thr,
+                 cudaStream_t st, const Fixed& F)
+{
+	auto go = [&](auto tplc)
+	{
+		constexpr int TPL = decltype(tplc)::value;
+		const uint64_t threads = R.count * TPL;
+		const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, (threads + B - 1) / B));
+		k_events<OP, K, T, C, false, B, TPL><<<grid, B, 0, st>>>(h->P, E, R, in, out, gs,
+		                                                        thr, h->d_err, F);
+	};
+	const int tpl = h->launch.threads_per_lor;
+	if constexpr (C)
+	{
+		if (tpl == 4)
+			go(std::integral_constant<int, 4>{});
+		else if (tpl == 2)
+			go(std::integral_constant<int, 2>{});
+		else
+			go(std::integral_constant<int, 1>{});
+	}
+	else
+	{
+		go(std::integral_constant<int, 1>{});
+	}
 }
 
 template <int OP>
@@ -1088,44 +1431,46 @@ yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
 	const Events E = toDev(ev);
 	const Range R{range.start, range.stride, range.count};
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-	const bool tof = h->hasTof;
-	const bool comp = h->comp;
-#define YRTB_DISPATCH(KIND)                                                    \
-	do                                                                         \
-	{                                                                          \
-		if (tof)                                                               \
-		{                                                                      \
-			if (comp)                                                          \
-				launchEvents<OP, KIND, true, true>(h, E, R, in, out, gs, thr, st); \
-			else                                                               \
-				launchEvents<OP, KIND, true, false>(h, E, R, in, out, gs, thr, st); \
-		}                                                                      \
-		else                                                                   \
-		{                                                                      \
-			if (comp)                                                          \
-				launchEvents<OP, KIND, false, true>(h, E, R, in, out, gs, thr, st); \
-			else                                                               \
-				launchEvents<OP, KIND, false, false>(h, E, R, in, out, gs, thr, st); \
-		}                                                                      \
-	} while (0)
-	switch (h->kind)
+	constexpr bool kScatter = OP == OP_BWD || OP == OP_EM;
+	Fixed F{};
+	if (kScatter && h->det)
+		if ((s = fixedBegin(h, R.count, st, F)) != YRTB_OK)
+			return s;
+	const unsigned grid = gridAll(R.count);
+	withConfig(h, [&](auto kind, auto tof, auto comp)
 	{
-	case K_SIDDON: YRTB_DISPATCH(K_SIDDON); break;
-	case K_SIDDON_MR: YRTB_DISPATCH(K_SIDDON_MR); break;
-	case K_DD:
-		if (tof)
-			launchEvents<OP, K_DD, true, false>(h, E, R, in, out, gs, thr, st);
-		else
-			launchEvents<OP, K_DD, false, false>(h, E, R, in, out, gs, thr, st);
-		break;
-	default:
-		if (tof)
-			launchEvents<OP, K_DD_PSF, true, false>(h, E, R, in, out, gs, thr, st);
-		else
-			launchEvents<OP, K_DD_PSF, false, false>(h, E, R, in, out, gs, thr, st);
-		break;
-	}
-#undef YRTB_DISPATCH
+		constexpr int K = decltype(kind)::value;
+		constexpr bool T = decltype(tof)::value;
+		constexpr bool C = decltype(comp)::value;
+		if constexpr (K == K_SIDDON && OP != OP_COUNT)
+		{
+			if (!(kScatter && h->det))
+			{
+				if (h->launch.block == 128)
+					launchTuned<OP, K, T, C, 128>(h, E, R, in, out, gs, thr, st, F);
+				else if (h->launch.block == 512)
+					launchTuned<OP, K, T, C, 512>(h, E, R, in, out, gs, thr, st, F);
+				else
+					launchTuned<OP, K, T, C, 256>(h, E, R, in, out, gs, thr, st, F);
+				return;
+			}
+		}
+		if constexpr (kScatter)
+		{
+			if (h->det)
+			{
+				k_events_bound<OP == OP_EM, K, T, C><<<grid, kBlock, 0, st>>>(
+				    h->P, E, R, in, gs, thr, h->d_fixMax);
+				k_events<OP, K, T, C, true><<<grid, kBlock, 0, st>>>(
+				    h->P, E, R, in, out, gs, thr, h->d_err, F);
+				return;
+			}
+		}
+		k_events<OP, K, T, C><<<grid, kBlock, 0, st>>>(h->P, E, R, in, out, gs,
+		                                               thr, h->d_err, F);
+	});
+	if (kScatter && h->det)
+		fixedEnd(h, F, out, st);
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
@@ -1152,19 +1497,113 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 	const Geom mg = mu ? makeGeom(*muParams) : Geom{};
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	const unsigned grid = gridAll(count);
-#define YRTB_HISTO(KIND)                                                       \
-	k_histo<KIND, EM><<<grid, kBlock, 0, st>>>(h->P, h->h3d, count, nps,       \
-	                                           numSubsets, subset, img, out,  \
-	                                           meas, sensH, acfH, addH, mg, mu, \
-	                                           gs, thr)
+	Fixed F{};
+	if (h->det)
+	{
+		const yrtb_status s = fixedBegin(h, count, st, F);
+		if (s != YRTB_OK)
+			return s;
+	}
+	auto launch = [&](auto kind)
+	{
+		constexpr int K = decltype(kind)::value;
+		if (h->det)
+		{
+			k_histo<K, EM, H_BOUND><<<grid, kBlock, 0, st>>>(
+			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
+			    acfH, addH, mg, mu, gs, thr, F, h->d_fixMax);
+			k_histo<K, EM, H_FIX><<<grid, kBlock, 0, st>>>(
+			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
+			    acfH, addH, mg, mu, gs, thr, F, nullptr);
+		}
+		else
+		{
+			k_histo<K, EM><<<grid, kBlock, 0, st>>>(
+			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
+			    acfH, addH, mg, mu, gs, thr, F, nullptr);
+		}
+	};
 	switch (h->kind)
 	{
-	case K_SIDDON: YRTB_HISTO(K_SIDDON); break;
-	case K_SIDDON_MR: YRTB_HISTO(K_SIDDON_MR); break;
-	case K_DD: YRTB_HISTO(K_DD); break;
-	default: YRTB_HISTO(K_DD_PSF); break;
+	case K_SIDDON: launch(std::integral_constant<int, K_SIDDON>{}); break;
+	case K_SIDDON_MR: launch(std::integral_constant<int, K_SIDDON_MR>{}); break;
+	case K_DD: launch(std::integral_constant<int, K_DD>{}); break;
+	default: launch(std::integral_constant<int, K_DD_PSF>{}); break;
 	}
-#undef YRTB_HISTO
+	if (h->det)
+		fixedEnd(h, F, out, st);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+// Subset-major permutation of the events (see yrtb_events_subset_order)
+// with ray-length buckets of 2^bucketShift crossings.
+yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
+                        int bucketShift, uint64_t* d_perm, cudaStream_t st)
+{
+	const uint64_t n = ev->count;
+	if (n == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	unsigned long long *keys = nullptr, *keys2 = nullptr, *vals = nullptr;
+	void* temp = nullptr;
+	size_t tempBytes = 0;
+	auto release = [&]
+	{
+		cudaFreeAsync(keys, st);
+		cudaFreeAsync(keys2, st);
+		cudaFreeAsync(vals, st);
+		cudaFreeAsync(temp, st);
+	};
+	cudaError_t ce = cudaMallocAsync(&keys, n * 8, st);
+	if (ce == cudaSuccess)
+		ce = cudaMallocAsync(&keys2, n * 8, st);
+	if (ce == cudaSuccess)
+		ce = cudaMallocAsync(&vals, n * 8, st);
+	if (ce != cudaSuccess)
+	{
+		release();
+		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+	}
+	// Crossing counts of the single-ray Siddon projector (into keys2, which
+	// the sort overwrites afterwards).
+	const uint32_t* counts = nullptr;
+	if (h->kind == K_SIDDON && (!h->hasTof || ev->tof_ps))
+	{
+		const yrtb_status cs = dispatchEvents<OP_COUNT>(
+		    h, ev, yrtb_range{0, 1, n}, nullptr, reinterpret_cast<float*>(keys2),
+		    1.f, 0.f, reinterpret_cast<yrtb_stream>(st));
+		if (cs != YRTB_OK)
+		{
+			release();
+			return cs;
+		}
+		counts = reinterpret_cast<const uint32_t*>(keys2);
+	}
+	// LOR keys wider than their field keep their high bits.
+	const int lorBits = ev->frame ? 29 : 33;
+	const uint64_t nd = h->h3d.numDets;
+	const uint64_t maxKey = h->h3 ? h->h3->numZBin * h->h3->numPhi * h->h3->numR
+	                              : nd * nd;
+	int keyBits = 0;
+	while (keyBits < 64 && (maxKey >> keyBits) != 0)
+		keyBits++;
+	const int lorShift = std::max(0, keyBits - lorBits);
+	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(
+	    h->h3d, h->h3 != nullptr, toDev(ev), n, S, counts, bucketShift, lorShift,
+	    keys, vals);
+	ce = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals,
+	                                     reinterpret_cast<unsigned long long*>(d_perm),
+	                                     n, 0, 64, st);
+	if (ce == cudaSuccess)
+		ce = cudaMallocAsync(&temp, tempBytes, st);
+	if (ce == cudaSuccess)
+		ce = cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals,
+		                                     reinterpret_cast<unsigned long long*>(d_perm),
+		                                     n, 0, 64, st);
+	release();
+	if (ce != cudaSuccess)
+		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
@@ -1332,6 +1771,13 @@ yrtb_status yrtb_projector_create(const yrtb_scanner* s, const float* lut,
 		P.tof.norm = static_cast<float>(1 / (std::sqrt(2 * 3.14159265358979) * P.tof.sigma));
 	}
 	h->comp = pp->precision == YRTB_COMPENSATED;
+	h->det = pp->deterministic != 0;
+	if (h->det)
+	{
+		const uint64_t J = static_cast<uint64_t>(P.g.nvox) * ip->nt;
+		YRTB_CUDA(cudaMalloc(&h->d_fix, J * sizeof(unsigned long long)));
+		YRTB_CUDA(cudaMalloc(&h->d_fixMax, sizeof(unsigned)));
+	}
 	if (pp->projector == YRTB_SIDDON)
 		h->kind = pp->num_rays > 1 ? K_SIDDON_MR : K_SIDDON;
 	else
@@ -1351,6 +1797,7 @@ yrtb_status yrtb_projector_create(const yrtb_scanner* s, const float* lut,
 		P.psf = Psf{h->d_taps, h->d_flipped, pp->psf_num_s, pp->psf_size,
 		            pp->psf_s_step, pp->psf_k_spacing};
 	}
+	h->h3d.numDets = static_cast<uint32_t>(nd);
 	if (s->dets_per_ring % 2 == 0)
 	{
 		h->h3 = std::make_unique<H3Host>(*s);
@@ -1372,6 +1819,34 @@ yrtb_status yrtb_projector_create(const yrtb_scanner* s, const float* lut,
 void yrtb_projector_destroy(yrtb_projector* h)
 {
 	delete h;
+}
+
+yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
+                                      const yrtb_launch_config* c)
+{
+	if (!h || !c)
+		return fail(YRTB_ERR_ARGUMENT, "null argument");
+	if (c->block != 128 && c->block != 256 && c->block != 512)
+		return fail(YRTB_ERR_ARGUMENT, "block must be 128, 256 or 512");
+	if (c->threads_per_lor != 1 && c->threads_per_lor != 2 && c->threads_per_lor != 4)
+		return fail(YRTB_ERR_ARGUMENT, "threads_per_lor must be 1, 2 or 4");
+	if (c->threads_per_lor > 1 && !(h->kind == K_SIDDON && h->comp))
+		return fail(YRTB_ERR_ARGUMENT,
+		            "threads_per_lor > 1 needs a single-ray Siddon projector in "
+		            "YRTB_COMPENSATED precision");
+	if (c->bucket_shift < 0 || c->bucket_shift > 6)
+		return fail(YRTB_ERR_ARGUMENT, "bucket_shift must be in 0..6");
+	h->launch = *c;
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_projector_get_launch(const yrtb_projector* h,
+                                      yrtb_launch_config* c)
+{
+	if (!h || !c)
+		return fail(YRTB_ERR_ARGUMENT, "null argument");
+	*c = h->launch;
+	return YRTB_OK;
 }
 
 yrtb_status yrtb_multiray_offsets(yrtb_projector* h, uint64_t count,
@@ -1402,61 +1877,8 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
 	subset_offsets[0] = 0;
 	for (uint64_t s = 0; s < S; s++)
 		subset_offsets[s + 1] = subset_offsets[s] + (n > s ? (n - s + S - 1) / S : 0);
-	if (n == 0)
-		return YRTB_OK;
-	YRTB_CUDA(cudaSetDevice(h->device));
-	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-	unsigned long long *keys = nullptr, *keys2 = nullptr, *vals = nullptr;
-	void* temp = nullptr;
-	size_t tempBytes = 0;
-	auto release = [&]
-	{
-		cudaFreeAsync(keys, st);
-		cudaFreeAsync(keys2, st);
-		cudaFreeAsync(vals, st);
-		cudaFreeAsync(temp, st);
-	};
-	cudaError_t ce = cudaMallocAsync(&keys, n * 8, st);
-	if (ce == cudaSuccess)
-		ce = cudaMallocAsync(&keys2, n * 8, st);
-	if (ce == cudaSuccess)
-		ce = cudaMallocAsync(&vals, n * 8, st);
-	if (ce != cudaSuccess)
-	{
-		release();
-		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
-	}
-	// Crossing counts of the single-ray Siddon projector (into keys2, which
-	// the sort overwrites afterwards).
-	const uint32_t* counts = nullptr;
-	if (h->kind == K_SIDDON && (!h->hasTof || ev->tof_ps))
-	{
-		const yrtb_status cs = dispatchEvents<OP_COUNT>(
-		    h, ev, yrtb_range{0, 1, n}, nullptr, reinterpret_cast<float*>(keys2),
-		    1.f, 0.f, stream);
-		if (cs != YRTB_OK)
-		{
-			release();
-			return cs;
-		}
-		counts = reinterpret_cast<const uint32_t*>(keys2);
-	}
-	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(
-	    h->h3d, h->h3 != nullptr, toDev(ev), n, S, counts, keys, vals);
-	ce = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals,
-	                                     reinterpret_cast<unsigned long long*>(d_perm),
-	                                     n, 0, 64, st);
-	if (ce == cudaSuccess)
-		ce = cudaMallocAsync(&temp, tempBytes, st);
-	if (ce == cudaSuccess)
-		ce = cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals,
-		                                     reinterpret_cast<unsigned long long*>(d_perm),
-		                                     n, 0, 64, st);
-	release();
-	if (ce != cudaSuccess)
-		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
-	YRTB_LAUNCHED();
-	return YRTB_OK;
+	return orderEvents(h, ev, S, h->launch.bucket_shift, d_perm,
+	                   reinterpret_cast<cudaStream_t>(stream));
 }
 
 yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
@@ -1878,6 +2300,146 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 			}
 		}
 	cleanup();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
+                          const yrtb_events* ev, int num_subsets,
+                          uint64_t max_sample, yrtb_tune_report* report,
+                          yrtb_stream stream)
+{
+	if (!h || !d_image || !ev || !report || num_subsets <= 0)
+		return fail(YRTB_ERR_ARGUMENT, "invalid autotune arguments");
+	*report = yrtb_tune_report{};
+	report->best = h->launch;
+	if (h->kind != K_SIDDON)
+		return YRTB_OK;
+	yrtb_range all{0, 1, 0};
+	yrtb_status s = checkEvents(h, ev, all, true);
+	if (s != YRTB_OK)
+		return s;
+	const uint64_t S = static_cast<uint64_t>(num_subsets);
+	uint64_t n = ev->count == 0 ? 0 : (ev->count + S - 1) / S;  // subset 0
+	if (max_sample > 0 && n > max_sample)
+		n = max_sample;
+	if (n == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+
+	// Temporaries: the sample twice (as drawn, and ordered per candidate),
+	// two permutations, one EM image.
+	std::vector<void*> bufs;
+	auto release = [&]
+	{
+		for (void* b : bufs)
+			cudaFreeAsync(b, st);
+		bufs.clear();
+	};
+	auto alloc = [&](size_t bytes, void** out) -> bool
+	{
+		*out = nullptr;
+		if (cudaMallocAsync(out, bytes, st) != cudaSuccess)
+			return false;
+		bufs.push_back(*out);
+		return true;
+	};
+	yrtb_events A = *ev, B = *ev;
+	A.count = B.count = n;
+	bool ok = true;
+	auto twin = [&](const void* src, size_t width, const void** a, const void** b)
+	{
+		if (!src || !ok)
+			return;
+		void *pa = nullptr, *pb = nullptr;
+		ok = alloc(n * width, &pa) && alloc(n * width, &pb);
+		*a = pa;
+		*b = pb;
+	};
+	twin(ev->d1, 4, reinterpret_cast<const void**>(&A.d1), reinterpret_cast<const void**>(&B.d1));
+	twin(ev->d2, 4, reinterpret_cast<const void**>(&A.d2), reinterpret_cast<const void**>(&B.d2));
+	twin(ev->lor, 24, reinterpret_cast<const void**>(&A.lor), reinterpret_cast<const void**>(&B.lor));
+	twin(ev->tof_ps, 4, reinterpret_cast<const void**>(&A.tof_ps), reinterpret_cast<const void**>(&B.tof_ps));
+	twin(ev->frame, 4, reinterpret_cast<const void**>(&A.frame), reinterpret_cast<const void**>(&B.frame));
+	twin(ev->motion_frame, 4, reinterpret_cast<const void**>(&A.motion_frame), reinterpret_cast<const void**>(&B.motion_frame));
+	twin(ev->measurement, 4, reinterpret_cast<const void**>(&A.measurement), reinterpret_cast<const void**>(&B.measurement));
+	twin(ev->sens, 4, reinterpret_cast<const void**>(&A.sens), reinterpret_cast<const void**>(&B.sens));
+	twin(ev->att, 4, reinterpret_cast<const void**>(&A.att), reinterpret_cast<const void**>(&B.att));
+	twin(ev->additive, 4, reinterpret_cast<const void**>(&A.additive), reinterpret_cast<const void**>(&B.additive));
+	void *perm = nullptr, *perm2 = nullptr, *em = nullptr;
+	const uint64_t J = static_cast<uint64_t>(h->P.g.nvox) * h->ip.nt;
+	ok = ok && alloc(n * 8, &perm) && alloc(n * 8, &perm2) && alloc(J * 4, &em);
+	if (!ok)
+	{
+		release();
+		return fail(YRTB_ERR_CUDA, "autotune: device allocation failed");
+	}
+	// Sample = events 0, S, 2S, ... (subset 0 of the interleaved subsets).
+	k_iota_stride<<<gridFor(n, 8), kBlock, 0, st>>>(
+	    static_cast<unsigned long long*>(perm), n, S);
+	yrtb_events src = *ev;
+	src.count = n;
+	if ((s = yrtb_events_gather(&src, static_cast<uint64_t*>(perm), &A, stream)) != YRTB_OK)
+	{
+		release();
+		return s;
+	}
+	cudaMemsetAsync(em, 0, J * 4, st);
+
+	std::vector<yrtb_launch_config> cands;
+	const bool split = h->comp && !h->det;
+	for (int shift : {2, 3, 4, 5})
+		for (int block : {128, 256, 512})
+			for (int tpl : {1, 2, 4})
+				if ((tpl == 1 || split) && (!h->det || (block == 256 && tpl == 1)))
+					cands.push_back(yrtb_launch_config{block, tpl, shift});
+	const yrtb_launch_config saved = h->launch;
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	const yrtb_range r{0, 1, n};
+	int bestIdx = -1;
+	int lastShift = -1;
+	for (const yrtb_launch_config& c : cands)
+	{
+		if (c.bucket_shift != lastShift)
+		{
+			lastShift = c.bucket_shift;
+			if ((s = orderEvents(h, &A, 1, c.bucket_shift, static_cast<uint64_t*>(perm2), st)) != YRTB_OK ||
+			    (s = yrtb_events_gather(&A, static_cast<uint64_t*>(perm2), &B, stream)) != YRTB_OK)
+				break;
+		}
+		h->launch = c;
+		float best = 3.4e38f;
+		for (int rep = 0; rep < 4 && s == YRTB_OK; rep++)
+		{
+			cudaEventRecord(e0, st);
+			s = yrtb_em_step(h, d_image, static_cast<float*>(em), &B, r, 1.f, 1e-35f, stream);
+			cudaEventRecord(e1, st);
+			const cudaError_t ce = cudaEventSynchronize(e1);
+			if (ce != cudaSuccess)
+				s = fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+			float ms = 0.f;
+			if (s == YRTB_OK && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+				best = std::min(best, ms);  // rep 0 warms up
+		}
+		if (s != YRTB_OK)
+			break;
+		const int i = report->num_tried++;
+		report->tried[i] = c;
+		report->ms[i] = best;
+		if (bestIdx < 0 || best < report->ms[bestIdx])
+			bestIdx = i;
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	release();
+	h->launch = bestIdx >= 0 ? report->tried[bestIdx] : saved;
+	report->best = h->launch;
+	report->sample_events = n;
+	if (s != YRTB_OK)
+		return s;
+	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
 

@@ -49,7 +49,8 @@ class yrtb_projector_params(ctypes.Structure):
                 ("tof_fwhm_ps", c_f), ("tof_n_std", ctypes.c_int),
                 ("psf_num_s", ctypes.c_int), ("psf_size", ctypes.c_int),
                 ("psf_s_step", c_f), ("psf_k_spacing", c_f),
-                ("psf_taps", c_vp), ("precision", ctypes.c_int)]
+                ("psf_taps", c_vp), ("precision", ctypes.c_int),
+                ("deterministic", ctypes.c_int)]
 
 
 class yrtb_events(ctypes.Structure):
@@ -71,6 +72,21 @@ class yrtb_osem_params(ctypes.Structure):
                 ("subset_offsets", c_vp)]
 
 
+class yrtb_launch_config(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int), ("threads_per_lor", ctypes.c_int),
+                ("bucket_shift", ctypes.c_int)]
+
+
+YRTB_TUNE_MAX = 64
+
+
+class yrtb_tune_report(ctypes.Structure):
+    _fields_ = [("best", yrtb_launch_config), ("num_tried", ctypes.c_int),
+                ("sample_events", c_u64),
+                ("tried", yrtb_launch_config * YRTB_TUNE_MAX),
+                ("ms", c_f * YRTB_TUNE_MAX)]
+
+
 # (name, argtypes) of every entry point of include/yrt_b200.h.
 _P = ctypes.POINTER
 SIGNATURES = {
@@ -83,6 +99,10 @@ SIGNATURES = {
                                _P(yrtb_projector_params), _P(c_vp)],
                               ctypes.c_int),
     "yrtb_projector_destroy": ([c_vp], None),
+    "yrtb_projector_set_launch": ([c_vp, _P(yrtb_launch_config)], ctypes.c_int),
+    "yrtb_projector_get_launch": ([c_vp, _P(yrtb_launch_config)], ctypes.c_int),
+    "yrtb_autotune": ([c_vp, c_vp, _P(yrtb_events), ctypes.c_int, c_u64,
+                       _P(yrtb_tune_report), c_vp], ctypes.c_int),
     "yrtb_multiray_offsets": ([c_vp, c_u64, c_vp, c_vp], ctypes.c_int),
     "yrtb_forward": ([c_vp, c_vp, _P(yrtb_events), yrtb_range, c_vp, c_vp],
                      ctypes.c_int),

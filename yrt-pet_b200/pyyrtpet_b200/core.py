@@ -211,6 +211,8 @@ class ProjectorParams:
         self.projPsf_fname = ""
         self.updaterType = "DEFAULT4D"
         self.precision = L.YRTB_MIRROR
+        # Two-pass fixed-point back projection (order-independent results).
+        self.deterministic = False
         self._tofWidth_ps = 0.0
         self._tofNumStd = 0
         self._psf = None
@@ -258,7 +260,7 @@ class ProjectorParams:
         p = L.yrtb_projector_params(
             L.YRTB_SIDDON if self.projectorType == "S" else L.YRTB_DD,
             int(self.numRays), self._tofWidth_ps, self._tofNumStd, 0, 0, 0.0,
-            0.0, None, int(self.precision))
+            0.0, None, int(self.precision), int(bool(self.deterministic)))
         if psf is not None:
             s_step, k_spacing, taps = psf
             keep = np.ascontiguousarray(taps, np.float32)
@@ -727,6 +729,35 @@ class DeviceProjector:
                                      float(global_scale),
                                      float(denom_threshold), _stream()))
         return em
+
+    # ------------------------------------------------ launch configuration --
+    def set_launch(self, block: int = 256, threads_per_lor: int = 1,
+                   bucket_shift: int = 3):
+        c = L.yrtb_launch_config(int(block), int(threads_per_lor), int(bucket_shift))
+        L.check(L.lib().yrtb_projector_set_launch(self.h, ctypes.byref(c)))
+
+    def get_launch(self) -> dict:
+        c = L.yrtb_launch_config()
+        L.check(L.lib().yrtb_projector_get_launch(self.h, ctypes.byref(c)))
+        return {"block": c.block, "threads_per_lor": c.threads_per_lor,
+                "bucket_shift": c.bucket_shift}
+
+    def autotune(self, img, ev: DeviceEvents, num_subsets: int = 1,
+                 max_sample: int = 2_000_000) -> dict:
+        """Time the fused EM step over a sample of the events for every launch
+        configuration this projector admits and keep the fastest
+        (yrtb_autotune).  Returns {"best": cfg, "sample_events": n,
+        "tried": [(cfg, ms), ...]}."""
+        self._check_image(img)
+        rep = L.yrtb_tune_report()
+        L.check(L.lib().yrtb_autotune(self.h, img.data_ptr(), ctypes.byref(ev.c()),
+                                      int(num_subsets), int(max_sample),
+                                      ctypes.byref(rep), _stream()))
+        cfg = lambda c: {"block": c.block, "threads_per_lor": c.threads_per_lor,
+                         "bucket_shift": c.bucket_shift}
+        return {"best": cfg(rep.best), "sample_events": int(rep.sample_events),
+                "tried": [(cfg(rep.tried[i]), float(rep.ms[i]))
+                          for i in range(rep.num_tried)]}
 
     def order_events(self, ev: DeviceEvents, num_subsets: int):
         """Subset-major, LOR-sorted copy of the events (yrtb_events_subset_order

@@ -44,6 +44,11 @@ class OSEM_GPU:
         # coherence); results differ from file order only by FP summation
         # order.
         self.orderEvents = True
+        # Pick the launch configuration (block size, threads per LOR, ray
+        # length binning of the event order) by timing EM steps over a sample
+        # of the events before reconstructing (yrtb_autotune).
+        self.autotune = False
+        self.lastTuneReport = None
         self._data = None
         self._sens_images: List[torch.Tensor] = []
         self._sens_histo = None
@@ -148,6 +153,7 @@ class OSEM_GPU:
         pp.projPsf_fname = self.projectorParams.projPsf_fname
         pp._psf = self.projectorParams._psf
         pp.precision = self.projectorParams.precision
+        pp.deterministic = self.projectorParams.deterministic
         return DeviceProjector(self.scanner, self.imageParams.withFrames(1), pp)
 
     def _histo_dev(self, h):
@@ -239,6 +245,11 @@ class OSEM_GPU:
         proj = DeviceProjector(self.scanner, ip, self.projectorParams)
         ev = self._listmode_events(proj, lm)
         offsets = None
+        if self.autotune:
+            probe = torch.full(ip.shape, self.INITIAL_VALUE_MLEM,
+                               dtype=torch.float32, device="cuda")
+            self.lastTuneReport = proj.autotune(probe, ev, self.num_OSEM_subsets)
+            del probe
         if self.orderEvents:
             ev, offsets = proj.order_events(ev, self.num_OSEM_subsets)
         J = ip.numVoxels
