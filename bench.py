@@ -51,6 +51,13 @@ def parse():
     ap.add_argument("--precision", default="compensated",
                     choices=["mirror", "compensated"])
     ap.add_argument("--parity-sample", type=int, default=200_000)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch configuration instead of "
+                         "timing the candidates on a sample first")
+    ap.add_argument("--tune-report", default="",
+                    help="write every autotuner candidate and its time (JSON)")
+    ap.add_argument("--deterministic", action="store_true",
+                    help="two-pass fixed-point back projection")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default) is the headline workload; the others "
                          "run bench_configs.py")
@@ -257,6 +264,7 @@ def main():
     pp.addTOF(TOF_FWHM, TOF_NSTD)
     pp.precision = (L.YRTB_COMPENSATED if args.precision == "compensated"
                     else L.YRTB_MIRROR)
+    pp.deterministic = bool(args.deterministic)
     proj = yrt.DeviceProjector(sc, ip, pp)
     # Correction factors per event, on device (sens = eff1*eff2 histogram
     # gather is equivalent to the direct product here; ACF via Siddon
@@ -283,6 +291,17 @@ def main():
     img = torch.full((J,), 0.125, device="cuda")
     img.mul_((sens > 0).float())
     em = torch.zeros(J, device="cuda")
+
+    # Launch configuration: timed on a sample of subset 0 (setup, not timed;
+    # a calibration done once per projector, like a library's algorithm
+    # search), then used by the ordered and end-to-end forms.
+    tune = None
+    if not args.no_autotune:
+        tune = proj.autotune(img, ev, SUBSETS)
+        if args.tune_report and rank == 0:
+            with open(args.tune_report, "w") as f:
+                json.dump(tune, f, indent=1)
+    launch = proj.get_launch()
 
     # Plain form: events in file order, subset = interleaved stride (the
     # reference's batching).  Ordered form: subset-major, LOR-sorted copy.
@@ -365,7 +384,10 @@ def main():
     value = total_events / (ms * 1e-3)
     timed_launches = launches[0]
 
-    # Plain (file-order) form on the same GPU, for the batched-vs-plain ratio.
+    # Plain (file-order) form on the same GPU, for the batched-vs-plain ratio,
+    # with the reference's launch shape (one thread per event, 256-thread
+    # blocks).
+    proj.set_launch(256, 1, launch["bucket_shift"])
     for _ in range(1):
         step(plain=True)
     pa = torch.cuda.Event(enable_timing=True)
@@ -380,6 +402,7 @@ def main():
         tt = torch.tensor([plain_ms], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         plain_ms = tt.item()
+    proj.set_launch(**launch)
 
     # ---- e2e: public OSEM API from pinned host buffers (1 iteration/step).
     e2e = None
@@ -487,6 +510,15 @@ def main():
                                        "10 subsets",
                            "events_per_gpu": ev.count, "subsets": SUBSETS,
                            "precision": args.precision,
+                           "deterministic": bool(args.deterministic),
+                           "launch": launch,
+                           "autotune": None if tune is None else {
+                               "sample_events": tune["sample_events"],
+                               "candidates": len(tune["tried"]),
+                               "best_ms": min(ms for _, ms in tune["tried"]) if tune["tried"] else None,
+                               "default_ms": next((ms for c, ms in tune["tried"]
+                                                   if c == {"block": 256, "threads_per_lor": 1,
+                                                            "bucket_shift": 3}), None)},
                            "l2": "event arrays (1.2 GB) larger than L2; "
                                  "image (42 MB) L2-resident by design",
                            "parallelism": f"dp{world} (events sharded, EM image "

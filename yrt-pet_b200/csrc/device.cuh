@@ -298,19 +298,21 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	const float fdz = static_cast<float>(dir_z) * dz;
 
 	// 3. Incremental walk: step to the nearest crossing; ties step together
-	// (<= on the crossing values from the start of the step).  Written with
-	// selects instead of branches so that the threads of a warp, whose rays
-	// step along different axes, stay converged; every value is the one the
-	// branchy formulation computes.  A ray crosses at most nx+ny+nz+3 planes
-	// inside the grid; the step cap only guards against non-finite input.
+	// (<= on the crossing values from the start of the step, i.e. every axis
+	// whose crossing equals the minimum).  Written with selects instead of
+	// branches so that the threads of a warp, whose rays step along different
+	// axes, stay converged; every value is the one the branchy formulation
+	// computes.  Every segment moves the voxel along at least one axis, always
+	// the same way, so the walk leaves the grid after at most nx+ny+nz
+	// segments; the step cap bounds the zero-length steps in between.
 	const int maxSteps = 2 * (nx + ny + nz) + 16;
-	auto advance = [&]() -> int
+	auto advance = [&](bool& sx, bool& sy, bool& sz)
 	{
 		const float ax = ax_next, ay = ay_next, az = az_next;
-		const bool sx = (ax <= ay) && (ax <= az);
-		const bool sy = (ay <= ax) && (ay <= az);
-		const bool sz = (az <= ax) && (az <= ay);
-		a_next = sz ? az : (sy ? ay : (sx ? ax : a_next));
+		const float m = fminf(fminf(ax, ay), az);
+		sx = ax == m;
+		sy = ay == m;
+		sz = az == m;
 		const float xn = x_cur + fdx, yn = y_cur + fdy, zn = z_cur + fdz;
 		const float axn = (xn - p1.x) * inv_x;
 		const float ayn = (yn - p1.y) * inv_y;
@@ -321,44 +323,51 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		ax_next = sx ? axn : ax_next;
 		ay_next = sy ? ayn : ay_next;
 		az_next = sz ? azn : az_next;
-		a_next = (a_next > amax) ? amax : a_next;
-		return (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
+		a_next = fminf(m, amax);
 	};
 	// TOF kernel centre along the LOR (mm from p1), loop invariant.
 	const float pc = TOF ? tofCenter(d_norm, tofValue) : 0.f;
 	const float inv_sigma = TOF ? 1.0f / tp.sigma : 0.f;
-	auto emit = [&]()
+	// Compensated TOF weight, per segment [a, b]:
+	//   (b - a) * L * norm * 2^(-x^2 log2(e) / 2),  x = ((a + b) L/2 - pc) / sigma
+	// with x = (a + b) * hs - pcs in one fused multiply-add and the hardware
+	// base-2 exponential (relative error below 2^-21).
+	const float hs = 0.5f * d_norm * inv_sigma;
+	const float pcs = pc * inv_sigma;
+	const float dnn = d_norm * tp.norm;
+	auto emit = [&](int o)
 	{
-		float w = (a_next - a_cur) * d_norm;
-		if constexpr (TOF)
+		float w;
+		if constexpr (TOF && COMP)
 		{
-			if constexpr (COMP)
-			{
-				// Gaussian at the segment midpoint with a multiply by 1/sigma
-				// and the fast exponential (<= 2 + 1.2|x| ulp); the error of
-				// the projection stays far below the FP64 budget.
-				const float xc = (0.5f * (a_cur + a_next) * d_norm - pc) * inv_sigma;
-				w *= __expf(-0.5f * xc * xc) * tp.norm;
-			}
-			else
-			{
-				const float lo = a_cur * d_norm, hi = a_next * d_norm;
-				const float xc = (0.5f * (lo + hi) - pc) / tp.sigma;
-				w *= expf(-0.5f * xc * xc) * tp.norm;
-			}
+			const float xc = __fmaf_rn(a_cur + a_next, hs, -pcs);
+			float g2;
+			asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(g2) : "f"(xc * xc * -0.72134752044448170f));
+			w = (a_next - a_cur) * dnn * g2;
 		}
-		visit(vx + off, w);
+		else
+		{
+			w = (a_next - a_cur) * d_norm;
+		}
+		if constexpr (TOF && !COMP)
+		{
+			// The reference's expression order (TimeOfFlight.hpp:74-84).
+			const float lo = a_cur * d_norm, hi = a_next * d_norm;
+			const float xc = (0.5f * (lo + hi) - pc) / tp.sigma;
+			w *= expf(-0.5f * xc * xc) * tp.norm;
+		}
+		visit(o, w);
 		a_cur = a_next;
 	};
 
 	// First non-empty segment: its voxel comes from the segment midpoint.
 	int step = 0;
-	int dir_next = 0;
+	bool sx = false, sy = false, sz = false;
 	for (;; step++)
 	{
 		if (!(a_cur < amax) || step >= maxSteps)
 			return;
-		dir_next = advance();
+		advance(sx, sy, sz);
 		if (a_cur < a_next)
 			break;
 	}
@@ -391,9 +400,9 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 				const int ip = static_cast<int>(rintf((pre - q0) / d));
 				v = dir > 0 ? ip - 1 : ip;
 			};
-			fromPlanes(flat_x, dir_next & 1, x_cur, fdx, x0, dx, dir_x, vx);
-			fromPlanes(flat_y, dir_next & 2, y_cur, fdy, y0, dy, dir_y, vy);
-			fromPlanes(flat_z, dir_next & 4, z_cur, fdz, z0, dz, dir_z, vz);
+			fromPlanes(flat_x, sx, x_cur, fdx, x0, dx, dir_x, vx);
+			fromPlanes(flat_y, sy, y_cur, fdy, y0, dy, dir_y, vy);
+			fromPlanes(flat_z, sz, z_cur, fdz, z0, dz, dir_z, vz);
 		}
 	}
 	else
@@ -405,27 +414,62 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	}
 	if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
 		return;
-	off = vz * nxy + vy * nx;
-	dir_prev = dir_next;
-	emit();
 
 	// Following segments: move the voxel along the axes stepped last time.
-	for (; a_cur < amax && step < maxSteps; step++)
+	if constexpr (COMP)
 	{
-		dir_next = advance();
-		if (a_cur >= a_next)
-			continue;
-		const int mx = dir_prev & 1, my = (dir_prev >> 1) & 1, mz = (dir_prev >> 2) & 1;
-		vx += mx * dir_x;
-		vy += my * dir_y;
-		vz += mz * dir_z;
-		off += my * dir_y * nx + mz * dir_z * nxy;
-		if (static_cast<unsigned>(vx) >= static_cast<unsigned>(nx) ||
-		    static_cast<unsigned>(vy) >= static_cast<unsigned>(ny) ||
-		    static_cast<unsigned>(vz) >= static_cast<unsigned>(nz))
-			break;
-		dir_prev = dir_next;
-		emit();
+		// Linear voxel index moved by a per-step delta.  The walk ends at the
+		// grid exit (amax); only a rounding-sized last segment can step past
+		// a face, and the index check keeps every access inside the image
+		// (such a segment adds a weight of ~1e-4 mm to a neighbouring voxel
+		// where the mirror walk stops).
+		const int dny = dir_y * nx, dnz = dir_z * nxy;
+		const unsigned nvox = static_cast<unsigned>(nxy * nz);
+		int lin = vz * nxy + vy * nx + vx;
+		int dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
+		emit(lin);
+		while (a_cur < amax)
+		{
+			advance(sx, sy, sz);
+			if (a_cur >= a_next)
+			{
+				if (++step >= maxSteps)
+					break;
+				continue;
+			}
+			lin += dprev;
+			if (static_cast<unsigned>(lin) >= nvox)
+				break;
+			dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
+			emit(lin);
+		}
+	}
+	else
+	{
+		off = vz * nxy + vy * nx;
+		dir_prev = (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
+		emit(vx + off);
+		while (a_cur < amax)
+		{
+			advance(sx, sy, sz);
+			if (a_cur >= a_next)
+			{
+				if (++step >= maxSteps)
+					break;
+				continue;
+			}
+			const int mx = dir_prev & 1, my = (dir_prev >> 1) & 1, mz = (dir_prev >> 2) & 1;
+			vx += mx * dir_x;
+			vy += my * dir_y;
+			vz += mz * dir_z;
+			off += my * dir_y * nx + mz * dir_z * nxy;
+			if (static_cast<unsigned>(vx) >= static_cast<unsigned>(nx) ||
+			    static_cast<unsigned>(vy) >= static_cast<unsigned>(ny) ||
+			    static_cast<unsigned>(vz) >= static_cast<unsigned>(nz))
+				break;
+			dir_prev = (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
+			emit(vx + off);
+		}
 	}
 }
 

@@ -401,17 +401,16 @@ __device__ __forceinline__ float forwardEvent(const KParams& P,
 	{
 		if constexpr (TRACK)
 			mw = fmaxf(mw, fabsf(w));
-		const float term = w * __ldg(img + o);
 		if constexpr (COMP)
 		{
-			const float y = term - comp;
+			const float y = __fmaf_rn(w, __ldg(img + o), -comp);
 			const float t = ray + y;
 			comp = (t - ray) - y;
 			ray = t;
 		}
 		else
 		{
-			ray += term;
+			ray += w * __ldg(img + o);
 		}
 	};
 	auto endRay = [&]
