@@ -491,12 +491,15 @@ def test_event_ordering_is_subset_major_permutation():
     assert rel_l2(em_b.cpu().numpy(), em_a.cpu().numpy()) < 1e-5
 
 
+@pytest.mark.parametrize("precision", [L.YRTB_MIRROR, L.YRTB_COMPENSATED])
 @pytest.mark.parametrize("support", ["cylinder", "offcentre", "empty"])
-def test_attenuation_factors_vs_oracle(support):
+def test_attenuation_factors_vs_oracle(support, precision):
     from pyyrtpet_b200 import synthetic as S
     sc = S.scanner_c1()
     ip = yrt.ImageParams(64, 64, 32, 256, 256, 128)
-    p = yrt.DeviceProjector(sc, ip, yrt.ProjectorParams(sc))
+    pp = yrt.ProjectorParams(sc)
+    pp.precision = precision
+    p = yrt.DeviceProjector(sc, ip, pp)
     evs = S.generate_events(sc, 30000, 91)
     e = evs.numpy()
     mu = S.Phantom(cyl_half_length=32).mu_image(ip).numpy()

@@ -473,6 +473,69 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	}
 }
 
+// Number of voxel crossings of the single-ray Siddon walk, estimated in O(1):
+// one plus the planes of each axis inside the ray's window (FOV cylinder,
+// image slabs, TOF window).  Ties (planes crossed together) count once per
+// axis here and once in the walk, so the estimate can exceed the walk's
+// count by the number of ties.  Used to group rays of similar length.
+template <bool TOF>
+__device__ __forceinline__ unsigned crossingEstimate(const Geom& g, float3 p1,
+                                                     float3 p2, const TofP& tp,
+                                                     float tofValue)
+{
+	const float ddx = p2.x - p1.x, ddy = p2.y - p1.y, ddz = p2.z - p1.z;
+	const float A = ddx * ddx + ddy * ddy;
+	float t0 = 0.f, t1 = 1.f;
+	if (A != 0.f)
+	{
+		const float B = 2.0f * (ddx * p1.x + ddy * p1.y);
+		const float C = p1.x * p1.x + p1.y * p1.y - g.fovRadius * g.fovRadius;
+		const float D = B * B - 4.0f * A * C;
+		if (D <= 0.f)
+			return 0u;
+		const float sq = sqrtf(D);
+		t0 = (-B - sq) / (2.0f * A);
+		t1 = (-B + sq) / (2.0f * A);
+	}
+	float amin = fmaxf(0.f, t0), amax = fminf(1.f, t1);
+	auto slab = [&](float p, float d, float half)
+	{
+		if (d != 0.f)
+		{
+			const float inv = 1.0f / d;
+			const float a0 = (-half - p) * inv, a1 = (half - p) * inv;
+			amin = fmaxf(amin, fminf(a0, a1));
+			amax = fminf(amax, fmaxf(a0, a1));
+		}
+		else if (p < -half || p > half)
+		{
+			amax = -1.f;
+		}
+	};
+	slab(p1.x, ddx, 0.5f * g.lx);
+	slab(p1.y, ddy, 0.5f * g.ly);
+	slab(p1.z, ddz, 0.5f * g.lz);
+	if constexpr (TOF)
+	{
+		float a0, a1;
+		tofAlphaRange(tp, sqrtf(A + ddz * ddz), tofValue, a0, a1);
+		amin = fmaxf(amin, a0);
+		amax = fminf(amax, a1);
+	}
+	if (!(amin < amax))
+		return 0u;
+	auto planes = [&](float p, float d, float q0, float dq) -> unsigned
+	{
+		if (d == 0.f)
+			return 0u;
+		const float u = floorf((p + amin * d - q0) / dq);
+		const float v = floorf((p + amax * d - q0) / dq);
+		return static_cast<unsigned>(fabsf(v - u));
+	};
+	return 1u + planes(p1.x, ddx, -0.5f * g.lx, g.vx) +
+	       planes(p1.y, ddy, -0.5f * g.ly, g.vy) + planes(p1.z, ddz, -0.5f * g.lz, g.vz);
+}
+
 // Parametric window of the ray p1 -> p2 inside the box of voxels
 // [b[0], b[3]] x [b[1], b[4]] x [b[2], b[5]] (inclusive) of grid g; an empty
 // box or a miss gives wlo > whi.

@@ -722,6 +722,24 @@ __global__ void k_fixed_finish(const unsigned long long* __restrict__ acc,
 	}
 }
 
+// Estimated crossings per event (crossingEstimate) for the event ordering.
+template <bool TOF>
+__global__ void k_count_estimate(KParams P, Events E, uint64_t n,
+                                 uint32_t* __restrict__ out)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t e = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     e < n; e += nthreads)
+	{
+		const int frame = E.frame ? __ldg(E.frame + e) : 0;
+		float3 p1, p2, n1, n2;
+		uint32_t c = 0;
+		if (frame >= 0 && frame < P.g.nt && fetchEvent(P, E, e, p1, p2, n1, n2))
+			c = crossingEstimate<TOF>(P.g, p1, p2, P.tof, TOF ? __ldg(E.tof + e) : 0.f);
+		out[e] = c;
+	}
+}
+
 __global__ void k_box_init(int* box)
 {
 	if (threadIdx.x < 6)
@@ -765,7 +783,9 @@ __global__ void k_support_box(const float* __restrict__ img, Geom g, int* box)
 	}
 }
 
-// Attenuation factor per event: exp(-0.1 * line integral of mu).
+// Attenuation factor per event: exp(-0.1 * line integral of mu), walked with
+// the projector's arithmetic (COMP: compensated walk).
+template <bool COMP>
 __global__ void __launch_bounds__(kBlock)
     k_attenuation(KParams P, Geom mu, Events E, Range R,
                   const float* __restrict__ muImg, const int* __restrict__ box,
@@ -797,7 +817,7 @@ __global__ void __launch_bounds__(kBlock)
 		float acc = 0.f;
 		auto visit = [&](int o, float w) { acc += w * __ldg(muImg + o); };
 		if (wlo < whi)
-			siddonWalk<false, false>(mu, p1, p2, P.tof, 0.f, visit, wlo, whi);
+			siddonWalk<false, COMP>(mu, p1, p2, P.tof, 0.f, visit, wlo, whi);
 		out[e] = expf(-acc * 0.1f);
 	}
 }
@@ -987,6 +1007,35 @@ __global__ void k_iota_stride(unsigned long long* __restrict__ perm, uint64_t n,
 	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
 	     i < n; i += nthreads)
 		perm[i] = i * stride;
+}
+
+// All 32-bit event arrays of a permutation in one pass: one perm read per
+// event and up to nine independent loads in flight per thread.
+struct GatherSet
+{
+	const uint32_t* src[9];
+	uint32_t* dst[9];
+	int count;
+};
+
+__global__ void k_gather_set(GatherSet G, const unsigned long long* __restrict__ perm,
+                             uint64_t n)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+	{
+		const unsigned long long p = __ldg(perm + i);
+		uint32_t v[9];
+#pragma unroll
+		for (int a = 0; a < 9; a++)
+			if (a < G.count)
+				v[a] = __ldg(G.src[a] + p);
+#pragma unroll
+		for (int a = 0; a < 9; a++)
+			if (a < G.count)
+				G.dst[a][i] = v[a];
+	}
 }
 
 template <typename T>
@@ -1204,6 +1253,49 @@ unsigned gridFor(uint64_t n, int perSM = 8)
 	const uint64_t need = (n + kBlock - 1) / kBlock;
 	const uint64_t cap = static_cast<uint64_t>(g_numSMs) * perSM;
 	return static_cast<unsigned>(std::max<uint64_t>(1, std::min(need, cap)));
+}
+
+// Temporaries of the event ordering, the attenuation factors and the
+// autotuner come from a stream-ordered pool the library keeps per device,
+// with freed blocks retained for later calls (the default pool returns them
+// to the driver at every synchronisation, and re-mapping a gigabyte of
+// ordering keys costs more than the sort itself).
+cudaError_t poolAlloc(void** p, size_t bytes, cudaStream_t st)
+{
+	constexpr int kMaxDevices = 64;
+	static std::mutex lock;
+	static cudaMemPool_t pools[kMaxDevices] = {};
+	int dev = 0;
+	cudaError_t e = cudaGetDevice(&dev);
+	if (e != cudaSuccess)
+		return e;
+	if (dev < 0 || dev >= kMaxDevices)
+		return cudaMallocAsync(p, bytes, st);
+	{
+		std::lock_guard<std::mutex> guard(lock);
+		if (pools[dev] == nullptr)
+		{
+			cudaMemPoolProps props{};
+			props.allocType = cudaMemAllocationTypePinned;
+			props.location.type = cudaMemLocationTypeDevice;
+			props.location.id = dev;
+			cudaMemPool_t pool = nullptr;
+			if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess)
+				return e;
+			uint64_t keep = ~uint64_t(0);
+			if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) !=
+			    cudaSuccess)
+				return e;
+			pools[dev] = pool;
+		}
+	}
+	return cudaMallocFromPoolAsync(p, bytes, pools[dev], st);
+}
+
+template <typename T>
+cudaError_t poolAlloc(T** p, size_t bytes, cudaStream_t st)
+{
+	return poolAlloc(reinterpret_cast<void**>(p), bytes, st);
 }
 
 Geom makeGeom(const yrtb_image_params& ip)
@@ -1554,30 +1646,27 @@ yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
 		cudaFreeAsync(vals, st);
 		cudaFreeAsync(temp, st);
 	};
-	cudaError_t ce = cudaMallocAsync(&keys, n * 8, st);
+	cudaError_t ce = poolAlloc(&keys, n * 8, st);
 	if (ce == cudaSuccess)
-		ce = cudaMallocAsync(&keys2, n * 8, st);
+		ce = poolAlloc(&keys2, n * 8, st);
 	if (ce == cudaSuccess)
-		ce = cudaMallocAsync(&vals, n * 8, st);
+		ce = poolAlloc(&vals, n * 8, st);
 	if (ce != cudaSuccess)
 	{
 		release();
 		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
 	}
-	// Crossing counts of the single-ray Siddon projector (into keys2, which
-	// the sort overwrites afterwards).
+	// Estimated crossings of the single-ray Siddon walk (into keys2, which
+	// the sort overwrites afterwards): O(1) per event instead of a walk.
 	const uint32_t* counts = nullptr;
 	if (h->kind == K_SIDDON && (!h->hasTof || ev->tof_ps))
 	{
-		const yrtb_status cs = dispatchEvents<OP_COUNT>(
-		    h, ev, yrtb_range{0, 1, n}, nullptr, reinterpret_cast<float*>(keys2),
-		    1.f, 0.f, reinterpret_cast<yrtb_stream>(st));
-		if (cs != YRTB_OK)
-		{
-			release();
-			return cs;
-		}
-		counts = reinterpret_cast<const uint32_t*>(keys2);
+		uint32_t* c32 = reinterpret_cast<uint32_t*>(keys2);
+		if (h->hasTof)
+			k_count_estimate<true><<<gridFor(n, 16), kBlock, 0, st>>>(h->P, toDev(ev), n, c32);
+		else
+			k_count_estimate<false><<<gridFor(n, 16), kBlock, 0, st>>>(h->P, toDev(ev), n, c32);
+		counts = c32;
 	}
 	// LOR keys wider than their field keep their high bits.
 	const int lorBits = ev->frame ? 29 : 33;
@@ -1595,7 +1684,7 @@ yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
 	                                     reinterpret_cast<unsigned long long*>(d_perm),
 	                                     n, 0, 64, st);
 	if (ce == cudaSuccess)
-		ce = cudaMallocAsync(&temp, tempBytes, st);
+		ce = poolAlloc(&temp, tempBytes, st);
 	if (ce == cudaSuccess)
 		ce = cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals,
 		                                     reinterpret_cast<unsigned long long*>(d_perm),
@@ -1901,15 +1990,28 @@ yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
 		    const_cast<uint32_t*>(static_cast<const uint32_t*>(b)));
 		return YRTB_OK;
 	};
+	GatherSet G{};
+	auto add = [&](const void* a, const void* b) -> yrtb_status
+	{
+		if (a == nullptr)
+			return YRTB_OK;
+		if (b == nullptr)
+			return fail(YRTB_ERR_ARGUMENT, "gather output array missing");
+		G.src[G.count] = static_cast<const uint32_t*>(a);
+		G.dst[G.count] = const_cast<uint32_t*>(static_cast<const uint32_t*>(b));
+		G.count++;
+		return YRTB_OK;
+	};
 	yrtb_status r;
-	if ((r = g32(in->d1, out->d1, 1)) || (r = g32(in->d2, out->d2, 1)) ||
-	    (r = g32(in->lor, out->lor, 6)) || (r = g32(in->tof_ps, out->tof_ps, 1)) ||
-	    (r = g32(in->frame, out->frame, 1)) ||
-	    (r = g32(in->motion_frame, out->motion_frame, 1)) ||
-	    (r = g32(in->measurement, out->measurement, 1)) ||
-	    (r = g32(in->sens, out->sens, 1)) || (r = g32(in->att, out->att, 1)) ||
-	    (r = g32(in->additive, out->additive, 1)))
+	if ((r = add(in->d1, out->d1)) || (r = add(in->d2, out->d2)) ||
+	    (r = add(in->tof_ps, out->tof_ps)) || (r = add(in->frame, out->frame)) ||
+	    (r = add(in->motion_frame, out->motion_frame)) ||
+	    (r = add(in->measurement, out->measurement)) ||
+	    (r = add(in->sens, out->sens)) || (r = add(in->att, out->att)) ||
+	    (r = add(in->additive, out->additive)) || (r = g32(in->lor, out->lor, 6)))
 		return r;
+	if (G.count > 0)
+		k_gather_set<<<gridFor(n, 16), kBlock, 0, st>>>(G, perm, n);
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
@@ -1982,12 +2084,16 @@ yrtb_status yrtb_attenuation_factors(yrtb_projector* h, const float* d_mu,
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	const Geom mg = makeGeom(*mu_params);
 	int* d_box = nullptr;
-	YRTB_CUDA(cudaMallocAsync(&d_box, 6 * sizeof(int), st));
+	YRTB_CUDA(poolAlloc(&d_box, 6 * sizeof(int), st));
 	k_box_init<<<1, 32, 0, st>>>(d_box);
 	k_support_box<<<gridFor(mg.nvox, 4), kBlock, 0, st>>>(d_mu, mg, d_box);
-	k_attenuation<<<gridAll(range.count), kBlock, 0, st>>>(
-	    h->P, mg, toDev(ev), Range{range.start, range.stride, range.count},
-	    d_mu, d_box, d_out, h->d_err);
+	const Range R{range.start, range.stride, range.count};
+	if (h->comp)
+		k_attenuation<true><<<gridAll(range.count), kBlock, 0, st>>>(
+		    h->P, mg, toDev(ev), R, d_mu, d_box, d_out, h->d_err);
+	else
+		k_attenuation<false><<<gridAll(range.count), kBlock, 0, st>>>(
+		    h->P, mg, toDev(ev), R, d_mu, d_box, d_out, h->d_err);
 	YRTB_LAUNCHED();
 	YRTB_CUDA(cudaFreeAsync(d_box, st));
 	return YRTB_OK;
@@ -2055,7 +2161,7 @@ yrtb_status yrtb_listmode_to_histo3d(yrtb_projector* h, const uint32_t* d1,
 	YRTB_CUDA(cudaSetDevice(h->device));
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	unsigned long long* d_bad = nullptr;
-	YRTB_CUDA(cudaMallocAsync(&d_bad, sizeof(unsigned long long), st));
+	YRTB_CUDA(poolAlloc(&d_bad, sizeof(unsigned long long), st));
 	YRTB_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), st));
 	if (n > 0)
 	{
@@ -2091,7 +2197,7 @@ yrtb_status yrtb_unpack_listmode(const void* d_raw, uint64_t n, int has_tof,
 		return YRTB_OK;
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	unsigned long long* d_bad = nullptr;
-	YRTB_CUDA(cudaMallocAsync(&d_bad, sizeof(unsigned long long), st));
+	YRTB_CUDA(poolAlloc(&d_bad, sizeof(unsigned long long), st));
 	YRTB_CUDA(cudaMemsetAsync(d_bad, 0xFF, sizeof(unsigned long long), st));
 	const int fields = 3 + (has_tof ? 1 : 0) + (has_randoms ? 1 : 0);
 	k_unpack_listmode<<<gridFor(n, 16), kBlock, 0, st>>>(
@@ -2338,7 +2444,7 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	auto alloc = [&](size_t bytes, void** out) -> bool
 	{
 		*out = nullptr;
-		if (cudaMallocAsync(out, bytes, st) != cudaSuccess)
+		if (poolAlloc(out, bytes, st) != cudaSuccess)
 			return false;
 		bufs.push_back(*out);
 		return true;

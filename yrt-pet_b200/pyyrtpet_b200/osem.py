@@ -191,11 +191,27 @@ class OSEM_GPU:
         return out
 
     # ------------------------------------------------------- reconstruct --
-    def _listmode_events(self, proj: DeviceProjector, lm: ListModeLUT):
+    def _listmode_events(self, proj: DeviceProjector, lm: ListModeLUT,
+                         order_subsets: int = 0):
+        """Device events with their correction factors.  With order_subsets,
+        the events are first put in subset-major order (yrtb_events_subset_
+        order) and the corrections are computed on the ordered arrays, so
+        that the attenuation walks also run on grouped rays; returns
+        (events, subset offsets or None)."""
         base = lm.device_events()
         ev = DeviceEvents(base.count, base.d1, base.d2, base.lor, base.tof,
                           base.frame, base.motion_frame, base.motion)
-        n = ev.count
+        if lm.randoms is not None:
+            ev.additive = base.additive if base.additive is not None else _dev(
+                lm.randoms, torch.float32)
+        offsets = None
+        if self.autotune:
+            probe = torch.full(proj.img_params.shape, self.INITIAL_VALUE_MLEM,
+                               dtype=torch.float32, device="cuda")
+            self.lastTuneReport = proj.autotune(probe, ev, max(order_subsets, 1))
+            del probe
+        if order_subsets:
+            ev, offsets = proj.order_events(ev, order_subsets)
         if self._sens_histo is not None:
             sh = self._histo_dev(self._sens_histo)
             ev.sens = proj.gather_histo3d(sh, ev, invert=self._invert_sens)
@@ -204,11 +220,8 @@ class OSEM_GPU:
         elif self._att_image is not None:
             ev.att = proj.attenuation_factors(self._att_image, self._att_params,
                                               ev)
-        add = None
-        if lm.randoms is not None:
-            add = base.additive if base.additive is not None else _dev(
-                lm.randoms, torch.float32)
-        elif self._randoms_histo is not None:
+        add = ev.additive
+        if add is None and self._randoms_histo is not None:
             add = proj.gather_histo3d(self._histo_dev(self._randoms_histo), ev)
         if self._scatter_histo is not None:
             sc = proj.gather_histo3d(self._histo_dev(self._scatter_histo), ev)
@@ -218,7 +231,7 @@ class OSEM_GPU:
             raise RuntimeError("A Line-Of-Response might not respect the "
                                "Minimum-Angle-Difference restriction of the "
                                "scanner (or a detector id is out of range)")
-        return ev
+        return ev, offsets
 
     def reconstruct(self, out_fname: str = "") -> torch.Tensor:
         if self._data is None:
@@ -243,15 +256,8 @@ class OSEM_GPU:
         nt = lm.getNumDynamicFrames()
         ip = self.imageParams.withFrames(nt)
         proj = DeviceProjector(self.scanner, ip, self.projectorParams)
-        ev = self._listmode_events(proj, lm)
-        offsets = None
-        if self.autotune:
-            probe = torch.full(ip.shape, self.INITIAL_VALUE_MLEM,
-                               dtype=torch.float32, device="cuda")
-            self.lastTuneReport = proj.autotune(probe, ev, self.num_OSEM_subsets)
-            del probe
-        if self.orderEvents:
-            ev, offsets = proj.order_events(ev, self.num_OSEM_subsets)
+        ev, offsets = self._listmode_events(
+            proj, lm, self.num_OSEM_subsets if self.orderEvents else 0)
         J = ip.numVoxels
         img = torch.empty(nt * J, dtype=torch.float32, device="cuda")
         init = 0
