@@ -370,11 +370,13 @@ def main():
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     em_events = []
+    torch.cuda.nvtx.range_push("timed")  # lets a profiler select these launches
     t0.record(st)
     for _ in range(args.steps):
         step(record=em_events)
     t1.record(st)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     if dist is not None:
         dist.barrier()
     if sampler is not None:
@@ -393,7 +395,8 @@ def main():
     # Plain (file-order) form on the same GPU, for the batched-vs-plain ratio,
     # with the reference's launch shape (one thread per event, 256-thread
     # blocks).
-    proj.set_launch(256, 1, launch["bucket_shift"])
+    proj.set_launch(256, 1, launch["bucket_shift"], launch["order"],
+                    launch["tile_shift"])
     for _ in range(1):
         step(plain=True)
     pa = torch.cuda.Event(enable_timing=True)
@@ -529,7 +532,8 @@ def main():
                                "best_ms": min(ms for _, ms in tune["tried"]) if tune["tried"] else None,
                                "default_ms": next((ms for c, ms in tune["tried"]
                                                    if c == {"block": 256, "threads_per_lor": 1,
-                                                            "bucket_shift": 3}), None)},
+                                                            "bucket_shift": 3, "order": 0,
+                                                            "tile_shift": 1}), None)},
                            "l2": "event arrays (1.2 GB) larger than L2; "
                                  "image (42 MB) L2-resident by design",
                            "parallelism": f"dp{world} (events sharded, EM image "

@@ -173,7 +173,11 @@ void yrtb_projector_destroy(yrtb_projector* h);
  * yrtb_backward, yrtb_em_step and the OSEM driver) and of the event ordering.
  * No reference counterpart: the reference launches one thread per event in
  * 256-thread blocks (GPUBatchSetup, include/yrt-pet/utils/GPUTypes.cuh:17-55)
- * on events in file order.  Default: {256, 1, 3}. */
+ * on events in file order.  Default: {256, 1, 3, YRTB_ORDER_LOR, 1}. */
+#define YRTB_ORDER_LOR 0      /* inside a ray-length bucket: by LOR (Histogram3D bin), then TOF */
+#define YRTB_ORDER_SPATIAL 1  /* inside a ray-length bucket: by direction sector (16 azimuthal x
+                                 2 axial), then the Morton code of the TOF kernel centre (the
+                                 LOR midpoint without TOF) on cells of tile_shift */
 typedef struct
 {
 	int block;            /* threads per block: 128, 256 or 512 */
@@ -183,7 +187,9 @@ typedef struct
 	                         pieces' sums round differently from one walk) and
 	                         is not used by deterministic back projections */
 	int bucket_shift;     /* yrtb_events_subset_order groups rays by
-	                         (voxel crossings >> bucket_shift), 0..6 */
+	                         (voxel crossings >> bucket_shift), 0..7 */
+	int order;            /* YRTB_ORDER_LOR or YRTB_ORDER_SPATIAL */
+	int tile_shift;       /* YRTB_ORDER_SPATIAL: cells of (voxel size * 2^tile_shift), 0..4 */
 } yrtb_launch_config;
 
 yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
@@ -204,10 +210,11 @@ typedef struct
 
 /* Autotuner (no reference counterpart).  Times the fused EM step of this
  * projector over a sample of the events -- subset 0 of num_subsets
- * interleaved subsets, at most max_sample events -- for every launch
- * configuration the projector admits (block x threads_per_lor x bucket_shift,
- * each bucket_shift on the sample ordered with it), keeps the fastest
- * (yrtb_projector_set_launch) and reports all timings.  d_image: the image
+ * interleaved subsets, at most max_sample events -- in two stages: first
+ * every event order (bucket_shift x order x tile_shift, the sample ordered
+ * with each) with the current block size and threads per LOR, then every
+ * block size x threads per LOR the projector admits on the fastest order.
+ * Keeps the fastest (yrtb_projector_set_launch) and reports all timings.  d_image: the image
  * the EM steps read (nx*ny*nz*nt floats; its values do not change the work).
  * Setup-time call: allocates temporaries and synchronises the stream, so it
  * must not run under stream capture.  Projectors other than single-ray

@@ -71,7 +71,7 @@ def test_every_launch_config_vs_oracle(tof):
     for block, tpl in CONFIGS:
         p.set_launch(block, tpl, 3)
         assert p.get_launch() == {"block": block, "threads_per_lor": tpl,
-                                  "bucket_shift": 3}
+                                  "bucket_shift": 3, "order": 0, "tile_shift": 1}
         v = p.forward(gimg, ev).cpu().numpy()
         b = p.backward(gy, ev).cpu().numpy()
         assert rel_l2(v, f64) < 1e-5, (block, tpl)
@@ -97,15 +97,20 @@ def test_threads_per_lor_needs_compensated_mode():
         p.set_launch(384, 1, 3)
     with pytest.raises(yrt.YrtbError, match="bucket_shift"):
         p.set_launch(256, 1, 9)
+    with pytest.raises(yrt.YrtbError, match="order must be"):
+        p.set_launch(256, 1, 3, order=2)
+    with pytest.raises(yrt.YrtbError, match="tile_shift"):
+        p.set_launch(256, 1, 3, order=1, tile_shift=5)
 
 
-@pytest.mark.parametrize("shift", [0, 2, 5])
-def test_ordering_with_bucket_shift_is_a_subset_major_permutation(shift):
+@pytest.mark.parametrize("shift,order,tile", [(0, 0, 1), (2, 0, 1), (5, 0, 1),
+                                              (3, 1, 0), (5, 1, 2), (7, 1, 3)])
+def test_ordering_with_bucket_shift_is_a_subset_major_permutation(shift, order, tile):
     sc, ip, p = make((214.0, 5))
     d1, d2 = random_events(50000, 43)
     tv = np.random.default_rng(44).normal(0, 300, len(d1)).astype(np.float32)
     ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv)
-    p.set_launch(256, 1, shift)
+    p.set_launch(256, 1, shift, order, tile)
     S = 7
     out, offs = p.order_events(ev, S)
     perm = out.perm.cpu().numpy()
@@ -145,7 +150,30 @@ def test_autotune_keeps_fastest_and_reconstruction_matches():
         reports.append(osem.lastTuneReport)
     rep = reports[1]
     assert 0 < rep["sample_events"] <= (len(e["d1"]) + 2) // 3
-    assert len(rep["tried"]) == 36
+    assert len(rep["tried"]) == 25 + 8
     best_ms = min(ms for _, ms in rep["tried"])
     assert [c for c, ms in rep["tried"] if ms == best_ms][0] == rep["best"]
     assert rel_l2(outs[1], outs[0]) < 1e-5
+
+
+def test_em_step_same_under_every_order():
+    """The EM image of a subset does not depend on the order of its events
+    beyond float summation order (image budget 1e-4; here far below)."""
+    sc, ip, p = make((214.0, 5))
+    d1, d2 = random_events(60000, 47)
+    rng = np.random.default_rng(48)
+    tv = rng.normal(0, 300, len(d1)).astype(np.float32)
+    img = torch.from_numpy(rng.uniform(0.5, 1.5, ip.shape).astype(np.float32)).cuda()
+    ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv)
+    S = 3
+    ref = None
+    for order, tile in [(0, 1), (1, 0), (1, 2)]:
+        p.set_launch(256, 1, 3, order, tile)
+        out, offs = p.order_events(ev, S)
+        em = torch.zeros(ip.shape, device="cuda")
+        p.em_step(img, em, out, rng=L.yrtb_range(int(offs[1]), 1, int(offs[2] - offs[1])))
+        em = em.cpu().numpy()
+        if ref is None:
+            ref = em
+        else:
+            assert rel_l2(em, ref) < 1e-6

@@ -946,16 +946,55 @@ __global__ void __launch_bounds__(kBlock)
 		warpMaxInto(maxBits, bound != bound ? __uint_as_float(0x7fffffffu) : bound);
 }
 
+// 8-bit value spread to every third bit (Morton interleave).
+__device__ __forceinline__ uint32_t spread3(uint32_t v)
+{
+	v &= 0xffu;
+	v = (v | (v << 8)) & 0x0300F00Fu;
+	v = (v | (v << 4)) & 0x030C30C3u;
+	v = (v | (v << 2)) & 0x09249249u;
+	return v;
+}
+
+// Spatial LOR key (29 bits): azimuthal sector of the direction (16 over
+// [0, pi), direction folded to dx > 0) in bits 25..28, the sign of its axial
+// component in bit 24, then the Morton code of the TOF kernel centre (the
+// LOR midpoint without TOF) on cells of cell mm, 256 per axis from the grid's
+// lower corner.  Rays of one warp then start near each other and run nearly
+// parallel, so their voxels overlap.
+__device__ __forceinline__ uint64_t spatialKey(const KParams& P, float3 p1, float3 p2,
+                                               bool tof, float tofv, float cell)
+{
+	float3 d = f3sub(p2, p1);
+	const float L = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+	const float ac = (tof && L > 0.f) ? tofCenter(L, tofv) / L : 0.5f;
+	const float3 c = make_float3(p1.x + ac * d.x, p1.y + ac * d.y, p1.z + ac * d.z);
+	if (d.x < 0.f || (d.x == 0.f && d.y < 0.f))
+		d = make_float3(-d.x, -d.y, -d.z);
+	const float phi = atan2f(d.y, d.x);  // (-pi/2, pi/2]
+	const uint32_t sector = min(15u, static_cast<uint32_t>(fmaxf(0.f, (phi + 1.5707964f) * 5.0929582f)));
+	const uint32_t up = d.z >= 0.f ? 1u : 0u;
+	auto cellOf = [&](float q, float len) -> uint32_t
+	{
+		const float u = (q + 0.5f * len) / cell;
+		return u <= 0.f ? 0u : (u >= 255.f ? 255u : static_cast<uint32_t>(u));
+	};
+	const uint32_t m = spread3(cellOf(c.x, P.g.lx)) | (spread3(cellOf(c.y, P.g.ly)) << 1) |
+	                   (spread3(cellOf(c.z, P.g.lz)) << 2);
+	return (static_cast<uint64_t>(sector) << 25) | (static_cast<uint64_t>(up) << 24) | m;
+}
+
 // Sort key of event e.  Without dynamic frames: subset (e mod S) in bits
 // 48..63, ray length bucket (voxel crossings >> bucketShift, at most 127, when
-// counts are given) in bits 41..47, LOR (Histogram3D bin, or the ordered
-// detector pair, >> lorShift to fit) in bits 8..40, TOF in 16 ps steps in bits
-// 0..7.  With dynamic frames: subset in bits 52..63, frame in 44..51, bucket
-// in 37..43, LOR in 8..36.  Grouping rays of similar length keeps the threads
-// of a warp iterating together; the LOR key keeps neighbouring rays together.
-__global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
+// counts are given) in bits 41..47, LOR key in bits 8..40, TOF in 16 ps steps
+// in bits 0..7.  With dynamic frames: subset in bits 52..63, frame in 44..51,
+// bucket in 37..43, LOR key in 8..36.  The LOR key is the Histogram3D bin (or
+// the ordered detector pair) >> lorShift, or the spatial key.  Grouping rays
+// of similar length keeps the threads of a warp iterating together; the LOR
+// key keeps neighbouring rays together.
+__global__ void k_order_keys(KParams P, H3Dev H, bool hasH3, Events E, uint64_t n,
                              uint64_t numSubsets, const uint32_t* __restrict__ counts,
-                             int bucketShift, int lorShift,
+                             int bucketShift, int lorShift, int spatial, float cell,
                              unsigned long long* __restrict__ keys,
                              unsigned long long* __restrict__ vals)
 {
@@ -964,7 +1003,14 @@ __global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
 	     e < n; e += nthreads)
 	{
 		uint64_t lorKey = 0;
-		if (E.d1 != nullptr)
+		const float tofv = E.tof != nullptr ? __ldg(E.tof + e) : 0.f;
+		if (spatial)
+		{
+			float3 p1, p2, n1, n2;
+			if (fetchEvent(P, E, e, p1, p2, n1, n2))
+				lorKey = spatialKey(P, p1, p2, E.tof != nullptr, tofv, cell);
+		}
+		else if (E.d1 != nullptr)
 		{
 			const uint32_t a = __ldg(E.d1 + e), b = __ldg(E.d2 + e);
 			uint64_t bin;
@@ -972,12 +1018,12 @@ __global__ void k_order_keys(H3Dev H, bool hasH3, Events E, uint64_t n,
 				lorKey = bin;
 			else
 				lorKey = static_cast<uint64_t>(min(a, b)) * H.numDets + max(a, b);
+			lorKey >>= lorShift;
 		}
-		lorKey >>= lorShift;
 		uint64_t q = 128;
 		if (E.tof != nullptr)
 		{
-			const float t = __ldg(E.tof + e) / 16.0f + 128.0f;
+			const float t = tofv / 16.0f + 128.0f;
 			q = t <= 0.f ? 0 : (t >= 255.f ? 255 : static_cast<uint64_t>(t));
 		}
 		const uint64_t bucket = counts ? min(__ldg(counts + e) >> bucketShift, 127u) : 0u;
@@ -1352,7 +1398,7 @@ struct yrtb_projector
 	int2* d_z = nullptr;
 	unsigned long long* d_err = nullptr;
 	// Launch configuration of the single-ray Siddon event kernels.
-	yrtb_launch_config launch{256, 1, 3};
+	yrtb_launch_config launch{256, 1, 3, YRTB_ORDER_LOR, 1};
 	// Deterministic back projection: fixed-point image (nvox * nt) and bound.
 	bool det = false;
 	unsigned long long* d_fix = nullptr;
@@ -1628,9 +1674,10 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 }
 
 // Subset-major permutation of the events (see yrtb_events_subset_order)
-// with ray-length buckets of 2^bucketShift crossings.
+// with the ordering parameters of cfg.
 yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
-                        int bucketShift, uint64_t* d_perm, cudaStream_t st)
+                        const yrtb_launch_config& cfg, uint64_t* d_perm,
+                        cudaStream_t st)
 {
 	const uint64_t n = ev->count;
 	if (n == 0)
@@ -1677,9 +1724,11 @@ yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
 	while (keyBits < 64 && (maxKey >> keyBits) != 0)
 		keyBits++;
 	const int lorShift = std::max(0, keyBits - lorBits);
+	const float voxel = std::max(h->P.g.vx, std::max(h->P.g.vy, h->P.g.vz));
+	const float cell = voxel * static_cast<float>(1 << cfg.tile_shift);
 	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(
-	    h->h3d, h->h3 != nullptr, toDev(ev), n, S, counts, bucketShift, lorShift,
-	    keys, vals);
+	    h->P, h->h3d, h->h3 != nullptr, toDev(ev), n, S, counts, cfg.bucket_shift,
+	    lorShift, cfg.order == YRTB_ORDER_SPATIAL ? 1 : 0, cell, keys, vals);
 	ce = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals,
 	                                     reinterpret_cast<unsigned long long*>(d_perm),
 	                                     n, 0, 64, st);
@@ -1922,8 +1971,12 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 		return fail(YRTB_ERR_ARGUMENT,
 		            "threads_per_lor > 1 needs a single-ray Siddon projector in "
 		            "YRTB_COMPENSATED precision");
-	if (c->bucket_shift < 0 || c->bucket_shift > 6)
-		return fail(YRTB_ERR_ARGUMENT, "bucket_shift must be in 0..6");
+	if (c->bucket_shift < 0 || c->bucket_shift > 7)
+		return fail(YRTB_ERR_ARGUMENT, "bucket_shift must be in 0..7");
+	if (c->order != YRTB_ORDER_LOR && c->order != YRTB_ORDER_SPATIAL)
+		return fail(YRTB_ERR_ARGUMENT, "order must be YRTB_ORDER_LOR or YRTB_ORDER_SPATIAL");
+	if (c->tile_shift < 0 || c->tile_shift > 4)
+		return fail(YRTB_ERR_ARGUMENT, "tile_shift must be in 0..4");
 	h->launch = *c;
 	return YRTB_OK;
 }
@@ -1965,7 +2018,7 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
 	subset_offsets[0] = 0;
 	for (uint64_t s = 0; s < S; s++)
 		subset_offsets[s + 1] = subset_offsets[s] + (n > s ? (n - s + S - 1) / S : 0);
-	return orderEvents(h, ev, S, h->launch.bucket_shift, d_perm,
+	return orderEvents(h, ev, S, h->launch, d_perm,
 	                   reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -2491,50 +2544,87 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	}
 	cudaMemsetAsync(em, 0, J * 4, st);
 
-	std::vector<yrtb_launch_config> cands;
-	const bool split = h->comp && !h->det;
-	for (int shift : {2, 3, 4, 5})
-		for (int block : {128, 256, 512})
-			for (int tpl : {1, 2, 4})
-				if ((tpl == 1 || split) && (!h->det || (block == 256 && tpl == 1)))
-					cands.push_back(yrtb_launch_config{block, tpl, shift});
 	const yrtb_launch_config saved = h->launch;
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	cudaEventCreate(&e0);
 	cudaEventCreate(&e1);
 	const yrtb_range r{0, 1, n};
 	int bestIdx = -1;
-	int lastShift = -1;
-	for (const yrtb_launch_config& c : cands)
+	// Orders the sample for c (unless it is ordered so already) and times the
+	// EM step with c: best of 3 after one warm-up.
+	yrtb_launch_config ordered{};
+	bool haveOrder = false;
+	auto timeOne = [&](const yrtb_launch_config& c) -> yrtb_status
 	{
-		if (c.bucket_shift != lastShift)
+		if (report->num_tried >= YRTB_TUNE_MAX)
+			return YRTB_OK;
+		yrtb_status q;
+		if (!haveOrder || c.bucket_shift != ordered.bucket_shift ||
+		    c.order != ordered.order || c.tile_shift != ordered.tile_shift)
 		{
-			lastShift = c.bucket_shift;
-			if ((s = orderEvents(h, &A, 1, c.bucket_shift, static_cast<uint64_t*>(perm2), st)) != YRTB_OK ||
-			    (s = yrtb_events_gather(&A, static_cast<uint64_t*>(perm2), &B, stream)) != YRTB_OK)
-				break;
+			if ((q = orderEvents(h, &A, 1, c, static_cast<uint64_t*>(perm2), st)) != YRTB_OK ||
+			    (q = yrtb_events_gather(&A, static_cast<uint64_t*>(perm2), &B, stream)) != YRTB_OK)
+				return q;
+			ordered = c;
+			haveOrder = true;
 		}
 		h->launch = c;
 		float best = 3.4e38f;
-		for (int rep = 0; rep < 4 && s == YRTB_OK; rep++)
+		for (int rep = 0; rep < 4; rep++)
 		{
 			cudaEventRecord(e0, st);
-			s = yrtb_em_step(h, d_image, static_cast<float*>(em), &B, r, 1.f, 1e-35f, stream);
+			q = yrtb_em_step(h, d_image, static_cast<float*>(em), &B, r, 1.f, 1e-35f, stream);
 			cudaEventRecord(e1, st);
 			const cudaError_t ce = cudaEventSynchronize(e1);
+			if (q != YRTB_OK)
+				return q;
 			if (ce != cudaSuccess)
-				s = fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
+				return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
 			float ms = 0.f;
-			if (s == YRTB_OK && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+			if (rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
 				best = std::min(best, ms);  // rep 0 warms up
 		}
-		if (s != YRTB_OK)
-			break;
 		const int i = report->num_tried++;
 		report->tried[i] = c;
 		report->ms[i] = best;
 		if (bestIdx < 0 || best < report->ms[bestIdx])
 			bestIdx = i;
+		return YRTB_OK;
+	};
+	// Stage 1: event orders, with the current block size and threads per LOR.
+	for (int shift : {2, 3, 4, 5, 7})
+	{
+		yrtb_launch_config c = saved;
+		c.bucket_shift = shift;
+		c.order = YRTB_ORDER_LOR;
+		if (s == YRTB_OK)
+			s = timeOne(c);
+		for (int tile : {0, 1, 2, 3})
+		{
+			c.order = YRTB_ORDER_SPATIAL;
+			c.tile_shift = tile;
+			if (s == YRTB_OK)
+				s = timeOne(c);
+		}
+	}
+	// Stage 2: block size x threads per LOR on the fastest order.
+	if (s == YRTB_OK && bestIdx >= 0)
+	{
+		const yrtb_launch_config o = report->tried[bestIdx];
+		const bool split = h->comp && !h->det;
+		for (int block : {128, 256, 512})
+			for (int tpl : {1, 2, 4})
+			{
+				if ((tpl > 1 && !split) || (h->det && (block != 256 || tpl != 1)))
+					continue;
+				if (block == o.block && tpl == o.threads_per_lor)
+					continue;
+				yrtb_launch_config c = o;
+				c.block = block;
+				c.threads_per_lor = tpl;
+				if (s == YRTB_OK)
+					s = timeOne(c);
+			}
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);

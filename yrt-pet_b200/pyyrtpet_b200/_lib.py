@@ -22,6 +22,8 @@ YRTB_DD = 1
 YRTB_OSEM_STATIC_MAX_FLOATS = 4 * 1024 * 1024
 YRTB_MIRROR = 0
 YRTB_COMPENSATED = 1
+YRTB_ORDER_LOR = 0
+YRTB_ORDER_SPATIAL = 1
 
 c_f = ctypes.c_float
 c_u64 = ctypes.c_uint64
@@ -74,7 +76,8 @@ class yrtb_osem_params(ctypes.Structure):
 
 class yrtb_launch_config(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int), ("threads_per_lor", ctypes.c_int),
-                ("bucket_shift", ctypes.c_int)]
+                ("bucket_shift", ctypes.c_int), ("order", ctypes.c_int),
+                ("tile_shift", ctypes.c_int)]
 
 
 YRTB_TUNE_MAX = 64

@@ -732,15 +732,21 @@ class DeviceProjector:
 
     # ------------------------------------------------ launch configuration --
     def set_launch(self, block: int = 256, threads_per_lor: int = 1,
-                   bucket_shift: int = 3):
-        c = L.yrtb_launch_config(int(block), int(threads_per_lor), int(bucket_shift))
+                   bucket_shift: int = 3, order: int = 0, tile_shift: int = 1):
+        c = L.yrtb_launch_config(int(block), int(threads_per_lor), int(bucket_shift),
+                                 int(order), int(tile_shift))
         L.check(L.lib().yrtb_projector_set_launch(self.h, ctypes.byref(c)))
+
+    @staticmethod
+    def _launch_dict(c) -> dict:
+        return {"block": c.block, "threads_per_lor": c.threads_per_lor,
+                "bucket_shift": c.bucket_shift, "order": c.order,
+                "tile_shift": c.tile_shift}
 
     def get_launch(self) -> dict:
         c = L.yrtb_launch_config()
         L.check(L.lib().yrtb_projector_get_launch(self.h, ctypes.byref(c)))
-        return {"block": c.block, "threads_per_lor": c.threads_per_lor,
-                "bucket_shift": c.bucket_shift}
+        return self._launch_dict(c)
 
     def autotune(self, img, ev: DeviceEvents, num_subsets: int = 1,
                  max_sample: int = 2_000_000) -> dict:
@@ -753,8 +759,7 @@ class DeviceProjector:
         L.check(L.lib().yrtb_autotune(self.h, img.data_ptr(), ctypes.byref(ev.c()),
                                       int(num_subsets), int(max_sample),
                                       ctypes.byref(rep), _stream()))
-        cfg = lambda c: {"block": c.block, "threads_per_lor": c.threads_per_lor,
-                         "bucket_shift": c.bucket_shift}
+        cfg = self._launch_dict
         return {"best": cfg(rep.best), "sample_events": int(rep.sample_events),
                 "tried": [(cfg(rep.tried[i]), float(rep.ms[i]))
                           for i in range(rep.num_tried)]}
