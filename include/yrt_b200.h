@@ -178,6 +178,8 @@ void yrtb_projector_destroy(yrtb_projector* h);
 #define YRTB_ORDER_SPATIAL 1  /* inside a ray-length bucket: by direction sector (16 azimuthal x
                                  2 axial), then the Morton code of the TOF kernel centre (the
                                  LOR midpoint without TOF) on cells of tile_shift */
+#define YRTB_ORDER_SPATIAL_FINE 2  /* as YRTB_ORDER_SPATIAL with 64 azimuthal sectors (and 128
+                                      centre cells per axis instead of 256) */
 typedef struct
 {
 	int block;            /* threads per block: 128, 256 or 512 */
@@ -188,7 +190,7 @@ typedef struct
 	                         is not used by deterministic back projections */
 	int bucket_shift;     /* yrtb_events_subset_order groups rays by
 	                         (voxel crossings >> bucket_shift), 0..7 */
-	int order;            /* YRTB_ORDER_LOR or YRTB_ORDER_SPATIAL */
+	int order;            /* YRTB_ORDER_LOR, YRTB_ORDER_SPATIAL or YRTB_ORDER_SPATIAL_FINE */
 	int tile_shift;       /* YRTB_ORDER_SPATIAL: cells of (voxel size * 2^tile_shift), 0..4 */
 } yrtb_launch_config;
 

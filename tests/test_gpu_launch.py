@@ -98,13 +98,14 @@ def test_threads_per_lor_needs_compensated_mode():
     with pytest.raises(yrt.YrtbError, match="bucket_shift"):
         p.set_launch(256, 1, 9)
     with pytest.raises(yrt.YrtbError, match="order must be"):
-        p.set_launch(256, 1, 3, order=2)
+        p.set_launch(256, 1, 3, order=3)
     with pytest.raises(yrt.YrtbError, match="tile_shift"):
         p.set_launch(256, 1, 3, order=1, tile_shift=5)
 
 
 @pytest.mark.parametrize("shift,order,tile", [(0, 0, 1), (2, 0, 1), (5, 0, 1),
-                                              (3, 1, 0), (5, 1, 2), (7, 1, 3)])
+                                              (3, 1, 0), (5, 1, 2), (7, 1, 3),
+                                              (4, 2, 1), (7, 2, 0)])
 def test_ordering_with_bucket_shift_is_a_subset_major_permutation(shift, order, tile):
     sc, ip, p = make((214.0, 5))
     d1, d2 = random_events(50000, 43)
@@ -150,7 +151,7 @@ def test_autotune_keeps_fastest_and_reconstruction_matches():
         reports.append(osem.lastTuneReport)
     rep = reports[1]
     assert 0 < rep["sample_events"] <= (len(e["d1"]) + 2) // 3
-    assert len(rep["tried"]) == 25 + 8
+    assert len(rep["tried"]) == 4 * 7 + 8
     best_ms = min(ms for _, ms in rep["tried"])
     assert [c for c, ms in rep["tried"] if ms == best_ms][0] == rep["best"]
     assert rel_l2(outs[1], outs[0]) < 1e-5
@@ -167,7 +168,7 @@ def test_em_step_same_under_every_order():
     ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv)
     S = 3
     ref = None
-    for order, tile in [(0, 1), (1, 0), (1, 2)]:
+    for order, tile in [(0, 1), (1, 0), (1, 2), (2, 1)]:
         p.set_launch(256, 1, 3, order, tile)
         out, offs = p.order_events(ev, S)
         em = torch.zeros(ip.shape, device="cuda")

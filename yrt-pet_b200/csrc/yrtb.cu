@@ -956,14 +956,15 @@ __device__ __forceinline__ uint32_t spread3(uint32_t v)
 	return v;
 }
 
-// Spatial LOR key (29 bits): azimuthal sector of the direction (16 over
-// [0, pi), direction folded to dx > 0) in bits 25..28, the sign of its axial
-// component in bit 24, then the Morton code of the TOF kernel centre (the
-// LOR midpoint without TOF) on cells of cell mm, 256 per axis from the grid's
-// lower corner.  Rays of one warp then start near each other and run nearly
-// parallel, so their voxels overlap.
+// Spatial LOR key (29 bits): azimuthal sector of the direction (16 or 64
+// over [0, pi), direction folded to dx > 0), the sign of its axial component,
+// then the Morton code of the TOF kernel centre (the LOR midpoint without TOF)
+// on cells of cell mm from the grid's lower corner (256 per axis with 16
+// sectors, 128 with 64).  Rays of one warp then start near each other and run
+// nearly parallel, so their voxels overlap.
 __device__ __forceinline__ uint64_t spatialKey(const KParams& P, float3 p1, float3 p2,
-                                               bool tof, float tofv, float cell)
+                                               bool tof, float tofv, float cell,
+                                               bool fine)
 {
 	float3 d = f3sub(p2, p1);
 	const float L = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
@@ -972,16 +973,21 @@ __device__ __forceinline__ uint64_t spatialKey(const KParams& P, float3 p1, floa
 	if (d.x < 0.f || (d.x == 0.f && d.y < 0.f))
 		d = make_float3(-d.x, -d.y, -d.z);
 	const float phi = atan2f(d.y, d.x);  // (-pi/2, pi/2]
-	const uint32_t sector = min(15u, static_cast<uint32_t>(fmaxf(0.f, (phi + 1.5707964f) * 5.0929582f)));
+	const uint32_t ns = fine ? 64u : 16u;
+	const uint32_t sector = min(ns - 1u, static_cast<uint32_t>(fmaxf(
+	                                         0.f, (phi + 1.5707964f) * (static_cast<float>(ns) * 0.31830989f))));
 	const uint32_t up = d.z >= 0.f ? 1u : 0u;
+	const float top = fine ? 127.f : 255.f;
 	auto cellOf = [&](float q, float len) -> uint32_t
 	{
 		const float u = (q + 0.5f * len) / cell;
-		return u <= 0.f ? 0u : (u >= 255.f ? 255u : static_cast<uint32_t>(u));
+		return u <= 0.f ? 0u : (u >= top ? static_cast<uint32_t>(top) : static_cast<uint32_t>(u));
 	};
 	const uint32_t m = spread3(cellOf(c.x, P.g.lx)) | (spread3(cellOf(c.y, P.g.ly)) << 1) |
 	                   (spread3(cellOf(c.z, P.g.lz)) << 2);
-	return (static_cast<uint64_t>(sector) << 25) | (static_cast<uint64_t>(up) << 24) | m;
+	// 16 sectors: sector | up | 24-bit Morton; 64 sectors: sector | up | 21-bit Morton.
+	return fine ? (static_cast<uint64_t>(sector) << 22) | (static_cast<uint64_t>(up) << 21) | m
+	            : (static_cast<uint64_t>(sector) << 25) | (static_cast<uint64_t>(up) << 24) | m;
 }
 
 // Sort key of event e.  Without dynamic frames: subset (e mod S) in bits
@@ -1008,7 +1014,7 @@ __global__ void k_order_keys(KParams P, H3Dev H, bool hasH3, Events E, uint64_t 
 		{
 			float3 p1, p2, n1, n2;
 			if (fetchEvent(P, E, e, p1, p2, n1, n2))
-				lorKey = spatialKey(P, p1, p2, E.tof != nullptr, tofv, cell);
+				lorKey = spatialKey(P, p1, p2, E.tof != nullptr, tofv, cell, spatial == 2);
 		}
 		else if (E.d1 != nullptr)
 		{
@@ -1728,7 +1734,7 @@ yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
 	const float cell = voxel * static_cast<float>(1 << cfg.tile_shift);
 	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(
 	    h->P, h->h3d, h->h3 != nullptr, toDev(ev), n, S, counts, cfg.bucket_shift,
-	    lorShift, cfg.order == YRTB_ORDER_SPATIAL ? 1 : 0, cell, keys, vals);
+	    lorShift, cfg.order, cell, keys, vals);
 	ce = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals,
 	                                     reinterpret_cast<unsigned long long*>(d_perm),
 	                                     n, 0, 64, st);
@@ -1973,8 +1979,10 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 		            "YRTB_COMPENSATED precision");
 	if (c->bucket_shift < 0 || c->bucket_shift > 7)
 		return fail(YRTB_ERR_ARGUMENT, "bucket_shift must be in 0..7");
-	if (c->order != YRTB_ORDER_LOR && c->order != YRTB_ORDER_SPATIAL)
-		return fail(YRTB_ERR_ARGUMENT, "order must be YRTB_ORDER_LOR or YRTB_ORDER_SPATIAL");
+	if (c->order != YRTB_ORDER_LOR && c->order != YRTB_ORDER_SPATIAL &&
+	    c->order != YRTB_ORDER_SPATIAL_FINE)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "order must be YRTB_ORDER_LOR, YRTB_ORDER_SPATIAL or YRTB_ORDER_SPATIAL_FINE");
 	if (c->tile_shift < 0 || c->tile_shift > 4)
 		return fail(YRTB_ERR_ARGUMENT, "tile_shift must be in 0..4");
 	h->launch = *c;
@@ -2592,20 +2600,21 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 		return YRTB_OK;
 	};
 	// Stage 1: event orders, with the current block size and threads per LOR.
-	for (int shift : {2, 3, 4, 5, 7})
+	for (int shift : {3, 4, 5, 7})
 	{
 		yrtb_launch_config c = saved;
 		c.bucket_shift = shift;
 		c.order = YRTB_ORDER_LOR;
 		if (s == YRTB_OK)
 			s = timeOne(c);
-		for (int tile : {0, 1, 2, 3})
-		{
-			c.order = YRTB_ORDER_SPATIAL;
-			c.tile_shift = tile;
-			if (s == YRTB_OK)
-				s = timeOne(c);
-		}
+		for (int order : {YRTB_ORDER_SPATIAL, YRTB_ORDER_SPATIAL_FINE})
+			for (int tile : {0, 1, 2})
+			{
+				c.order = order;
+				c.tile_shift = tile;
+				if (s == YRTB_OK)
+					s = timeOne(c);
+			}
 	}
 	// Stage 2: block size x threads per LOR on the fastest order.
 	if (s == YRTB_OK && bestIdx >= 0)

@@ -24,6 +24,7 @@ YRTB_MIRROR = 0
 YRTB_COMPENSATED = 1
 YRTB_ORDER_LOR = 0
 YRTB_ORDER_SPATIAL = 1
+YRTB_ORDER_SPATIAL_FINE = 2
 
 c_f = ctypes.c_float
 c_u64 = ctypes.c_uint64
