@@ -396,7 +396,7 @@ def main():
     # with the reference's launch shape (one thread per event, 256-thread
     # blocks).
     proj.set_launch(256, 1, launch["bucket_shift"], launch["order"],
-                    launch["tile_shift"])
+                    launch["tile_shift"], 0)
     for _ in range(1):
         step(plain=True)
     pa = torch.cuda.Event(enable_timing=True)
@@ -533,7 +533,8 @@ def main():
                                "default_ms": next((ms for c, ms in tune["tried"]
                                                    if c == {"block": 256, "threads_per_lor": 1,
                                                             "bucket_shift": 3, "order": 0,
-                                                            "tile_shift": 1}), None)},
+                                                            "tile_shift": 1,
+                                                            "vector_groups": 1}), None)},
                            "l2": "event arrays (1.2 GB) larger than L2; "
                                  "image (42 MB) L2-resident by design",
                            "parallelism": f"dp{world} (events sharded, EM image "

@@ -47,7 +47,8 @@ def random_events(n, seed):
     return d1[ok][:n], d2[ok][:n]
 
 
-CONFIGS = [(b, t) for b in (128, 256, 512) for t in (1, 2, 4)]
+CONFIGS = [(b, t, v) for b in (128, 256, 512) for t in (1, 2, 4) for v in (1, 0)
+           if not (t > 1 and v == 0)]
 
 
 @pytest.mark.parametrize("tof", [None, (214.0, 5)])
@@ -68,10 +69,11 @@ def test_every_launch_config_vs_oracle(tof):
     gimg = torch.from_numpy(img).cuda()
     gy = torch.from_numpy(y).cuda()
     base = None
-    for block, tpl in CONFIGS:
-        p.set_launch(block, tpl, 3)
+    for block, tpl, vec in CONFIGS:
+        p.set_launch(block, tpl, 3, vector_groups=vec)
         assert p.get_launch() == {"block": block, "threads_per_lor": tpl,
-                                  "bucket_shift": 3, "order": 0, "tile_shift": 1}
+                                  "bucket_shift": 3, "order": 0, "tile_shift": 1,
+                                  "vector_groups": vec}
         v = p.forward(gimg, ev).cpu().numpy()
         b = p.backward(gy, ev).cpu().numpy()
         assert rel_l2(v, f64) < 1e-5, (block, tpl)
@@ -151,7 +153,9 @@ def test_autotune_keeps_fastest_and_reconstruction_matches():
         reports.append(osem.lastTuneReport)
     rep = reports[1]
     assert 0 < rep["sample_events"] <= (len(e["d1"]) + 2) // 3
-    assert len(rep["tried"]) == 4 * 7 + 8
+    # 3 bucket shifts x 5 orders x vector groups on/off, then 3 blocks x
+    # 3 threads/LOR minus the stage-1 shape.
+    assert len(rep["tried"]) == 3 * 5 * 2 + 3 * 3 - 1
     best_ms = min(ms for _, ms in rep["tried"])
     assert [c for c, ms in rep["tried"] if ms == best_ms][0] == rep["best"]
     assert rel_l2(outs[1], outs[0]) < 1e-5

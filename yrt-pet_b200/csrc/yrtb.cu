@@ -387,7 +387,9 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
 // traversal order, compensated mode uses Kahan summation.  With TRACK, maxw
 // receives the largest |weight| of the event's rays (the sum itself is
 // computed exactly as without TRACK).
-template <int KIND, bool TOF, bool COMP, bool TRACK = false>
+// VEC: the image is read as aligned float4 groups, and consecutive
+// crossings inside one group (x steps) reuse the group held in registers.
+template <int KIND, bool TOF, bool COMP, bool TRACK = false, bool VEC = false>
 __device__ __forceinline__ float forwardEvent(const KParams& P,
                                               const float* __restrict__ img,
                                               float3 p1, float3 p2, float3 n1,
@@ -397,20 +399,40 @@ __device__ __forceinline__ float forwardEvent(const KParams& P,
                                               int part = 0, int parts = 1)
 {
 	float acc = 0.f, ray = 0.f, comp = 0.f, mw = 0.f;
+	int gb = -1;
+	float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
+	auto fetch = [&](int o) -> float
+	{
+		if constexpr (VEC)
+		{
+			const int g = o & ~3;
+			if (g != gb)
+			{
+				q4 = __ldg(reinterpret_cast<const float4*>(img + g));
+				gb = g;
+			}
+			const int l = o & 3;
+			return l == 0 ? q4.x : (l == 1 ? q4.y : (l == 2 ? q4.z : q4.w));
+		}
+		else
+		{
+			return __ldg(img + o);
+		}
+	};
 	auto visit = [&](int o, float w)
 	{
 		if constexpr (TRACK)
 			mw = fmaxf(mw, fabsf(w));
 		if constexpr (COMP)
 		{
-			const float y = __fmaf_rn(w, __ldg(img + o), -comp);
+			const float y = __fmaf_rn(w, fetch(o), -comp);
 			const float t = ray + y;
 			comp = (t - ray) - y;
 			ray = t;
 		}
 		else
 		{
-			ray += w * __ldg(img + o);
+			ray += w * fetch(o);
 		}
 	};
 	auto endRay = [&]
@@ -486,7 +508,16 @@ __device__ __forceinline__ void warpMaxInto(unsigned* out, float b)
 		atomicMax(out, bits);
 }
 
-template <int KIND, bool TOF, bool COMP, bool FIX = false>
+// VEC: contributions to one aligned group of 4 voxels (consecutive x steps)
+// are summed in registers and sent as one red.global.add.v4.f32 (the other
+// lanes add zero), which cuts the L2 reduction requests.
+__device__ __forceinline__ void redV4(float* p, float4 v)
+{
+	asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};"
+	             :: "l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
+}
+
+template <int KIND, bool TOF, bool COMP, bool FIX = false, bool VEC = false>
 __device__ __forceinline__ void backwardEvent(const KParams& P,
                                               float* __restrict__ img,
                                               float v, float3 p1, float3 p2,
@@ -509,6 +540,36 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 		};
 		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
 		                              endRay, part, parts);
+	}
+	else if constexpr (VEC)
+	{
+		int gb = -1;
+		float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
+		auto visit = [&](int o, float w)
+		{
+			const float c = v * w;
+			const int g = o & ~3;
+			if (g != gb)
+			{
+				if (gb >= 0)
+					redV4(img + gb, a4);
+				gb = g;
+				a4 = make_float4(0.f, 0.f, 0.f, 0.f);
+			}
+			const int l = o & 3;
+			a4.x += l == 0 ? c : 0.f;
+			a4.y += l == 1 ? c : 0.f;
+			a4.z += l == 2 ? c : 0.f;
+			a4.w += l == 3 ? c : 0.f;
+		};
+		auto flush = [&]
+		{
+			if (gb >= 0)
+				redV4(img + gb, a4);
+			gb = -1;
+		};
+		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+		                              flush, part, parts);
 	}
 	else
 	{
@@ -549,7 +610,7 @@ __device__ __forceinline__ float groupSum(float v)
 // the compiler's register choice.  FIX (OP_BWD, OP_EM): pass 2 of the
 // deterministic back projection.
 template <int OP, int KIND, bool TOF, bool COMP, bool FIX = false,
-          int BLOCK = kBlock, int TPL = 1>
+          int BLOCK = kBlock, int TPL = 1, bool VEC = false>
 __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
     k_events(KParams P, Events E, Range R, const float* __restrict__ in,
              float* __restrict__ out, float globalScale, float denomThr,
@@ -593,7 +654,7 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 		}
 		else if constexpr (OP == OP_FWD)
 		{
-			const float v = groupSum<TPL>(forwardEvent<KIND, TOF, COMP>(
+			const float v = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, VEC>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			if (part == 0)
 				out[e] = v;
@@ -605,9 +666,9 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 				                                     p2, n1, n2, tofv, k,
 				                                     F.acc + fo, fixedScale(F));
 			else
-				backwardEvent<KIND, TOF, COMP>(P, out + fo, __ldg(in + e), p1, p2,
-				                               n1, n2, tofv, k, nullptr, 0.0, part,
-				                               TPL);
+				backwardEvent<KIND, TOF, COMP, false, VEC>(P, out + fo, __ldg(in + e),
+				                                           p1, p2, n1, n2, tofv, k,
+				                                           nullptr, 0.0, part, TPL);
 		}
 		else
 		{
@@ -616,7 +677,7 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 			const float a = E.att ? __ldg(E.att + e) : 1.0f;
 			if (m == 0.f || s == 0.f || a == 0.f)
 				return;
-			float u = groupSum<TPL>(forwardEvent<KIND, TOF, COMP>(
+			float u = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, VEC>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			u *= s;
 			u *= a;
@@ -634,8 +695,9 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 					                                     n2, tofv, k, F.acc + fo,
 					                                     fixedScale(F));
 				else
-					backwardEvent<KIND, TOF, COMP>(P, out + fo, u, p1, p2, n1, n2,
-					                               tofv, k, nullptr, 0.0, part, TPL);
+					backwardEvent<KIND, TOF, COMP, false, VEC>(P, out + fo, u, p1, p2,
+					                                           n1, n2, tofv, k, nullptr,
+					                                           0.0, part, TPL);
 			}
 		}
 	}
@@ -1404,7 +1466,7 @@ struct yrtb_projector
 	int2* d_z = nullptr;
 	unsigned long long* d_err = nullptr;
 	// Launch configuration of the single-ray Siddon event kernels.
-	yrtb_launch_config launch{256, 1, 3, YRTB_ORDER_LOR, 1};
+	yrtb_launch_config launch{256, 1, 3, YRTB_ORDER_LOR, 1, 1};
 	// Deterministic back projection: fixed-point image (nvox * nt) and bound.
 	bool det = false;
 	unsigned long long* d_fix = nullptr;
@@ -1536,11 +1598,26 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
                  const float* in, float* out, float gs, float thr,
                  cudaStream_t st, const Fixed& F)
 {
+	// Float4 groups need 16-byte aligned frames of the images read and
+	// written (every frame starts at a multiple of nvox floats).
+	const float* img = OP == OP_BWD ? out : in;
+	const bool aligned = (reinterpret_cast<uintptr_t>(img) % 16 == 0) &&
+	                     (OP != OP_EM || reinterpret_cast<uintptr_t>(out) % 16 == 0) &&
+	                     (h->P.g.nvox % 4 == 0);
 	auto go = [&](auto tplc)
 	{
 		constexpr int TPL = decltype(tplc)::value;
 		const uint64_t threads = R.count * TPL;
 		const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, (threads + B - 1) / B));
+		if constexpr (TPL == 1)
+		{
+			if (aligned && h->launch.vector_groups)
+			{
+				k_events<OP, K, T, C, false, B, 1, true><<<grid, B, 0, st>>>(
+				    h->P, E, R, in, out, gs, thr, h->d_err, F);
+				return;
+			}
+		}
 		k_events<OP, K, T, C, false, B, TPL><<<grid, B, 0, st>>>(h->P, E, R, in, out, gs,
 		                                                        thr, h->d_err, F);
 	};
@@ -1985,6 +2062,8 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 		            "order must be YRTB_ORDER_LOR, YRTB_ORDER_SPATIAL or YRTB_ORDER_SPATIAL_FINE");
 	if (c->tile_shift < 0 || c->tile_shift > 4)
 		return fail(YRTB_ERR_ARGUMENT, "tile_shift must be in 0..4");
+	if (c->vector_groups != 0 && c->vector_groups != 1)
+		return fail(YRTB_ERR_ARGUMENT, "vector_groups must be 0 or 1");
 	h->launch = *c;
 	return YRTB_OK;
 }
@@ -2599,23 +2678,24 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 			bestIdx = i;
 		return YRTB_OK;
 	};
-	// Stage 1: event orders, with the current block size and threads per LOR.
-	for (int shift : {3, 4, 5, 7})
-	{
-		yrtb_launch_config c = saved;
-		c.bucket_shift = shift;
-		c.order = YRTB_ORDER_LOR;
-		if (s == YRTB_OK)
-			s = timeOne(c);
-		for (int order : {YRTB_ORDER_SPATIAL, YRTB_ORDER_SPATIAL_FINE})
-			for (int tile : {0, 1, 2})
+	// Stage 1: event orders x vector groups, with the current block size and
+	// threads per LOR (one thread per LOR when the projector splits none).
+	const int orders[5][2] = {{YRTB_ORDER_LOR, 1}, {YRTB_ORDER_SPATIAL, 0},
+	                          {YRTB_ORDER_SPATIAL, 1}, {YRTB_ORDER_SPATIAL, 2},
+	                          {YRTB_ORDER_SPATIAL_FINE, 1}};
+	for (int shift : {3, 4, 5})
+		for (const auto& ot : orders)
+			for (int vec : {1, 0})
 			{
-				c.order = order;
-				c.tile_shift = tile;
+				yrtb_launch_config c = saved;
+				c.threads_per_lor = 1;
+				c.bucket_shift = shift;
+				c.order = ot[0];
+				c.tile_shift = ot[1];
+				c.vector_groups = vec;
 				if (s == YRTB_OK)
 					s = timeOne(c);
 			}
-	}
 	// Stage 2: block size x threads per LOR on the fastest order.
 	if (s == YRTB_OK && bestIdx >= 0)
 	{

@@ -78,7 +78,7 @@ class yrtb_osem_params(ctypes.Structure):
 class yrtb_launch_config(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int), ("threads_per_lor", ctypes.c_int),
                 ("bucket_shift", ctypes.c_int), ("order", ctypes.c_int),
-                ("tile_shift", ctypes.c_int)]
+                ("tile_shift", ctypes.c_int), ("vector_groups", ctypes.c_int)]
 
 
 YRTB_TUNE_MAX = 64

@@ -732,16 +732,17 @@ class DeviceProjector:
 
     # ------------------------------------------------ launch configuration --
     def set_launch(self, block: int = 256, threads_per_lor: int = 1,
-                   bucket_shift: int = 3, order: int = 0, tile_shift: int = 1):
+                   bucket_shift: int = 3, order: int = 0, tile_shift: int = 1,
+                   vector_groups: int = 1):
         c = L.yrtb_launch_config(int(block), int(threads_per_lor), int(bucket_shift),
-                                 int(order), int(tile_shift))
+                                 int(order), int(tile_shift), int(vector_groups))
         L.check(L.lib().yrtb_projector_set_launch(self.h, ctypes.byref(c)))
 
     @staticmethod
     def _launch_dict(c) -> dict:
         return {"block": c.block, "threads_per_lor": c.threads_per_lor,
                 "bucket_shift": c.bucket_shift, "order": c.order,
-                "tile_shift": c.tile_shift}
+                "tile_shift": c.tile_shift, "vector_groups": c.vector_groups}
 
     def get_launch(self) -> dict:
         c = L.yrtb_launch_config()
