@@ -53,9 +53,11 @@ def project(x, projector, events):
 
 def poisson_nll(x, projector, events, sens_image, eps: float = 1e-12):
     """List-mode Poisson negative log-likelihood:
-    sum_j s_j x_j - sum_e log(y_e) with y = A x."""
-    y = project(x, projector, events)
+    sum_j s_j x_j - sum_e log(y_e) with y = A x.  Both reductions run in
+    FP64 (millions of terms); the projections and gradients stay FP32."""
+    y = project(x, projector, events).double()
+    xd = x.double()
     if x.dim() == 5:
-        lin = (sens_image[None] * x).sum(dim=tuple(range(1, x.dim())))
+        lin = (sens_image[None].double() * xd).sum(dim=tuple(range(1, x.dim())))
         return lin - torch.log(y.clamp_min(eps)).sum(dim=-1)
-    return (sens_image * x).sum() - torch.log(y.clamp_min(eps)).sum()
+    return (sens_image.double() * xd).sum() - torch.log(y.clamp_min(eps)).sum()

@@ -49,6 +49,10 @@ class OSEM_GPU:
         # of the events before reconstructing (yrtb_autotune).
         self.autotune = False
         self.lastTuneReport = None
+        # Fixed launch configuration (a dict as returned by
+        # DeviceProjector.get_launch, e.g. lastTuneReport["best"] of an
+        # earlier reconstruction); used when autotune is off.
+        self.launchConfig = None
         self._data = None
         self._sens_images: List[torch.Tensor] = []
         self._sens_histo = None
@@ -205,6 +209,8 @@ class OSEM_GPU:
             ev.additive = base.additive if base.additive is not None else _dev(
                 lm.randoms, torch.float32)
         offsets = None
+        if self.launchConfig is not None and not self.autotune:
+            proj.set_launch(**self.launchConfig)
         if self.autotune:
             probe = torch.full(proj.img_params.shape, self.INITIAL_VALUE_MLEM,
                                dtype=torch.float32, device="cuda")
