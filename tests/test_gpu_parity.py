@@ -241,11 +241,17 @@ def test_multiray_vs_oracle_with_device_offsets():
 
 
 # ---------------------------------------------------------------- DD ------
-@pytest.mark.parametrize("tof,psf", [(None, False), ((214.0, 5), False),
-                                     (None, True), ((214.0, 5), True)])
-def test_dd_vs_oracle(tof, psf):
+@pytest.mark.parametrize("tof,psf,prec", [(None, False, L.YRTB_MIRROR),
+                                          ((214.0, 5), False, L.YRTB_MIRROR),
+                                          (None, True, L.YRTB_MIRROR),
+                                          ((214.0, 5), True, L.YRTB_MIRROR),
+                                          (None, True, L.YRTB_COMPENSATED),
+                                          ((214.0, 5), True, L.YRTB_COMPENSATED)])
+def test_dd_vs_oracle(tof, psf, prec):
+    # Compensated DD + PSF takes the PSF integrals from prefix sums of the
+    # kernel's trapezoid bins instead of the bin-by-bin loop.
     table = gaussian_psf() if psf else None
-    sc, ip, p = make(projector="DD", tof=tof, psf=table)
+    sc, ip, p = make(projector="DD", tof=tof, psf=table, precision=prec)
     d1, d2 = random_events(SC_ARGS, 6000, 14)
     rng = np.random.default_rng(15)
     tv = rng.normal(0, 300, len(d1)).astype(np.float32) if tof else None
@@ -265,6 +271,12 @@ def test_dd_vs_oracle(tof, psf):
     assert rel_l2(v, f64) < 1e-5
     if tof is None and not psf:
         assert np.array_equal(bits(v), bits(f32))
+    # Adjoint identity of the device operator pair.
+    yv = rng.random(len(d1)).astype(np.float32)
+    bv = p.backward(torch.from_numpy(yv).cuda(), ev).cpu().numpy()
+    lhs = float(np.dot(v.astype(np.float64), yv))
+    rhs = float(np.sum(bv.astype(np.float64) * img))
+    assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
     y = rng.random(len(d1)).astype(np.float32)
     b = p.backward(torch.from_numpy(y).cuda(), ev).cpu().numpy()
     b64 = po.project(oip, pr, lors, values=y.astype(np.float64), orients=ori,

@@ -49,6 +49,10 @@ struct Psf
 	const float* flipped;  // adjoint taps
 	int num_s, size;
 	float sStep, kSpacing;
+	// Prefix sums of the trapezoid bins of each kernel row (num_s * (size +
+	// 3)): prefix[m] = sum over bins xi = -1 .. m-2 of step (v(xi) + v(xi+1)) / 2.
+	const float* prefix;
+	const float* prefixFlipped;
 };
 
 struct Scan
@@ -611,9 +615,14 @@ struct MultiRay
 };
 
 // ---------------------------------------------------------------- DD -----
+// Integral of the linearly interpolated kernel over [x0, x1]: partial bins at
+// both ends plus the whole bins between them, summed bin by bin in the
+// reference's order, or (prefix given) as a difference of the row's prefix
+// sums, one subtraction instead of a loop over the taps.
 __device__ __forceinline__ float psfIntegral(const float* kernel,
                                              int kernelSize, float kernelStep,
-                                             float x0, float x1)
+                                             float x0, float x1,
+                                             const float* prefix = nullptr)
 {
 	const int halfSize = (kernelSize - 1) / 2;
 	if (x0 > (halfSize + 1) * kernelStep || x1 < -(halfSize + 1) * kernelStep ||
@@ -643,11 +652,19 @@ __device__ __forceinline__ float psfIntegral(const float* kernel,
 		// Bins entirely outside [-1, kernelSize] contribute exactly zero.
 		const int xi_lo = max(x0_i + 1, -1);
 		const int xi_hi = min(x1_i, kernelSize + 1);
-		for (int xi = xi_lo; xi < xi_hi; xi++)
+		if (prefix != nullptr)
 		{
-			const float v_lo = (xi < 0 || xi >= kernelSize) ? 0.f : __ldg(kernel + xi);
-			const float v_hi = (xi + 1 < 0 || xi + 1 >= kernelSize) ? 0.f : __ldg(kernel + xi + 1);
-			out += kernelStep * 0.5f * (v_lo + v_hi);
+			if (xi_hi > xi_lo)
+				out += __ldg(prefix + xi_hi + 1) - __ldg(prefix + xi_lo + 1);
+		}
+		else
+		{
+			for (int xi = xi_lo; xi < xi_hi; xi++)
+			{
+				const float v_lo = (xi < 0 || xi >= kernelSize) ? 0.f : __ldg(kernel + xi);
+				const float v_hi = (xi + 1 < 0 || xi + 1 >= kernelSize) ? 0.f : __ldg(kernel + xi + 1);
+				out += kernelStep * 0.5f * (v_lo + v_hi);
+			}
 		}
 	}
 	return out;
@@ -655,7 +672,8 @@ __device__ __forceinline__ float psfIntegral(const float* kernel,
 
 // Distance-driven footprint of one LOR.  d1, d2: crystal centres relative to
 // the image centre; n1, n2: crystal orientations.  visit(offset, weight).
-template <bool TOF, bool PSF, typename Visit>
+// FASTPSF: PSF integrals from the prefix sums (compensated precision).
+template <bool TOF, bool PSF, bool FASTPSF, typename Visit>
 __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
                                        const float3 d2, const float3 n1,
                                        const float3 n2, float thickness_trans,
@@ -667,6 +685,7 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 	const bool flag_y = fabsf(d12.y) > fabsf(d12.x);
 	const float d_norm = sqrtf(d12.x * d12.x + d12.y * d12.y + d12.z * d12.z);
 	const float* kern = nullptr;
+	const float* kpre = nullptr;
 	float ext = 0.f;
 	if constexpr (PSF)
 	{
@@ -684,6 +703,8 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 			                                                    static_cast<int>(si);
 		}
 		kern = (forward ? psf.taps : psf.flipped) + s_idx * psf.size;
+		if constexpr (FASTPSF)
+			kpre = (forward ? psf.prefix : psf.prefixFlipped) + s_idx * (psf.size + 3);
 		ext = static_cast<float>((psf.size + 1) / 2) * psf.kSpacing;
 	}
 	const float dx = g.vx, dy = g.vy, dz = g.vz;
@@ -821,7 +842,8 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 				if (xa > halfWidth * psf.kSpacing || xb < -halfWidth * psf.kSpacing || xa >= xb)
 					wxy = 0.f;
 				else
-					wxy = psfIntegral(kern, psf.size, psf.kSpacing, xa, xb);
+					wxy = psfIntegral(kern, psf.size, psf.kSpacing, xa, xb,
+					                  FASTPSF ? kpre : nullptr);
 			}
 			else
 			{

@@ -375,7 +375,7 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
 	}
 	else
 	{
-		ddWalk<TOF, KIND == K_DD_PSF>(P.g, p1, p2, n1, n2, P.scan.crystalTrans,
+		ddWalk<TOF, KIND == K_DD_PSF, COMP && KIND == K_DD_PSF>(P.g, p1, p2, n1, n2, P.scan.crystalTrans,
 		                              P.scan.crystalZ, P.tof, tofv, P.psf,
 		                              forward, visit);
 		endRay();
@@ -921,7 +921,7 @@ enum HistoMode
 	H_FIX = 2
 };
 
-template <int KIND, bool EM, int MODE = H_PLAIN>
+template <int KIND, bool EM, int MODE = H_PLAIN, bool COMP = false>
 __global__ void __launch_bounds__(kBlock)
     k_histo(KParams P, H3Dev H, uint64_t count, uint64_t numPhiSubset,
             uint64_t numSubsets, uint64_t subset, const float* __restrict__ img,
@@ -974,10 +974,10 @@ __global__ void __launch_bounds__(kBlock)
 		{
 			float u;
 			if constexpr (MODE == H_BOUND)
-				u = forwardEvent<KIND, false, false, true>(P, img, p1, p2, n1, n2,
-				                                           0.f, k, &mw);
+				u = forwardEvent<KIND, false, COMP, true>(P, img, p1, p2, n1, n2,
+				                                          0.f, k, &mw);
 			else
-				u = forwardEvent<KIND, false, false>(P, img, p1, p2, n1, n2, 0.f, k);
+				u = forwardEvent<KIND, false, COMP>(P, img, p1, p2, n1, n2, 0.f, k);
 			u *= s;
 			u *= a;
 			u *= globalScale;
@@ -994,15 +994,15 @@ __global__ void __launch_bounds__(kBlock)
 		else if constexpr (MODE == H_BOUND)
 		{
 			if (v != 0.f)
-				mw = maxWeightEvent<KIND, false, false>(P, p1, p2, n1, n2, 0.f, k);
+				mw = maxWeightEvent<KIND, false, COMP>(P, p1, p2, n1, n2, 0.f, k);
 		}
 		if constexpr (MODE == H_BOUND)
 			bound = fabsf(v) * mw;
 		else if constexpr (MODE == H_FIX)
-			backwardEvent<KIND, false, false, true>(P, nullptr, v, p1, p2, n1, n2,
-			                                        0.f, k, F.acc, fixedScale(F));
+			backwardEvent<KIND, false, COMP, true>(P, nullptr, v, p1, p2, n1, n2,
+			                                       0.f, k, F.acc, fixedScale(F));
 		else
-			backwardEvent<KIND, false, false>(P, out, v, p1, p2, n1, n2, 0.f, k);
+			backwardEvent<KIND, false, COMP>(P, out, v, p1, p2, n1, n2, 0.f, k);
 	} while (false);
 	if constexpr (MODE == H_BOUND)
 		warpMaxInto(maxBits, bound != bound ? __uint_as_float(0x7fffffffu) : bound);
@@ -1462,6 +1462,8 @@ struct yrtb_projector
 	float4* d_ori = nullptr;
 	float* d_taps = nullptr;
 	float* d_flipped = nullptr;
+	float* d_prefix = nullptr;
+	float* d_prefixFlipped = nullptr;
 	int32_t* d_ring = nullptr;
 	int2* d_z = nullptr;
 	unsigned long long* d_err = nullptr;
@@ -1481,6 +1483,8 @@ struct yrtb_projector
 		cudaFree(d_ori);
 		cudaFree(d_taps);
 		cudaFree(d_flipped);
+		cudaFree(d_prefix);
+		cudaFree(d_prefixFlipped);
 		cudaFree(d_ring);
 		cudaFree(d_z);
 		cudaFree(d_err);
@@ -1538,7 +1542,8 @@ yrtb_status checkEvents(const yrtb_projector* h, const yrtb_events* ev,
 
 // Calls fn(kind, tof, comp) with the projector's configuration as
 // std::integral_constant / bool_constant values (compensated arithmetic
-// exists for the Siddon projectors only).
+// exists for the Siddon projectors and, as prefix-sum PSF integrals, for
+// distance-driven projection with a PSF).
 template <typename Fn>
 void withConfig(const yrtb_projector* h, Fn&& fn)
 {
@@ -1546,7 +1551,8 @@ void withConfig(const yrtb_projector* h, Fn&& fn)
 	auto go = [&](auto kind)
 	{
 		using K = decltype(kind);
-		if constexpr (K::value == K_SIDDON || K::value == K_SIDDON_MR)
+		if constexpr (K::value == K_SIDDON || K::value == K_SIDDON_MR ||
+		              K::value == K_DD_PSF)
 		{
 			if (tof && comp)
 				fn(kind, std::true_type{}, std::true_type{});
@@ -1724,31 +1730,43 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 		if (s != YRTB_OK)
 			return s;
 	}
-	auto launch = [&](auto kind)
+	auto launch = [&](auto kind, auto comp)
 	{
 		constexpr int K = decltype(kind)::value;
+		constexpr bool C = decltype(comp)::value;
 		if (h->det)
 		{
-			k_histo<K, EM, H_BOUND><<<grid, kBlock, 0, st>>>(
+			k_histo<K, EM, H_BOUND, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
 			    acfH, addH, mg, mu, gs, thr, F, h->d_fixMax);
-			k_histo<K, EM, H_FIX><<<grid, kBlock, 0, st>>>(
+			k_histo<K, EM, H_FIX, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
 			    acfH, addH, mg, mu, gs, thr, F, nullptr);
 		}
 		else
 		{
-			k_histo<K, EM><<<grid, kBlock, 0, st>>>(
+			k_histo<K, EM, H_PLAIN, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
 			    acfH, addH, mg, mu, gs, thr, F, nullptr);
 		}
 	};
+	// Histogram mode honours the precision for single-ray Siddon and DD + PSF.
 	switch (h->kind)
 	{
-	case K_SIDDON: launch(std::integral_constant<int, K_SIDDON>{}); break;
-	case K_SIDDON_MR: launch(std::integral_constant<int, K_SIDDON_MR>{}); break;
-	case K_DD: launch(std::integral_constant<int, K_DD>{}); break;
-	default: launch(std::integral_constant<int, K_DD_PSF>{}); break;
+	case K_SIDDON:
+		if (h->comp)
+			launch(std::integral_constant<int, K_SIDDON>{}, std::true_type{});
+		else
+			launch(std::integral_constant<int, K_SIDDON>{}, std::false_type{});
+		break;
+	case K_SIDDON_MR: launch(std::integral_constant<int, K_SIDDON_MR>{}, std::false_type{}); break;
+	case K_DD: launch(std::integral_constant<int, K_DD>{}, std::false_type{}); break;
+	default:
+		if (h->comp)
+			launch(std::integral_constant<int, K_DD_PSF>{}, std::true_type{});
+		else
+			launch(std::integral_constant<int, K_DD_PSF>{}, std::false_type{});
+		break;
 	}
 	if (h->det)
 		fixedEnd(h, F, out, st);
@@ -2014,8 +2032,34 @@ yrtb_status yrtb_projector_create(const yrtb_scanner* s, const float* lut,
 		YRTB_CUDA(cudaMalloc(&h->d_flipped, n * sizeof(float)));
 		YRTB_CUDA(cudaMemcpy(h->d_taps, pp->psf_taps, n * sizeof(float), cudaMemcpyHostToDevice));
 		YRTB_CUDA(cudaMemcpy(h->d_flipped, flipped.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+		// Prefix sums of the trapezoid bins per kernel row (FP64, stored FP32).
+		const int K = pp->psf_size, W = K + 3;
+		auto prefixOf = [&](const std::vector<float>& t, std::vector<float>& out)
+		{
+			out.assign(static_cast<size_t>(pp->psf_num_s) * W, 0.f);
+			for (int i = 0; i < pp->psf_num_s; i++)
+			{
+				auto v = [&](int k) { return (k < 0 || k >= K) ? 0.0 : double(t[size_t(i) * K + k]); };
+				double acc = 0.0;
+				out[size_t(i) * W + 0] = 0.f;
+				for (int m = 1; m < W; m++)
+				{
+					const int xi = m - 2;
+					if (xi >= -1)
+						acc += double(pp->psf_k_spacing) * 0.5 * (v(xi) + v(xi + 1));
+					out[size_t(i) * W + m] = static_cast<float>(acc);
+				}
+			}
+		};
+		std::vector<float> taps(pp->psf_taps, pp->psf_taps + n), pre, preF;
+		prefixOf(taps, pre);
+		prefixOf(flipped, preF);
+		YRTB_CUDA(cudaMalloc(&h->d_prefix, pre.size() * sizeof(float)));
+		YRTB_CUDA(cudaMalloc(&h->d_prefixFlipped, preF.size() * sizeof(float)));
+		YRTB_CUDA(cudaMemcpy(h->d_prefix, pre.data(), pre.size() * sizeof(float), cudaMemcpyHostToDevice));
+		YRTB_CUDA(cudaMemcpy(h->d_prefixFlipped, preF.data(), preF.size() * sizeof(float), cudaMemcpyHostToDevice));
 		P.psf = Psf{h->d_taps, h->d_flipped, pp->psf_num_s, pp->psf_size,
-		            pp->psf_s_step, pp->psf_k_spacing};
+		            pp->psf_s_step, pp->psf_k_spacing, h->d_prefix, h->d_prefixFlipped};
 	}
 	h->h3d.numDets = static_cast<uint32_t>(nd);
 	if (s->dets_per_ring % 2 == 0)
