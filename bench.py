@@ -534,7 +534,7 @@ def main():
                                                    if c == {"block": 256, "threads_per_lor": 1,
                                                             "bucket_shift": 3, "order": 0,
                                                             "tile_shift": 1,
-                                                            "vector_groups": 1}), None)},
+                                                            "vector_groups": 2}), None)},
                            "l2": "event arrays (1.2 GB) larger than L2; "
                                  "image (42 MB) L2-resident by design",
                            "parallelism": f"dp{world} (events sharded, EM image "

@@ -173,7 +173,7 @@ void yrtb_projector_destroy(yrtb_projector* h);
  * yrtb_backward, yrtb_em_step and the OSEM driver) and of the event ordering.
  * No reference counterpart: the reference launches one thread per event in
  * 256-thread blocks (GPUBatchSetup, include/yrt-pet/utils/GPUTypes.cuh:17-55)
- * on events in file order.  Default: {256, 1, 3, YRTB_ORDER_LOR, 1, 1}. */
+ * on events in file order.  Default: {256, 1, 3, YRTB_ORDER_LOR, 1, 2}. */
 #define YRTB_ORDER_LOR 0      /* inside a ray-length bucket: by LOR (Histogram3D bin), then TOF */
 #define YRTB_ORDER_SPATIAL 1  /* inside a ray-length bucket: by direction sector (16 azimuthal x
                                  2 axial), then the Morton code of the TOF kernel centre (the
@@ -182,7 +182,7 @@ void yrtb_projector_destroy(yrtb_projector* h);
                                       centre cells per axis instead of 256) */
 typedef struct
 {
-	int block;            /* threads per block: 128, 256 or 512 */
+	int block;            /* threads per block: 128 or 256 */
 	int threads_per_lor;  /* 1, 2 or 4 threads walk one LOR, each a piece cut
 	                         at voxel planes, the forward sum reduced over the
 	                         group; > 1 needs YRTB_COMPENSATED precision (the
@@ -192,10 +192,11 @@ typedef struct
 	                         (voxel crossings >> bucket_shift), 0..7 */
 	int order;            /* YRTB_ORDER_LOR, YRTB_ORDER_SPATIAL or YRTB_ORDER_SPATIAL_FINE */
 	int tile_shift;       /* YRTB_ORDER_SPATIAL: cells of (voxel size * 2^tile_shift), 0..4 */
-	int vector_groups;    /* 1: one-thread-per-LOR walks read the image as aligned float4
-	                         groups and send the contributions to one group as a single
-	                         red.global.add.v4.f32 (images 16-byte aligned, voxels per frame a
-	                         multiple of 4; otherwise scalar accesses are used) */
+	int vector_groups;    /* bit 0: one-thread-per-LOR walks read the image as aligned
+	                         float4 groups (consecutive x steps reuse the group held in
+	                         registers); bit 1: they send the contributions to one group as a
+	                         single red.global.add.v4.f32.  Images must be 16-byte aligned with
+	                         a multiple of 4 voxels per frame, else scalar accesses are used */
 } yrtb_launch_config;
 
 yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
@@ -217,10 +218,10 @@ typedef struct
 /* Autotuner (no reference counterpart).  Times the fused EM step of this
  * projector over a sample of the events -- subset 0 of num_subsets
  * interleaved subsets, at most max_sample events -- in two stages: first
- * 15 event orders (bucket_shift x order x tile_shift, the sample ordered
- * with each) x vector_groups with the current block size and one thread per
- * LOR, then every block size x threads per LOR the projector admits on the
- * fastest of those.
+ * 12 event orders (bucket_shift x order x tile_shift, the sample ordered
+ * with each) x 4 vector_groups with the current block size and one thread
+ * per LOR, then every block size x threads per LOR the projector admits on
+ * the fastest of those.
  * Keeps the fastest (yrtb_projector_set_launch) and reports all timings.  d_image: the image
  * the EM steps read (nx*ny*nz*nt floats; its values do not change the work).
  * Setup-time call: allocates temporaries and synchronises the stream, so it

@@ -47,8 +47,8 @@ def random_events(n, seed):
     return d1[ok][:n], d2[ok][:n]
 
 
-CONFIGS = [(b, t, v) for b in (128, 256, 512) for t in (1, 2, 4) for v in (1, 0)
-           if not (t > 1 and v == 0)]
+CONFIGS = [(b, t, v) for b in (128, 256) for t in (1, 2, 4) for v in (3, 2, 1, 0)
+           if not (t > 1 and v != 0)]
 
 
 @pytest.mark.parametrize("tof", [None, (214.0, 5)])
@@ -92,17 +92,19 @@ def test_every_launch_config_vs_oracle(tof):
 
 def test_threads_per_lor_needs_compensated_mode():
     sc, ip, p = make((214.0, 5), precision=L.YRTB_MIRROR)
-    p.set_launch(512, 1, 2)
+    p.set_launch(128, 1, 2)
     with pytest.raises(yrt.YrtbError, match="threads_per_lor > 1"):
         p.set_launch(256, 2, 3)
     with pytest.raises(yrt.YrtbError, match="block must be"):
-        p.set_launch(384, 1, 3)
+        p.set_launch(512, 1, 3)
     with pytest.raises(yrt.YrtbError, match="bucket_shift"):
         p.set_launch(256, 1, 9)
     with pytest.raises(yrt.YrtbError, match="order must be"):
         p.set_launch(256, 1, 3, order=3)
     with pytest.raises(yrt.YrtbError, match="tile_shift"):
         p.set_launch(256, 1, 3, order=1, tile_shift=5)
+    with pytest.raises(yrt.YrtbError, match="vector_groups"):
+        p.set_launch(256, 1, 3, vector_groups=4)
 
 
 @pytest.mark.parametrize("shift,order,tile", [(0, 0, 1), (2, 0, 1), (5, 0, 1),
@@ -153,9 +155,9 @@ def test_autotune_keeps_fastest_and_reconstruction_matches():
         reports.append(osem.lastTuneReport)
     rep = reports[1]
     assert 0 < rep["sample_events"] <= (len(e["d1"]) + 2) // 3
-    # 3 bucket shifts x 5 orders x vector groups on/off, then 3 blocks x
+    # 3 bucket shifts x 4 orders x 4 vector-group modes, then 2 blocks x
     # 3 threads/LOR minus the stage-1 shape.
-    assert len(rep["tried"]) == 3 * 5 * 2 + 3 * 3 - 1
+    assert len(rep["tried"]) == 3 * 4 * 4 + 2 * 3 - 1
     best_ms = min(ms for _, ms in rep["tried"])
     assert [c for c, ms in rep["tried"] if ms == best_ms][0] == rep["best"]
     assert rel_l2(outs[1], outs[0]) < 1e-5

@@ -610,7 +610,7 @@ __device__ __forceinline__ float groupSum(float v)
 // the compiler's register choice.  FIX (OP_BWD, OP_EM): pass 2 of the
 // deterministic back projection.
 template <int OP, int KIND, bool TOF, bool COMP, bool FIX = false,
-          int BLOCK = kBlock, int TPL = 1, bool VEC = false>
+          int BLOCK = kBlock, int TPL = 1, int VEC = 0>
 __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
     k_events(KParams P, Events E, Range R, const float* __restrict__ in,
              float* __restrict__ out, float globalScale, float denomThr,
@@ -654,7 +654,7 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 		}
 		else if constexpr (OP == OP_FWD)
 		{
-			const float v = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, VEC>(
+			const float v = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			if (part == 0)
 				out[e] = v;
@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 				                                     p2, n1, n2, tofv, k,
 				                                     F.acc + fo, fixedScale(F));
 			else
-				backwardEvent<KIND, TOF, COMP, false, VEC>(P, out + fo, __ldg(in + e),
+				backwardEvent<KIND, TOF, COMP, false, (VEC & 2) != 0>(P, out + fo, __ldg(in + e),
 				                                           p1, p2, n1, n2, tofv, k,
 				                                           nullptr, 0.0, part, TPL);
 		}
@@ -677,7 +677,7 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 			const float a = E.att ? __ldg(E.att + e) : 1.0f;
 			if (m == 0.f || s == 0.f || a == 0.f)
 				return;
-			float u = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, VEC>(
+			float u = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			u *= s;
 			u *= a;
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 					                                     n2, tofv, k, F.acc + fo,
 					                                     fixedScale(F));
 				else
-					backwardEvent<KIND, TOF, COMP, false, VEC>(P, out + fo, u, p1, p2,
+					backwardEvent<KIND, TOF, COMP, false, (VEC & 2) != 0>(P, out + fo, u, p1, p2,
 					                                           n1, n2, tofv, k, nullptr,
 					                                           0.0, part, TPL);
 			}
@@ -1468,7 +1468,7 @@ struct yrtb_projector
 	int2* d_z = nullptr;
 	unsigned long long* d_err = nullptr;
 	// Launch configuration of the single-ray Siddon event kernels.
-	yrtb_launch_config launch{256, 1, 3, YRTB_ORDER_LOR, 1, 1};
+	yrtb_launch_config launch{256, 1, 3, YRTB_ORDER_LOR, 1, 2};
 	// Deterministic back projection: fixed-point image (nvox * nt) and bound.
 	bool det = false;
 	unsigned long long* d_fix = nullptr;
@@ -1617,10 +1617,25 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 		const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, (threads + B - 1) / B));
 		if constexpr (TPL == 1)
 		{
-			if (aligned && h->launch.vector_groups)
+			// Bit 0: float4 gathers (forward), bit 1: float4 reductions
+			// (back projection); each op instantiates only the bits it uses.
+			constexpr int kUse = OP == OP_FWD ? 1 : (OP == OP_BWD ? 2 : 3);
+			const int vg = aligned ? (h->launch.vector_groups & kUse) : 0;
+			if (vg == 1 || vg == 2 || vg == 3)
 			{
-				k_events<OP, K, T, C, false, B, 1, true><<<grid, B, 0, st>>>(
-				    h->P, E, R, in, out, gs, thr, h->d_err, F);
+				auto vlaunch = [&](auto vc)
+				{
+					constexpr int V = decltype(vc)::value;
+					if constexpr ((V & kUse) == V)
+						k_events<OP, K, T, C, false, B, 1, V><<<grid, B, 0, st>>>(
+						    h->P, E, R, in, out, gs, thr, h->d_err, F);
+				};
+				if (vg == 1)
+					vlaunch(std::integral_constant<int, 1>{});
+				else if (vg == 2)
+					vlaunch(std::integral_constant<int, 2>{});
+				else
+					vlaunch(std::integral_constant<int, 3>{});
 				return;
 			}
 		}
@@ -1674,8 +1689,6 @@ yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
 			{
 				if (h->launch.block == 128)
 					launchTuned<OP, K, T, C, 128>(h, E, R, in, out, gs, thr, st, F);
-				else if (h->launch.block == 512)
-					launchTuned<OP, K, T, C, 512>(h, E, R, in, out, gs, thr, st, F);
 				else
 					launchTuned<OP, K, T, C, 256>(h, E, R, in, out, gs, thr, st, F);
 				return;
@@ -2090,8 +2103,8 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 {
 	if (!h || !c)
 		return fail(YRTB_ERR_ARGUMENT, "null argument");
-	if (c->block != 128 && c->block != 256 && c->block != 512)
-		return fail(YRTB_ERR_ARGUMENT, "block must be 128, 256 or 512");
+	if (c->block != 128 && c->block != 256)
+		return fail(YRTB_ERR_ARGUMENT, "block must be 128 or 256");
 	if (c->threads_per_lor != 1 && c->threads_per_lor != 2 && c->threads_per_lor != 4)
 		return fail(YRTB_ERR_ARGUMENT, "threads_per_lor must be 1, 2 or 4");
 	if (c->threads_per_lor > 1 && !(h->kind == K_SIDDON && h->comp))
@@ -2106,8 +2119,8 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 		            "order must be YRTB_ORDER_LOR, YRTB_ORDER_SPATIAL or YRTB_ORDER_SPATIAL_FINE");
 	if (c->tile_shift < 0 || c->tile_shift > 4)
 		return fail(YRTB_ERR_ARGUMENT, "tile_shift must be in 0..4");
-	if (c->vector_groups != 0 && c->vector_groups != 1)
-		return fail(YRTB_ERR_ARGUMENT, "vector_groups must be 0 or 1");
+	if (c->vector_groups < 0 || c->vector_groups > 3)
+		return fail(YRTB_ERR_ARGUMENT, "vector_groups must be in 0..3");
 	h->launch = *c;
 	return YRTB_OK;
 }
@@ -2724,12 +2737,11 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	};
 	// Stage 1: event orders x vector groups, with the current block size and
 	// threads per LOR (one thread per LOR when the projector splits none).
-	const int orders[5][2] = {{YRTB_ORDER_LOR, 1}, {YRTB_ORDER_SPATIAL, 0},
-	                          {YRTB_ORDER_SPATIAL, 1}, {YRTB_ORDER_SPATIAL, 2},
-	                          {YRTB_ORDER_SPATIAL_FINE, 1}};
+	const int orders[4][2] = {{YRTB_ORDER_LOR, 1}, {YRTB_ORDER_SPATIAL, 0},
+	                          {YRTB_ORDER_SPATIAL, 1}, {YRTB_ORDER_SPATIAL, 2}};
 	for (int shift : {3, 4, 5})
 		for (const auto& ot : orders)
-			for (int vec : {1, 0})
+			for (int vec : {3, 2, 1, 0})
 			{
 				yrtb_launch_config c = saved;
 				c.threads_per_lor = 1;
@@ -2745,7 +2757,7 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	{
 		const yrtb_launch_config o = report->tried[bestIdx];
 		const bool split = h->comp && !h->det;
-		for (int block : {128, 256, 512})
+		for (int block : {128, 256})
 			for (int tpl : {1, 2, 4})
 			{
 				if ((tpl > 1 && !split) || (h->det && (block != 256 || tpl != 1)))

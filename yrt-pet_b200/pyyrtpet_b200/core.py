@@ -733,7 +733,7 @@ class DeviceProjector:
     # ------------------------------------------------ launch configuration --
     def set_launch(self, block: int = 256, threads_per_lor: int = 1,
                    bucket_shift: int = 3, order: int = 0, tile_shift: int = 1,
-                   vector_groups: int = 1):
+                   vector_groups: int = 2):
         c = L.yrtb_launch_config(int(block), int(threads_per_lor), int(bucket_shift),
                                  int(order), int(tile_shift), int(vector_groups))
         L.check(L.lib().yrtb_projector_set_launch(self.h, ctypes.byref(c)))
