@@ -438,13 +438,19 @@ def main():
             e.sens = (eff_d[e.d1.long()] * eff_d[e.d2.long()]).contiguous()
             e.att = proj.attenuation_factors(mu_flat, ip, e)
             x = torch.full((J,), 0.125, device="cuda")
-            work = torch.empty(2 * J, device="cuda")
-            p = L.yrtb_osem_params(ITERATIONS, SUBSETS, 1.0, 1e-35, 1.19209e-07,
-                                   0, 0, None, offs.ctypes.data)
-            L.check(lib.yrtb_osem_listmode(proj.h, ctypes.byref(e.c()),
-                                           sens.data_ptr(), x.data_ptr(),
-                                           work.data_ptr(), ctypes.byref(p),
-                                           s_ptr))
+            if dist is None:
+                work = torch.empty(2 * J, device="cuda")
+                p = L.yrtb_osem_params(ITERATIONS, SUBSETS, 1.0, 1e-35, 1.19209e-07,
+                                       0, 0, None, offs.ctypes.data)
+                L.check(lib.yrtb_osem_listmode(proj.h, ctypes.byref(e.c()),
+                                               sens.data_ptr(), x.data_ptr(),
+                                               work.data_ptr(), ctypes.byref(p),
+                                               s_ptr))
+            else:
+                # Sharded reconstruction: the EM image is summed over ranks
+                # once per subset (NCCL) between the EM pass and the update.
+                from pyyrtpet_b200.distributed import osem_listmode
+                osem_listmode(proj, e, offs, sens, x, ITERATIONS, SUBSETS)
             h_img.copy_(x, non_blocking=True)
 
         for _ in range(max(1, args.warmup)):
@@ -466,7 +472,9 @@ def main():
                "h2d_bytes_per_step": int(h_d1.numel() * 12),
                "d2h_bytes_per_step": int(J * 4), "ms_per_step": e2e_ms,
                "iterations_per_step": ITERATIONS,
-               "path": "yrtb_osem_listmode (C ABI) from pinned host events; "
+               "path": ("yrtb_osem_listmode (C ABI)" if dist is None else
+                        "pyyrtpet_b200.distributed.osem_listmode (C ABI EM "
+                        "passes, NCCL all-reduce per subset)") + " from pinned host events; "
                        "per step: H2D events, event ordering, device "
                        "corrections, one reconstruction of 3 OSEM iterations "
                        "x 10 subsets, D2H image"}

@@ -227,3 +227,35 @@ def test_listmode_file_unpacked_on_gpu(tmp_path, tof, randoms):
     raw.tofile(f)
     with pytest.raises(yrt.YrtbError, match="list-mode event 777"):
         yrt.ListModeLUT(sc, tof, randoms).readFromFile(f, device=True)
+
+
+def test_distributed_osem_driver_matches_c_driver_on_one_rank():
+    """pyyrtpet_b200.distributed.osem_listmode (the sharded driver, run here
+    without a process group) against yrtb_osem_listmode on the same ordered
+    events: same steps, so the images agree to float summation order."""
+    import ctypes
+    from pyyrtpet_b200 import synthetic as S
+    from pyyrtpet_b200.core import _stream
+    from pyyrtpet_b200.distributed import osem_listmode
+    sc = S.scanner_c1()
+    ip = yrt.ImageParams(32, 32, 16, 256, 256, 128)
+    pp = yrt.ProjectorParams(sc)
+    pp.addTOF(214.0, 5)
+    pp.precision = L.YRTB_COMPENSATED
+    proj = yrt.DeviceProjector(sc, ip, pp)
+    e = S.generate_events(sc, 40000, 77, tof_fwhm_ps=214.0, device="cuda")
+    ev = yrt.DeviceEvents.from_arrays(e.d1.to(torch.int32), e.d2.to(torch.int32),
+                                      tof=e.tof)
+    ev, offs = proj.order_events(ev, 4)
+    sens = torch.zeros(ip.numVoxels, device="cuda")
+    sp = yrt.DeviceProjector(sc, ip, yrt.ProjectorParams(sc))
+    sp.sensitivity_histo3d(sens, 1, 0)
+    a = torch.empty(ip.numVoxels, device="cuda")
+    osem_listmode(proj, ev, offs, sens, a, 2, 4)
+    b = torch.empty(ip.numVoxels, device="cuda")
+    work = torch.empty(2 * ip.numVoxels, device="cuda")
+    p = L.yrtb_osem_params(2, 4, 1.0, 1e-35, 1.19209e-07, 0, 0, None, offs.ctypes.data)
+    L.check(L.lib().yrtb_osem_listmode(proj.h, ctypes.byref(ev.c()), sens.data_ptr(),
+                                       b.data_ptr(), work.data_ptr(), ctypes.byref(p),
+                                       _stream()))
+    assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-6

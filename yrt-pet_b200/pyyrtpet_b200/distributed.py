@@ -41,3 +41,47 @@ def sharded_subset_update(em_local: Callable[[torch.Tensor], None],
         torch.distributed.all_reduce(em, group=group)
     update(em)
     return em
+
+
+def osem_listmode(proj, events, offsets, sens: torch.Tensor, img: torch.Tensor,
+                  iterations: int, subsets: int, global_scale: float = 1.0,
+                  denom_threshold: float = 1e-35, init_from_image: bool = False,
+                  group=None) -> torch.Tensor:
+    """List-mode OSEM over this rank's share of the events (already in
+    subset-major order, subset s = events [offsets[s], offsets[s+1])), with
+    the EM-ratio image summed over ranks once per subset.  Same steps as
+    yrtb_osem_listmode (x0 = 0.125 masked by sens > 0, sensitivity / subsets,
+    EM update with threshold EPS_FLT), driven from Python so that the
+    collective sits between the EM pass and the update."""
+    import ctypes
+    from . import _lib as L
+    from .core import _stream
+    lib = L.lib()
+    ip = proj.img_params
+    J, nt = ip.numVoxels, ip.nt
+    em = torch.empty(nt * J, dtype=torch.float32, device=img.device)
+    sens_sub = (sens.reshape(-1)[:J] / float(subsets)).contiguous()
+    s_ptr = _stream()
+    if not init_from_image:
+        L.check(lib.yrtb_fill(img.data_ptr(), nt * J, 0.125, s_ptr))
+    L.check(lib.yrtb_apply_threshold(img.data_ptr(), sens.data_ptr(), J, nt, 1,
+                                     0.0, 0.0, 0.0, 1.0, 0.0, s_ptr))
+    evc = events.c()
+
+    def em_local(s):
+        def run(buf):
+            r = L.yrtb_range(int(offsets[s]), 1, int(offsets[s + 1] - offsets[s]))
+            if r.count:
+                L.check(lib.yrtb_em_step(proj.h, img.data_ptr(), buf.data_ptr(),
+                                         ctypes.byref(evc), r, float(global_scale),
+                                         float(denom_threshold), s_ptr))
+        return run
+
+    def update(buf):
+        L.check(lib.yrtb_em_update(img.data_ptr(), buf.data_ptr(), sens_sub.data_ptr(),
+                                   J, nt, 1, 1.19209e-07, None, s_ptr))
+
+    for _ in range(iterations):
+        for s in range(subsets):
+            sharded_subset_update(em_local(s), update, em, group=group)
+    return img
