@@ -157,7 +157,11 @@ class OSEM_GPU:
         pp.projPsf_fname = self.projectorParams.projPsf_fname
         pp._psf = self.projectorParams._psf
         pp.precision = self.projectorParams.precision
-        pp.deterministic = self.projectorParams.deterministic
+        # Compensated precision accumulates the sensitivity image exactly
+        # (64-bit fixed point, the deterministic two-pass back projection):
+        # it sums every histogram bin's contribution once per reconstruction.
+        pp.deterministic = (self.projectorParams.deterministic or
+                            self.projectorParams.precision == L.YRTB_COMPENSATED)
         return DeviceProjector(self.scanner, self.imageParams.withFrames(1), pp)
 
     def _histo_dev(self, h):
