@@ -184,3 +184,14 @@ def test_em_step_same_under_every_order():
             ref = em
         else:
             assert rel_l2(em, ref) < 1e-6
+
+
+def test_release_cached_memory_after_ordering():
+    sc, ip, p = make((214.0, 5))
+    d1, d2 = random_events(20000, 49)
+    tv = np.random.default_rng(50).normal(0, 300, len(d1)).astype(np.float32)
+    ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv)
+    out, offs = p.order_events(ev, 2)
+    yrt.release_cached_memory()
+    out2, offs2 = p.order_events(ev, 2)   # the pool grows again on demand
+    assert torch.equal(out.perm, out2.perm)

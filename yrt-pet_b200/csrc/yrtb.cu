@@ -1374,11 +1374,15 @@ unsigned gridFor(uint64_t n, int perSM = 8)
 // with freed blocks retained for later calls (the default pool returns them
 // to the driver at every synchronisation, and re-mapping a gigabyte of
 // ordering keys costs more than the sort itself).
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_poolLock;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+
 cudaError_t poolAlloc(void** p, size_t bytes, cudaStream_t st)
 {
-	constexpr int kMaxDevices = 64;
-	static std::mutex lock;
-	static cudaMemPool_t pools[kMaxDevices] = {};
+	constexpr int kMaxDevices = kMaxPoolDevices;
+	std::mutex& lock = g_poolLock;
+	cudaMemPool_t* pools = g_pools;
 	int dev = 0;
 	cudaError_t e = cudaGetDevice(&dev);
 	if (e != cudaSuccess)
@@ -2096,6 +2100,22 @@ yrtb_status yrtb_projector_create(const yrtb_scanner* s, const float* lut,
 void yrtb_projector_destroy(yrtb_projector* h)
 {
 	delete h;
+}
+
+yrtb_status yrtb_release_cached_memory(void)
+{
+	std::lock_guard<std::mutex> guard(g_poolLock);
+	for (int d = 0; d < kMaxPoolDevices; d++)
+		if (g_pools[d] != nullptr)
+		{
+			int cur = 0;
+			YRTB_CUDA(cudaGetDevice(&cur));
+			YRTB_CUDA(cudaSetDevice(d));
+			YRTB_CUDA(cudaDeviceSynchronize());
+			YRTB_CUDA(cudaMemPoolTrimTo(g_pools[d], 0));
+			YRTB_CUDA(cudaSetDevice(cur));
+		}
+	return YRTB_OK;
 }
 
 yrtb_status yrtb_projector_set_launch(yrtb_projector* h,

@@ -11,7 +11,7 @@ from .core import (BinIteratorChronologicalInterleaved,  # noqa: F401
                    OperatorProjectorDevice, ProjectionOper, ProjectorParams,
                    Scanner, UniformHistogram, convertToHistogram3D,
                    histo3d_bins, histo3d_detpairs, read_psf_csv,
-                   write_psf_csv)
+                   release_cached_memory, write_psf_csv)
 from .osem import OSEM_GPU, createOSEM  # noqa: F401
 
 ListModeLUTOwned = ListModeLUT

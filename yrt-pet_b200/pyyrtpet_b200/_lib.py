@@ -105,6 +105,7 @@ SIGNATURES = {
     "yrtb_projector_destroy": ([c_vp], None),
     "yrtb_projector_set_launch": ([c_vp, _P(yrtb_launch_config)], ctypes.c_int),
     "yrtb_projector_get_launch": ([c_vp, _P(yrtb_launch_config)], ctypes.c_int),
+    "yrtb_release_cached_memory": ([], ctypes.c_int),
     "yrtb_autotune": ([c_vp, c_vp, _P(yrtb_events), ctypes.c_int, c_u64,
                        _P(yrtb_tune_report), c_vp], ctypes.c_int),
     "yrtb_multiray_offsets": ([c_vp, c_u64, c_vp, c_vp], ctypes.c_int),

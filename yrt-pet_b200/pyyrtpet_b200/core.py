@@ -647,6 +647,12 @@ class DeviceEvents:
 
 
 # ---------------------------------------------------------------- projector --
+def release_cached_memory():
+    """Return the library's cached device temporaries to the driver
+    (yrtb_release_cached_memory)."""
+    L.check(L.lib().yrtb_release_cached_memory())
+
+
 class DeviceProjector:
     """Owns one yrtb_projector handle (scanner + image grid + options)."""
 
