@@ -195,8 +195,10 @@ typedef struct
 	int vector_groups;    /* bit 0: one-thread-per-LOR walks read the image as aligned
 	                         float4 groups (consecutive x steps reuse the group held in
 	                         registers); bit 1: they send the contributions to one group as a
-	                         single red.global.add.v4.f32.  Images must be 16-byte aligned with
-	                         a multiple of 4 voxels per frame, else scalar accesses are used */
+	                         single red.global.add.v4.f32, summed in registers; bit 2: the
+	                         same with the group staged in shared memory (wins over bit 1).
+	                         Images must be 16-byte aligned with a multiple of 4 voxels per
+	                         frame, else scalar accesses are used */
 } yrtb_launch_config;
 
 yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
@@ -225,9 +227,9 @@ typedef struct
 /* Autotuner (no reference counterpart).  Times the fused EM step of this
  * projector over a sample of the events -- subset 0 of num_subsets
  * interleaved subsets, at most max_sample events -- in two stages: first
- * 12 event orders (bucket_shift x order x tile_shift, the sample ordered
- * with each) x 4 vector_groups with the current block size and one thread
- * per LOR, then every block size x threads per LOR the projector admits on
+ * 9 event orders (bucket_shift x order x tile_shift, the sample ordered
+ * with each) x 4 vector_groups modes with the current block size and one
+ * thread per LOR, then every block size x threads per LOR the projector admits on
  * the fastest of those.
  * Keeps the fastest (yrtb_projector_set_launch) and reports all timings.  d_image: the image
  * the EM steps read (nx*ny*nz*nt floats; its values do not change the work).

@@ -47,7 +47,7 @@ def random_events(n, seed):
     return d1[ok][:n], d2[ok][:n]
 
 
-CONFIGS = [(b, t, v) for b in (128, 256) for t in (1, 2, 4) for v in (3, 2, 1, 0)
+CONFIGS = [(b, t, v) for b in (128, 256) for t in (1, 2, 4) for v in (3, 2, 1, 0, 4, 5)
            if not (t > 1 and v != 0)]
 
 
@@ -104,7 +104,7 @@ def test_threads_per_lor_needs_compensated_mode():
     with pytest.raises(yrt.YrtbError, match="tile_shift"):
         p.set_launch(256, 1, 3, order=1, tile_shift=5)
     with pytest.raises(yrt.YrtbError, match="vector_groups"):
-        p.set_launch(256, 1, 3, vector_groups=4)
+        p.set_launch(256, 1, 3, vector_groups=8)
 
 
 @pytest.mark.parametrize("shift,order,tile", [(0, 0, 1), (2, 0, 1), (5, 0, 1),
@@ -155,9 +155,9 @@ def test_autotune_keeps_fastest_and_reconstruction_matches():
         reports.append(osem.lastTuneReport)
     rep = reports[1]
     assert 0 < rep["sample_events"] <= (len(e["d1"]) + 2) // 3
-    # 3 bucket shifts x 4 orders x 4 vector-group modes, then 2 blocks x
+    # 3 bucket shifts x 3 orders x 4 vector-group modes, then 2 blocks x
     # 3 threads/LOR minus the stage-1 shape.
-    assert len(rep["tried"]) == 3 * 4 * 4 + 2 * 3 - 1
+    assert len(rep["tried"]) == 3 * 3 * 4 + 2 * 3 - 1
     best_ms = min(ms for _, ms in rep["tried"])
     assert [c for c, ms in rep["tried"] if ms == best_ms][0] == rep["best"]
     assert rel_l2(outs[1], outs[0]) < 1e-5

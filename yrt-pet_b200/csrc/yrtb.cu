@@ -517,7 +517,11 @@ __device__ __forceinline__ void redV4(float* p, float4 v)
 	             :: "l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
 }
 
-template <int KIND, bool TOF, bool COMP, bool FIX = false, bool VEC = false>
+// VEC 1: the group is summed in registers; VEC 2: the group's four values
+// are staged in this thread's shared-memory slots (vslot[l * vstride]; a
+// single-ray walk visits each voxel once, so a slot is written at most once
+// per group) and read back only to send the group.
+template <int KIND, bool TOF, bool COMP, bool FIX = false, int VEC = 0>
 __device__ __forceinline__ void backwardEvent(const KParams& P,
                                               float* __restrict__ img,
                                               float v, float3 p1, float3 p2,
@@ -525,7 +529,9 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
                                               uint64_t rid,
                                               unsigned long long* fix = nullptr,
                                               double scale = 0.0, int part = 0,
-                                              int parts = 1)
+                                              int parts = 1,
+                                              float* vslot = nullptr,
+                                              int vstride = 0)
 {
 	if constexpr (KIND == K_SIDDON_MR)
 		v = v / static_cast<float>(P.numRays);
@@ -541,7 +547,41 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
 		                              endRay, part, parts);
 	}
-	else if constexpr (VEC)
+	else if constexpr (VEC == 2)
+	{
+		static_assert(KIND == K_SIDDON, "slots hold one value per voxel of one ray");
+		int gb = -1;
+		auto send = [&]
+		{
+			const float4 a = make_float4(vslot[0], vslot[vstride], vslot[2 * vstride],
+			                             vslot[3 * vstride]);
+			redV4(img + gb, a);
+		};
+		auto visit = [&](int o, float w)
+		{
+			const int g = o & ~3;
+			if (g != gb)
+			{
+				if (gb >= 0)
+					send();
+				vslot[0] = 0.f;
+				vslot[vstride] = 0.f;
+				vslot[2 * vstride] = 0.f;
+				vslot[3 * vstride] = 0.f;
+				gb = g;
+			}
+			vslot[(o & 3) * vstride] = v * w;
+		};
+		auto flush = [&]
+		{
+			if (gb >= 0)
+				send();
+			gb = -1;
+		};
+		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+		                              flush, part, parts);
+	}
+	else if constexpr (VEC == 1)
 	{
 		int gb = -1;
 		float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -623,6 +663,14 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 	const uint64_t gt = static_cast<uint64_t>(blockIdx.x) * BLOCK + threadIdx.x;
 	const uint64_t k = gt / TPL;
 	const int part = static_cast<int>(gt % TPL);
+	// Shared-memory slots of the staged float4 reductions (VEC bit 2).
+	constexpr int kRedMode = (VEC & 4) ? 2 : ((VEC & 2) ? 1 : 0);
+	float* vslot = nullptr;
+	if constexpr (kRedMode == 2)
+	{
+		__shared__ float vacc[4 * BLOCK];
+		vslot = vacc + threadIdx.x;
+	}
 	if (k < R.count)
 	{
 		const uint64_t e = R.start + k * R.stride;
@@ -666,9 +714,10 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 				                                     p2, n1, n2, tofv, k,
 				                                     F.acc + fo, fixedScale(F));
 			else
-				backwardEvent<KIND, TOF, COMP, false, (VEC & 2) != 0>(P, out + fo, __ldg(in + e),
-				                                           p1, p2, n1, n2, tofv, k,
-				                                           nullptr, 0.0, part, TPL);
+				backwardEvent<KIND, TOF, COMP, false, kRedMode>(P, out + fo, __ldg(in + e),
+				                                                p1, p2, n1, n2, tofv, k,
+				                                                nullptr, 0.0, part, TPL,
+				                                                vslot, BLOCK);
 		}
 		else
 		{
@@ -695,9 +744,10 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 					                                     n2, tofv, k, F.acc + fo,
 					                                     fixedScale(F));
 				else
-					backwardEvent<KIND, TOF, COMP, false, (VEC & 2) != 0>(P, out + fo, u, p1, p2,
-					                                           n1, n2, tofv, k, nullptr,
-					                                           0.0, part, TPL);
+					backwardEvent<KIND, TOF, COMP, false, kRedMode>(P, out + fo, u, p1, p2,
+					                                                n1, n2, tofv, k, nullptr,
+					                                                0.0, part, TPL, vslot,
+					                                                BLOCK);
 			}
 		}
 	}
@@ -1621,11 +1671,14 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 		const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, (threads + B - 1) / B));
 		if constexpr (TPL == 1)
 		{
-			// Bit 0: float4 gathers (forward), bit 1: float4 reductions
-			// (back projection); each op instantiates only the bits it uses.
-			constexpr int kUse = OP == OP_FWD ? 1 : (OP == OP_BWD ? 2 : 3);
-			const int vg = aligned ? (h->launch.vector_groups & kUse) : 0;
-			if (vg == 1 || vg == 2 || vg == 3)
+			// Bit 0: float4 gathers (forward); bit 1: float4 reductions summed
+			// in registers, bit 2: staged in shared memory (back projection,
+			// bit 2 wins).  Each op instantiates only the modes it uses.
+			constexpr int kUse = OP == OP_FWD ? 1 : (OP == OP_BWD ? 6 : 7);
+			int vg = aligned ? (h->launch.vector_groups & kUse) : 0;
+			if (vg & 4)
+				vg &= ~2;
+			if (vg != 0)
 			{
 				auto vlaunch = [&](auto vc)
 				{
@@ -1634,12 +1687,14 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 						k_events<OP, K, T, C, false, B, 1, V><<<grid, B, 0, st>>>(
 						    h->P, E, R, in, out, gs, thr, h->d_err, F);
 				};
-				if (vg == 1)
-					vlaunch(std::integral_constant<int, 1>{});
-				else if (vg == 2)
-					vlaunch(std::integral_constant<int, 2>{});
-				else
-					vlaunch(std::integral_constant<int, 3>{});
+				switch (vg)
+				{
+				case 1: vlaunch(std::integral_constant<int, 1>{}); break;
+				case 2: vlaunch(std::integral_constant<int, 2>{}); break;
+				case 3: vlaunch(std::integral_constant<int, 3>{}); break;
+				case 4: vlaunch(std::integral_constant<int, 4>{}); break;
+				default: vlaunch(std::integral_constant<int, 5>{}); break;
+				}
 				return;
 			}
 		}
@@ -2139,8 +2194,8 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 		            "order must be YRTB_ORDER_LOR, YRTB_ORDER_SPATIAL or YRTB_ORDER_SPATIAL_FINE");
 	if (c->tile_shift < 0 || c->tile_shift > 4)
 		return fail(YRTB_ERR_ARGUMENT, "tile_shift must be in 0..4");
-	if (c->vector_groups < 0 || c->vector_groups > 3)
-		return fail(YRTB_ERR_ARGUMENT, "vector_groups must be in 0..3");
+	if (c->vector_groups < 0 || c->vector_groups > 7)
+		return fail(YRTB_ERR_ARGUMENT, "vector_groups must be in 0..7");
 	h->launch = *c;
 	return YRTB_OK;
 }
@@ -2757,11 +2812,11 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	};
 	// Stage 1: event orders x vector groups, with the current block size and
 	// threads per LOR (one thread per LOR when the projector splits none).
-	const int orders[4][2] = {{YRTB_ORDER_LOR, 1}, {YRTB_ORDER_SPATIAL, 0},
-	                          {YRTB_ORDER_SPATIAL, 1}, {YRTB_ORDER_SPATIAL, 2}};
+	const int orders[3][2] = {{YRTB_ORDER_LOR, 1}, {YRTB_ORDER_SPATIAL, 1},
+	                          {YRTB_ORDER_SPATIAL, 2}};
 	for (int shift : {3, 4, 5})
 		for (const auto& ot : orders)
-			for (int vec : {3, 2, 1, 0})
+			for (int vec : {2, 4, 1, 0})
 			{
 				yrtb_launch_config c = saved;
 				c.threads_per_lor = 1;
