@@ -74,3 +74,41 @@ def test_no_cpu_fallback_when_library_missing(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
     with pytest.raises(RuntimeError, match="libyrtb.so not found"):
         _lib.lib()
+
+
+def test_ctypes_structs_match_the_c_header_layout(tmp_path):
+    """Every struct the Python binding passes through the C ABI has the size
+    and field offsets the C compiler gives it from include/yrt_b200.h."""
+    import shutil
+    import subprocess
+    from pyyrtpet_b200 import _lib
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    structs = {
+        "yrtb_scanner": _lib.yrtb_scanner, "yrtb_image_params": _lib.yrtb_image_params,
+        "yrtb_projector_params": _lib.yrtb_projector_params,
+        "yrtb_events": _lib.yrtb_events, "yrtb_range": _lib.yrtb_range,
+        "yrtb_launch_config": _lib.yrtb_launch_config,
+        "yrtb_tune_report": _lib.yrtb_tune_report,
+        "yrtb_osem_params": _lib.yrtb_osem_params,
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "yrt_b200.h"',
+             "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'printf("{name} size %zu\\n", sizeof({name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'printf("{name} {field} %zu\\n", offsetof({name}, {field}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["gcc", "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    for line in out.splitlines():
+        name, what, value = line.split()
+        cls = structs[name]
+        if what == "size":
+            assert ctypes.sizeof(cls) == int(value), name
+        else:
+            assert getattr(cls, what).offset == int(value), (name, what)
