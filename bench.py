@@ -22,6 +22,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -359,8 +360,7 @@ def main():
         step()
     torch.cuda.synchronize()
 
-    clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-    os.makedirs(os.path.dirname(clk_path), exist_ok=True)
+    clk_path = os.path.join(tempfile.mkdtemp(prefix="yrtb_clocks_"), f"clocks_rank{rank}.csv")
     sampler = clocks_sampler(clk_path) if rank == 0 else None
     time.sleep(0.5)
     if dist is not None:
@@ -520,9 +520,8 @@ def main():
     cpu = None
     parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        # Checker (CPU baseline leg): forward projections of a sample of the
-        # workload's events in this run's precision mode against the FP64
-        # oracle.
+        # CPU leg: forward projections of a sample of the workload's events in
+        # this run's precision mode against the FP64 oracle.
         try:
             parity = fp64_parity(sc, ip, proj, ev_plain, args.parity_sample,
                                  args.precision)

@@ -20,9 +20,9 @@ each printing one JSON line:
       subsets) against the plain form (one single-frame reconstruction per
       frame).
 
-Inputs are seeded synthetic events (SURVEY: no datasets are available); the
-reference CPU measurements use oracle/_ref, the reference library built from
-its sources, where present.
+Inputs are seeded synthetic events (the reference's datasets are not
+available); the reference CPU measurements use oracle/_ref, the reference
+library built from its sources, where present.
 """
 from __future__ import annotations
 

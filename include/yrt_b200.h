@@ -209,7 +209,7 @@ yrtb_status yrtb_projector_get_launch(const yrtb_projector* h,
 /* Temporaries of yrtb_events_subset_order, yrtb_attenuation_factors and
  * yrtb_autotune come from a stream-ordered memory pool per device that keeps
  * freed blocks for later calls (ordering 50M events holds about 3.6 GB).
- * This returns them to the driver (synchronises every device that has a
+ * This returns them to the CUDA driver (synchronises every device that has a
  * pool).  No reference counterpart. */
 yrtb_status yrtb_release_cached_memory(void);
 

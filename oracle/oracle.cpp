@@ -1,7 +1,7 @@
 // TEST INFRASTRUCTURE — NOT PART OF THE PRODUCT.
 //
-// CPU restatement of the YRT-PET 2.0.7 projection hot path, used only as the
-// checker by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg.
+// CPU restatement of the YRT-PET 2.0.7 projection hot path, used only to check
+// results in tests/ and __graft_entry__.smoke() and in bench.py's CPU leg.
 // The product (yrt-pet_b200/) never links, loads or calls this file.
 //
 // Every routine is templated on the arithmetic type T:

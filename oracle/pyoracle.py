@@ -1,8 +1,8 @@
 """Test infrastructure: ctypes front-end of the CPU oracle and of the reference.
 
 Two CPU implementations of the YRT-PET projection hot path are reachable from
-here, both used only as checkers (tests/, ``__graft_entry__.smoke()`` and the
-CPU-baseline leg of ``bench.py``):
+here, both used only to check results (tests/, ``__graft_entry__.smoke()``)
+and to time the CPU baseline (``bench.py``):
 
 * ``liboracle.so``   -- the restatement in ``oracle/oracle.cpp`` (float mirror
   of the reference's FP32 order, and an FP64 oracle);

@@ -1,6 +1,6 @@
 # Builds the reference's CPU path (YRT-PET 2.0.7) straight from its sources with
 # g++, without its CMake project, into oracle/_ref/.  Test infrastructure only:
-# the outputs are the checker and the timed CPU baseline, never the product.
+# the outputs check results and give the timed CPU baseline, never the product.
 #
 #   make -f oracle/ref.mk -j8 REF=/root/reference/yrt-pet
 #

@@ -1422,7 +1422,7 @@ unsigned gridFor(uint64_t n, int perSM = 8)
 // Temporaries of the event ordering, the attenuation factors and the
 // autotuner come from a stream-ordered pool the library keeps per device,
 // with freed blocks retained for later calls (the default pool returns them
-// to the driver at every synchronisation, and re-mapping a gigabyte of
+// to the CUDA driver at every synchronisation, and re-mapping a gigabyte of
 // ordering keys costs more than the sort itself).
 constexpr int kMaxPoolDevices = 64;
 std::mutex g_poolLock;

@@ -648,7 +648,7 @@ class DeviceEvents:
 
 # ---------------------------------------------------------------- projector --
 def release_cached_memory():
-    """Return the library's cached device temporaries to the driver
+    """Return the library's cached device temporaries to the CUDA driver
     (yrtb_release_cached_memory)."""
     L.check(L.lib().yrtb_release_cached_memory())
 

@@ -280,7 +280,7 @@ class OSEM_GPU:
             mask_src = self._mask
         else:
             mask_src = sens
-        # The driver masks with its sensitivity argument; give it the mask
+        # yrtb_osem_listmode masks with its sensitivity argument; give it the mask
         # first when a separate mask image is set.
         p = L.yrtb_osem_params(self.num_MLEM_iterations, self.num_OSEM_subsets,
                                self._global, self.denomThreshold, self.EPS_FLT,
