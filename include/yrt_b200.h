@@ -317,7 +317,8 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
                                      yrtb_stream stream);
 
 /* out->X[i] = in->X[d_perm[i]] for every array present in `in` (output
- * buffers allocated by the caller; out->count == in->count). */
+ * buffers allocated by the caller; out->count == in->count).  d_perm must be
+ * a permutation of 0..count-1, as yrtb_events_subset_order produces. */
 yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
                                const yrtb_events* out, yrtb_stream stream);
 

@@ -1202,6 +1202,42 @@ __global__ void k_gather_set(GatherSet G, const unsigned long long* __restrict__
 	}
 }
 
+// Up to four 32-bit arrays interleaved into one 16-byte record per event
+// (a streaming pass), so that the permutation then reads one sector per event
+// instead of one per array.
+__global__ void k_pack4(GatherSet G, int first, int count, uint64_t n,
+                        uint4* __restrict__ packed)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+	{
+		uint32_t v[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+		for (int a = 0; a < 4; a++)
+			if (a < count)
+				v[a] = __ldg(G.src[first + a] + i);
+		packed[i] = make_uint4(v[0], v[1], v[2], v[3]);
+	}
+}
+
+__global__ void k_unpack4_gather(GatherSet G, int first, int count, uint64_t n,
+                                 const uint4* __restrict__ packed,
+                                 const unsigned long long* __restrict__ perm)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < n; i += nthreads)
+	{
+		const uint4 r = __ldg(packed + __ldg(perm + i));
+		const uint32_t v[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+		for (int a = 0; a < 4; a++)
+			if (a < count)
+				G.dst[first + a][i] = v[a];
+	}
+}
+
 template <typename T>
 __global__ void k_gather(const T* __restrict__ in, const unsigned long long* __restrict__ perm,
                          uint64_t n, int width, T* __restrict__ out)
@@ -1902,15 +1938,21 @@ yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
 	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(
 	    h->P, h->h3d, h->h3 != nullptr, toDev(ev), n, S, counts, cfg.bucket_shift,
 	    lorShift, cfg.order, cell, keys, vals);
+	// Only the key bits in use are sorted: the subset field ends at bit
+	// (frames ? 52 : 48) + bits(S - 1).
+	int sBits = 0;
+	while (sBits < 16 && ((S - 1) >> sBits) != 0)
+		sBits++;
+	const int endBit = std::min(64, (ev->frame ? 52 : 48) + sBits);
 	ce = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals,
 	                                     reinterpret_cast<unsigned long long*>(d_perm),
-	                                     n, 0, 64, st);
+	                                     n, 0, endBit, st);
 	if (ce == cudaSuccess)
 		ce = poolAlloc(&temp, tempBytes, st);
 	if (ce == cudaSuccess)
 		ce = cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals,
 		                                     reinterpret_cast<unsigned long long*>(d_perm),
-		                                     n, 0, 64, st);
+		                                     n, 0, endBit, st);
 	release();
 	if (ce != cudaSuccess)
 		return fail(YRTB_ERR_CUDA, cudaGetErrorString(ce));
@@ -2241,8 +2283,17 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
 	                   reinterpret_cast<cudaStream_t>(stream));
 }
 
-yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
-                               const yrtb_events* out, yrtb_stream stream)
+}  // extern "C"
+
+namespace
+{
+// out->X[i] = in->X[d_perm[i]].  packable: d_perm is a permutation of
+// 0..count-1, so the source arrays may be interleaved into 16-byte records
+// first (one random sector per event); otherwise (a perm that reaches
+// beyond count, e.g. every S-th event of a longer array) the arrays are read
+// directly.
+yrtb_status gatherEvents(const yrtb_events* in, const uint64_t* d_perm,
+                         const yrtb_events* out, yrtb_stream stream, bool packable)
 {
 	if (!in || !out || !d_perm)
 		return fail(YRTB_ERR_ARGUMENT, "invalid gather arguments");
@@ -2282,10 +2333,49 @@ yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
 	    (r = add(in->sens, out->sens)) || (r = add(in->att, out->att)) ||
 	    (r = add(in->additive, out->additive)) || (r = g32(in->lor, out->lor, 6)))
 		return r;
-	if (G.count > 0)
+	if (G.count == 1)
+	{
 		k_gather_set<<<gridFor(n, 16), kBlock, 0, st>>>(G, perm, n);
+	}
+	else if (G.count > 1 && !packable)
+	{
+		k_gather_set<<<gridFor(n, 16), kBlock, 0, st>>>(G, perm, n);
+	}
+	else if (G.count > 1)
+	{
+		// Groups of up to four arrays: pack, then one 16-byte random read per
+		// event (four 4-byte random reads cost four sectors).
+		uint4* packed = nullptr;
+		const cudaError_t ce = poolAlloc(&packed, n * sizeof(uint4), st);
+		if (ce != cudaSuccess)
+		{
+			(void)cudaGetLastError();  // no room for the records: read directly
+			k_gather_set<<<gridFor(n, 16), kBlock, 0, st>>>(G, perm, n);
+		}
+		else
+		{
+			for (int first = 0; first < G.count; first += 4)
+			{
+				const int cnt = std::min(4, G.count - first);
+				k_pack4<<<gridFor(n, 16), kBlock, 0, st>>>(G, first, cnt, n, packed);
+				k_unpack4_gather<<<gridFor(n, 16), kBlock, 0, st>>>(G, first, cnt, n,
+				                                                      packed, perm);
+			}
+			cudaFreeAsync(packed, st);
+		}
+	}
 	YRTB_LAUNCHED();
 	return YRTB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
+                               const yrtb_events* out, yrtb_stream stream)
+{
+	return gatherEvents(in, d_perm, out, stream, true);
 }
 
 yrtb_status yrtb_projector_take_event_errors(yrtb_projector* h, uint64_t* count)
@@ -2756,7 +2846,7 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	    static_cast<unsigned long long*>(perm), n, S);
 	yrtb_events src = *ev;
 	src.count = n;
-	if ((s = yrtb_events_gather(&src, static_cast<uint64_t*>(perm), &A, stream)) != YRTB_OK)
+	if ((s = gatherEvents(&src, static_cast<uint64_t*>(perm), &A, stream, false)) != YRTB_OK)
 	{
 		release();
 		return s;
