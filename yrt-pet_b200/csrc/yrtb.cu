@@ -898,7 +898,7 @@ __global__ void k_support_box(const float* __restrict__ img, Geom g, int* box)
 // Attenuation factor per event: exp(-0.1 * line integral of mu), walked with
 // the projector's arithmetic (COMP: compensated walk).
 template <bool COMP>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 8)
     k_attenuation(KParams P, Geom mu, Events E, Range R,
                   const float* __restrict__ muImg, const int* __restrict__ box,
                   float* __restrict__ out, unsigned long long* err)
