@@ -583,6 +583,7 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 	}
 	else if constexpr (VEC == 1)
 	{
+		static_assert(KIND == K_SIDDON, "lanes hold one value per voxel of one ray");
 		int gb = -1;
 		float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
 		auto visit = [&](int o, float w)
@@ -596,11 +597,13 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 				gb = g;
 				a4 = make_float4(0.f, 0.f, 0.f, 0.f);
 			}
+			// A single-ray walk visits each voxel once: a lane is set, never
+			// summed, inside a group.
 			const int l = o & 3;
-			a4.x += l == 0 ? c : 0.f;
-			a4.y += l == 1 ? c : 0.f;
-			a4.z += l == 2 ? c : 0.f;
-			a4.w += l == 3 ? c : 0.f;
+			a4.x = l == 0 ? c : a4.x;
+			a4.y = l == 1 ? c : a4.y;
+			a4.z = l == 2 ? c : a4.z;
+			a4.w = l == 3 ? c : a4.w;
 		};
 		auto flush = [&]
 		{
