@@ -590,20 +590,17 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 		{
 			const float c = v * w;
 			const int g = o & ~3;
-			if (g != gb)
-			{
-				if (gb >= 0)
-					redV4(img + gb, a4);
-				gb = g;
-				a4 = make_float4(0.f, 0.f, 0.f, 0.f);
-			}
+			const bool nw = g != gb;
+			if (nw && gb >= 0)
+				redV4(img + gb, a4);
+			gb = g;
 			// A single-ray walk visits each voxel once: a lane is set, never
-			// summed, inside a group.
+			// summed, inside a group (and cleared when a new group starts).
 			const int l = o & 3;
-			a4.x = l == 0 ? c : a4.x;
-			a4.y = l == 1 ? c : a4.y;
-			a4.z = l == 2 ? c : a4.z;
-			a4.w = l == 3 ? c : a4.w;
+			a4.x = l == 0 ? c : (nw ? 0.f : a4.x);
+			a4.y = l == 1 ? c : (nw ? 0.f : a4.y);
+			a4.z = l == 2 ? c : (nw ? 0.f : a4.z);
+			a4.w = l == 3 ? c : (nw ? 0.f : a4.w);
 		};
 		auto flush = [&]
 		{
