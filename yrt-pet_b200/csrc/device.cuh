@@ -333,20 +333,23 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	const float pc = TOF ? tofCenter(d_norm, tofValue) : 0.f;
 	const float inv_sigma = TOF ? 1.0f / tp.sigma : 0.f;
 	// Compensated TOF weight, per segment [a, b]:
-	//   (b - a) * L * norm * 2^(-x^2 log2(e) / 2),  x = ((a + b) L/2 - pc) / sigma
-	// with x = (a + b) * hs - pcs in one fused multiply-add and the hardware
-	// base-2 exponential (relative error below 2^-21).
-	const float hs = 0.5f * d_norm * inv_sigma;
-	const float pcs = pc * inv_sigma;
+	//   (b - a) * L * norm * 2^(-y^2),  y = x sqrt(log2(e) / 2),
+	//   x = ((a + b) L/2 - pc) / sigma
+	// with y = (a + b) * hs - pcs in one fused multiply-add (the constant
+	// folded into hs and pcs) and the hardware base-2 exponential (relative
+	// error below 2^-21).
+	constexpr float kHalfLog2e = 0.84932180028801904f;  // sqrt(log2(e) / 2)
+	const float hs = 0.5f * d_norm * inv_sigma * kHalfLog2e;
+	const float pcs = pc * inv_sigma * kHalfLog2e;
 	const float dnn = d_norm * tp.norm;
 	auto emit = [&](int o)
 	{
 		float w;
 		if constexpr (TOF && COMP)
 		{
-			const float xc = __fmaf_rn(a_cur + a_next, hs, -pcs);
+			const float y = __fmaf_rn(a_cur + a_next, hs, -pcs);
 			float g2;
-			asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(g2) : "f"(xc * xc * -0.72134752044448170f));
+			asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(g2) : "f"(-(y * y)));
 			w = (a_next - a_cur) * dnn * g2;
 		}
 		else
