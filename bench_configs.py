@@ -19,6 +19,8 @@ each printing one JSON line:
       batched form (all frames in one EM launch per subset, CUDA-graph
       subsets) against the plain form (one single-frame reconstruction per
       frame).
+  psf image-space PSF (applyA + applyAH) on the C2 image, bit-exact against
+      the reference operator.
 
 Inputs are seeded synthetic events (the reference's datasets are not
 available); the reference CPU measurements use oracle/_ref, the reference
@@ -417,4 +419,81 @@ def run_c4(args):
                   "precision": "compensated", "launch": tune["best"]})
 
 
-RUNNERS = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}
+# ------------------------------------------------------- image-space PSF --
+def run_psf(args):
+    """Image-space PSF (OperatorPsfDevice applyA + applyAH) on the C2 image,
+    4 mm FWHM Gaussian; bit-exact check and CPU time of the reference
+    operator on the same image."""
+    yrt, L, S, _stream = _yrt()
+    ip = S.image_c2()
+    psf = yrt.OperatorPsfDevice.createGaussianFromFWHM(4.0, 4.0, 4.0, ip.vx, ip.vy, ip.vz)
+    g = torch.Generator(device="cuda").manual_seed(20261203)
+    x = torch.rand(ip.shape, generator=g, device="cuda")
+    a = torch.empty_like(x)
+    ah = torch.empty_like(x)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    V = ip.numVoxels
+
+    def step():
+        psf.applyA(x, a, ip)
+        psf.applyAH(a, ah, ip)
+
+    for _ in range(args.warmup):
+        step()
+    resident, cold = [], []
+    for _ in range(args.steps):
+        with Timer() as t:
+            step()
+        resident.append(t.ms)
+        flush.fill_(1)
+        with Timer() as t:
+            step()
+        cold.append(t.ms)
+    ms_res = float(np.median(resident))
+    ms_cold = float(np.median(cold))
+    # Three passes per apply, each reading and writing every voxel once.
+    alg = 2 * 3 * 8 * V
+    peaks = _measured_peaks()
+    out = _base("image-space PSF (separable 3-D convolution, circular borders), "
+                "C2 image 256x256x160 @2mm, 4 mm FWHM Gaussian (5 taps per axis)",
+                "voxels/s (applyA + applyAH per voxel)", V / (ms_res * 1e-3),
+                "voxels/s", args.steps, args.warmup, ms_res,
+                {"kernel_taps": [len(psf.getKernelX()), len(psf.getKernelY()),
+                                 len(psf.getKernelZ())],
+                 "image_bytes": 4 * V, "l2": "image L2-resident (42 MB); "
+                 "cold = after a 256 MB flush"})
+    out["roofline"] = {"bound": "hbm", "achieved": alg / (ms_cold * 1e-3) / 1e9,
+                       "peak": peaks, "unit": "GB/s",
+                       "frac": alg / (ms_cold * 1e-3) / 1e9 / peaks,
+                       "traffic": None, "note": "cold (flushed) step; 48 B/voxel "
+                       "algorithmic (3 passes x 2 applies x read + write)"}
+    out["ms_per_step_cold"] = ms_cold
+    po = _po()
+    if po.ref_available():
+        host = x.cpu().numpy()
+        oip = _po_image(po, ip)
+        t0 = time.perf_counter()
+        ref = po.ref_psf_convolve(oip, host, psf.getKernelX(), psf.getKernelY(),
+                                  psf.getKernelZ())
+        ref = po.ref_psf_convolve(oip, ref, psf.getKernelX(), psf.getKernelY(),
+                                  psf.getKernelZ(), adjoint=True)
+        sec = time.perf_counter() - t0
+        out["bitexact_vs_reference"] = bool(np.array_equal(
+            ref.view(np.uint32), ah.cpu().numpy().view(np.uint32)))
+        out["cpu_baseline"] = {"value": V / sec, "unit": "voxels/s", "cores": 1,
+                               "kind": "reference",
+                               "sample": "the same image, applyA + applyAH "
+                               "(OperatorPsf, single-threaded)"}
+    return out
+
+
+def _measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+RUNNERS = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5,
+           "psf": run_psf}

@@ -418,6 +418,29 @@ yrtb_status yrtb_fill(float* d_x, uint64_t n, float value, yrtb_stream stream);
 yrtb_status yrtb_scale(float* d_x, uint64_t n, float scale,
                        yrtb_stream stream);
 
+/* ---------------------------------------------------- image-space PSF --- */
+/* Spatially invariant, separable image-space PSF: OperatorPsf /
+ * OperatorPsfDevice (include/yrt-pet/operators/OperatorPsf.hpp:19-70,
+ * src/operators/OperatorPsf.cpp:288-375, src/operators/OperatorPsfDevice.cu).
+ * Three 1-D kernels of odd length (x, y, z); applyA convolves with them,
+ * applyAH with the flipped kernels. */
+typedef struct yrtb_psf yrtb_psf;
+
+yrtb_status yrtb_psf_create(const float* kernel_x, int size_x,
+                            const float* kernel_y, int size_y,
+                            const float* kernel_z, int size_z, yrtb_psf** out);
+void yrtb_psf_destroy(yrtb_psf* psf);
+
+/* d_out = PSF d_in (adjoint = 0) or PSF^H d_in (adjoint = 1), every frame:
+ * passes along x, y, z, each out[i] = sum_kk k[kk + c] in[circ(i - kk)],
+ * kk = -c..c, with circular borders and FP32 sums in tap order (bit-identical
+ * to the reference CPU operator).  d_in != d_out; d_tmp: nx*ny*nz*nt floats
+ * of scratch, or NULL (taken from the library's pool).  A kernel half-width
+ * must be smaller than the image along its axis. */
+yrtb_status yrtb_psf_apply(const yrtb_psf* psf, const float* d_in, float* d_out,
+                           const yrtb_image_params* image, int adjoint,
+                           float* d_tmp, yrtb_stream stream);
+
 /* ------------------------------------------------------ OSEM (driver) --- */
 /* List-mode OSEM over device-resident events.  Mirrors OSEM::reconstruct
  * (src/recon/OSEM.cpp:315-365) with the GPU hooks of OSEM_GPU
@@ -426,7 +449,8 @@ yrtb_status yrtb_scale(float* d_x, uint64_t n, float scale,
  * subsets = chronologically interleaved events.  d_image holds nt frames and
  * is both the initial estimate (when init_from_image != 0) and the result.
  * d_sens: one image (voxels_per_frame floats).  d_work: scratch of
- * nt*voxels_per_frame floats + voxels_per_frame floats.  use_graph != 0
+ * nt*voxels_per_frame floats + voxels_per_frame floats, plus
+ * 2*nt*voxels_per_frame floats with an image-space PSF.  use_graph != 0
  * captures each subset (reset, EM pass, update) into a CUDA graph and
  * replays it. */
 typedef struct
@@ -440,6 +464,11 @@ typedef struct
 	                                   events (stride = subsets); else subset s
 	                                   = events [off[s], off[s+1]) as produced
 	                                   by yrtb_events_subset_order */
+	const yrtb_psf* psf;  /* image-space PSF or NULL: each subset projects PSF x and
+	                         applies PSF^H to the EM image before the update
+	                         (OSEM_GPU::computeEMUpdateImage, src/recon/OSEM_GPU.cu:456-509);
+	                         d_sens must already include PSF^H, as
+	                         OSEM::generateSensitivityImages makes it */
 } yrtb_osem_params;
 
 yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,

@@ -1259,3 +1259,77 @@ int orc_em_step_f64(const Image* im, const orc_proj* p, uint64_t n,
 }
 
 }  // extern "C"
+
+// Image-space PSF: separable convolution along x, then y, then z, with
+// circular borders and sums in tap order, out[i] = sum_kk k[kk + c] *
+// in[circ(i - kk)], kk = -c..c (OperatorPsf::convolve,
+// src/operators/OperatorPsf.cpp:288-375; util::circular, src/utils/Tools.cpp:160-167).
+// T = float mirrors the reference's FP32 sums; T = double is the FP64 oracle.
+template <typename T>
+static void psfConvolve(int64_t nx, int64_t ny, int64_t nz, int64_t nt,
+                        const float* in, T* out, const float* kx, int nkx,
+                        const float* ky, int nky, const float* kz, int nkz,
+                        bool flip)
+{
+	auto tap = [&](const float* k, int n, int j) -> T
+	{ return static_cast<T>(flip ? k[n - 1 - j] : k[j]); };
+	auto circ = [](int64_t M, int64_t x) { return x < 0 ? x + M : (x >= M ? x - M : x); };
+	const int64_t V = nx * ny * nz;
+	std::vector<T> a(V), b(V);
+	for (int64_t t = 0; t < nt; t++)
+	{
+		const float* src = in + t * V;
+		T* dst = out + t * V;
+		const int cx = nkx / 2, cy = nky / 2, cz = nkz / 2;
+		for (int64_t z = 0; z < nz; z++)
+			for (int64_t y = 0; y < ny; y++)
+				for (int64_t x = 0; x < nx; x++)
+				{
+					T sum = 0;
+					for (int kk = -cx; kk <= cx; kk++)
+						sum += tap(kx, nkx, kk + cx) *
+						       static_cast<T>(src[(z * ny + y) * nx + circ(nx, x - kk)]);
+					a[(z * ny + y) * nx + x] = sum;
+				}
+		for (int64_t z = 0; z < nz; z++)
+			for (int64_t x = 0; x < nx; x++)
+				for (int64_t y = 0; y < ny; y++)
+				{
+					T sum = 0;
+					for (int kk = -cy; kk <= cy; kk++)
+						sum += tap(ky, nky, kk + cy) * a[(z * ny + circ(ny, y - kk)) * nx + x];
+					b[(z * ny + y) * nx + x] = sum;
+				}
+		for (int64_t x = 0; x < nx; x++)
+			for (int64_t y = 0; y < ny; y++)
+				for (int64_t z = 0; z < nz; z++)
+				{
+					T sum = 0;
+					for (int kk = -cz; kk <= cz; kk++)
+						sum += tap(kz, nkz, kk + cz) * b[(circ(nz, z - kk) * ny + y) * nx + x];
+					dst[(z * ny + y) * nx + x] = sum;
+				}
+	}
+}
+
+extern "C" {
+
+int orc_psf_convolve_f32(int64_t nx, int64_t ny, int64_t nz, int64_t nt,
+                         const float* in, float* out, const float* kx, int nkx,
+                         const float* ky, int nky, const float* kz, int nkz,
+                         int adjoint)
+{
+	psfConvolve<float>(nx, ny, nz, nt, in, out, kx, nkx, ky, nky, kz, nkz, adjoint != 0);
+	return 0;
+}
+
+int orc_psf_convolve_f64(int64_t nx, int64_t ny, int64_t nz, int64_t nt,
+                         const float* in, double* out, const float* kx, int nkx,
+                         const float* ky, int nky, const float* kz, int nkz,
+                         int adjoint)
+{
+	psfConvolve<double>(nx, ny, nz, nt, in, out, kx, nkx, ky, nky, kz, nkz, adjoint != 0);
+	return 0;
+}
+
+}  // extern "C"

@@ -63,7 +63,8 @@ class OsemDesc(ctypes.Structure):
                 ("tof_fwhm_ps", ctypes.c_float), ("tof_n_std", ctypes.c_int),
                 ("iterations", ctypes.c_int), ("subsets", ctypes.c_int),
                 ("threads", ctypes.c_int), ("global_scale", ctypes.c_float),
-                ("hard_threshold", ctypes.c_float), ("listmode", ctypes.c_int)]
+                ("hard_threshold", ctypes.c_float), ("listmode", ctypes.c_int),
+                ("image_psf_csv", ctypes.c_char_p)]
 
 
 @dataclass
@@ -480,10 +481,11 @@ def ref_lm_to_histo3d(sc: Scanner, d1, d2, threads=8):
 
 def _osem_desc(projector="S", num_rays=1, tof_fwhm_ps=0.0, tof_n_std=0,
                iterations=1, subsets=1, threads=8, global_scale=1.0,
-               hard_threshold=1.0, listmode=True):
+               hard_threshold=1.0, listmode=True, image_psf_csv=None):
     return OsemDesc(0 if projector == "S" else 1, num_rays, tof_fwhm_ps,
                     tof_n_std, iterations, subsets, threads, global_scale,
-                    hard_threshold, int(listmode))
+                    hard_threshold, int(listmode),
+                    None if image_psf_csv is None else image_psf_csv.encode())
 
 
 def ref_sensitivity(sc: Scanner, ip: ImageParams, *, sens_histo=None,
@@ -573,3 +575,47 @@ def ref_osem_histo3d(sc: Scanner, ip: ImageParams, sens_images, histo, *,
             ctypes.byref(sec))
     _ref_check(rc)
     return out, sec.value
+
+
+# ------------------------------------------------------ image-space PSF ---
+def psf_convolve(ip: ImageParams, image, kx, ky, kz, adjoint=False,
+                 precision="f32"):
+    """Oracle separable PSF convolution (OperatorPsf::convolve restated)."""
+    img = np.ascontiguousarray(image, np.float32)
+    kx, ky, kz = (np.ascontiguousarray(k, np.float32) for k in (kx, ky, kz))
+    dt = np.float32 if precision == "f32" else np.float64
+    out = np.zeros(img.shape, dt)
+    fn = (oracle_lib().orc_psf_convolve_f32 if precision == "f32"
+          else oracle_lib().orc_psf_convolve_f64)
+    rc = fn(ctypes.c_int64(ip.nx), ctypes.c_int64(ip.ny), ctypes.c_int64(ip.nz),
+            ctypes.c_int64(ip.nt), _p(img), _p(out), _p(kx), ctypes.c_int(len(kx)),
+            _p(ky), ctypes.c_int(len(ky)), _p(kz), ctypes.c_int(len(kz)),
+            ctypes.c_int(int(adjoint)))
+    assert rc == 0
+    return out
+
+
+def ref_psf_convolve(ip: ImageParams, image, kx, ky, kz, adjoint=False):
+    """The reference's OperatorPsf::applyA / applyAH."""
+    img = np.ascontiguousarray(image, np.float32)
+    kx, ky, kz = (np.ascontiguousarray(k, np.float32) for k in (kx, ky, kz))
+    out = np.zeros(img.shape, np.float32)
+    with quiet():
+        rc = ref_lib().ref_psf_convolve(
+            ctypes.byref(ip.desc()), _p(img), _p(out), _p(kx), ctypes.c_int(len(kx)),
+            _p(ky), ctypes.c_int(len(ky)), _p(kz), ctypes.c_int(len(kz)),
+            ctypes.c_int(int(adjoint)))
+    _ref_check(rc)
+    return out
+
+
+def ref_psf_gaussian_kernel(sigma, voxel, size=0):
+    """The reference's OperatorPsf::createGaussianKernel1D."""
+    buf = np.zeros(4096, np.float32)
+    n = ctypes.c_uint64()
+    with quiet():
+        rc = ref_lib().ref_psf_gaussian_kernel(
+            ctypes.c_float(sigma), ctypes.c_float(voxel), ctypes.c_uint64(size),
+            _p(buf), ctypes.c_uint64(len(buf)), ctypes.byref(n))
+    _ref_check(rc)
+    return buf[:n.value].copy()

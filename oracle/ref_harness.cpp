@@ -23,6 +23,7 @@
 #include "yrt-pet/datastruct/projection/ListModeLUT.hpp"
 #include "yrt-pet/datastruct/projection/UniformHistogram.hpp"
 #include "yrt-pet/datastruct/scanner/Scanner.hpp"
+#include "yrt-pet/operators/OperatorPsf.hpp"
 #include "yrt-pet/operators/ProjectionPsfManager.hpp"
 #include "yrt-pet/operators/ProjectorDD.hpp"
 #include "yrt-pet/operators/ProjectorParams.hpp"
@@ -400,6 +401,45 @@ int64_t ref_read_listmode(const ref_scanner_desc* s, const char* fname,
 	return rc == 0 ? n : -1;
 }
 
+// Image-space PSF: OperatorPsf::applyA / applyAH (separable convolution with
+// circular borders, src/operators/OperatorPsf.cpp:288-375).
+int ref_psf_convolve(const ref_image_desc* d, const float* in, float* out,
+                     const float* kx, int nkx, const float* ky, int nky,
+                     const float* kz, int nkz, int adjoint)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto a = makeImage(d, in);
+		    auto b = makeImage(d, nullptr);
+		    OperatorPsf op(std::vector<float>(kx, kx + nkx),
+		                   std::vector<float>(ky, ky + nky),
+		                   std::vector<float>(kz, kz + nkz));
+		    if (adjoint)
+			    op.applyAH(a.get(), b.get());
+		    else
+			    op.applyA(a.get(), b.get());
+		    const size_t n = d->nx * d->ny * d->nz * d->nt;
+		    std::memcpy(out, b->getRawPointer(), n * sizeof(float));
+	    });
+}
+
+// OperatorPsf::createGaussianKernel1D; size 0 = the reference's default.
+int ref_psf_gaussian_kernel(float sigma, float vox, uint64_t size, float* out,
+                            uint64_t cap, uint64_t* outSize)
+{
+	return guarded(
+	    [&]
+	    {
+		    const size_t sz = size;
+		    const auto k = OperatorPsf::createGaussianKernel1D(
+		        sigma, vox, size ? &sz : nullptr);
+		    *outSize = k.size();
+		    for (size_t i = 0; i < k.size() && i < cap; i++)
+			    out[i] = k[i];
+	    });
+}
+
 float ref_dd_overlap(float p0, float p1, float d0, float d1)
 {
 	return ProjectorDD::getOverlap(p0, p1, d0, d1, nullptr, nullptr);
@@ -445,6 +485,7 @@ struct ref_osem_desc
 	float global_scale;
 	float hard_threshold;
 	int listmode;  // 1: list-mode events, 0: histogram input
+	const char* image_psf_csv;  // image-space PSF (OSEM::addImagePSF), or NULL
 };
 
 // Sensitivity image (reference OSEM::generateSensitivityImages).  sens_histo
@@ -472,6 +513,8 @@ int ref_sensitivity(const ref_scanner_desc* s, const ref_image_desc* d,
 		    osem->setNumRays(o->num_rays);
 		    if (psf_csv && psf_csv[0])
 			    osem->addProjPSF(psf_csv);
+		    if (o->image_psf_csv && o->image_psf_csv[0])
+			    osem->addImagePSF(o->image_psf_csv);
 		    osem->setGlobalScalingFactor(o->global_scale);
 		    std::unique_ptr<Histogram3DOwned> sh;
 		    if (sens_histo)
@@ -574,6 +617,8 @@ int ref_osem_listmode_ex(const ref_scanner_desc* s, const ref_image_desc* d,
 		    osem->setNumRays(o->num_rays);
 		    if (o->tof_fwhm_ps > 0)
 			    osem->addTOF(o->tof_fwhm_ps, o->tof_n_std);
+		    if (o->image_psf_csv && o->image_psf_csv[0])
+			    osem->addImagePSF(o->image_psf_csv);
 		    osem->setGlobalScalingFactor(o->global_scale);
 		    std::unique_ptr<Histogram3DOwned> sh;
 		    if (sens_histo)
@@ -643,6 +688,8 @@ int ref_osem_histo3d(const ref_scanner_desc* s, const ref_image_desc* d,
 		    osem->setNumRays(o->num_rays);
 		    if (psf_csv && psf_csv[0])
 			    osem->addProjPSF(psf_csv);
+		    if (o->image_psf_csv && o->image_psf_csv[0])
+			    osem->addImagePSF(o->image_psf_csv);
 		    if (o->tof_fwhm_ps > 0)
 			    osem->addTOF(o->tof_fwhm_ps, o->tof_n_std);
 		    const size_t nv = d->nx * d->ny * d->nz;

@@ -246,3 +246,32 @@ def test_live_reference_lm_to_histogram_bitexact():
     assert bad == 0
     r, _ = po.ref_lm_to_histo3d(SC, d1[ok], d2[ok])
     assert np.array_equal(bits(h), bits(r))
+
+
+# ------------------------------------------------------- image-space PSF --
+@needs_ref
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_psf_convolution_oracle_bitexact_vs_reference(adjoint):
+    """The oracle's separable convolution (FP32, tap order, circular borders)
+    against the reference's OperatorPsf::applyA / applyAH, bit for bit; the
+    FP64 restatement within float rounding."""
+    rng = np.random.default_rng(61)
+    ip = po.ImageParams(20, 16, 12, 40, 32, 24, nt=2)
+    img = rng.random((2, 12, 16, 20), dtype=np.float32)
+    kx = rng.random(5).astype(np.float32)
+    ky = rng.random(7).astype(np.float32)
+    kz = rng.random(3).astype(np.float32)
+    ref = po.ref_psf_convolve(ip, img, kx, ky, kz, adjoint=adjoint)
+    f32 = po.psf_convolve(ip, img, kx, ky, kz, adjoint=adjoint)
+    f64 = po.psf_convolve(ip, img, kx, ky, kz, adjoint=adjoint, precision="f64")
+    assert np.array_equal(ref.view(np.uint32), f32.view(np.uint32))
+    assert np.linalg.norm(f64 - ref) / np.linalg.norm(f64) < 1e-6
+
+
+@needs_ref
+def test_psf_gaussian_kernel_matches_reference():
+    k = po.ref_psf_gaussian_kernel(1.7, 2.0, 7)
+    x = (np.arange(7) - 3).astype(np.float32)
+    mine = np.exp(-0.5 * (x * np.float32(2.0) / np.float32(1.7)) ** 2).astype(np.float32)
+    mine /= mine.sum(dtype=np.float32)
+    assert np.allclose(k, mine, rtol=1e-6)

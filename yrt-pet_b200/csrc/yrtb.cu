@@ -1432,6 +1432,188 @@ __global__ void k_scale(float* __restrict__ x, uint64_t n, float v)
 		x[i] *= v;
 }
 
+// One pass of the separable image-space PSF along AXIS (0 x, 1 y, 2 z):
+// dst[i] = sum_kk k[kk + c] * src[circ(i - kk)], kk = -c..c, circular border,
+// FP32 sums in tap order (OperatorPsf::convolve, src/operators/OperatorPsf.cpp:288-375).
+// Blocks of kPsfBX x kPsfBY threads cover an (x, y) tile; each thread takes
+// kPsfPlanes consecutive (z, frame) planes at a time, so every tap issues
+// kPsfPlanes independent loads, and no thread divides a 64-bit index.  A warp
+// reads 32 consecutive x for every tap (coalesced along every axis).
+// NK > 0 fixes the number of taps at compile time (the tap loop unrolls and
+// all loads of a plane group are in flight together); NK = 0 reads nk.
+constexpr int kPsfBX = 32, kPsfBY = 8, kPsfPlanes = 4;
+template <int AXIS, int NK>
+__global__ void __launch_bounds__(kPsfBX * kPsfBY)
+k_psf_pass(const float* __restrict__ src, float* __restrict__ dst, int nx, int ny, int nz,
+           int planes, const float* __restrict__ k, int nkRuntime)
+{
+	const int nk = NK > 0 ? NK : nkRuntime;
+	const int x = blockIdx.x * kPsfBX + threadIdx.x;
+	const int y = blockIdx.y * kPsfBY + threadIdx.y;
+	if (x >= nx || y >= ny)
+		return;
+	const int c = nk / 2;
+	const int n = AXIS == 0 ? nx : (AXIS == 1 ? ny : nz);
+	const int64_t plane = static_cast<int64_t>(nx) * ny;
+	const int64_t stride = AXIS == 0 ? 1 : (AXIS == 1 ? nx : plane);
+	for (int zt0 = blockIdx.z * kPsfPlanes; zt0 < planes; zt0 += gridDim.z * kPsfPlanes)
+	{
+		const float* base[kPsfPlanes];
+		int coord[kPsfPlanes];
+		float sum[kPsfPlanes];
+#pragma unroll
+		for (int q = 0; q < kPsfPlanes; q++)
+		{
+			// Past the last plane, repeat it (loads stay in bounds, no store).
+			const int zt = min(zt0 + q, planes - 1);
+			const int64_t i = zt * plane + static_cast<int64_t>(y) * nx + x;
+			coord[q] = AXIS == 0 ? x : (AXIS == 1 ? y : zt % nz);
+			base[q] = src + (i - coord[q] * stride);
+			sum[q] = 0.f;
+		}
+#pragma unroll
+		for (int kk = -c; kk <= c; kk++)
+		{
+			const float tap = __ldg(k + kk + c);
+#pragma unroll
+			for (int q = 0; q < kPsfPlanes; q++)
+			{
+				int r = coord[q] - kk;
+				r = r < 0 ? r + n : (r >= n ? r - n : r);
+				// Rounded product and sum, no contraction into an FMA: the
+				// reference operator multiplies and adds separately.
+				sum[q] = __fadd_rn(sum[q], __fmul_rn(tap, __ldg(base[q] + r * stride)));
+			}
+		}
+#pragma unroll
+		for (int q = 0; q < kPsfPlanes; q++)
+			if (zt0 + q < planes)
+				dst[(zt0 + q) * plane + static_cast<int64_t>(y) * nx + x] = sum[q];
+	}
+}
+
+// Vector form of k_psf_pass for rows of a multiple of 4 voxels (16-byte
+// aligned images): each thread produces 4 consecutive x of kPsfPlanes planes
+// with 16-byte loads.  Along y and z every tap is one float4 load; along x the
+// thread loads the 2D+1 aligned chunks around its own (circular chunk index,
+// which wraps by whole periods because nx is a multiple of 4) and slides the
+// taps over them in registers.  Same products and sums in the same order as
+// the scalar form, so the results are bit-identical.
+template <int AXIS, int NK>
+__global__ void __launch_bounds__(kPsfBX * kPsfBY)
+k_psf_pass4(const float* __restrict__ src, float* __restrict__ dst, int nx, int ny, int nz,
+            int planes, const float* __restrict__ k)
+{
+	constexpr int C = NK / 2;
+	constexpr int D = (C + 3) / 4;
+	const int nxc = nx >> 2;
+	const int jx = blockIdx.x * kPsfBX + threadIdx.x;
+	const int y = blockIdx.y * kPsfBY + threadIdx.y;
+	if (jx >= nxc || y >= ny)
+		return;
+	float taps[NK];
+#pragma unroll
+	for (int i = 0; i < NK; i++)
+		taps[i] = __ldg(k + i);
+	const int64_t plane = static_cast<int64_t>(nx) * ny;
+	for (int zt0 = blockIdx.z * kPsfPlanes; zt0 < planes; zt0 += gridDim.z * kPsfPlanes)
+	{
+		float4 acc[kPsfPlanes];
+#pragma unroll
+		for (int q = 0; q < kPsfPlanes; q++)
+		{
+			const int zt = min(zt0 + q, planes - 1);
+			const float* row = src + zt * plane + static_cast<int64_t>(y) * nx;
+			float out[4];
+			if constexpr (AXIS == 0)
+			{
+				float w[4 * (2 * D + 1)];
+#pragma unroll
+				for (int d = -D; d <= D; d++)
+				{
+					int j = jx + d;
+					j = j < 0 ? j + nxc : (j >= nxc ? j - nxc : j);
+					const float4 v = __ldg(reinterpret_cast<const float4*>(row) + j);
+					w[4 * (d + D) + 0] = v.x;
+					w[4 * (d + D) + 1] = v.y;
+					w[4 * (d + D) + 2] = v.z;
+					w[4 * (d + D) + 3] = v.w;
+				}
+#pragma unroll
+				for (int m = 0; m < 4; m++)
+				{
+					float sum = 0.f;
+#pragma unroll
+					for (int kk = -C; kk <= C; kk++)
+						sum = __fadd_rn(sum, __fmul_rn(taps[kk + C], w[4 * D + m - kk]));
+					out[m] = sum;
+				}
+			}
+			else
+			{
+				const int n = AXIS == 1 ? ny : nz;
+				const int coord = AXIS == 1 ? y : zt % nz;
+				const int64_t stride = AXIS == 1 ? nx : plane;
+				const float* col = row - coord * stride + 4 * jx;
+				out[0] = out[1] = out[2] = out[3] = 0.f;
+#pragma unroll
+				for (int kk = -C; kk <= C; kk++)
+				{
+					int r = coord - kk;
+					r = r < 0 ? r + n : (r >= n ? r - n : r);
+					const float4 v = __ldg(reinterpret_cast<const float4*>(col + r * stride));
+					const float t = taps[kk + C];
+					out[0] = __fadd_rn(out[0], __fmul_rn(t, v.x));
+					out[1] = __fadd_rn(out[1], __fmul_rn(t, v.y));
+					out[2] = __fadd_rn(out[2], __fmul_rn(t, v.z));
+					out[3] = __fadd_rn(out[3], __fmul_rn(t, v.w));
+				}
+			}
+			acc[q] = make_float4(out[0], out[1], out[2], out[3]);
+		}
+#pragma unroll
+		for (int q = 0; q < kPsfPlanes; q++)
+			if (zt0 + q < planes)
+				*reinterpret_cast<float4*>(dst + (zt0 + q) * plane +
+				                           static_cast<int64_t>(y) * nx + 4 * jx) = acc[q];
+	}
+}
+
+// Kernel sizes up to 15 taps run the unrolled instantiation.
+// vec: rows of a multiple of 4 voxels and 16-byte aligned buffers; grid.x
+// then counts chunks of 4 x.
+template <int AXIS>
+void psfPass(dim3 grid, dim3 block, cudaStream_t st, const float* src, float* dst,
+             const int* dims, int planes, const float* k, int nk, bool vec)
+{
+	dim3 grid4 = grid;
+	grid4.x = (dims[0] / 4 + kPsfBX - 1) / kPsfBX;
+#define YRTB_PSF_CASE(N)                                                                  \
+	case N:                                                                               \
+		if (vec)                                                                          \
+			k_psf_pass4<AXIS, N><<<grid4, block, 0, st>>>(src, dst, dims[0], dims[1],     \
+			                                              dims[2], planes, k);            \
+		else                                                                              \
+			k_psf_pass<AXIS, N><<<grid, block, 0, st>>>(src, dst, dims[0], dims[1],       \
+			                                            dims[2], planes, k, nk);          \
+		return;
+	switch (nk)
+	{
+		YRTB_PSF_CASE(1)
+		YRTB_PSF_CASE(3)
+		YRTB_PSF_CASE(5)
+		YRTB_PSF_CASE(7)
+		YRTB_PSF_CASE(9)
+		YRTB_PSF_CASE(11)
+		YRTB_PSF_CASE(13)
+		YRTB_PSF_CASE(15)
+	default:
+		k_psf_pass<AXIS, 0><<<grid, block, 0, st>>>(src, dst, dims[0], dims[1], dims[2],
+		                                            planes, k, nk);
+	}
+#undef YRTB_PSF_CASE
+}
+
 int g_numSMs = 0;
 
 // Blocks for one item per thread.
@@ -1578,6 +1760,23 @@ struct yrtb_projector
 		cudaFree(d_ring);
 		cudaFree(d_z);
 		cudaFree(d_err);
+	}
+};
+
+// Separable image-space PSF: kernels and flipped kernels per axis.
+struct yrtb_psf
+{
+	float* k[3] = {nullptr, nullptr, nullptr};
+	float* kf[3] = {nullptr, nullptr, nullptr};
+	int n[3] = {0, 0, 0};
+	int device = 0;
+	~yrtb_psf()
+	{
+		for (int a = 0; a < 3; a++)
+		{
+			cudaFree(k[a]);
+			cudaFree(kf[a]);
+		}
 	}
 };
 
@@ -2655,6 +2854,78 @@ yrtb_status yrtb_scale(float* x, uint64_t n, float v, yrtb_stream stream)
 	return YRTB_OK;
 }
 
+yrtb_status yrtb_psf_create(const float* kx, int nkx, const float* ky, int nky,
+                            const float* kz, int nkz, yrtb_psf** out)
+{
+	if (!out)
+		return fail(YRTB_ERR_ARGUMENT, "null output handle");
+	*out = nullptr;
+	const float* ks[3] = {kx, ky, kz};
+	const int ns[3] = {nkx, nky, nkz};
+	for (int a = 0; a < 3; a++)
+		if (!ks[a] || ns[a] <= 0 || ns[a] % 2 == 0)
+			return fail(YRTB_ERR_ARGUMENT, "Kernel size must be odd");
+	auto p = std::make_unique<yrtb_psf>();
+	cudaGetDevice(&p->device);
+	for (int a = 0; a < 3; a++)
+	{
+		std::vector<float> f(ks[a], ks[a] + ns[a]);
+		std::reverse(f.begin(), f.end());
+		p->n[a] = ns[a];
+		YRTB_CUDA(cudaMalloc(&p->k[a], ns[a] * sizeof(float)));
+		YRTB_CUDA(cudaMalloc(&p->kf[a], ns[a] * sizeof(float)));
+		YRTB_CUDA(cudaMemcpy(p->k[a], ks[a], ns[a] * sizeof(float), cudaMemcpyHostToDevice));
+		YRTB_CUDA(cudaMemcpy(p->kf[a], f.data(), ns[a] * sizeof(float), cudaMemcpyHostToDevice));
+	}
+	*out = p.release();
+	return YRTB_OK;
+}
+
+void yrtb_psf_destroy(yrtb_psf* p)
+{
+	delete p;
+}
+
+yrtb_status yrtb_psf_apply(const yrtb_psf* p, const float* d_in, float* d_out,
+                           const yrtb_image_params* ip, int adjoint,
+                           float* d_tmp, yrtb_stream stream)
+{
+	if (!p || !d_in || !d_out || !validImage(ip))
+		return fail(YRTB_ERR_ARGUMENT, "invalid PSF arguments");
+	if (d_in == d_out)
+		return fail(YRTB_ERR_ARGUMENT, "PSF input and output must differ");
+	const int dims[3] = {static_cast<int>(ip->nx), static_cast<int>(ip->ny),
+	                     static_cast<int>(ip->nz)};
+	if ((dims[1] + kPsfBY - 1) / kPsfBY > 65535 ||
+	    static_cast<int64_t>(ip->nz) * ip->nt > INT32_MAX)
+		return fail(YRTB_ERR_ARGUMENT, "image too large for the PSF launch");
+	for (int a = 0; a < 3; a++)
+		if (p->n[a] / 2 >= dims[a])
+			return fail(YRTB_ERR_ARGUMENT,
+			            "PSF kernel half-width must be smaller than the image along each axis");
+	YRTB_CUDA(cudaSetDevice(p->device));
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	const uint64_t total = static_cast<uint64_t>(ip->nx) * ip->ny * ip->nz * ip->nt;
+	float* tmp = d_tmp;
+	if (!tmp)
+		YRTB_CUDA(poolAlloc(&tmp, total * sizeof(float), st));
+	float* const* k = adjoint ? p->kf : p->k;
+	const int planes = static_cast<int>(ip->nz * ip->nt);
+	const dim3 block(kPsfBX, kPsfBY);
+	const dim3 grid((dims[0] + kPsfBX - 1) / kPsfBX, (dims[1] + kPsfBY - 1) / kPsfBY,
+	                std::min((planes + kPsfPlanes - 1) / kPsfPlanes, 65535));
+	auto aligned = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+	const bool vec = dims[0] % 4 == 0 && aligned(d_in) && aligned(d_out) && aligned(tmp);
+	// x: in -> out, y: out -> tmp, z: tmp -> out.
+	psfPass<0>(grid, block, st, d_in, d_out, dims, planes, k[0], p->n[0], vec);
+	psfPass<1>(grid, block, st, d_out, tmp, dims, planes, k[1], p->n[1], vec);
+	psfPass<2>(grid, block, st, tmp, d_out, dims, planes, k[2], p->n[2], vec);
+	if (!d_tmp)
+		YRTB_CUDA(cudaFreeAsync(tmp, st));
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
 yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
                                const float* d_sens, float* d_image,
                                float* d_work, const yrtb_osem_params* p,
@@ -2669,6 +2940,10 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 	const int64_t nt = h->ip.nt;
 	float* em = d_work;
 	float* sens = d_work + J * nt;
+	// With an image-space PSF: the blurred image (also the blurred EM image
+	// after the pass) and the PSF's temporary follow.
+	float* xpsf = sens + J;
+	float* ptmp = xpsf + J * nt;
 	// List-mode sensitivity is shared by all subsets and divided by their
 	// number (OSEM::initializeSensImageBuffer, OSEM.cpp:1007-1035).
 	YRTB_CUDA(cudaMemcpyAsync(sens, d_sens, J * sizeof(float),
@@ -2703,6 +2978,19 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 			if (range.count == 0)
 				return yrtb_em_update(d_image, em, sens, J, nt, 1, p->em_threshold,
 				                      p->d_frame_scale, stream);
+		}
+		if (p->psf)
+		{
+			// OSEM_GPU::computeEMUpdateImage with image PSF
+			// (src/recon/OSEM_GPU.cu:456-509): project PSF(x), back-project
+			// the ratio, apply PSF^H to the EM image.
+			if ((r = yrtb_psf_apply(p->psf, d_image, xpsf, &h->ip, 0, ptmp, stream)) != YRTB_OK ||
+			    (r = yrtb_em_step(h, xpsf, em, ev, range, p->global_scale,
+			                      p->denom_threshold, stream)) != YRTB_OK ||
+			    (r = yrtb_psf_apply(p->psf, em, xpsf, &h->ip, 1, ptmp, stream)) != YRTB_OK)
+				return r;
+			return yrtb_em_update(d_image, xpsf, sens, J, nt, 1, p->em_threshold,
+			                      p->d_frame_scale, stream);
 		}
 		if ((r = yrtb_em_step(h, d_image, em, ev, range, p->global_scale,
 		                      p->denom_threshold, stream)) != YRTB_OK)
@@ -2999,7 +3287,8 @@ extern "C" yrtb_status yrtb_osem_listmode_static(yrtb_projector* h,
 		            "yrtb_osem_listmode_static does not build CUDA graphs "
 		            "(instantiating one allocates); set use_graph = 0");
 	const uint64_t J = static_cast<uint64_t>(h->P.g.nvox);
-	const uint64_t need = J * static_cast<uint64_t>(h->ip.nt) + J;
+	const uint64_t need = J * static_cast<uint64_t>(h->ip.nt) + J +
+	                      (p->psf ? 2 * J * static_cast<uint64_t>(h->ip.nt) : 0);
 	if (need > YRTB_OSEM_STATIC_MAX_FLOATS)
 		return fail(YRTB_ERR_ARGUMENT,
 		            "image too large for yrtb_osem_listmode_static: needs " +

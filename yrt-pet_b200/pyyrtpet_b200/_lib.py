@@ -72,7 +72,7 @@ class yrtb_osem_params(ctypes.Structure):
                 ("global_scale", c_f), ("denom_threshold", c_f),
                 ("em_threshold", c_f), ("init_from_image", ctypes.c_int),
                 ("use_graph", ctypes.c_int), ("d_frame_scale", c_vp),
-                ("subset_offsets", c_vp)]
+                ("subset_offsets", c_vp), ("psf", c_vp)]
 
 
 class yrtb_launch_config(ctypes.Structure):
@@ -146,6 +146,11 @@ SIGNATURES = {
                               c_f, c_f, c_f, c_vp], ctypes.c_int),
     "yrtb_fill": ([c_vp, c_u64, c_f, c_vp], ctypes.c_int),
     "yrtb_scale": ([c_vp, c_u64, c_f, c_vp], ctypes.c_int),
+    "yrtb_psf_create": ([c_vp, ctypes.c_int, c_vp, ctypes.c_int, c_vp, ctypes.c_int,
+                         _P(c_vp)], ctypes.c_int),
+    "yrtb_psf_destroy": ([c_vp], None),
+    "yrtb_psf_apply": ([c_vp, c_vp, c_vp, _P(yrtb_image_params), ctypes.c_int, c_vp,
+                        c_vp], ctypes.c_int),
     "yrtb_osem_listmode": ([c_vp, _P(yrtb_events), c_vp, c_vp, c_vp,
                             _P(yrtb_osem_params), c_vp], ctypes.c_int),
     "yrtb_osem_listmode_static": ([c_vp, _P(yrtb_events), c_vp, c_vp,

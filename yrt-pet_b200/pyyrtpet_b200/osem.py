@@ -22,6 +22,7 @@ import torch
 from . import _lib as L
 from .core import (DeviceEvents, DeviceProjector, Histogram3D, ImageParams,
                    ListModeLUT, ProjectorParams, Scanner, _dev, _ptr, _stream)
+from .psf import OperatorPsfDevice
 
 
 class OSEM_GPU:
@@ -66,6 +67,8 @@ class OSEM_GPU:
         self._initial = None
         self._mask = None
         self._frame_scale = None
+        self.imagePsf = None
+        self.flagImagePSF = False
 
     # ----------------------------------------------------------- setters --
     def setImageParams(self, p: ImageParams):
@@ -98,6 +101,45 @@ class OSEM_GPU:
 
     def addProjPSF(self, fname: str):
         self.projectorParams.projPsf_fname = fname
+
+    # --------------------------------------------------- image-space PSF --
+    # OSEM_GPU::addImagePSF / addUniformGaussianImagePSFFrom{FWHM,Sigma}
+    # (src/recon/OSEM_GPU.cu:48-95).  Spatially invariant (UNIFORM) only.
+    def addImagePSF(self, image_psf_fname: str, image_psf_mode: str = "UNIFORM"):
+        if not image_psf_fname:
+            raise RuntimeError("Empty filename for Image-space PSF")
+        mode = getattr(image_psf_mode, "name", image_psf_mode)
+        if str(mode).upper() != "UNIFORM":
+            raise RuntimeError("Only the spatially invariant (UNIFORM) "
+                               "image-space PSF is supported")
+        self.imagePsf = OperatorPsfDevice(image_psf_fname)
+        self.flagImagePSF = True
+
+    def addUniformGaussianImagePSFFromFWHM(self, fwhm_x, fwhm_y, fwhm_z,
+                                           kernel_size_x=None, kernel_size_y=None,
+                                           kernel_size_z=None):
+        ip = self._require_image_params()
+        self.imagePsf = OperatorPsfDevice.createGaussianFromFWHM(
+            fwhm_x, fwhm_y, fwhm_z, ip.vx, ip.vy, ip.vz,
+            kernel_size_x, kernel_size_y, kernel_size_z)
+        self.flagImagePSF = True
+
+    def addUniformGaussianImagePSFFromSigma(self, sigma_x, sigma_y, sigma_z,
+                                            kernel_size_x=None, kernel_size_y=None,
+                                            kernel_size_z=None):
+        ip = self._require_image_params()
+        self.imagePsf = OperatorPsfDevice.createGaussianFromSigma(
+            sigma_x, sigma_y, sigma_z, ip.vx, ip.vy, ip.vz,
+            kernel_size_x, kernel_size_y, kernel_size_z)
+        self.flagImagePSF = True
+
+    def hasImagePSF(self) -> bool:
+        return self.flagImagePSF
+
+    def _require_image_params(self) -> ImageParams:
+        if self.imageParams is None:
+            raise RuntimeError("Image parameters not set")
+        return self.imageParams
 
     def setGlobalScalingFactor(self, g: float):
         self._global = float(g)
@@ -173,8 +215,10 @@ class OSEM_GPU:
 
     # ----------------------------------------------- sensitivity images --
     def generateSensitivityImages(self) -> List[torch.Tensor]:
-        """Back projection of sens x ACF over every Histogram3D bin (non-TOF),
-        thresholded: <= hardThreshold -> 0, else x globalScale."""
+        """Back projection of sens x ACF over every Histogram3D bin (non-TOF);
+        with an image-space PSF, PSF^H of it zeroed where the back projection
+        is <= EPS_FLT (OSEM_GPU.cu:228-236); then thresholded: <= hardThreshold
+        -> 0, else x globalScale."""
         if self.imageParams is None:
             raise RuntimeError("Image parameters not valid/set")
         nsub = 1 if self.usingListModeInput else self.num_OSEM_subsets
@@ -190,6 +234,13 @@ class OSEM_GPU:
             proj.sensitivity_histo3d(img, nsub, s, sens_histo=sh, acf_histo=acf,
                                      mu=None if acf is not None else self._att_image,
                                      mu_params=self._att_params)
+            if self.flagImagePSF:
+                blurred = torch.empty_like(img)
+                self.imagePsf.applyAH(img, blurred, ip.withFrames(1))
+                L.check(L.lib().yrtb_apply_threshold(
+                    blurred.data_ptr(), img.data_ptr(), ip.numVoxels, 1, 0,
+                    float(self.EPS_FLT), 0.0, 0.0, 1.0, 0.0, _stream()))
+                img = blurred
             L.check(L.lib().yrtb_apply_threshold(
                 img.data_ptr(), img.data_ptr(), ip.numVoxels, 1, 0,
                 float(self.hardThreshold), 0.0, 0.0, float(self._global), 0.0,
@@ -274,7 +325,9 @@ class OSEM_GPU:
         if self._initial is not None:
             img.copy_(self._initial.reshape(-1))
             init = 1
-        work = torch.empty(nt * J + J, dtype=torch.float32, device="cuda")
+        psf = self.imagePsf if self.flagImagePSF else None
+        work = torch.empty((3 * nt + 1) * J if psf else nt * J + J,
+                           dtype=torch.float32, device="cuda")
         sens = self._sens_images[0]
         if self._mask is not None:
             mask_src = self._mask
@@ -286,7 +339,8 @@ class OSEM_GPU:
                                self._global, self.denomThreshold, self.EPS_FLT,
                                init, int(self.useGraphs),
                                _ptr(self._frame_scale),
-                               None if offsets is None else offsets.ctypes.data)
+                               None if offsets is None else offsets.ctypes.data,
+                               None if psf is None else psf.handle)
         stream = torch.cuda.current_stream()
         use_side = self.useGraphs and stream.cuda_stream == 0
         s = torch.cuda.Stream() if use_side else stream
@@ -340,16 +394,27 @@ class OSEM_GPU:
                                              1, 1, 0.0, 0.0, 0.0, 1.0, 0.0,
                                              _stream()))
         em = torch.empty(J, dtype=torch.float32, device="cuda")
+        psf = self.imagePsf if self.flagImagePSF else None
+        if psf is not None:
+            # Project PSF x, apply PSF^H to the EM image
+            # (OSEM_GPU::computeEMUpdateImage, OSEM_GPU.cu:456-509).
+            xpsf = torch.empty_like(img)
+            em_psf = torch.empty_like(em)
         for _ in range(self.num_MLEM_iterations):
             for s in range(self.num_OSEM_subsets):
                 em.zero_()
-                proj.em_step_histo3d(img, em, meas, self.num_OSEM_subsets, s,
+                if psf is not None:
+                    psf.applyA(img, xpsf, ip)
+                proj.em_step_histo3d(img if psf is None else xpsf, em, meas,
+                                     self.num_OSEM_subsets, s,
                                      sens_histo=sh, acf_histo=acf,
                                      additive_histo=add,
                                      global_scale=self._global,
                                      denom_threshold=self.denomThreshold)
+                if psf is not None:
+                    psf.applyAH(em, em_psf, ip)
                 L.check(L.lib().yrtb_em_update(
-                    img.data_ptr(), em.data_ptr(),
+                    img.data_ptr(), (em if psf is None else em_psf).data_ptr(),
                     self._sens_images[s].data_ptr(), J, 1, 1, self.EPS_FLT,
                     None, _stream()))
         return img.reshape(ip.shape)
