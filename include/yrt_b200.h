@@ -392,7 +392,8 @@ yrtb_status yrtb_histo3d_detpairs(yrtb_projector* h, const uint64_t* d_bins,
 /* -------------------------------------------------------- image space --- */
 /* x *= u / s where s > threshold.  sens_nt == 1 broadcasts one sensitivity
  * image over nt frames; d_frame_scale (nullable, nt floats) divides u and
- * the threshold per frame.  Replaces Image::updateEMThreshold{Static,
+ * the threshold per frame and, as updateEMThresholdDynamic with sensScaling,
+ * always reads the first sensitivity frame.  Replaces Image::updateEMThreshold{Static,
  * DynamicWithScaling,DynamicWith4DSens} (src/datastruct/image/Image.cpp:651-833)
  * and updateEM_kernel / updateEMDynamic_kernel
  * (src/datastruct/image/ImageSpaceKernels.cu:13-76). */
@@ -440,6 +441,41 @@ void yrtb_psf_destroy(yrtb_psf* psf);
 yrtb_status yrtb_psf_apply(const yrtb_psf* psf, const float* d_in, float* d_out,
                            const yrtb_image_params* image, int adjoint,
                            float* d_tmp, yrtb_stream stream);
+
+/* ------------------------------------------- low-rank dynamic images --- */
+/* Low-rank image model of the LR updater (ProjectorUpdaterLR,
+ * src/operators/ProjectorUpdater.cpp:228-280; ProjectorUpdaterDeviceLR,
+ * include/yrt-pet/operators/ProjectorUpdaterDevice.cuh:53-225; LREM,
+ * src/recon/LREM.cpp:175-260): frame t of the image is
+ * x_t = sum_l H[l][t] W_l, with W = rank images of voxels_per_frame floats
+ * (rank-major) and H = rank x frames floats (row-major, HBasis[r][t]).
+ * Instead of the rank sum at every voxel crossing, a projection of the
+ * low-rank image projects the expanded frames (yrtb_lr_expand, then any
+ * frame-indexed projector call with nt = frames), and a back projection is
+ * contracted onto the basis afterwards (yrtb_lr_contract_w for W,
+ * yrtb_lr_contract_h for H).  rank <= 32. */
+
+/* X[t][j] = sum_l W[l][j] H[l][t], l ascending, FP32 products and sums in the
+ * reference updater's order (X: frames x voxels_per_frame floats). */
+yrtb_status yrtb_lr_expand(const float* d_W, const float* d_H, int rank, int frames,
+                           uint64_t voxels_per_frame, float* d_X, yrtb_stream stream);
+
+/* Wn[l][j] = sum_t E[t][j] H[l][t] (E: frames x voxels_per_frame, e.g. the
+ * EM image of an EM step over the expanded frames; Wn: rank images). */
+yrtb_status yrtb_lr_contract_w(const float* d_E, const float* d_H, int rank, int frames,
+                               uint64_t voxels_per_frame, float* d_Wn, yrtb_stream stream);
+
+/* Hn[l][t] = sum_j W[l][j] E[t][j] (FP32 products, FP64 sums in a fixed order:
+ * deterministic).  rank x frames <= 2048 and rank + frames <= 440.  With
+ * frames = 1 and E = a sensitivity image it gives LREM's H-update scaling
+ * c_r = sum_j W[r][j] s[j] (LREM::generateHUpdateSensScaling). */
+yrtb_status yrtb_lr_contract_h(const float* d_W, const float* d_E, int rank, int frames,
+                               uint64_t voxels_per_frame, double* d_Hn, yrtb_stream stream);
+
+/* H[r][t] *= float(Hn[r][t]) * (1 / max(c[r], eps))  (LREM::applyHUpdate,
+ * src/recon/LREM.cpp:175-199).  d_c: rank floats. */
+yrtb_status yrtb_lr_update_h(float* d_H, const double* d_Hn, const float* d_c, int rank,
+                             int frames, float eps, yrtb_stream stream);
 
 /* ------------------------------------------------------ OSEM (driver) --- */
 /* List-mode OSEM over device-resident events.  Mirrors OSEM::reconstruct

@@ -619,3 +619,91 @@ def ref_psf_gaussian_kernel(sigma, voxel, size=0):
             _p(buf), ctypes.c_uint64(len(buf)), ctypes.byref(n))
     _ref_check(rc)
     return buf[:n.value].copy()
+
+
+# ------------------------------------------------------ low-rank images ----
+def lr_expand(W, H):
+    """Frames of a low-rank image, x_t = sum_l W_l H[l][t] with FP32 products
+    and sums in l order (ProjectorUpdaterLR::forwardUpdate,
+    src/operators/ProjectorUpdater.cpp:228-243).  W: (R, ...) float32,
+    H: (R, T).  Returns (T, ...)."""
+    W = np.ascontiguousarray(W, np.float32)
+    H = np.ascontiguousarray(H, np.float32)
+    R, T = H.shape
+    out = np.zeros((T,) + W.shape[1:], np.float32)
+    for t in range(T):
+        acc = np.zeros(W.shape[1:], np.float32)
+        for l in range(R):
+            acc = (acc + (W[l] * H[l, t]).astype(np.float32)).astype(np.float32)
+        out[t] = acc
+    return out
+
+
+def lr_contract_w_f64(E, H):
+    """W-side back projection of a low-rank image from a frame-indexed one:
+    Wn_l = sum_t H[l][t] E_t, in FP64 (the reference adds H[l][t] times each
+    crossing's value, ProjectorUpdater.cpp:245-266)."""
+    E = np.asarray(E, np.float64)
+    H = np.asarray(H, np.float64)
+    return np.tensordot(H, E, (1, 0))
+
+
+def lr_contract_h_f64(W, E):
+    """H-side back projection: Hn[l][t] = sum_j W[l][j] E[t][j], in FP64."""
+    W = np.asarray(W, np.float64).reshape(W.shape[0], -1)
+    E = np.asarray(E, np.float64).reshape(E.shape[0], -1)
+    return W @ E.T
+
+
+def ref_siddon_lr(sc: Scanner, ip: ImageParams, lors, frames, H, *, image=None,
+                  values=None, tof=None, tof_fwhm_ps=0.0, tof_n_std=0,
+                  forward=True, threads=8):
+    """The reference's incremental Siddon with its LR updater: ip.nt = rank
+    (image = W), H: rank x frames, frames[i] = each LOR's dynamic frame."""
+    lors = _c(lors, np.float32)
+    n = len(lors)
+    tof = _c(tof, np.float32)
+    frames = _c(frames, np.int32)
+    Hc = np.ascontiguousarray(H, np.float32).copy()
+    R, T = Hc.shape
+    if forward:
+        img = np.ascontiguousarray(image, np.float32).copy()
+        vals = np.zeros(n, np.float32)
+    else:
+        img = np.zeros(ip.shape, np.float32)
+        vals = np.ascontiguousarray(values, np.float32).copy()
+    with quiet():
+        rc = ref_lib().ref_siddon_lr(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), _p(img),
+            ctypes.c_uint64(n), _p(lors), _p(tof), ctypes.c_float(tof_fwhm_ps),
+            ctypes.c_int(tof_n_std), _p(frames), _p(Hc), ctypes.c_int(R),
+            ctypes.c_int(T), ctypes.c_int(int(forward)), ctypes.c_int(threads),
+            _p(vals))
+    _ref_check(rc)
+    return vals if forward else img
+
+
+def ref_lrem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, timestamps,
+                      frame_ts, H, *, tof=None, update_h=False, init=None, **kw):
+    """Reference low-rank EM (LREM_CPU): ip.nt = rank.  Returns (W, H after
+    the reconstruction, seconds); H changes only with update_h."""
+    o = _osem_desc(**kw)
+    out = np.zeros(ip.shape, np.float32)
+    sec = ctypes.c_double()
+    d1 = _c(d1, np.uint32)
+    d2 = _c(d2, np.uint32)
+    ts = _c(timestamps, np.uint32)
+    fts = _c(frame_ts, np.uint32)
+    tof = _c(tof, np.float32)
+    s = _c(sens, np.float32)
+    Hc = np.ascontiguousarray(H, np.float32).copy()
+    R, T = Hc.shape
+    ini = _c(init, np.float32)
+    with quiet():
+        rc = ref_lib().ref_lrem_listmode(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
+            _p(s), ctypes.c_uint64(len(d1)), _p(d1), _p(d2), _p(tof), _p(ts),
+            _p(fts), _p(Hc), ctypes.c_int(R), ctypes.c_int(T),
+            ctypes.c_int(int(update_h)), _p(ini), _p(out), ctypes.byref(sec))
+    _ref_check(rc)
+    return out, Hc, sec.value

@@ -15,6 +15,8 @@
 //   TimeOfFlightHelper              include/yrt-pet/operators/TimeOfFlight.hpp:19-85
 //   convertToHistogram3D            src/utils/ReconstructionUtils.cpp:659-800
 //   OSEM (CPU)                      src/recon/OSEM.cpp:315-365, OSEM_CPU.cpp:127-403
+//   LR updater, LREM (CPU)          src/operators/ProjectorUpdater.cpp:228-280,
+//                                   src/recon/LREM.cpp, LREM_CPU.cpp
 
 #include "yrt-pet/datastruct/image/Image.hpp"
 #include "yrt-pet/datastruct/projection/DynamicFraming.hpp"
@@ -29,6 +31,7 @@
 #include "yrt-pet/operators/ProjectorParams.hpp"
 #include "yrt-pet/operators/ProjectorSiddon.hpp"
 #include "yrt-pet/operators/TimeOfFlight.hpp"
+#include "yrt-pet/recon/LREM.hpp"
 #include "yrt-pet/recon/OSEM.hpp"
 #include "yrt-pet/utils/Globals.hpp"
 #include "yrt-pet/utils/ReconstructionUtils.hpp"
@@ -705,6 +708,122 @@ int ref_osem_histo3d(const ref_scanner_desc* s, const ref_image_desc* d,
 		    const auto t1 = std::chrono::steady_clock::now();
 		    if (seconds)
 			    *seconds = std::chrono::duration<double>(t1 - t0).count();
+		    std::memcpy(out, res->getRawPointer(), nv * sizeof(float));
+	    });
+}
+
+// Incremental Siddon forward (fwd=1: values[i] = A x) or back projection
+// (fwd=0: W += A^T values) of a low-rank image through the reference's
+// ProjectorUpdaterLR: image holds rank frames W (d->nt = rank), H is
+// rank x frames (row-major), frames[i] is each LOR's dynamic frame.
+int ref_siddon_lr(const ref_scanner_desc* s, const ref_image_desc* d, float* image,
+                  uint64_t n, const float* lors, const float* tof, float tof_fwhm_ps,
+                  int tof_n_std, const int32_t* frames, float* H, int rank,
+                  int num_frames, int fwd, int threads, float* values)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    auto img = makeImage(d, image);
+		    ProjectorParams pp(*sc);
+		    pp.updaterType = UpdaterType::LR;
+		    pp.bindHBasis(H, rank, num_frames);
+		    globals::setNumThreads(threads);
+		    ProjectorSiddon proj(pp);
+		    std::unique_ptr<TimeOfFlightHelper> tofh;
+		    if (tof)
+			    tofh = std::make_unique<TimeOfFlightHelper>(tof_fwhm_ps, tof_n_std);
+		    const Vector3D zero{};
+		    parallelFor(
+		        n, threads,
+		        [&](size_t i, int tid)
+		        {
+			        Line3D lor{{lors[i * 6 + 0], lors[i * 6 + 1], lors[i * 6 + 2]},
+			                   {lors[i * 6 + 3], lors[i * 6 + 4], lors[i * 6 + 5]}};
+			        const frame_t fr = frames[i];
+			        const float tv = tof ? tof[i] : 0.f;
+			        if (fwd)
+				        values[i] = proj.forwardProjection(img.get(), lor, zero, zero,
+				                                           tid, fr, tofh.get(), tv);
+			        else
+				        proj.backProjection(img.get(), lor, zero, zero, values[i], tid,
+				                            fr, tofh.get(), tv);
+		        });
+		    if (!fwd)
+		    {
+			    const size_t nv = d->nx * d->ny * d->nz * d->nt;
+			    std::memcpy(image, img->getRawPointer(), nv * sizeof(float));
+		    }
+	    });
+}
+
+// List-mode low-rank EM with the reference CPU path (LREM_CPU through
+// util::createOSEM(scanner, false, true)): d->nt = rank; H (rank x frames,
+// row-major) is bound as the HBasis and, with update_h, updated in place.
+// timestamps / frame_ts give the events' dynamic frames (DynamicFraming with
+// frames+1 boundaries).  init (nullable): initial W.  out: W (rank images).
+int ref_lrem_listmode(const ref_scanner_desc* s, const ref_image_desc* d,
+                      const ref_osem_desc* o, const float* sens, uint64_t n,
+                      const uint32_t* d1, const uint32_t* d2, const float* tof,
+                      const uint32_t* timestamps, const uint32_t* frame_ts,
+                      float* H, int rank, int num_frames, int update_h,
+                      const float* init, float* out, double* seconds)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    globals::setNumThreads(o->threads);
+		    ListModeLUTOwned lm(*sc, tof != nullptr, false);
+		    lm.allocate(n);
+		    for (uint64_t i = 0; i < n; i++)
+		    {
+			    lm.setDetectorIdsOfEvent(i, d1[i], d2[i]);
+			    if (tof)
+				    lm.setTOFValueOfEvent(i, tof[i]);
+			    lm.setTimestampOfEvent(i, timestamps[i]);
+		    }
+		    std::vector<timestamp_t> v(frame_ts, frame_ts + num_frames + 1);
+		    lm.addDynamicFraming(v);
+		    auto osem = util::createOSEM(*sc, false, true);
+		    auto* lr = dynamic_cast<LREM*>(osem.get());
+		    if (!lr)
+			    throw std::runtime_error("createOSEM did not return an LREM");
+		    ImageParams ip = makeParams(d);
+		    osem->setImageParams(ip);
+		    osem->num_OSEM_subsets = o->subsets;
+		    osem->num_MLEM_iterations = o->iterations;
+		    osem->setListModeEnabled(true);
+		    osem->setProjector(o->projector == 0 ? ProjectorType::SIDDON :
+		                                           ProjectorType::DD);
+		    osem->setNumRays(o->num_rays);
+		    if (o->tof_fwhm_ps > 0)
+			    osem->addTOF(o->tof_fwhm_ps, o->tof_n_std);
+		    osem->setGlobalScalingFactor(o->global_scale);
+		    osem->setProjectorUpdaterType(UpdaterType::LR);
+		    Array2DAlias<float> hb;
+		    hb.bind(H, rank, num_frames);
+		    lr->setHBasis(hb);
+		    lr->setUpdateH(update_h != 0);
+		    std::unique_ptr<ImageOwned> initImg;
+		    if (init)
+		    {
+			    initImg = makeImage(d, init);
+			    osem->setInitialEstimate(initImg.get());
+		    }
+		    ref_image_desc sd = *d;
+		    sd.nt = 1;
+		    auto sensImg = makeImage(&sd, sens);
+		    osem->setSensitivityImage(sensImg.get(), 0);
+		    osem->setDataInput(&lm);
+		    const auto t0 = std::chrono::steady_clock::now();
+		    auto res = osem->reconstruct("");
+		    const auto t1 = std::chrono::steady_clock::now();
+		    if (seconds)
+			    *seconds = std::chrono::duration<double>(t1 - t0).count();
+		    const ImageParams& rp = res->getParams();
+		    const size_t nv = rp.nx * rp.ny * rp.nz * rp.nt;
 		    std::memcpy(out, res->getRawPointer(), nv * sizeof(float));
 	    });
 }

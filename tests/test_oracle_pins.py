@@ -275,3 +275,69 @@ def test_psf_gaussian_kernel_matches_reference():
     mine = np.exp(-0.5 * (x * np.float32(2.0) / np.float32(1.7)) ** 2).astype(np.float32)
     mine /= mine.sum(dtype=np.float32)
     assert np.allclose(k, mine, rtol=1e-6)
+
+
+# ------------------------------------------------------ low-rank images ----
+def _lr_case(seed, n=6000, R=3, T=5):
+    rng = np.random.default_rng(seed)
+    lut = po.scanner_lut(SC)
+    d1 = rng.integers(0, SC.num_dets, n)
+    d2 = rng.integers(0, SC.num_dets, n)
+    ok = d1 % 256 != d2 % 256
+    lors, _ = po.lors_from_detpairs(lut, d1[ok], d2[ok])
+    frames = rng.integers(0, T, len(lors)).astype(np.int32)
+    W = rng.random((R,) + IP.shape[1:], dtype=np.float32)
+    H = rng.random((R, T), dtype=np.float32)
+    return lors, frames, W, H
+
+
+@needs_ref
+@pytest.mark.parametrize("tofw", [0.0, 214.0])
+def test_lr_forward_is_forward_of_expanded_frames(tofw):
+    """The reference's LR updater forward (rank sum at each crossing) equals,
+    bit for bit, its plain forward projection of the expanded frames."""
+    lors, frames, W, H = _lr_case(31)
+    R, T = H.shape
+    rng = np.random.default_rng(32)
+    tof = rng.normal(0, 300, len(lors)).astype(np.float32) if tofw else None
+    ipw = po.ImageParams(32, 32, 16, 128, 128, 64, nt=R)
+    ipx = po.ImageParams(32, 32, 16, 128, 128, 64, nt=T)
+    a = po.ref_siddon_lr(SC, ipw, lors, frames, H, image=W, tof=tof,
+                         tof_fwhm_ps=tofw, tof_n_std=5)
+    X = po.lr_expand(W, H)
+    b = po.ref_siddon(SC, ipx, lors, image=X, tof=tof, tof_fwhm_ps=tofw,
+                      tof_n_std=5, frames=frames)
+    assert np.array_equal(bits(a), bits(b))
+
+
+@needs_ref
+def test_lr_backward_is_contraction_of_frame_backprojection():
+    """The reference's LR updater back projection (rank atomics per crossing)
+    equals the contraction of its frame-indexed back projection, up to the
+    order of FP32 sums."""
+    lors, frames, W, H = _lr_case(33)
+    R, T = H.shape
+    vals = np.random.default_rng(34).random(len(lors), dtype=np.float32)
+    ipw = po.ImageParams(32, 32, 16, 128, 128, 64, nt=R)
+    ipx = po.ImageParams(32, 32, 16, 128, 128, 64, nt=T)
+    a = po.ref_siddon_lr(SC, ipw, lors, frames, H, values=vals, forward=False,
+                         threads=1)
+    E = po.ref_siddon(SC, ipx, lors, values=vals, frames=frames, forward=False,
+                      threads=1)
+    b = po.lr_contract_w_f64(E, H)
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-6
+
+
+def test_lr_oracle_expand_and_contractions_agree():
+    """<A_lr W, y> identities of the restatement: the expansion and the two
+    contractions are adjoint to each other in FP64."""
+    rng = np.random.default_rng(35)
+    R, T, J = 4, 7, 300
+    W = rng.random((R, J), dtype=np.float32)
+    H = rng.random((R, T), dtype=np.float32)
+    E = rng.random((T, J), dtype=np.float32)
+    X = po.lr_expand(W, H)
+    lhs = float(np.sum(X.astype(np.float64) * E))
+    rhs_w = float(np.sum(W.astype(np.float64) * po.lr_contract_w_f64(E, H)))
+    rhs_h = float(np.sum(H.astype(np.float64) * po.lr_contract_h_f64(W, E)))
+    assert abs(lhs - rhs_w) / lhs < 1e-6 and abs(lhs - rhs_h) / lhs < 1e-6

@@ -1378,13 +1378,13 @@ __global__ void k_em_update(float* __restrict__ x, const float* __restrict__ u,
 	{
 		const uint64_t j = i % J;
 		const uint64_t r = i / J;
-		if (sens_nt == nt && nt > 1)
+		if (!scale && sens_nt == nt && nt > 1)
 		{
 			const float sv = __ldg(s + i);
 			if (sv > thr)
 				x[i] *= __ldg(u + i) / sv;
 		}
-		else if (nt == 1)
+		else if (!scale && nt == 1)
 		{
 			const float sv = __ldg(s + j);
 			if (sv > thr)
@@ -1612,6 +1612,159 @@ void psfPass(dim3 grid, dim3 block, cudaStream_t st, const float* src, float* ds
 		                                            planes, k, nk);
 	}
 #undef YRTB_PSF_CASE
+}
+
+// ------------------------------------------------- low-rank dynamic image --
+// Frame t of a low-rank image is x_t = sum_l H[l][t] W_l (W: rank images, H:
+// rank x frames basis), the ProjectorUpdaterLR / ProjectorUpdaterDeviceLR
+// model (src/operators/ProjectorUpdater.cpp:228-280,
+// include/yrt-pet/operators/ProjectorUpdaterDevice.cuh:53-225).  The reference
+// applies the rank sum at every voxel crossing (rank gathers forward, rank
+// atomics backward).  Here the frames are expanded once per subset, the
+// frame-indexed projection kernels run on them (one gather / one atomic per
+// crossing), and the frame-indexed EM image is contracted back onto W or H.
+constexpr int kLrMaxRank = 32;
+constexpr int kLrTile = 128;      // voxels per shared-memory tile (H contraction)
+constexpr int kLrPairs = 8;       // (rank, frame) pairs per thread, 256 threads
+constexpr int kLrBlock = 256;
+
+// X[t][j] = sum_l W[l][j] * H[l][t], l ascending, rounded products and sums
+// (the CPU updater's forwardUpdate order).
+template <int RMAX>
+__global__ void __launch_bounds__(kBlock)
+k_lr_expand(const float* __restrict__ W, const float* __restrict__ H, int R, int T, uint64_t J,
+            float* __restrict__ X)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < J;
+	     j += nthreads)
+	{
+		float w[RMAX];
+#pragma unroll
+		for (int l = 0; l < RMAX; l++)
+			w[l] = l < R ? __ldg(W + l * J + j) : 0.f;
+		for (int t = 0; t < T; t++)
+		{
+			float x = 0.f;
+#pragma unroll
+			for (int l = 0; l < RMAX; l++)
+				if (l < R)
+					x = __fadd_rn(x, __fmul_rn(w[l], __ldg(H + l * T + t)));
+			X[static_cast<uint64_t>(t) * J + j] = x;
+		}
+	}
+}
+
+// Wn[l][j] = sum_t E[t][j] * H[l][t], t ascending.
+template <int RMAX>
+__global__ void __launch_bounds__(kBlock)
+k_lr_contract_w(const float* __restrict__ E, const float* __restrict__ H, int R, int T,
+                uint64_t J, float* __restrict__ Wn)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < J;
+	     j += nthreads)
+	{
+		float acc[RMAX];
+#pragma unroll
+		for (int l = 0; l < RMAX; l++)
+			acc[l] = 0.f;
+		for (int t = 0; t < T; t++)
+		{
+			const float e = __ldg(E + static_cast<uint64_t>(t) * J + j);
+#pragma unroll
+			for (int l = 0; l < RMAX; l++)
+				if (l < R)
+					acc[l] = __fadd_rn(acc[l], __fmul_rn(e, __ldg(H + l * T + t)));
+		}
+#pragma unroll
+		for (int l = 0; l < RMAX; l++)
+			if (l < R)
+				Wn[l * J + j] = acc[l];
+	}
+}
+
+// Split-J contraction: partial[b][l*T + t] = sum over block b's voxels of
+// W[l][j] * E[t][j] (rounded FP32 product, FP64 sum).  Tiles of kLrTile voxels
+// of every W row and E row sit in shared memory (rows padded to kLrTile + 1
+// floats: the 32 threads of a warp read 32 different E rows without bank
+// conflicts); each thread owns up to kLrPairs (l, t) pairs.
+__global__ void __launch_bounds__(kLrBlock)
+k_lr_contract_h(const float* __restrict__ W, const float* __restrict__ E, int R, int T,
+                uint64_t J, double* __restrict__ partial)
+{
+	extern __shared__ float lrTile[];
+	constexpr int ld = kLrTile + 1;
+	const int P = R * T;
+	double acc[kLrPairs];
+#pragma unroll
+	for (int q = 0; q < kLrPairs; q++)
+		acc[q] = 0.0;
+	for (uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * kLrTile; j0 < J;
+	     j0 += static_cast<uint64_t>(gridDim.x) * kLrTile)
+	{
+		const uint64_t left = J - j0;
+		const int n = left < static_cast<uint64_t>(kLrTile) ? static_cast<int>(left) : kLrTile;
+		__syncthreads();
+		for (int idx = threadIdx.x; idx < (R + T) * kLrTile; idx += blockDim.x)
+		{
+			const int row = idx / kLrTile, col = idx - row * kLrTile;
+			float v = 0.f;
+			if (col < n)
+				v = row < R ? __ldg(W + row * J + j0 + col)
+				            : __ldg(E + static_cast<uint64_t>(row - R) * J + j0 + col);
+			lrTile[row * ld + col] = v;
+		}
+		__syncthreads();
+#pragma unroll
+		for (int q = 0; q < kLrPairs; q++)
+		{
+			const int k = threadIdx.x + q * kLrBlock;
+			if (k < P)
+			{
+				const int l = k / T, t = k - (k / T) * T;
+				const float* a = lrTile + l * ld;
+				const float* b = lrTile + (R + t) * ld;
+				double sum = 0.0;
+				for (int i = 0; i < n; i++)
+					sum += static_cast<double>(__fmul_rn(a[i], b[i]));
+				acc[q] += sum;
+			}
+		}
+	}
+#pragma unroll
+	for (int q = 0; q < kLrPairs; q++)
+	{
+		const int k = threadIdx.x + q * kLrBlock;
+		if (k < P)
+			partial[static_cast<uint64_t>(blockIdx.x) * P + k] = acc[q];
+	}
+}
+
+// out[k] = sum over blocks b (ascending) of partial[b][k].
+__global__ void k_lr_finish(const double* __restrict__ partial, int blocks, int P,
+                            double* __restrict__ out)
+{
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P; k += gridDim.x * blockDim.x)
+	{
+		double s = 0.0;
+		for (int b = 0; b < blocks; b++)
+			s += partial[static_cast<uint64_t>(b) * P + k];
+		out[k] = s;
+	}
+}
+
+// H[r][t] *= float(Hn[r][t]) * (1 / max(cH[r], eps))  (LREM::applyHUpdate,
+// src/recon/LREM.cpp:175-199: the numerator is held in FP32 there).
+__global__ void k_lr_update_h(float* __restrict__ H, const double* __restrict__ Hn,
+                              const float* __restrict__ cH, int R, int T, float eps)
+{
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < R * T; k += gridDim.x * blockDim.x)
+	{
+		const int r = k / T;
+		const float inv = 1.0f / fmaxf(cH[r], eps);
+		H[k] = __fmul_rn(H[k], __fmul_rn(static_cast<float>(Hn[k]), inv));
+	}
 }
 
 int g_numSMs = 0;
@@ -2922,6 +3075,101 @@ yrtb_status yrtb_psf_apply(const yrtb_psf* p, const float* d_in, float* d_out,
 	psfPass<2>(grid, block, st, tmp, d_out, dims, planes, k[2], p->n[2], vec);
 	if (!d_tmp)
 		YRTB_CUDA(cudaFreeAsync(tmp, st));
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+#define YRTB_LR_LAUNCH(KERNEL, ...)                                                        \
+	do                                                                                     \
+	{                                                                                      \
+		const unsigned grid_ = gridFor(J, 8);                                              \
+		if (R <= 4)                                                                        \
+			KERNEL<4><<<grid_, kBlock, 0, st>>>(__VA_ARGS__);                              \
+		else if (R <= 8)                                                                   \
+			KERNEL<8><<<grid_, kBlock, 0, st>>>(__VA_ARGS__);                              \
+		else if (R <= 16)                                                                  \
+			KERNEL<16><<<grid_, kBlock, 0, st>>>(__VA_ARGS__);                             \
+		else                                                                               \
+			KERNEL<32><<<grid_, kBlock, 0, st>>>(__VA_ARGS__);                             \
+	} while (0)
+
+static yrtb_status lrCheck(int R, int T, uint64_t J)
+{
+	if (R <= 0 || R > kLrMaxRank)
+		return fail(YRTB_ERR_ARGUMENT, "low-rank basis: rank must be in 1..32");
+	if (T <= 0 || J == 0)
+		return fail(YRTB_ERR_ARGUMENT, "low-rank basis: empty frames or image");
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_lr_expand(const float* d_W, const float* d_H, int R, int T, uint64_t J,
+                           float* d_X, yrtb_stream stream)
+{
+	if (!d_W || !d_H || !d_X)
+		return fail(YRTB_ERR_ARGUMENT, "null low-rank argument");
+	yrtb_status s = lrCheck(R, T, J);
+	if (s != YRTB_OK)
+		return s;
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	YRTB_LR_LAUNCH(k_lr_expand, d_W, d_H, R, T, J, d_X);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_lr_contract_w(const float* d_E, const float* d_H, int R, int T, uint64_t J,
+                               float* d_Wn, yrtb_stream stream)
+{
+	if (!d_E || !d_H || !d_Wn)
+		return fail(YRTB_ERR_ARGUMENT, "null low-rank argument");
+	yrtb_status s = lrCheck(R, T, J);
+	if (s != YRTB_OK)
+		return s;
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	YRTB_LR_LAUNCH(k_lr_contract_w, d_E, d_H, R, T, J, d_Wn);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_lr_contract_h(const float* d_W, const float* d_E, int R, int T, uint64_t J,
+                               double* d_Hn, yrtb_stream stream)
+{
+	if (!d_W || !d_E || !d_Hn)
+		return fail(YRTB_ERR_ARGUMENT, "null low-rank argument");
+	yrtb_status s = lrCheck(R, T, J);
+	if (s != YRTB_OK)
+		return s;
+	const int P = R * T;
+	const size_t smem = static_cast<size_t>(R + T) * (kLrTile + 1) * sizeof(float);
+	if (P > kLrPairs * kLrBlock || smem > 227 * 1024)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "low-rank basis too large for the H contraction "
+		            "(rank x frames <= 2048, rank + frames <= 440)");
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	if (smem > 48 * 1024)
+		YRTB_CUDA(cudaFuncSetAttribute(k_lr_contract_h,
+		                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                               static_cast<int>(smem)));
+	const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(
+	    (J + kLrTile - 1) / kLrTile, static_cast<uint64_t>(gridFor(1 << 30, 2))));
+	double* partial = nullptr;
+	YRTB_CUDA(poolAlloc(&partial, static_cast<size_t>(blocks) * P * sizeof(double), st));
+	k_lr_contract_h<<<blocks, kLrBlock, smem, st>>>(d_W, d_E, R, T, J, partial);
+	k_lr_finish<<<(P + kBlock - 1) / kBlock, kBlock, 0, st>>>(partial, blocks, P, d_Hn);
+	YRTB_CUDA(cudaFreeAsync(partial, st));
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_lr_update_h(float* d_H, const double* d_Hn, const float* d_cH, int R, int T,
+                             float eps, yrtb_stream stream)
+{
+	if (!d_H || !d_Hn || !d_cH)
+		return fail(YRTB_ERR_ARGUMENT, "null low-rank argument");
+	yrtb_status s = lrCheck(R, T, 1);
+	if (s != YRTB_OK)
+		return s;
+	k_lr_update_h<<<(R * T + kBlock - 1) / kBlock, kBlock, 0,
+	                reinterpret_cast<cudaStream_t>(stream)>>>(d_H, d_Hn, d_cH, R, T, eps);
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }

@@ -14,6 +14,7 @@ from .core import (BinIteratorChronologicalInterleaved,  # noqa: F401
                    release_cached_memory, write_psf_csv)
 from .osem import OSEM_GPU, createOSEM  # noqa: F401
 from .psf import OperatorPsfDevice, write_image_psf_csv  # noqa: F401
+from .lrem import LREM_GPU, LowRankProjector  # noqa: F401
 
 ListModeLUTOwned = ListModeLUT
 ListModeLUTAlias = ListModeLUT

@@ -146,6 +146,14 @@ SIGNATURES = {
                               c_f, c_f, c_f, c_vp], ctypes.c_int),
     "yrtb_fill": ([c_vp, c_u64, c_f, c_vp], ctypes.c_int),
     "yrtb_scale": ([c_vp, c_u64, c_f, c_vp], ctypes.c_int),
+    "yrtb_lr_expand": ([c_vp, c_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, c_vp, c_vp],
+                       ctypes.c_int),
+    "yrtb_lr_contract_w": ([c_vp, c_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, c_vp,
+                            c_vp], ctypes.c_int),
+    "yrtb_lr_contract_h": ([c_vp, c_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, c_vp,
+                            c_vp], ctypes.c_int),
+    "yrtb_lr_update_h": ([c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, c_vp],
+                         ctypes.c_int),
     "yrtb_psf_create": ([c_vp, ctypes.c_int, c_vp, ctypes.c_int, c_vp, ctypes.c_int,
                          _P(c_vp)], ctypes.c_int),
     "yrtb_psf_destroy": ([c_vp], None),

@@ -210,6 +210,10 @@ class ProjectorParams:
         self.numRays = 1
         self.projPsf_fname = ""
         self.updaterType = "DEFAULT4D"
+        # Low-rank updater: HBasis (rank x frames float32) and whether a back
+        # projection accumulates onto H instead of W.
+        self.HBasis = None
+        self.updateH = False
         self.precision = L.YRTB_MIRROR
         # Two-pass fixed-point back projection (order-independent results).
         self.deterministic = False
@@ -225,6 +229,14 @@ class ProjectorParams:
             self.projectorType = "DD"
         else:
             raise RuntimeError(f"Unknown projector: {name}")
+
+    def setHBasisFromNumpy(self, HBasis):
+        h = np.asarray(HBasis)
+        if h.ndim != 2:
+            raise RuntimeError("HBasis must be 2D (rank x time).")
+        if h.dtype != np.float32:
+            raise RuntimeError("HBasis must be float32.")
+        self.HBasis = np.ascontiguousarray(h)
 
     def addTOF(self, tofWidth_ps: float, tofNumStd: int):
         self._tofWidth_ps = float(tofWidth_ps)
@@ -956,8 +968,9 @@ class ProjectionOper:
                  num_subsets=1, tof_width_ps=None, tof_n_std=0,
                  proj_psf_fname=None, num_rays=1, H_basis=None,
                  update_H=False, use_gpu=True):
-        if updater_type != "DEFAULT4D":
-            raise RuntimeError("only the DEFAULT4D updater is supported")
+        updater_type = getattr(updater_type, "name", str(updater_type)).upper()
+        if updater_type not in ("DEFAULT4D", "LR"):
+            raise RuntimeError("Projector updater type not valid")
         self._scanner = scanner
         self._img_params = img_params
         self._projData = projData
@@ -971,14 +984,51 @@ class ProjectionOper:
         self._proj_params = pp
         self._oper = OperatorProjectorDevice.create(pp, self._binIter)
         self._image_shape = img_params.shape
+        self._lr = None
+        if updater_type == "LR":
+            # Low-rank image: x holds rank images W, the frames are
+            # x_t = sum_l H[l][t] W_l (the LR updater); events carry their
+            # dynamic frame (ListModeLUT.addDynamicFraming).
+            if H_basis is None:
+                raise RuntimeError("LR updater was requested but HBasis is empty")
+            pp.updaterType = "LR"
+            pp.setHBasisFromNumpy(H_basis)
+            pp.updateH = bool(update_H)
+            R, T = pp.HBasis.shape
+            self._image_shape = (R,) + img_params.shape[1:]
+            self._frames_params = img_params.withFrames(T)
+
+    def _lr_projector(self):
+        from .lrem import LowRankProjector
+        if self._lr is None:
+            dp = self._oper._projector(self._frames_params)
+            self._lr = LowRankProjector(dp, self._proj_params.HBasis)
+        return self._lr
 
     def A(self, x):
         xx = torch.as_tensor(np.require(x, np.float32)).reshape(
             self._image_shape).cuda()
+        if self._proj_params.updaterType == "LR":
+            ev, rng = self._oper._events(self._projData)
+            out = torch.zeros(ev.count, dtype=torch.float32, device="cuda")
+            return self._lr_projector().forward(xx, ev, out=out, rng=rng).cpu().numpy()
         y = self._oper.applyA(xx, self._projData, self._img_params)
         return y.cpu().numpy()
 
-    def At(self, y):
+    def At(self, y, W=None):
+        """Back projection.  With the LR updater: onto W (rank images), or,
+        with update_H, onto the temporal basis given the rank images W
+        (returns the rank x frames numerator sum value * weight * W[l][j])."""
         yy = torch.as_tensor(np.require(y, np.float32)).cuda()
+        if self._proj_params.updaterType == "LR":
+            ev, rng = self._oper._events(self._projData)
+            lrp = self._lr_projector()
+            if self._proj_params.updateH:
+                if W is None:
+                    raise RuntimeError("the H back projection needs the rank images W")
+                Wt = torch.as_tensor(np.require(W, np.float32)).reshape(
+                    self._image_shape).cuda()
+                return lrp.backward_h(yy, Wt, ev, rng=rng).cpu().numpy()
+            return lrp.backward(yy, ev, rng=rng).cpu().numpy()
         x = self._oper.applyAH(yy, self._projData, self._img_params)
         return x.cpu().numpy()

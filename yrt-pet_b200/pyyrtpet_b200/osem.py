@@ -424,5 +424,6 @@ def createOSEM(scanner: Scanner, useGPU: bool = True, isLowRank: bool = False):
     if not useGPU:
         raise RuntimeError("pyyrtpet_b200 provides the GPU reconstruction only")
     if isLowRank:
-        raise RuntimeError("low-rank (LREM) reconstruction is not provided")
+        from .lrem import LREM_GPU
+        return LREM_GPU(scanner)
     return OSEM_GPU(scanner)
