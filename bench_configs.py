@@ -21,6 +21,8 @@ each printing one JSON line:
       frame).
   psf image-space PSF (applyA + applyAH) on the C2 image, bit-exact against
       the reference operator.
+  lrem low-rank list-mode EM (rank 8, 20 frames) on the C2 scanner and image,
+      20M TOF events: per-stage times of expand / EM pass / contraction.
 
 Inputs are seeded synthetic events (the reference's datasets are not
 available); the reference CPU measurements use oracle/_ref, the reference
@@ -487,6 +489,131 @@ def run_psf(args):
     return out
 
 
+# ---------------------------------------------------------- low-rank EM ----
+def run_lrem(args):
+    """Low-rank list-mode EM (W update): rank 8, 20 dynamic frames, C2 scanner
+    and image, 20M TOF events spread evenly over the frames, 4 subsets."""
+    yrt, L, S, _stream = _yrt()
+    from pyyrtpet_b200 import lrem
+    sc = S.scanner_c2()
+    ip1 = S.image_c2()
+    R, T, subsets = 8, 20, 4
+    n = args.cfg_events or 20_000_000
+    ev = S.generate_events(sc, n, 20261203 + 60, tof_fwhm_ps=214.0, device="cuda",
+                           chunk=1 << 24)
+    frames = ((torch.arange(n, device="cuda", dtype=torch.int64) * T) // n).to(torch.int32)
+    pp = yrt.ProjectorParams(sc)
+    pp.addTOF(214.0, 5)
+    pp.precision = L.YRTB_COMPENSATED
+    ipT = ip1.withFrames(T)
+    proj = yrt.DeviceProjector(sc, ipT, pp)
+    base = yrt.DeviceEvents.from_arrays(ev.d1.to(torch.int32), ev.d2.to(torch.int32),
+                                        tof=ev.tof, frame=frames)
+    J = ip1.numVoxels
+    sens_proj = yrt.DeviceProjector(sc, ip1, yrt.ProjectorParams(sc))
+    sens = torch.zeros(J, device="cuda")
+    sens_proj.sensitivity_histo3d(sens, 20, 0)
+    sens.mul_(20.0)
+    lib = L.lib()
+    st = _stream()
+    g = torch.Generator(device="cuda").manual_seed(20261203 + 61)
+    H = (0.2 + torch.rand((R, T), generator=g, device="cuda")).contiguous()
+    c = torch.from_numpy(lrem.w_update_scaling(H.cpu().numpy())).cuda()
+    sens_sub = (sens * np.float32(1.0 / subsets)).contiguous()
+    X = torch.empty(T * J, device="cuda")
+    E = torch.empty(T * J, device="cuda")
+    Wn = torch.empty(R * J, device="cuda")
+    W = torch.full((R * J,), 0.125, device="cuda")
+    # Set-up (not timed): launch configuration and subset-major event order.
+    lrem.lr_expand(W, H, out=X)
+    tune = proj.autotune(X, base, subsets)
+    ordered, offs = proj.order_events(base, subsets)
+    evc = ordered.c()
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    stage = np.zeros(4)
+
+    def subset(sidx, record):
+        r = L.yrtb_range(int(offs[sidx]), 1, int(offs[sidx + 1] - offs[sidx]))
+        if record:
+            marks[0].record()
+        lrem.lr_expand(W, H, out=X)
+        if record:
+            marks[1].record()
+        E.zero_()
+        L.check(lib.yrtb_em_step(proj.h, X.data_ptr(), E.data_ptr(), ctypes.byref(evc), r,
+                                 1.0, 1e-35, st))
+        if record:
+            marks[2].record()
+        lrem.lr_contract_w(E, H, out=Wn)
+        if record:
+            marks[3].record()
+        L.check(lib.yrtb_em_update(W.data_ptr(), Wn.data_ptr(), sens_sub.data_ptr(), J, R,
+                                   1, 1.19209e-07, c.data_ptr(), st))
+        if record:
+            marks[4].record()
+
+    def step(record=False):
+        for sidx in range(subsets):
+            subset(sidx, record)
+            if record:
+                torch.cuda.synchronize()
+                for k in range(4):
+                    stage[k] += marks[k].elapsed_time(marks[k + 1])
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        with Timer() as t:
+            step()
+        times.append(t.ms)
+    stage[:] = 0
+    step(record=True)
+    per_subset = stage / subsets
+    ms = float(np.median(times))
+    out = _base("low-rank list-mode EM (W update), rank 8 x 20 frames, C2 scanner "
+                "80x672, 256x256x160 @2mm, 20M TOF events, 4 subsets",
+                "events/s (one EM iteration over all events, low-rank image)",
+                n / (ms * 1e-3), "events/s", args.steps, args.warmup, ms,
+                {"rank": R, "frames": T, "subsets": subsets, "events": n,
+                 "precision": "compensated", "launch": tune["best"],
+                 "l2": "expanded frames 840 MB and rank images 336 MB exceed L2"})
+    peaks = _measured_peaks()
+    # expand: read R, write T images; contract: read T, write R images.
+    bytes_expand = 4.0 * J * (R + T)
+    bytes_contract = 4.0 * J * (T + R)
+    out["stages_ms_per_subset"] = {"expand": per_subset[0], "em_pass": per_subset[1],
+                                   "contract_w": per_subset[2], "update": per_subset[3]}
+    out["roofline"] = {"bound": "hbm",
+                       "achieved": bytes_expand / (per_subset[0] * 1e-3) / 1e9,
+                       "peak": peaks, "unit": "GB/s",
+                       "frac": bytes_expand / (per_subset[0] * 1e-3) / 1e9 / peaks,
+                       "traffic": None,
+                       "note": "yrtb_lr_expand: 4 (R + T) B per voxel; contract_w "
+                               "achieves %.0f GB/s" % (bytes_contract /
+                                                        (per_subset[2] * 1e-3) / 1e9)}
+    po = _po()
+    if po.ref_available():
+        m = 200_000
+        d1 = ev.d1[:m].cpu().numpy().astype(np.uint32)
+        d2 = ev.d2[:m].cpu().numpy().astype(np.uint32)
+        tof = ev.tof[:m].cpu().numpy()
+        ts = np.arange(m, dtype=np.uint32)
+        fts = np.linspace(0, m, T + 1).astype(np.uint32)
+        t0 = time.perf_counter()
+        po.ref_lrem_listmode(_po_scanner(po, sc), _po_image(po, ip1, nt=R),
+                             sens.cpu().numpy(), d1, d2, ts, fts,
+                             H.cpu().numpy(), tof=tof, iterations=1, subsets=1,
+                             tof_fwhm_ps=214.0, tof_n_std=5,
+                             threads=os.cpu_count() or 1)
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": m / sec, "unit": "events/s",
+                               "cores": os.cpu_count() or 1, "kind": "reference",
+                               "sample": "200k events of the workload, 1 iteration, "
+                                         "1 subset, LREM_CPU (wall time incl. set-up)"}
+    return out
+
+
 def _measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -496,4 +623,4 @@ def _measured_peaks():
 
 
 RUNNERS = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5,
-           "psf": run_psf}
+           "psf": run_psf, "lrem": run_lrem}

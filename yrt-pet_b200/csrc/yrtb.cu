@@ -1366,38 +1366,41 @@ __global__ void k_pairs(H3Dev H, const uint64_t* __restrict__ bins, uint64_t n,
 }
 
 // ---------------------------------------------------- image-space ops ----
+// One thread per voxel of a frame, frames in an inner loop: the broadcast
+// sensitivity value is read once per voxel and no index is divided.
 __global__ void k_em_update(float* __restrict__ x, const float* __restrict__ u,
                             const float* __restrict__ s, uint64_t J, int64_t nt,
                             int64_t sens_nt, float thr,
                             const float* __restrict__ scale)
 {
-	const uint64_t total = J * static_cast<uint64_t>(nt);
 	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-	     i < total; i += nthreads)
+	const bool perFrameSens = !scale && sens_nt == nt && nt > 1;
+	for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < J;
+	     j += nthreads)
 	{
-		const uint64_t j = i % J;
-		const uint64_t r = i / J;
-		if (!scale && sens_nt == nt && nt > 1)
+		const float s0 = __ldg(s + j);
+		for (int64_t r = 0; r < nt; r++)
 		{
-			const float sv = __ldg(s + i);
-			if (sv > thr)
-				x[i] *= __ldg(u + i) / sv;
-		}
-		else if (!scale && nt == 1)
-		{
-			const float sv = __ldg(s + j);
-			if (sv > thr)
-				x[i] *= __ldg(u + i) / sv;
-		}
-		else
-		{
-			// updateEMThresholdDynamicWithScaling (Image.cpp:760-800).
-			const float inv_c = scale ? 1.0f / __ldg(scale + r) : 1.0f;
-			const float thr_r = thr * inv_c;
-			const float sv = __ldg(s + j);
-			if (sv > thr_r)
-				x[i] *= (__ldg(u + i) * inv_c) / sv;
+			const uint64_t i = static_cast<uint64_t>(r) * J + j;
+			if (perFrameSens)
+			{
+				const float sv = __ldg(s + i);
+				if (sv > thr)
+					x[i] *= __ldg(u + i) / sv;
+			}
+			else if (!scale)
+			{
+				if (s0 > thr)
+					x[i] *= __ldg(u + i) / s0;
+			}
+			else
+			{
+				// updateEMThresholdDynamicWithScaling (Image.cpp:760-800).
+				const float inv_c = 1.0f / __ldg(scale + r);
+				const float thr_r = thr * inv_c;
+				if (s0 > thr_r)
+					x[i] *= (__ldg(u + i) * inv_c) / s0;
+			}
 		}
 	}
 }
@@ -1681,6 +1684,71 @@ k_lr_contract_w(const float* __restrict__ E, const float* __restrict__ H, int R,
 		for (int l = 0; l < RMAX; l++)
 			if (l < R)
 				Wn[l * J + j] = acc[l];
+	}
+}
+
+// Vector forms of k_lr_expand / k_lr_contract_w for images of a multiple of 4
+// voxels (16-byte aligned, rank <= 16): 4 consecutive voxels per thread with
+// 16-byte loads and stores, the same products and sums per voxel.
+__device__ __forceinline__ float4 lrMulAdd4(float4 acc, float4 v, float h)
+{
+	acc.x = __fadd_rn(acc.x, __fmul_rn(v.x, h));
+	acc.y = __fadd_rn(acc.y, __fmul_rn(v.y, h));
+	acc.z = __fadd_rn(acc.z, __fmul_rn(v.z, h));
+	acc.w = __fadd_rn(acc.w, __fmul_rn(v.w, h));
+	return acc;
+}
+
+template <int RMAX>
+__global__ void __launch_bounds__(kBlock)
+k_lr_expand4(const float4* __restrict__ W, const float* __restrict__ H, int R, int T,
+             uint64_t J4, float4* __restrict__ X)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < J4;
+	     j += nthreads)
+	{
+		float4 w[RMAX];
+#pragma unroll
+		for (int l = 0; l < RMAX; l++)
+			w[l] = l < R ? __ldg(W + l * J4 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+		for (int t = 0; t < T; t++)
+		{
+			float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+			for (int l = 0; l < RMAX; l++)
+				if (l < R)
+					x = lrMulAdd4(x, w[l], __ldg(H + l * T + t));
+			X[static_cast<uint64_t>(t) * J4 + j] = x;
+		}
+	}
+}
+
+template <int RMAX>
+__global__ void __launch_bounds__(kBlock)
+k_lr_contract_w4(const float4* __restrict__ E, const float* __restrict__ H, int R, int T,
+                 uint64_t J4, float4* __restrict__ Wn)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < J4;
+	     j += nthreads)
+	{
+		float4 acc[RMAX];
+#pragma unroll
+		for (int l = 0; l < RMAX; l++)
+			acc[l] = make_float4(0.f, 0.f, 0.f, 0.f);
+		for (int t = 0; t < T; t++)
+		{
+			const float4 e = __ldg(E + static_cast<uint64_t>(t) * J4 + j);
+#pragma unroll
+			for (int l = 0; l < RMAX; l++)
+				if (l < R)
+					acc[l] = lrMulAdd4(acc[l], e, __ldg(H + l * T + t));
+		}
+#pragma unroll
+		for (int l = 0; l < RMAX; l++)
+			if (l < R)
+				Wn[l * J4 + j] = acc[l];
 	}
 }
 
@@ -2964,7 +3032,7 @@ yrtb_status yrtb_em_update(float* x, const float* u, const float* s,
 {
 	if (!x || !u || !s || J == 0 || nt <= 0 || (sens_nt != 1 && sens_nt != nt))
 		return fail(YRTB_ERR_ARGUMENT, "invalid EM update arguments");
-	k_em_update<<<gridFor(J * nt, 16), kBlock, 0,
+	k_em_update<<<gridFor(J, 16), kBlock, 0,
 	              reinterpret_cast<cudaStream_t>(stream)>>>(x, u, s, J, nt, sens_nt,
 	                                                        thr, scale);
 	YRTB_LAUNCHED();
@@ -3093,6 +3161,13 @@ yrtb_status yrtb_psf_apply(const yrtb_psf* p, const float* d_in, float* d_out,
 			KERNEL<32><<<grid_, kBlock, 0, st>>>(__VA_ARGS__);                             \
 	} while (0)
 
+// Vector form: rank <= 16, images of a multiple of 4 voxels, 16-byte aligned.
+static bool lrVec(int R, uint64_t J, const void* a, const void* b)
+{
+	return R <= 16 && J % 4 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0 &&
+	       (reinterpret_cast<uintptr_t>(b) & 15) == 0;
+}
+
 static yrtb_status lrCheck(int R, int T, uint64_t J)
 {
 	if (R <= 0 || R > kLrMaxRank)
@@ -3111,7 +3186,21 @@ yrtb_status yrtb_lr_expand(const float* d_W, const float* d_H, int R, int T, uin
 	if (s != YRTB_OK)
 		return s;
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-	YRTB_LR_LAUNCH(k_lr_expand, d_W, d_H, R, T, J, d_X);
+	if (lrVec(R, J, d_W, d_X))
+	{
+		const uint64_t J4 = J / 4;
+		const unsigned grid_ = gridFor(J4, 8);
+		auto W4 = reinterpret_cast<const float4*>(d_W);
+		auto X4 = reinterpret_cast<float4*>(d_X);
+		if (R <= 4)
+			k_lr_expand4<4><<<grid_, kBlock, 0, st>>>(W4, d_H, R, T, J4, X4);
+		else if (R <= 8)
+			k_lr_expand4<8><<<grid_, kBlock, 0, st>>>(W4, d_H, R, T, J4, X4);
+		else
+			k_lr_expand4<16><<<grid_, kBlock, 0, st>>>(W4, d_H, R, T, J4, X4);
+	}
+	else
+		YRTB_LR_LAUNCH(k_lr_expand, d_W, d_H, R, T, J, d_X);
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
@@ -3125,7 +3214,21 @@ yrtb_status yrtb_lr_contract_w(const float* d_E, const float* d_H, int R, int T,
 	if (s != YRTB_OK)
 		return s;
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-	YRTB_LR_LAUNCH(k_lr_contract_w, d_E, d_H, R, T, J, d_Wn);
+	if (lrVec(R, J, d_E, d_Wn))
+	{
+		const uint64_t J4 = J / 4;
+		const unsigned grid_ = gridFor(J4, 8);
+		auto E4 = reinterpret_cast<const float4*>(d_E);
+		auto Wn4 = reinterpret_cast<float4*>(d_Wn);
+		if (R <= 4)
+			k_lr_contract_w4<4><<<grid_, kBlock, 0, st>>>(E4, d_H, R, T, J4, Wn4);
+		else if (R <= 8)
+			k_lr_contract_w4<8><<<grid_, kBlock, 0, st>>>(E4, d_H, R, T, J4, Wn4);
+		else
+			k_lr_contract_w4<16><<<grid_, kBlock, 0, st>>>(E4, d_H, R, T, J4, Wn4);
+	}
+	else
+		YRTB_LR_LAUNCH(k_lr_contract_w, d_E, d_H, R, T, J, d_Wn);
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
