@@ -442,6 +442,43 @@ yrtb_status yrtb_psf_apply(const yrtb_psf* psf, const float* d_in, float* d_out,
                            const yrtb_image_params* image, int adjoint,
                            float* d_tmp, yrtb_stream stream);
 
+/* -------------------------------------- spatially variant image PSF --- */
+/* OperatorVarPsf / OperatorVarPsfDevice
+ * (include/yrt-pet/operators/OperatorVarPsf.hpp:66-100,
+ * src/operators/OperatorVarPsf.cpp:290-455): voxel (i, j, k) is blurred by
+ * its own 3-D kernel, the LUT entry nearest to the voxel centre's distance
+ * from the image centre: index (a, b, c) = round(|d| / gap) per axis, clamped
+ * to floor(range / gap), LUT index a + A (b + B c). */
+typedef struct yrtb_varpsf yrtb_varpsf;
+
+/* One Gaussian (columns = 3: sigma x, y, z) or two-Gaussian mixture
+ * (columns = 7: sigma1 x y z, sigma2 x y z, weight2) kernel of the LUT
+ * (ConvolutionKernelGaussian / ConvolutionKernelGaussianMixture): half sizes
+ * max(1, floor(sigma_max nstd / v) - 1), weights z-major, then y, then x.
+ * Writes the half sizes (x, y, z) and the weight count; weights only when
+ * out != NULL (cap floats). Host-side, no device work. */
+yrtb_status yrtb_varpsf_gaussian_kernel(const float* sigmas, int columns, const float* nstd,
+                                        const yrtb_image_params* image, float* out,
+                                        uint64_t cap, int32_t* half_sizes, uint64_t* size);
+
+/* Kernel LUT: num_kernels kernels back to back in weights (kernel i:
+ * (2hz+1)(2hy+1)(2hx+1) floats, z-major), half_sizes 3 per kernel (x, y, z);
+ * range / gap: 3 floats (x, y, z) as OperatorVarPsf::setRangeAndGap. */
+yrtb_status yrtb_varpsf_create(const float* weights, const int32_t* half_sizes,
+                               int num_kernels, const float* range, const float* gap,
+                               yrtb_varpsf** out);
+void yrtb_varpsf_destroy(yrtb_varpsf* psf);
+
+/* d_out = A d_in (adjoint = 0: each output voxel sums its own kernel over
+ * the input, FP32 in the reference's z, y, x tap order, bit-identical) or
+ * A^H d_in (adjoint = 1: each input voxel's kernel spread to its
+ * neighbours, gathered per output voxel without atomics), circular borders,
+ * every frame.  d_out is overwritten (the reference accumulates into an
+ * output it zeroes first).  d_in != d_out. */
+yrtb_status yrtb_varpsf_apply(const yrtb_varpsf* psf, const float* d_in, float* d_out,
+                              const yrtb_image_params* image, int adjoint,
+                              yrtb_stream stream);
+
 /* ------------------------------------------- low-rank dynamic images --- */
 /* Low-rank image model of the LR updater (ProjectorUpdaterLR,
  * src/operators/ProjectorUpdater.cpp:228-280; ProjectorUpdaterDeviceLR,
@@ -505,6 +542,8 @@ typedef struct
 	                         (OSEM_GPU::computeEMUpdateImage, src/recon/OSEM_GPU.cu:456-509);
 	                         d_sens must already include PSF^H, as
 	                         OSEM::generateSensitivityImages makes it */
+	const yrtb_varpsf* varpsf; /* spatially variant image-space PSF or NULL (used
+	                              like psf; at most one of the two) */
 } yrtb_osem_params;
 
 yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,

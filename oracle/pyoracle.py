@@ -64,7 +64,7 @@ class OsemDesc(ctypes.Structure):
                 ("iterations", ctypes.c_int), ("subsets", ctypes.c_int),
                 ("threads", ctypes.c_int), ("global_scale", ctypes.c_float),
                 ("hard_threshold", ctypes.c_float), ("listmode", ctypes.c_int),
-                ("image_psf_csv", ctypes.c_char_p)]
+                ("image_psf_csv", ctypes.c_char_p), ("image_psf_variant", ctypes.c_int)]
 
 
 @dataclass
@@ -481,11 +481,13 @@ def ref_lm_to_histo3d(sc: Scanner, d1, d2, threads=8):
 
 def _osem_desc(projector="S", num_rays=1, tof_fwhm_ps=0.0, tof_n_std=0,
                iterations=1, subsets=1, threads=8, global_scale=1.0,
-               hard_threshold=1.0, listmode=True, image_psf_csv=None):
+               hard_threshold=1.0, listmode=True, image_psf_csv=None,
+               image_psf_variant=False):
     return OsemDesc(0 if projector == "S" else 1, num_rays, tof_fwhm_ps,
                     tof_n_std, iterations, subsets, threads, global_scale,
                     hard_threshold, int(listmode),
-                    None if image_psf_csv is None else image_psf_csv.encode())
+                    None if image_psf_csv is None else image_psf_csv.encode(),
+                    int(bool(image_psf_variant)))
 
 
 def ref_sensitivity(sc: Scanner, ip: ImageParams, *, sens_histo=None,
@@ -707,3 +709,76 @@ def ref_lrem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, timestamps,
             ctypes.c_int(int(update_h)), _p(ini), _p(out), ctypes.byref(sec))
     _ref_check(rc)
     return out, Hc, sec.value
+
+
+# -------------------------------------------- spatially variant image PSF --
+def ref_varpsf_gaussian_kernel(sigmas, nstd, ip: ImageParams):
+    """The reference's ConvolutionKernelGaussian (3 sigmas) or
+    ConvolutionKernelGaussianMixture (7 values): (weights (z, y, x), half
+    sizes (x, y, z))."""
+    sig = np.ascontiguousarray(sigmas, np.float32)
+    ns = np.ascontiguousarray(nstd, np.float32)
+    half = np.zeros(3, np.int32)
+    size = ctypes.c_uint64()
+    cap = 1 << 20
+    out = np.zeros(cap, np.float32)
+    rc = ref_lib().ref_varpsf_gaussian_kernel(
+        _p(sig), ctypes.c_int(len(sig)), _p(ns), ctypes.byref(ip.desc()), _p(out),
+        ctypes.c_uint64(cap), _p(half), ctypes.byref(size))
+    _ref_check(rc)
+    hx, hy, hz = (int(v) for v in half)
+    return out[:size.value].reshape(2 * hz + 1, 2 * hy + 1, 2 * hx + 1).copy(), (hx, hy, hz)
+
+
+def ref_varpsf_apply(ip: ImageParams, csv: str, image, adjoint=False, threads=8):
+    """OperatorVarPsf(csv, params).applyA / applyAH (output zeroed first)."""
+    img = np.ascontiguousarray(image, np.float32)
+    out = np.zeros(img.shape, np.float32)
+    with quiet():
+        rc = ref_lib().ref_varpsf_apply(ctypes.byref(ip.desc()), csv.encode(), _p(img),
+                                        _p(out), ctypes.c_int(int(adjoint)),
+                                        ctypes.c_int(threads))
+    _ref_check(rc)
+    return out
+
+
+def varpsf_apply_f64(ip: ImageParams, image, kernels, half_sizes, rng_gap, adjoint=False):
+    """FP64 restatement of OperatorVarPsf::varconvolve (one frame): kernels[i]
+    (z, y, x) with half sizes (x, y, z); rng_gap = (range x y z, gap x y z).
+    Pure-Python loops over the voxels: small images only."""
+    img = np.asarray(image, np.float64).reshape(ip.nz, ip.ny, ip.nx)
+    nx, ny, nz = ip.nx, ip.ny, ip.nz
+    f32 = np.float32
+    vx = f32(f32(ip.length_x) / f32(nx))
+    vy = f32(f32(ip.length_y) / f32(ny))
+    vz = f32(f32(ip.length_z) / f32(nz))
+    cx, cy, cz = (f32(f32(n) * v / f32(2)) for n, v in ((nx, vx), (ny, vy), (nz, vz)))
+    rx, ry, rz, gx, gy, gz = (f32(v) for v in rng_gap)
+    dims = [int(np.floor(f32(r / g))) + 1 for r, g in ((rx, gx), (ry, gy), (rz, gz))]
+
+    def lut(i, j, k):
+        t = [f32(abs((i + 0.5) * float(vx) - float(cx))),
+             f32(abs((j + 0.5) * float(vy) - float(cy))),
+             f32(abs((k + 0.5) * float(vz) - float(cz)))]
+        idx = []
+        for a, (tv, g) in enumerate(zip(t, (gx, gy, gz))):
+            q = f32(tv / g)
+            r = int(np.floor(float(q) + 0.5))  # round half away from zero (q >= 0)
+            idx.append(min(r, dims[a] - 1))
+        return idx[0] + dims[0] * (idx[1] + dims[1] * idx[2])
+
+    out = np.zeros_like(img)
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                ki = lut(i, j, k)
+                w = np.asarray(kernels[ki], np.float64)
+                hx, hy, hz = half_sizes[ki]
+                zz = (k + np.arange(-hz, hz + 1)) % nz
+                yy = (j + np.arange(-hy, hy + 1)) % ny
+                xx = (i + np.arange(-hx, hx + 1)) % nx
+                if not adjoint:
+                    out[k, j, i] = np.sum(img[np.ix_(zz, yy, xx)] * w)
+                else:
+                    out[np.ix_(zz, yy, xx)] += img[k, j, i] * w
+    return out

@@ -26,6 +26,7 @@
 #include "yrt-pet/datastruct/projection/UniformHistogram.hpp"
 #include "yrt-pet/datastruct/scanner/Scanner.hpp"
 #include "yrt-pet/operators/OperatorPsf.hpp"
+#include "yrt-pet/operators/OperatorVarPsf.hpp"
 #include "yrt-pet/operators/ProjectionPsfManager.hpp"
 #include "yrt-pet/operators/ProjectorDD.hpp"
 #include "yrt-pet/operators/ProjectorParams.hpp"
@@ -489,6 +490,7 @@ struct ref_osem_desc
 	float hard_threshold;
 	int listmode;  // 1: list-mode events, 0: histogram input
 	const char* image_psf_csv;  // image-space PSF (OSEM::addImagePSF), or NULL
+	int image_psf_variant;      // 1: the CSV is a spatially variant PSF LUT
 };
 
 // Sensitivity image (reference OSEM::generateSensitivityImages).  sens_histo
@@ -517,7 +519,9 @@ int ref_sensitivity(const ref_scanner_desc* s, const ref_image_desc* d,
 		    if (psf_csv && psf_csv[0])
 			    osem->addProjPSF(psf_csv);
 		    if (o->image_psf_csv && o->image_psf_csv[0])
-			    osem->addImagePSF(o->image_psf_csv);
+			    osem->addImagePSF(o->image_psf_csv, o->image_psf_variant ?
+			                                          ImagePSFMode::VARIANT :
+			                                          ImagePSFMode::UNIFORM);
 		    osem->setGlobalScalingFactor(o->global_scale);
 		    std::unique_ptr<Histogram3DOwned> sh;
 		    if (sens_histo)
@@ -621,7 +625,9 @@ int ref_osem_listmode_ex(const ref_scanner_desc* s, const ref_image_desc* d,
 		    if (o->tof_fwhm_ps > 0)
 			    osem->addTOF(o->tof_fwhm_ps, o->tof_n_std);
 		    if (o->image_psf_csv && o->image_psf_csv[0])
-			    osem->addImagePSF(o->image_psf_csv);
+			    osem->addImagePSF(o->image_psf_csv, o->image_psf_variant ?
+			                                          ImagePSFMode::VARIANT :
+			                                          ImagePSFMode::UNIFORM);
 		    osem->setGlobalScalingFactor(o->global_scale);
 		    std::unique_ptr<Histogram3DOwned> sh;
 		    if (sens_histo)
@@ -692,7 +698,9 @@ int ref_osem_histo3d(const ref_scanner_desc* s, const ref_image_desc* d,
 		    if (psf_csv && psf_csv[0])
 			    osem->addProjPSF(psf_csv);
 		    if (o->image_psf_csv && o->image_psf_csv[0])
-			    osem->addImagePSF(o->image_psf_csv);
+			    osem->addImagePSF(o->image_psf_csv, o->image_psf_variant ?
+			                                          ImagePSFMode::VARIANT :
+			                                          ImagePSFMode::UNIFORM);
 		    if (o->tof_fwhm_ps > 0)
 			    osem->addTOF(o->tof_fwhm_ps, o->tof_n_std);
 		    const size_t nv = d->nx * d->ny * d->nz;
@@ -825,6 +833,54 @@ int ref_lrem_listmode(const ref_scanner_desc* s, const ref_image_desc* d,
 		    const ImageParams& rp = res->getParams();
 		    const size_t nv = rp.nx * rp.ny * rp.nz * rp.nt;
 		    std::memcpy(out, res->getRawPointer(), nv * sizeof(float));
+	    });
+}
+
+// One kernel of the variant PSF LUT (ConvolutionKernelGaussian for
+// columns = 3, ConvolutionKernelGaussianMixture for columns = 7).
+int ref_varpsf_gaussian_kernel(const float* sig, int columns, const float* nstd,
+                               const ref_image_desc* d, float* out, uint64_t cap,
+                               int32_t* half_sizes, uint64_t* size)
+{
+	return guarded(
+	    [&]
+	    {
+		    const ImageParams ip = makeParams(d);
+		    std::unique_ptr<ConvolutionKernel> k;
+		    if (columns == 7)
+			    k = std::make_unique<ConvolutionKernelGaussianMixture>(
+			        sig[0], sig[1], sig[2], sig[3], sig[4], sig[5], sig[6], nstd[0],
+			        nstd[1], nstd[2], ip);
+		    else
+			    k = std::make_unique<ConvolutionKernelGaussian>(
+			        sig[0], sig[1], sig[2], nstd[0], nstd[1], nstd[2], ip);
+		    half_sizes[0] = static_cast<int32_t>(k->getHalfSizeX());
+		    half_sizes[1] = static_cast<int32_t>(k->getHalfSizeY());
+		    half_sizes[2] = static_cast<int32_t>(k->getHalfSizeZ());
+		    const auto& a = k->getArray();
+		    *size = a.getSizeTotal();
+		    for (size_t i = 0; i < a.getSizeTotal() && i < cap; i++)
+			    out[i] = a.getFlat(i);
+	    });
+}
+
+// OperatorVarPsf(csv, params).applyA / applyAH into a zeroed output.
+int ref_varpsf_apply(const ref_image_desc* d, const char* csv, const float* in, float* out,
+                     int adjoint, int threads)
+{
+	return guarded(
+	    [&]
+	    {
+		    globals::setNumThreads(threads);
+		    auto src = makeImage(d, in);
+		    auto dst = makeImage(d, nullptr);
+		    OperatorVarPsf op(csv, makeParams(d));
+		    if (adjoint)
+			    op.applyAH(src.get(), dst.get());
+		    else
+			    op.applyA(src.get(), dst.get());
+		    const size_t nv = d->nx * d->ny * d->nz * d->nt;
+		    std::memcpy(out, dst->getRawPointer(), nv * sizeof(float));
 	    });
 }
 

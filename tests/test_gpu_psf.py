@@ -231,3 +231,80 @@ def test_image_psf_graph_and_plain_agree(tmp_path):
         outs.append(osem.reconstruct().cpu().numpy())
     # Same launches in both; only the arrival order of float atomics differs.
     assert rel_l2(outs[1], outs[0]) < 1e-5
+
+
+# ------------------------------------------- spatially variant image PSF --
+def _varpsf_csv(path, two_gaussian, seed):
+    """LUT of the reference's VarPSF unit test: 5 x 5 x 5 kernels over range
+    200 mm, gap 50 mm, 4 sigmas, sigmas switching at 100 mm
+    (unit_tests/operators/test_PSF.cpp:290-360)."""
+    rng = np.random.default_rng(seed)
+    s1lo, s1hi = rng.uniform(0.5, 1.0, 3), rng.uniform(1.1, 1.5, 3)
+    s2lo, s2hi = rng.uniform(1.6, 2.0, 3), rng.uniform(2.1, 2.5, 3)
+    w2 = rng.uniform(0.2, 0.6)
+    vals = [5.1, 54.9, 105.3, 155.1, 205.5]
+    rows = []
+    for z in vals:
+        for y in vals:
+            for x in vals:
+                pos = (x, y, z)
+                s1 = [s1hi[a] if pos[a] > 100 else s1lo[a] for a in range(3)]
+                s2 = [s2hi[a] if pos[a] > 100 else s2lo[a] for a in range(3)]
+                rows.append(s1 + s2 + [w2] if two_gaussian else s1)
+    with open(path, "w") as f:
+        f.write("200,200,200\n50,50,50\n4,4,4\n")
+        for r in rows:
+            f.write(",".join(f"{float(v):.9g}" for v in r) + "\n")
+    return path
+
+
+@needs_ref
+@pytest.mark.parametrize("two_gaussian", [False, True])
+def test_varpsf_vs_reference_operator(tmp_path, two_gaussian):
+    ip = yrt.ImageParams(100, 100, 51, 400.0, 401.0, 421.0)
+    oip = po.ImageParams(100, 100, 51, 400.0, 401.0, 421.0)
+    csv = _varpsf_csv(str(tmp_path / "v.csv"), two_gaussian, 95)
+    rng = np.random.default_rng(96)
+    img = rng.random((51, 100, 100), dtype=np.float32)
+    op = yrt.OperatorVarPsfDevice(csv, ip)
+    d_in = torch.from_numpy(img).cuda()
+    fwd = op.applyA(d_in, torch.empty_like(d_in)).cpu().numpy()
+    ref = po.ref_varpsf_apply(oip, csv, img)
+    assert np.array_equal(bits(fwd), bits(ref))
+    adj = op.applyAH(d_in, torch.empty_like(d_in)).cpu().numpy()
+    ref_adj = po.ref_varpsf_apply(oip, csv, img, adjoint=True)
+    assert rel_l2(adj, ref_adj) < 1e-6
+    y = torch.from_numpy(rng.random((51, 100, 100), dtype=np.float32)).cuda()
+    lhs = float((torch.from_numpy(fwd).cuda().double() * y.double()).sum())
+    rhs = float((d_in.double() * op.applyAH(y, torch.empty_like(y)).double()).sum())
+    assert abs(lhs - rhs) / abs(rhs) < 1e-6
+
+
+@needs_ref
+def test_listmode_osem_with_variant_psf_vs_reference(tmp_path):
+    sc, ip, e = _c1_events(60000, 97)
+    rng = np.random.default_rng(98)
+    csv = str(tmp_path / "v.csv")
+    with open(csv, "w") as f:
+        f.write("60,60,30\n30,30,30\n3,3,3\n")
+        for _ in range(3 * 3 * 2):
+            f.write(",".join(f"{v:.6g}" for v in rng.uniform(6.0, 12.0, 3)) + "\n")
+    osem = yrt.createOSEM(sc)
+    osem.setImageParams(ip)
+    osem.num_MLEM_iterations = 2
+    osem.num_OSEM_subsets = 2
+    osem.setListModeEnabled(True)
+    osem.addImagePSF(csv, "VARIANT")
+    sens = osem.generateSensitivityImages()
+    osc = po.Scanner(*SC_ARGS)
+    oip = po.ImageParams(32, 32, 16, 256, 256, 128)
+    rs, _ = po.ref_sensitivity(osc, oip, listmode=True, image_psf_csv=csv,
+                               image_psf_variant=True)
+    assert rel_l2(sens[0].cpu().numpy(), rs[0]) < 1e-5
+    lm = yrt.ListModeLUT(sc)
+    lm.bind(e["d1"], e["d2"])
+    osem.setDataInput(lm)
+    img = osem.reconstruct().cpu().numpy()
+    ref, _ = po.ref_osem_listmode(osc, oip, rs[0], e["d1"], e["d2"], iterations=2,
+                                  subsets=2, image_psf_csv=csv, image_psf_variant=True)
+    assert rel_l2(img, ref) < 1e-4

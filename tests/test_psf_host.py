@@ -47,3 +47,49 @@ def test_image_psf_csv_layout(tmp_path):
     assert len(rows) == 4
     assert [int(v) for v in rows[3]] == [3, 5, 1]
     assert np.array_equal(np.array(rows[1], np.float32), ky)
+
+
+# ------------------------------------------- spatially variant image PSF --
+def _varpsf_csv(path, rows, rng_gap_nstd):
+    with open(path, "w") as f:
+        for r in rng_gap_nstd + rows:
+            f.write(",".join(f"{float(v):.9g}" for v in r) + "\n")
+
+
+@needs_ref
+@pytest.mark.parametrize("values", [[1.3, 0.8, 2.1], [0.7, 0.9, 1.2, 1.9, 2.2, 2.4, 0.35]])
+def test_varpsf_gaussian_kernels_bitexact_vs_reference(values):
+    from pyyrtpet_b200.core import ImageParams
+    from pyyrtpet_b200.psf import _gaussian_kernel
+    ip = ImageParams(40, 36, 20, 80.0, 75.6, 50.0)
+    oip = po.ImageParams(40, 36, 20, 80.0, 75.6, 50.0)
+    nstd = [4.0, 3.5, 4.0]
+    mine = _gaussian_kernel(values, nstd, ip)
+    ref, half = po.ref_varpsf_gaussian_kernel(values, nstd, oip)
+    assert mine.half_sizes == half
+    assert np.array_equal(mine.weights.view(np.uint32), ref.view(np.uint32))
+
+
+@needs_ref
+@pytest.mark.parametrize("gap", [4.0, 4.5])
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_varpsf_fp64_restatement_vs_reference(tmp_path, gap, adjoint):
+    """The FP64 restatement of varconvolve (kernel choice by nearest LUT
+    entry, circular borders) against the reference operator."""
+    from pyyrtpet_b200.core import ImageParams
+    from pyyrtpet_b200.psf import _gaussian_kernel
+    nx, ny, nz = 14, 12, 9
+    ip = ImageParams(nx, ny, nz, 14.0, 13.2, 11.7)
+    oip = po.ImageParams(nx, ny, nz, 14.0, 13.2, 11.7)
+    rng = np.random.default_rng(91)
+    rg = [[7.0, 7.0, 6.0], [gap, gap, gap], [3.0, 3.0, 3.0]]
+    dims = [int(np.floor(np.float32(r) / np.float32(gap))) + 1 for r in rg[0]]
+    rows = [list(rng.uniform(0.4, 1.2, 3)) for _ in range(dims[0] * dims[1] * dims[2])]
+    csv = str(tmp_path / "var.csv")
+    _varpsf_csv(csv, rows, rg)
+    ks = [_gaussian_kernel(r, rg[2], ip) for r in rows]
+    img = rng.random((nz, ny, nx), dtype=np.float32)
+    ref = po.ref_varpsf_apply(oip, csv, img, adjoint=adjoint, threads=1)
+    mine = po.varpsf_apply_f64(oip, img, [k.weights for k in ks],
+                               [k.half_sizes for k in ks], rg[0] + rg[1], adjoint=adjoint)
+    assert np.linalg.norm(mine - ref) / np.linalg.norm(ref) < 1e-6

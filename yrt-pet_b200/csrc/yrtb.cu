@@ -1617,6 +1617,105 @@ void psfPass(dim3 grid, dim3 block, cudaStream_t st, const float* src, float* ds
 #undef YRTB_PSF_CASE
 }
 
+// ------------------------------------------- spatially variant image PSF --
+// OperatorVarPsf (src/operators/OperatorVarPsf.cpp:290-455): every voxel has
+// its own 3-D kernel, the LUT entry nearest to |voxel centre - image centre|
+// (x, y, z gaps, clamped at the LUT's range).
+struct VarPsfDev
+{
+	const float* w;     // all kernels' weights, z-major, then y, then x
+	const int4* meta;   // per kernel: offset into w, half sizes x, y, z
+	int lutX, lutY, lutZ;
+	float gapX, gapY, gapZ;
+	float vx, vy, vz;
+	float cx, cy, cz;   // image centre: n * v / 2 in FP32
+	int maxHx, maxHy, maxHz;
+};
+
+// LUT entry of voxel (i, j, k) (OperatorVarPsf::findNearestKernel with the
+// distances of varconvolve: |(i + 0.5) v - centre| in FP64, then FP32).
+__device__ __forceinline__ int varPsfKernel(const VarPsfDev& P, int i, int j, int k)
+{
+	const float tx = static_cast<float>(fabs((i + 0.5) * static_cast<double>(P.vx) - P.cx));
+	const float ty = static_cast<float>(fabs((j + 0.5) * static_cast<double>(P.vy) - P.cy));
+	const float tz = static_cast<float>(fabs((k + 0.5) * static_cast<double>(P.vz) - P.cz));
+	int a = static_cast<int>(roundf(fabsf(tx) / P.gapX));
+	int b = static_cast<int>(roundf(fabsf(ty) / P.gapY));
+	int c = static_cast<int>(roundf(fabsf(tz) / P.gapZ));
+	a = a >= P.lutX ? P.lutX - 1 : a;
+	b = b >= P.lutY ? P.lutY - 1 : b;
+	c = c >= P.lutZ ? P.lutZ - 1 : c;
+	return a + P.lutX * (b + P.lutY * c);
+}
+
+__device__ __forceinline__ int circ1(int n, int x)
+{
+	return x < 0 ? x + n : (x >= n ? x - n : x);
+}
+
+// Forward (applyA): out[p] = sum over the kernel of p of in[p + d] w_p(d),
+// d in z, y, x order, FP32 products and sums as the reference's loop.
+// Adjoint (applyAH): the reference scatters in[q] w_q(d) to q + d; here each
+// output gathers out[p] = sum_d in[p - d] w_{p-d}(d) over the largest kernel
+// support (no atomics; the FP32 sum order differs from the scatter's).
+template <bool ADJ>
+__global__ void __launch_bounds__(kPsfBX * kPsfBY)
+k_varpsf(const float* __restrict__ src, float* __restrict__ dst, int nx, int ny, int nz,
+         int planes, VarPsfDev P)
+{
+	const int x = blockIdx.x * kPsfBX + threadIdx.x;
+	const int y = blockIdx.y * kPsfBY + threadIdx.y;
+	if (x >= nx || y >= ny)
+		return;
+	const int64_t plane = static_cast<int64_t>(nx) * ny;
+	for (int zt = blockIdx.z; zt < planes; zt += gridDim.z)
+	{
+		const int z = zt % nz;
+		const float* frame = src + (zt - z) * plane;
+		float sum = 0.f;
+		if (!ADJ)
+		{
+			const int4 m = __ldg(P.meta + varPsfKernel(P, x, y, z));
+			const float* w = P.w + m.x;
+			for (int dz = -m.w; dz <= m.w; dz++)
+			{
+				const float* pz = frame + circ1(nz, z + dz) * plane;
+				for (int dy = -m.z; dy <= m.z; dy++)
+				{
+					const float* py = pz + static_cast<int64_t>(circ1(ny, y + dy)) * nx;
+					for (int dx = -m.y; dx <= m.y; dx++, w++)
+						sum = __fadd_rn(sum, __fmul_rn(__ldg(py + circ1(nx, x + dx)), __ldg(w)));
+				}
+			}
+		}
+		else
+		{
+			for (int dz = -P.maxHz; dz <= P.maxHz; dz++)
+			{
+				const int qz = circ1(nz, z - dz);
+				for (int dy = -P.maxHy; dy <= P.maxHy; dy++)
+				{
+					const int qy = circ1(ny, y - dy);
+					for (int dx = -P.maxHx; dx <= P.maxHx; dx++)
+					{
+						const int qx = circ1(nx, x - dx);
+						const int4 m = __ldg(P.meta + varPsfKernel(P, qx, qy, qz));
+						if (dx < -m.y || dx > m.y || dy < -m.z || dy > m.z || dz < -m.w ||
+						    dz > m.w)
+							continue;
+						const int tap = ((dz + m.w) * (2 * m.z + 1) + (dy + m.z)) * (2 * m.y + 1) +
+						                (dx + m.y);
+						sum = __fadd_rn(sum, __fmul_rn(__ldg(frame + qz * plane +
+						                                     static_cast<int64_t>(qy) * nx + qx),
+						                               __ldg(P.w + m.x + tap)));
+					}
+				}
+			}
+		}
+		dst[static_cast<int64_t>(zt) * plane + static_cast<int64_t>(y) * nx + x] = sum;
+	}
+}
+
 // ------------------------------------------------- low-rank dynamic image --
 // Frame t of a low-rank image is x_t = sum_l H[l][t] W_l (W: rank images, H:
 // rank x frames basis), the ProjectorUpdaterLR / ProjectorUpdaterDeviceLR
@@ -1981,6 +2080,23 @@ struct yrtb_projector
 		cudaFree(d_ring);
 		cudaFree(d_z);
 		cudaFree(d_err);
+	}
+};
+
+// Spatially variant image-space PSF: kernel LUT on the device.
+struct yrtb_varpsf
+{
+	float* w = nullptr;
+	int4* meta = nullptr;
+	int numKernels = 0;
+	int lut[3] = {0, 0, 0};
+	float gap[3] = {0, 0, 0};
+	int maxH[3] = {0, 0, 0};
+	int device = 0;
+	~yrtb_varpsf()
+	{
+		cudaFree(w);
+		cudaFree(meta);
 	}
 };
 
@@ -3277,6 +3393,184 @@ yrtb_status yrtb_lr_update_h(float* d_H, const double* d_Hn, const float* d_cH, 
 	return YRTB_OK;
 }
 
+/* Spatially variant PSF (OperatorVarPsf): kernel construction mirrors
+ * ConvolutionKernelGaussian / ConvolutionKernelGaussianMixture::setSigmas
+ * (src/operators/OperatorVarPsf.cpp:75-240) in FP32 with the host libm. */
+yrtb_status yrtb_varpsf_gaussian_kernel(const float* sig, int columns, const float* nstd,
+                                        const yrtb_image_params* ip, float* out,
+                                        uint64_t cap, int32_t* half_sizes,
+                                        uint64_t* size)
+{
+	if (!sig || !nstd || !validImage(ip) || !half_sizes || !size ||
+	    (columns != 3 && columns != 7))
+		return fail(YRTB_ERR_ARGUMENT, "invalid Gaussian PSF kernel arguments");
+	const float vx = static_cast<float>(ip->length_x / ip->nx);
+	const float vy = static_cast<float>(ip->length_y / ip->ny);
+	const float vz = static_cast<float>(ip->length_z / ip->nz);
+	const bool two = columns == 7;
+	if (!(sig[0] > 0.f && sig[1] > 0.f && sig[2] > 0.f) ||
+	    (two && !(sig[3] > 0.f && sig[4] > 0.f && sig[5] > 0.f)))
+		return fail(YRTB_ERR_ARGUMENT, "Gaussian sigmas must be positive");
+	if (two && !(sig[6] >= 0.f && sig[6] <= 1.f))
+		return fail(YRTB_ERR_ARGUMENT, "Second Gaussian weight must be in [0, 1]");
+	const float sxm = two ? std::max(sig[0], sig[3]) : sig[0];
+	const float sym = two ? std::max(sig[1], sig[4]) : sig[1];
+	const float szm = two ? std::max(sig[2], sig[5]) : sig[2];
+	const int hx = std::max(1, static_cast<int>(std::floor((sxm * nstd[0]) / vx)) - 1);
+	const int hy = std::max(1, static_cast<int>(std::floor((sym * nstd[1]) / vy)) - 1);
+	const int hz = std::max(1, static_cast<int>(std::floor((szm * nstd[2]) / vz)) - 1);
+	half_sizes[0] = hx;
+	half_sizes[1] = hy;
+	half_sizes[2] = hz;
+	const uint64_t n = static_cast<uint64_t>(2 * hx + 1) * (2 * hy + 1) * (2 * hz + 1);
+	*size = n;
+	if (!out)
+		return YRTB_OK;
+	if (cap < n)
+		return fail(YRTB_ERR_ARGUMENT, "Gaussian PSF kernel buffer too small");
+	auto inv2 = [](float s) { return 1.0f / (2 * s * s); };
+	const float ix1 = inv2(sig[0]), iy1 = inv2(sig[1]), iz1 = inv2(sig[2]);
+	std::vector<float> k(n);
+	float sum1 = 0.f, sum2 = 0.f;
+	size_t idx = 0;
+	for (int dz = -hz; dz <= hz; ++dz)
+		for (int dy = -hy; dy <= hy; ++dy)
+			for (int dx = -hx; dx <= hx; ++dx, ++idx)
+			{
+				const float xo = dx * vx, yo = dy * vy, zo = dz * vz;
+				const float e1 = -(xo * xo * ix1 + yo * yo * iy1 + zo * zo * iz1);
+				k[idx] = std::exp(e1);
+				sum1 += k[idx];
+				if (two)
+				{
+					const float e2 = -(xo * xo * inv2(sig[3]) + yo * yo * inv2(sig[4]) +
+					                   zo * zo * inv2(sig[5]));
+					sum2 += std::exp(e2);
+				}
+			}
+	if (!two)
+	{
+		for (uint64_t i = 0; i < n; i++)
+			out[i] = k[i] / sum1;
+		return YRTB_OK;
+	}
+	if (!(sum1 > 0.f && sum2 > 0.f))
+		return fail(YRTB_ERR_ARGUMENT, "2-Gaussian kernel sums must be positive");
+	const float w1 = 1.0f - sig[6];
+	idx = 0;
+	for (int dz = -hz; dz <= hz; ++dz)
+		for (int dy = -hy; dy <= hy; ++dy)
+			for (int dx = -hx; dx <= hx; ++dx, ++idx)
+			{
+				const float xo = dx * vx, yo = dy * vy, zo = dz * vz;
+				const float e2 = -(xo * xo * inv2(sig[3]) + yo * yo * inv2(sig[4]) +
+				                   zo * zo * inv2(sig[5]));
+				out[idx] = w1 * k[idx] / sum1 + sig[6] * std::exp(e2) / sum2;
+				if (!(out[idx] >= 0.f))
+					return fail(YRTB_ERR_ARGUMENT, "2-Gaussian kernel value cannot be negative");
+			}
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_varpsf_create(const float* weights, const int32_t* half_sizes,
+                               int num_kernels, const float* range, const float* gap,
+                               yrtb_varpsf** out)
+{
+	if (!out)
+		return fail(YRTB_ERR_ARGUMENT, "null output handle");
+	*out = nullptr;
+	if (!weights || !half_sizes || num_kernels <= 0 || !range || !gap)
+		return fail(YRTB_ERR_ARGUMENT, "LUT not defined");
+	auto p = std::make_unique<yrtb_varpsf>();
+	for (int a = 0; a < 3; a++)
+	{
+		if (!(gap[a] > 0.f) || !(range[a] >= 0.f))
+			return fail(YRTB_ERR_ARGUMENT, "variant PSF ranges and gaps must be positive");
+		p->gap[a] = gap[a];
+		p->lut[a] = static_cast<int>(std::floor(range[a] / gap[a])) + 1;
+	}
+	if (static_cast<int64_t>(p->lut[0]) * p->lut[1] * p->lut[2] > num_kernels)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "variant PSF LUT has fewer kernels than its ranges and gaps need");
+	std::vector<int4> meta(num_kernels);
+	uint64_t total = 0;
+	for (int i = 0; i < num_kernels; i++)
+	{
+		const int hx = half_sizes[3 * i], hy = half_sizes[3 * i + 1], hz = half_sizes[3 * i + 2];
+		if (hx < 0 || hy < 0 || hz < 0)
+			return fail(YRTB_ERR_ARGUMENT, "negative PSF kernel half size");
+		meta[i] = make_int4(static_cast<int>(total), hx, hy, hz);
+		p->maxH[0] = std::max(p->maxH[0], hx);
+		p->maxH[1] = std::max(p->maxH[1], hy);
+		p->maxH[2] = std::max(p->maxH[2], hz);
+		total += static_cast<uint64_t>(2 * hx + 1) * (2 * hy + 1) * (2 * hz + 1);
+		if (total > static_cast<uint64_t>(INT32_MAX))
+			return fail(YRTB_ERR_ARGUMENT, "variant PSF kernels too large");
+	}
+	p->numKernels = num_kernels;
+	cudaGetDevice(&p->device);
+	YRTB_CUDA(cudaMalloc(&p->w, total * sizeof(float)));
+	YRTB_CUDA(cudaMalloc(&p->meta, num_kernels * sizeof(int4)));
+	YRTB_CUDA(cudaMemcpy(p->w, weights, total * sizeof(float), cudaMemcpyHostToDevice));
+	YRTB_CUDA(cudaMemcpy(p->meta, meta.data(), num_kernels * sizeof(int4),
+	                     cudaMemcpyHostToDevice));
+	*out = p.release();
+	return YRTB_OK;
+}
+
+void yrtb_varpsf_destroy(yrtb_varpsf* p)
+{
+	delete p;
+}
+
+yrtb_status yrtb_varpsf_apply(const yrtb_varpsf* p, const float* d_in, float* d_out,
+                              const yrtb_image_params* ip, int adjoint, yrtb_stream stream)
+{
+	if (!p || !d_in || !d_out || !validImage(ip))
+		return fail(YRTB_ERR_ARGUMENT, "invalid variant PSF arguments");
+	if (d_in == d_out)
+		return fail(YRTB_ERR_ARGUMENT, "PSF input and output must differ");
+	const int dims[3] = {static_cast<int>(ip->nx), static_cast<int>(ip->ny),
+	                     static_cast<int>(ip->nz)};
+	for (int a = 0; a < 3; a++)
+		if (p->maxH[a] >= dims[a])
+			return fail(YRTB_ERR_ARGUMENT,
+			            "PSF kernel half-width must be smaller than the image along each axis");
+	if ((dims[1] + kPsfBY - 1) / kPsfBY > 65535 ||
+	    static_cast<int64_t>(ip->nz) * ip->nt > INT32_MAX)
+		return fail(YRTB_ERR_ARGUMENT, "image too large for the PSF launch");
+	YRTB_CUDA(cudaSetDevice(p->device));
+	VarPsfDev P;
+	P.w = p->w;
+	P.meta = p->meta;
+	P.lutX = p->lut[0];
+	P.lutY = p->lut[1];
+	P.lutZ = p->lut[2];
+	P.gapX = p->gap[0];
+	P.gapY = p->gap[1];
+	P.gapZ = p->gap[2];
+	P.vx = static_cast<float>(ip->length_x / ip->nx);
+	P.vy = static_cast<float>(ip->length_y / ip->ny);
+	P.vz = static_cast<float>(ip->length_z / ip->nz);
+	P.cx = ip->nx * P.vx / 2.0f;
+	P.cy = ip->ny * P.vy / 2.0f;
+	P.cz = ip->nz * P.vz / 2.0f;
+	P.maxHx = p->maxH[0];
+	P.maxHy = p->maxH[1];
+	P.maxHz = p->maxH[2];
+	const int planes = static_cast<int>(ip->nz * ip->nt);
+	const dim3 block(kPsfBX, kPsfBY);
+	const dim3 grid((dims[0] + kPsfBX - 1) / kPsfBX, (dims[1] + kPsfBY - 1) / kPsfBY,
+	                std::min(planes, 65535));
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	if (adjoint)
+		k_varpsf<true><<<grid, block, 0, st>>>(d_in, d_out, dims[0], dims[1], dims[2], planes, P);
+	else
+		k_varpsf<false><<<grid, block, 0, st>>>(d_in, d_out, dims[0], dims[1], dims[2], planes, P);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
 yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
                                const float* d_sens, float* d_image,
                                float* d_work, const yrtb_osem_params* p,
@@ -3330,15 +3624,20 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 				return yrtb_em_update(d_image, em, sens, J, nt, 1, p->em_threshold,
 				                      p->d_frame_scale, stream);
 		}
-		if (p->psf)
+		if (p->psf || p->varpsf)
 		{
 			// OSEM_GPU::computeEMUpdateImage with image PSF
 			// (src/recon/OSEM_GPU.cu:456-509): project PSF(x), back-project
 			// the ratio, apply PSF^H to the EM image.
-			if ((r = yrtb_psf_apply(p->psf, d_image, xpsf, &h->ip, 0, ptmp, stream)) != YRTB_OK ||
+			auto blur = [&](const float* in, float* out, int adj)
+			{
+				return p->psf ? yrtb_psf_apply(p->psf, in, out, &h->ip, adj, ptmp, stream)
+				              : yrtb_varpsf_apply(p->varpsf, in, out, &h->ip, adj, stream);
+			};
+			if ((r = blur(d_image, xpsf, 0)) != YRTB_OK ||
 			    (r = yrtb_em_step(h, xpsf, em, ev, range, p->global_scale,
 			                      p->denom_threshold, stream)) != YRTB_OK ||
-			    (r = yrtb_psf_apply(p->psf, em, xpsf, &h->ip, 1, ptmp, stream)) != YRTB_OK)
+			    (r = blur(em, xpsf, 1)) != YRTB_OK)
 				return r;
 			return yrtb_em_update(d_image, xpsf, sens, J, nt, 1, p->em_threshold,
 			                      p->d_frame_scale, stream);
@@ -3639,7 +3938,7 @@ extern "C" yrtb_status yrtb_osem_listmode_static(yrtb_projector* h,
 		            "(instantiating one allocates); set use_graph = 0");
 	const uint64_t J = static_cast<uint64_t>(h->P.g.nvox);
 	const uint64_t need = J * static_cast<uint64_t>(h->ip.nt) + J +
-	                      (p->psf ? 2 * J * static_cast<uint64_t>(h->ip.nt) : 0);
+	                      ((p->psf || p->varpsf) ? 2 * J * static_cast<uint64_t>(h->ip.nt) : 0);
 	if (need > YRTB_OSEM_STATIC_MAX_FLOATS)
 		return fail(YRTB_ERR_ARGUMENT,
 		            "image too large for yrtb_osem_listmode_static: needs " +

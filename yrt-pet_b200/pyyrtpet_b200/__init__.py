@@ -13,7 +13,9 @@ from .core import (BinIteratorChronologicalInterleaved,  # noqa: F401
                    histo3d_bins, histo3d_detpairs, read_psf_csv,
                    release_cached_memory, write_psf_csv)
 from .osem import OSEM_GPU, createOSEM  # noqa: F401
-from .psf import OperatorPsfDevice, write_image_psf_csv  # noqa: F401
+from .psf import (ConvolutionKernel, ConvolutionKernelGaussian,  # noqa: F401
+                  ConvolutionKernelGaussianMixture, OperatorPsfDevice,
+                  OperatorVarPsfDevice, write_image_psf_csv)
 from .lrem import LREM_GPU, LowRankProjector  # noqa: F401
 
 ListModeLUTOwned = ListModeLUT

@@ -72,7 +72,7 @@ class yrtb_osem_params(ctypes.Structure):
                 ("global_scale", c_f), ("denom_threshold", c_f),
                 ("em_threshold", c_f), ("init_from_image", ctypes.c_int),
                 ("use_graph", ctypes.c_int), ("d_frame_scale", c_vp),
-                ("subset_offsets", c_vp), ("psf", c_vp)]
+                ("subset_offsets", c_vp), ("psf", c_vp), ("varpsf", c_vp)]
 
 
 class yrtb_launch_config(ctypes.Structure):
@@ -154,6 +154,12 @@ SIGNATURES = {
                             c_vp], ctypes.c_int),
     "yrtb_lr_update_h": ([c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, c_vp],
                          ctypes.c_int),
+    "yrtb_varpsf_gaussian_kernel": ([c_vp, ctypes.c_int, c_vp, _P(yrtb_image_params), c_vp,
+                                     ctypes.c_uint64, c_vp, c_vp], ctypes.c_int),
+    "yrtb_varpsf_create": ([c_vp, c_vp, ctypes.c_int, c_vp, c_vp, _P(c_vp)], ctypes.c_int),
+    "yrtb_varpsf_destroy": ([c_vp], None),
+    "yrtb_varpsf_apply": ([c_vp, c_vp, c_vp, _P(yrtb_image_params), ctypes.c_int, c_vp],
+                          ctypes.c_int),
     "yrtb_psf_create": ([c_vp, ctypes.c_int, c_vp, ctypes.c_int, c_vp, ctypes.c_int,
                          _P(c_vp)], ctypes.c_int),
     "yrtb_psf_destroy": ([c_vp], None),

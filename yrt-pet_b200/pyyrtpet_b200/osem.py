@@ -22,7 +22,7 @@ import torch
 from . import _lib as L
 from .core import (DeviceEvents, DeviceProjector, Histogram3D, ImageParams,
                    ListModeLUT, ProjectorParams, Scanner, _dev, _ptr, _stream)
-from .psf import OperatorPsfDevice
+from .psf import OperatorPsfDevice, OperatorVarPsfDevice
 
 
 class OSEM_GPU:
@@ -104,15 +104,22 @@ class OSEM_GPU:
 
     # --------------------------------------------------- image-space PSF --
     # OSEM_GPU::addImagePSF / addUniformGaussianImagePSFFrom{FWHM,Sigma}
-    # (src/recon/OSEM_GPU.cu:48-95).  Spatially invariant (UNIFORM) only.
+    # (src/recon/OSEM_GPU.cu:48-95): UNIFORM (separable, OperatorPsfDevice) or
+    # VARIANT (kernel LUT, OperatorVarPsfDevice; image parameters first).
     def addImagePSF(self, image_psf_fname: str, image_psf_mode: str = "UNIFORM"):
         if not image_psf_fname:
             raise RuntimeError("Empty filename for Image-space PSF")
-        mode = getattr(image_psf_mode, "name", image_psf_mode)
-        if str(mode).upper() != "UNIFORM":
-            raise RuntimeError("Only the spatially invariant (UNIFORM) "
-                               "image-space PSF is supported")
-        self.imagePsf = OperatorPsfDevice(image_psf_fname)
+        mode = str(getattr(image_psf_mode, "name", image_psf_mode)).upper()
+        if mode == "UNIFORM":
+            self.imagePsf = OperatorPsfDevice(image_psf_fname)
+        elif mode == "VARIANT":
+            if self.imageParams is None:
+                raise RuntimeError("For spatially variant PSF, image parameters have "
+                                   "to be set before calling addImagePSF")
+            self.imagePsf = OperatorVarPsfDevice(image_psf_fname,
+                                                 self.imageParams.withFrames(1))
+        else:
+            raise RuntimeError("Unknown image PSF mode")
         self.flagImagePSF = True
 
     def addUniformGaussianImagePSFFromFWHM(self, fwhm_x, fwhm_y, fwhm_z,
@@ -340,7 +347,8 @@ class OSEM_GPU:
                                init, int(self.useGraphs),
                                _ptr(self._frame_scale),
                                None if offsets is None else offsets.ctypes.data,
-                               None if psf is None else psf.handle)
+                               None if not isinstance(psf, OperatorPsfDevice) else psf.handle,
+                               None if not isinstance(psf, OperatorVarPsfDevice) else psf.handle)
         stream = torch.cuda.current_stream()
         use_side = self.useGraphs and stream.cuda_stream == 0
         s = torch.cuda.Stream() if use_side else stream

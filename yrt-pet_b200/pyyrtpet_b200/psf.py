@@ -184,3 +184,160 @@ def write_image_psf_csv(fname: str, kernel_x, kernel_y, kernel_z):
         for k in ks:
             f.write(",".join(f"{float(v):.9g}" for v in k) + "\n")
         f.write(",".join(str(k.size) for k in ks) + "\n")
+
+
+# ------------------------------------------- spatially variant image PSF ---
+class ConvolutionKernel:
+    """One kernel of a variant PSF LUT: weights (2hz+1, 2hy+1, 2hx+1)."""
+
+    def __init__(self, weights, half_sizes=None):
+        w = np.ascontiguousarray(weights, np.float32)
+        if w.ndim != 3 or any(n % 2 == 0 for n in w.shape):
+            raise RuntimeError("kernel must be 3-D with odd sizes")
+        self.weights = w
+        self.half_sizes = (w.shape[2] // 2, w.shape[1] // 2, w.shape[0] // 2)
+
+    def getHalfSizeX(self):
+        return self.half_sizes[0]
+
+    def getHalfSizeY(self):
+        return self.half_sizes[1]
+
+    def getHalfSizeZ(self):
+        return self.half_sizes[2]
+
+    def getArray(self):
+        return self.weights.copy()
+
+
+def _gaussian_kernel(values, nstd, params: ImageParams) -> ConvolutionKernel:
+    sig = np.ascontiguousarray(values, np.float32)
+    ns = np.ascontiguousarray(nstd, np.float32)
+    half = np.zeros(3, np.int32)
+    size = ctypes.c_uint64()
+    ip = params._c()
+    L.check(L.lib().yrtb_varpsf_gaussian_kernel(sig.ctypes.data, len(sig), ns.ctypes.data,
+                                                ctypes.byref(ip), None, 0, half.ctypes.data,
+                                                ctypes.byref(size)))
+    out = np.zeros(size.value, np.float32)
+    L.check(L.lib().yrtb_varpsf_gaussian_kernel(sig.ctypes.data, len(sig), ns.ctypes.data,
+                                                ctypes.byref(ip), out.ctypes.data, out.size,
+                                                half.ctypes.data, ctypes.byref(size)))
+    hx, hy, hz = (int(v) for v in half)
+    return ConvolutionKernel(out.reshape(2 * hz + 1, 2 * hy + 1, 2 * hx + 1))
+
+
+class ConvolutionKernelGaussian(ConvolutionKernel):
+    """ConvolutionKernelGaussian (src/operators/OperatorVarPsf.cpp:75-130)."""
+
+    def __init__(self, sigmaX, sigmaY, sigmaZ, nStdX, nStdY, nStdZ, params: ImageParams):
+        k = _gaussian_kernel([sigmaX, sigmaY, sigmaZ], [nStdX, nStdY, nStdZ], params)
+        super().__init__(k.weights)
+
+
+class ConvolutionKernelGaussianMixture(ConvolutionKernel):
+    """ConvolutionKernelGaussianMixture (src/operators/OperatorVarPsf.cpp:132-245)."""
+
+    def __init__(self, sigmaX1, sigmaY1, sigmaZ1, sigmaX2, sigmaY2, sigmaZ2, weight2,
+                 nStdX, nStdY, nStdZ, params: ImageParams):
+        k = _gaussian_kernel([sigmaX1, sigmaY1, sigmaZ1, sigmaX2, sigmaY2, sigmaZ2, weight2],
+                             [nStdX, nStdY, nStdZ], params)
+        super().__init__(k.weights)
+
+
+class OperatorVarPsfDevice:
+    """Spatially variant image-space PSF (OperatorVarPsf / OperatorVarPsfDevice):
+    OperatorVarPsfDevice(image_params) or OperatorVarPsfDevice(fname,
+    image_params).  CSV: range x y z; gap x y z; nstd x y z; then one row per
+    kernel with 3 sigmas (Gaussian) or 7 values (two-Gaussian mixture)."""
+
+    def __init__(self, *args):
+        self._h = None
+        self._kernels = []
+        self._range = None
+        self._gap = None
+        if len(args) == 1:
+            self.params = args[0]
+        elif len(args) == 2:
+            self.params = args[1]
+            self.readFromFile(args[0])
+        else:
+            raise RuntimeError("OperatorVarPsfDevice(image_params) or (fname, image_params)")
+
+    def setRangeAndGap(self, xRange, xGap, yRange, yGap, zRange, zGap):
+        self._range = np.array([xRange, yRange, zRange], np.float32)
+        self._gap = np.array([xGap, yGap, zGap], np.float32)
+        self._upload()
+
+    def setKernelCollection(self, kernels):
+        self._kernels = [k if isinstance(k, ConvolutionKernel) else ConvolutionKernel(k)
+                         for k in kernels]
+        self._upload()
+
+    def readFromFile(self, fname: str):
+        rows = []
+        with open(fname) as f:
+            for line in f:
+                vals = [v for v in line.replace(",", " ").split() if v]
+                if vals:
+                    rows.append([float(v) for v in vals])
+        if len(rows) <= 3:
+            raise RuntimeError("CSV file format error: At least 4 rows expected")
+        cols = max(len(r) for r in rows)
+        if cols not in (3, 7):
+            raise RuntimeError("CSV file format error: 3 columns expected for 1-Gaussian "
+                               "VarPSF or 7 columns expected for 2-Gaussian VarPSF")
+        rows = [r + [0.0] * (cols - len(r)) for r in rows]
+        self._range = np.array(rows[0][:3], np.float32)
+        self._gap = np.array(rows[1][:3], np.float32)
+        nstd = rows[2][:3]
+        self._kernels = [_gaussian_kernel(r[:cols], nstd, self.params) for r in rows[3:]]
+        self._upload()
+
+    def _upload(self):
+        if self._range is None or not self._kernels:
+            return
+        w = np.concatenate([k.weights.ravel() for k in self._kernels]).astype(np.float32)
+        half = np.array([k.half_sizes for k in self._kernels], np.int32).ravel()
+        h = ctypes.c_void_p()
+        L.check(L.lib().yrtb_varpsf_create(w.ctypes.data, half.ctypes.data,
+                                           len(self._kernels), self._range.ctypes.data,
+                                           self._gap.ctypes.data, ctypes.byref(h)))
+        self._release()
+        self._h = h
+
+    def _release(self):
+        if self._h is not None:
+            L.lib().yrtb_varpsf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self._release()
+        except Exception:
+            pass
+
+    def _apply(self, img_in, img_out, adjoint, params=None):
+        if self._h is None:
+            raise RuntimeError("LUT not defined")
+        for t in (img_in, img_out):
+            if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+                raise RuntimeError("images must be contiguous float32 CUDA tensors")
+        if img_in.numel() != img_out.numel():
+            raise RuntimeError("Dimensions mismatch between the two images")
+        ip = params or self.params
+        if img_in.numel() != ip.numVoxels * ip.nt:
+            ip = ip.withFrames(img_in.numel() // ip.numVoxels)
+        L.check(L.lib().yrtb_varpsf_apply(self._h, img_in.data_ptr(), img_out.data_ptr(),
+                                          ctypes.byref(ip._c()), int(adjoint), _stream()))
+        return img_out
+
+    def applyA(self, img_in, img_out, params: Optional[ImageParams] = None):
+        return self._apply(img_in, img_out, False, params)
+
+    def applyAH(self, img_in, img_out, params: Optional[ImageParams] = None):
+        return self._apply(img_in, img_out, True, params)
+
+    @property
+    def handle(self):
+        return self._h
