@@ -1632,20 +1632,16 @@ struct VarPsfDev
 	int maxHx, maxHy, maxHz;
 };
 
-// LUT entry of voxel (i, j, k) (OperatorVarPsf::findNearestKernel with the
-// distances of varconvolve: |(i + 0.5) v - centre| in FP64, then FP32).
-__device__ __forceinline__ int varPsfKernel(const VarPsfDev& P, int i, int j, int k)
+// LUT coordinate of index i along one axis (OperatorVarPsf::findNearestKernel
+// with the distances of varconvolve: |(i + 0.5) v - centre| in FP64, then
+// FP32, divided by the gap, rounded, clamped).  The LUT index of voxel
+// (i, j, k) is a(i) + A (b(j) + B c(k)): separable, so each block tabulates
+// the three axes once in shared memory.
+__device__ __forceinline__ int varPsfAxis(int i, float v, float centre, float gap, int dim)
 {
-	const float tx = static_cast<float>(fabs((i + 0.5) * static_cast<double>(P.vx) - P.cx));
-	const float ty = static_cast<float>(fabs((j + 0.5) * static_cast<double>(P.vy) - P.cy));
-	const float tz = static_cast<float>(fabs((k + 0.5) * static_cast<double>(P.vz) - P.cz));
-	int a = static_cast<int>(roundf(fabsf(tx) / P.gapX));
-	int b = static_cast<int>(roundf(fabsf(ty) / P.gapY));
-	int c = static_cast<int>(roundf(fabsf(tz) / P.gapZ));
-	a = a >= P.lutX ? P.lutX - 1 : a;
-	b = b >= P.lutY ? P.lutY - 1 : b;
-	c = c >= P.lutZ ? P.lutZ - 1 : c;
-	return a + P.lutX * (b + P.lutY * c);
+	const float t = static_cast<float>(fabs((i + 0.5) * static_cast<double>(v) - centre));
+	const int a = static_cast<int>(roundf(fabsf(t) / gap));
+	return a >= dim ? dim - 1 : a;
 }
 
 __device__ __forceinline__ int circ1(int n, int x)
@@ -1663,6 +1659,21 @@ __global__ void __launch_bounds__(kPsfBX * kPsfBY)
 k_varpsf(const float* __restrict__ src, float* __restrict__ dst, int nx, int ny, int nz,
          int planes, VarPsfDev P)
 {
+	extern __shared__ int varAxis[];  // nx + ny + nz: LUT offsets per axis
+	int* ax = varAxis;
+	int* ay = ax + nx;
+	int* az = ay + ny;
+	for (int t = threadIdx.y * kPsfBX + threadIdx.x; t < nx + ny + nz; t += kPsfBX * kPsfBY)
+	{
+		if (t < nx)
+			ax[t] = varPsfAxis(t, P.vx, P.cx, P.gapX, P.lutX);
+		else if (t < nx + ny)
+			ay[t - nx] = P.lutX * varPsfAxis(t - nx, P.vy, P.cy, P.gapY, P.lutY);
+		else
+			az[t - nx - ny] =
+			    P.lutX * P.lutY * varPsfAxis(t - nx - ny, P.vz, P.cz, P.gapZ, P.lutZ);
+	}
+	__syncthreads();
 	const int x = blockIdx.x * kPsfBX + threadIdx.x;
 	const int y = blockIdx.y * kPsfBY + threadIdx.y;
 	if (x >= nx || y >= ny)
@@ -1675,7 +1686,7 @@ k_varpsf(const float* __restrict__ src, float* __restrict__ dst, int nx, int ny,
 		float sum = 0.f;
 		if (!ADJ)
 		{
-			const int4 m = __ldg(P.meta + varPsfKernel(P, x, y, z));
+			const int4 m = __ldg(P.meta + ax[x] + ay[y] + az[z]);
 			const float* w = P.w + m.x;
 			for (int dz = -m.w; dz <= m.w; dz++)
 			{
@@ -1693,13 +1704,15 @@ k_varpsf(const float* __restrict__ src, float* __restrict__ dst, int nx, int ny,
 			for (int dz = -P.maxHz; dz <= P.maxHz; dz++)
 			{
 				const int qz = circ1(nz, z - dz);
+				const int cz = az[qz];
 				for (int dy = -P.maxHy; dy <= P.maxHy; dy++)
 				{
 					const int qy = circ1(ny, y - dy);
+					const int cyz = cz + ay[qy];
 					for (int dx = -P.maxHx; dx <= P.maxHx; dx++)
 					{
 						const int qx = circ1(nx, x - dx);
-						const int4 m = __ldg(P.meta + varPsfKernel(P, qx, qy, qz));
+						const int4 m = __ldg(P.meta + cyz + ax[qx]);
 						if (dx < -m.y || dx > m.y || dy < -m.z || dy > m.z || dz < -m.w ||
 						    dz > m.w)
 							continue;
@@ -3560,13 +3573,20 @@ yrtb_status yrtb_varpsf_apply(const yrtb_varpsf* p, const float* d_in, float* d_
 	P.maxHz = p->maxH[2];
 	const int planes = static_cast<int>(ip->nz * ip->nt);
 	const dim3 block(kPsfBX, kPsfBY);
-	const dim3 grid((dims[0] + kPsfBX - 1) / kPsfBX, (dims[1] + kPsfBY - 1) / kPsfBY,
-	                std::min(planes, 65535));
+	// Enough blocks for a few waves; each loops over planes so that the
+	// per-block axis tables are built a few thousand times, not per plane.
+	const int gx = (dims[0] + kPsfBX - 1) / kPsfBX, gy = (dims[1] + kPsfBY - 1) / kPsfBY;
+	const int want = static_cast<int>(gridFor(1u << 30, 16));
+	const int gz = std::max(1, std::min(planes, (want + gx * gy - 1) / (gx * gy)));
+	const dim3 grid(gx, gy, std::min(gz, 65535));
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	const size_t smem = static_cast<size_t>(dims[0] + dims[1] + dims[2]) * sizeof(int);
+	if (smem > 48 * 1024)
+		return fail(YRTB_ERR_ARGUMENT, "image too large for the variant PSF (nx + ny + nz > 12288)");
 	if (adjoint)
-		k_varpsf<true><<<grid, block, 0, st>>>(d_in, d_out, dims[0], dims[1], dims[2], planes, P);
+		k_varpsf<true><<<grid, block, smem, st>>>(d_in, d_out, dims[0], dims[1], dims[2], planes, P);
 	else
-		k_varpsf<false><<<grid, block, 0, st>>>(d_in, d_out, dims[0], dims[1], dims[2], planes, P);
+		k_varpsf<false><<<grid, block, smem, st>>>(d_in, d_out, dims[0], dims[1], dims[2], planes, P);
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
