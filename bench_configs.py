@@ -249,11 +249,16 @@ def run_c5(args):
         plain(1)
     bt, pt = [], []
     for _ in range(args.steps):
+        # NVTX ranges let a profiler select the timed launches of each form.
+        torch.cuda.nvtx.range_push("c5_batched")
         with Timer() as t:
             batched(1)
+        torch.cuda.nvtx.range_pop()
         bt.append(t.ms)
+        torch.cuda.nvtx.range_push("c5_plain")
         with Timer() as t:
             plain(1)
+        torch.cuda.nvtx.range_pop()
         pt.append(t.ms)
     ms_b = float(np.median(bt))
     ms_p = float(np.median(pt))

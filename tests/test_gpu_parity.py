@@ -461,6 +461,60 @@ def test_em_update_variants_vs_numpy():
     np.testing.assert_allclose(xt.cpu().numpy(), ref, rtol=1e-6)
 
 
+@pytest.mark.parametrize("J", [4096, 1001])  # float4 form, scalar form
+@pytest.mark.parametrize("mode", ["broadcast", "per_frame", "scaled"])
+def test_em_update_modes_bit_exact(J, mode):
+    # Image::updateEMThreshold{Static,Dynamic,DynamicWithScaling,
+    # DynamicWith4DSens} (Image.cpp:651-833): x *= u / s where s > thr, the
+    # same FP32 operations as numpy's, so the results are bit-identical.
+    rng = np.random.default_rng(31)
+    nt = 5
+    thr = np.float32(1.19209e-07)
+    x = rng.uniform(0.1, 2, (nt, J)).astype(np.float32)
+    u = rng.uniform(0.1, 2, (nt, J)).astype(np.float32)
+    sens_nt = nt if mode == "per_frame" else 1
+    s = rng.uniform(-0.1, 2, (sens_nt, J)).astype(np.float32)
+    s[:, ::7] = 0.0
+    c = rng.uniform(0.5, 2, nt).astype(np.float32)
+    xt = torch.from_numpy(x.copy()).cuda()
+    ut, st, ct = (torch.from_numpy(a).cuda() for a in (u, s, c))
+    L.check(L.lib().yrtb_em_update(xt.data_ptr(), ut.data_ptr(), st.data_ptr(), J, nt,
+                                   sens_nt, thr,
+                                   ct.data_ptr() if mode == "scaled" else None, None))
+    torch.cuda.synchronize()
+    ref = x.copy()
+    for r in range(nt):
+        sr = s[r] if mode == "per_frame" else s[0]
+        if mode == "scaled":
+            inv_c = np.float32(1) / c[r]
+            m = sr > thr * inv_c
+            ref[r, m] *= (u[r, m] * inv_c) / sr[m]
+        else:
+            m = sr > thr
+            ref[r, m] *= u[r, m] / sr[m]
+    assert np.array_equal(xt.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("J", [4096, 1001])
+@pytest.mark.parametrize("broadcast", [1, 0])
+def test_apply_threshold_bit_exact(J, broadcast):
+    # Image::applyThreshold[Broadcast] (Image.cpp:595-650): x = m <= thr ? x*les + leo
+    # : x*gts + gto, FP32 products and sums without contraction.
+    rng = np.random.default_rng(32)
+    nt = 3
+    x = rng.uniform(-1, 2, (nt, J)).astype(np.float32)
+    m = rng.uniform(-0.5, 1, (1 if broadcast else nt, J)).astype(np.float32)
+    a = [np.float32(v) for v in (0.25, 0.0, 1.5, -0.125, 0.5)]  # thr les leo gts gto
+    xt = torch.from_numpy(x.copy()).cuda()
+    mt = torch.from_numpy(m).cuda()
+    L.check(L.lib().yrtb_apply_threshold(xt.data_ptr(), mt.data_ptr(), J, nt, broadcast,
+                                         *a, None))
+    torch.cuda.synchronize()
+    mm = np.broadcast_to(m, x.shape)
+    ref = np.where(mm <= a[0], x * a[1] + a[2], x * a[3] + a[4]).astype(np.float32)
+    assert np.array_equal(xt.cpu().numpy(), ref)
+
+
 # ------------------------------------------------------------- errors -----
 def test_invalid_detector_ids_are_counted_not_read():
     sc, ip, p = make()

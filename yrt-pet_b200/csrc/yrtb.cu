@@ -1405,6 +1405,53 @@ __global__ void k_em_update(float* __restrict__ x, const float* __restrict__ u,
 	}
 }
 
+// Float4 form of k_em_update (J a multiple of 4; x, u, s 16-byte aligned):
+// each thread updates 4 consecutive voxels of every frame with 16-byte
+// accesses, several frames unrolled so that their loads are in flight
+// together.  The FP32 operations per voxel are those of k_em_update.
+__device__ __forceinline__ float emVoxel(float x, float u, float s, float thr,
+                                         bool scaled, float inv_c)
+{
+	if (scaled)
+		return s > thr ? x * ((u * inv_c) / s) : x;
+	return s > thr ? x * (u / s) : x;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_em_update4(float4* __restrict__ x, const float4* __restrict__ u,
+                 const float4* __restrict__ s, uint64_t J4, int64_t nt,
+                 int64_t sens_nt, float thr, const float* __restrict__ scale)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	const bool perFrameSens = !scale && sens_nt == nt && nt > 1;
+	const bool scaled = scale != nullptr;
+	for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < J4;
+	     j += nthreads)
+	{
+		const float4 s0 = __ldg(s + j);
+#pragma unroll 4
+		for (int64_t r = 0; r < nt; r++)
+		{
+			const uint64_t i = static_cast<uint64_t>(r) * J4 + j;
+			const float4 uv = __ldg(u + i);
+			const float4 sv = perFrameSens ? __ldg(s + i) : s0;
+			float inv_c = 1.f, tr = thr;
+			if (scaled)
+			{
+				// updateEMThresholdDynamicWithScaling (Image.cpp:760-800).
+				inv_c = 1.0f / __ldg(scale + r);
+				tr = thr * inv_c;
+			}
+			float4 xv = x[i];
+			xv.x = emVoxel(xv.x, uv.x, sv.x, tr, scaled, inv_c);
+			xv.y = emVoxel(xv.y, uv.y, sv.y, tr, scaled, inv_c);
+			xv.z = emVoxel(xv.z, uv.z, sv.z, tr, scaled, inv_c);
+			xv.w = emVoxel(xv.w, uv.w, sv.w, tr, scaled, inv_c);
+			x[i] = xv;
+		}
+	}
+}
+
 __global__ void k_threshold(float* __restrict__ x, const float* __restrict__ m,
                             uint64_t J, int64_t nt, int broadcast, float thr,
                             float les, float leo, float gts, float gto)
@@ -1416,6 +1463,40 @@ __global__ void k_threshold(float* __restrict__ x, const float* __restrict__ m,
 	{
 		const float mv = __ldg(m + (broadcast ? i % J : i));
 		x[i] = (mv <= thr) ? x[i] * les + leo : x[i] * gts + gto;
+	}
+}
+
+// Float4 form of k_threshold (J a multiple of 4; x, m 16-byte aligned): 4
+// consecutive voxels per thread, frames in an inner loop so that a broadcast
+// mask is read once per voxel group and no index is divided.
+__device__ __forceinline__ float thrVoxel(float x, float m, float thr, float les,
+                                          float leo, float gts, float gto)
+{
+	return (m <= thr) ? x * les + leo : x * gts + gto;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_threshold4(float4* __restrict__ x, const float4* __restrict__ m,
+                 uint64_t J4, int64_t nt, int broadcast, float thr, float les,
+                 float leo, float gts, float gto)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < J4;
+	     j += nthreads)
+	{
+		const float4 m0 = __ldg(m + j);
+#pragma unroll 4
+		for (int64_t r = 0; r < nt; r++)
+		{
+			const uint64_t i = static_cast<uint64_t>(r) * J4 + j;
+			const float4 mv = broadcast ? m0 : __ldg(m + i);
+			float4 xv = x[i];
+			xv.x = thrVoxel(xv.x, mv.x, thr, les, leo, gts, gto);
+			xv.y = thrVoxel(xv.y, mv.y, thr, les, leo, gts, gto);
+			xv.z = thrVoxel(xv.z, mv.z, thr, les, leo, gts, gto);
+			xv.w = thrVoxel(xv.w, mv.w, thr, les, leo, gts, gto);
+			x[i] = xv;
+		}
 	}
 }
 
@@ -3161,9 +3242,16 @@ yrtb_status yrtb_em_update(float* x, const float* u, const float* s,
 {
 	if (!x || !u || !s || J == 0 || nt <= 0 || (sens_nt != 1 && sens_nt != nt))
 		return fail(YRTB_ERR_ARGUMENT, "invalid EM update arguments");
-	k_em_update<<<gridFor(J, 16), kBlock, 0,
-	              reinterpret_cast<cudaStream_t>(stream)>>>(x, u, s, J, nt, sens_nt,
-	                                                        thr, scale);
+	auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+	if (J % 4 == 0 && a16(x) && a16(u) && a16(s))
+		k_em_update4<<<gridFor(J / 4, 16), kBlock, 0,
+		               reinterpret_cast<cudaStream_t>(stream)>>>(
+		    reinterpret_cast<float4*>(x), reinterpret_cast<const float4*>(u),
+		    reinterpret_cast<const float4*>(s), J / 4, nt, sens_nt, thr, scale);
+	else
+		k_em_update<<<gridFor(J, 16), kBlock, 0,
+		              reinterpret_cast<cudaStream_t>(stream)>>>(x, u, s, J, nt, sens_nt,
+		                                                        thr, scale);
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
@@ -3175,9 +3263,16 @@ yrtb_status yrtb_apply_threshold(float* x, const float* m, uint64_t J,
 {
 	if (!x || !m || J == 0 || nt <= 0)
 		return fail(YRTB_ERR_ARGUMENT, "invalid threshold arguments");
-	k_threshold<<<gridFor(J * nt, 16), kBlock, 0,
-	              reinterpret_cast<cudaStream_t>(stream)>>>(x, m, J, nt, broadcast,
-	                                                        thr, les, leo, gts, gto);
+	auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+	if (J % 4 == 0 && a16(x) && a16(m))
+		k_threshold4<<<gridFor(J / 4, 16), kBlock, 0,
+		               reinterpret_cast<cudaStream_t>(stream)>>>(
+		    reinterpret_cast<float4*>(x), reinterpret_cast<const float4*>(m), J / 4, nt,
+		    broadcast, thr, les, leo, gts, gto);
+	else
+		k_threshold<<<gridFor(J * nt, 16), kBlock, 0,
+		              reinterpret_cast<cudaStream_t>(stream)>>>(x, m, J, nt, broadcast,
+		                                                        thr, les, leo, gts, gto);
 	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
