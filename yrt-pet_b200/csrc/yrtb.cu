@@ -1429,6 +1429,11 @@ __global__ void __launch_bounds__(kBlock)
 	     j += nthreads)
 	{
 		const float4 s0 = __ldg(s + j);
+		// A group outside the mask in every frame is left untouched (no
+		// loads or stores), as the scalar form touches only voxels with s > thr.
+		if (!perFrameSens && !scaled &&
+		    !(s0.x > thr || s0.y > thr || s0.z > thr || s0.w > thr))
+			continue;
 #pragma unroll 4
 		for (int64_t r = 0; r < nt; r++)
 		{
