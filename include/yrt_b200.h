@@ -350,6 +350,32 @@ yrtb_status yrtb_em_step_histo3d(yrtb_projector* h, const float* d_image,
                                  float global_scale, float denom_threshold,
                                  yrtb_stream stream);
 
+/* The bins of one subset that the histogram EM pass does work for (valid
+ * detector pair, measurement != 0), as subset-local indices in increasing
+ * order: d_k (device, capacity >= the subset's bin count) receives them and
+ * *n_out their number (synchronises the stream).  Replaces the skip of
+ * zero-measurement bins inside the bin loop of computeEMUpdateImage_kernel
+ * (OSEM_GPU.cu:1224-1225) by selecting them once per reconstruction. */
+yrtb_status yrtb_histo3d_subset_nonzero(yrtb_projector* h,
+                                        const float* d_measurements,
+                                        int num_subsets, int subset,
+                                        uint64_t* d_k, uint64_t capacity,
+                                        uint64_t* n_out, yrtb_stream stream);
+
+/* yrtb_em_step_histo3d over the n listed bins of the subset only (the list of
+ * yrtb_histo3d_subset_nonzero): the same per-bin work, with warps that hold
+ * only bins that do work.  Same image as the full-subset pass (bit-identical
+ * in deterministic mode). */
+yrtb_status yrtb_em_step_histo3d_list(yrtb_projector* h, const float* d_image,
+                                      float* d_em, const float* d_measurements,
+                                      const float* d_sens_histo,
+                                      const float* d_acf_histo,
+                                      const float* d_additive_histo,
+                                      int num_subsets, int subset,
+                                      const uint64_t* d_k, uint64_t n,
+                                      float global_scale, float denom_threshold,
+                                      yrtb_stream stream);
+
 /* List-mode -> Histogram3D: d_histo[bin(d1,d2)] += value for value > 0 and
  * d1 != d2 (values NULL: 1).  Pairs outside the histogram (ring difference,
  * minimum angle) are skipped and counted in *n_invalid (the reference

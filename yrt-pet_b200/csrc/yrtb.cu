@@ -25,6 +25,8 @@
 #include "device.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -979,16 +981,19 @@ __global__ void __launch_bounds__(kBlock)
             const float* __restrict__ sensH, const float* __restrict__ acfH,
             const float* __restrict__ addH, Geom mu,
             const float* __restrict__ muImg, float globalScale, float denomThr,
-            Fixed F, unsigned* maxBits)
+            Fixed F, unsigned* maxBits, const uint64_t* __restrict__ list)
 {
 	// One item per thread: a warp's threads stay converged across items
-	// (a grid-stride loop lets them drift apart between items).
-	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	// (a grid-stride loop lets them drift apart between items).  With a list,
+	// thread t takes the subset-local bin index list[t] (count = list length),
+	// so that warps hold only the bins that do work.
+	const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
 	float bound = 0.f;  // H_BOUND: |v| * max|w| of this bin
 	do
 	{
-		if (k >= count)
+		if (t >= count)
 			break;
+		const uint64_t k = list ? __ldg(list + t) : t;
 		const uint64_t bin = h3SubsetBin(H, k, numPhiSubset, numSubsets, subset);
 		uint32_t d1, d2;
 		h3Pair(H, bin, d1, d2);
@@ -2444,13 +2449,33 @@ yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
 	return YRTB_OK;
 }
 
+// Bins of one subset that the histogram EM pass does work for: a valid
+// detector pair and a non-zero measurement (NaN included), exactly the bins
+// k_histo<EM> does not skip.
+struct NonzeroBin
+{
+	H3Dev H;
+	const float* meas;
+	uint64_t nps, numSubsets, subset;
+	__device__ bool operator()(uint64_t k) const
+	{
+		const uint64_t bin = h3SubsetBin(H, k, nps, numSubsets, subset);
+		uint32_t d1, d2;
+		h3Pair(H, bin, d1, d2);
+		if (d1 == 0 && d2 == 0)
+			return false;
+		return !(__ldg(meas + bin) == 0.f);
+	}
+};
+
 template <bool EM>
 yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
                           const float* img, float* out, const float* meas,
                           const float* sensH, const float* acfH,
                           const float* addH, const float* mu,
                           const yrtb_image_params* muParams, float gs,
-                          float thr, yrtb_stream stream)
+                          float thr, yrtb_stream stream,
+                          const uint64_t* list = nullptr, uint64_t listCount = 0)
 {
 	if (!h || !out || numSubsets <= 0 || subset < 0 || subset >= numSubsets)
 		return fail(YRTB_ERR_ARGUMENT, "invalid histogram subset or buffers");
@@ -2462,14 +2487,18 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 		return fail(YRTB_ERR_ARGUMENT, "histogram-mode projection is single-frame");
 	YRTB_CUDA(cudaSetDevice(h->device));
 	uint64_t nps = 0;
-	const uint64_t count = h3SubsetSize(*h->h3, numSubsets, subset, nps);
+	const uint64_t subsetCount = h3SubsetSize(*h->h3, numSubsets, subset, nps);
+	// Threads: one per listed bin, or one per bin of the subset.  The
+	// fixed-point scale of deterministic mode is set by the subset size in
+	// both forms, so that they give the same image.
+	const uint64_t count = list ? listCount : subsetCount;
 	const Geom mg = mu ? makeGeom(*muParams) : Geom{};
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	const unsigned grid = gridAll(count);
 	Fixed F{};
 	if (h->det)
 	{
-		const yrtb_status s = fixedBegin(h, count, st, F);
+		const yrtb_status s = fixedBegin(h, subsetCount, st, F);
 		if (s != YRTB_OK)
 			return s;
 	}
@@ -2481,16 +2510,16 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 		{
 			k_histo<K, EM, H_BOUND, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
-			    acfH, addH, mg, mu, gs, thr, F, h->d_fixMax);
+			    acfH, addH, mg, mu, gs, thr, F, h->d_fixMax, list);
 			k_histo<K, EM, H_FIX, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
-			    acfH, addH, mg, mu, gs, thr, F, nullptr);
+			    acfH, addH, mg, mu, gs, thr, F, nullptr, list);
 		}
 		else
 		{
 			k_histo<K, EM, H_PLAIN, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
-			    acfH, addH, mg, mu, gs, thr, F, nullptr);
+			    acfH, addH, mg, mu, gs, thr, F, nullptr, list);
 		}
 	};
 	// Histogram mode honours the precision for single-ray Siddon and DD + PSF.
@@ -3146,6 +3175,77 @@ yrtb_status yrtb_em_step_histo3d(yrtb_projector* h, const float* d_image,
 	return dispatchHisto<true>(h, num_subsets, subset, d_image, d_em, d_meas,
 	                           d_sens_histo, d_acf_histo, d_add_histo, nullptr,
 	                           nullptr, global_scale, denom_threshold, stream);
+}
+
+yrtb_status yrtb_histo3d_subset_nonzero(yrtb_projector* h, const float* d_meas,
+                                        int num_subsets, int subset,
+                                        uint64_t* d_k, uint64_t capacity,
+                                        uint64_t* n_out, yrtb_stream stream)
+{
+	if (!h || !h->h3)
+		return fail(YRTB_ERR_ARGUMENT, "projector has no Histogram3D (odd ring)");
+	if (!d_meas || !d_k || !n_out || num_subsets <= 0 || subset < 0 ||
+	    subset >= num_subsets)
+		return fail(YRTB_ERR_ARGUMENT, "invalid histogram subset or buffers");
+	uint64_t nps = 0;
+	const uint64_t count = h3SubsetSize(*h->h3, num_subsets, subset, nps);
+	if (capacity < count)
+		return fail(YRTB_ERR_ARGUMENT,
+		            "bin list capacity " + std::to_string(capacity) +
+		                " is below the subset size " + std::to_string(count));
+	*n_out = 0;
+	if (count == 0)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	const NonzeroBin pred{h->h3d, d_meas, nps, static_cast<uint64_t>(num_subsets),
+	                      static_cast<uint64_t>(subset)};
+	const thrust::counting_iterator<uint64_t> first(0);
+	unsigned long long* d_num = nullptr;
+	void* temp = nullptr;
+	size_t tempBytes = 0;
+	cudaError_t ce = cub::DeviceSelect::If(nullptr, tempBytes, first, d_k, d_num,
+	                                       static_cast<int64_t>(count), pred, st);
+	if (ce == cudaSuccess)
+		ce = poolAlloc(&d_num, sizeof(unsigned long long), st);
+	if (ce == cudaSuccess)
+		ce = poolAlloc(&temp, tempBytes, st);
+	if (ce == cudaSuccess)
+		ce = cub::DeviceSelect::If(temp, tempBytes, first, d_k, d_num,
+		                           static_cast<int64_t>(count), pred, st);
+	unsigned long long num = 0;
+	if (ce == cudaSuccess)
+		ce = cudaMemcpyAsync(&num, d_num, sizeof(num), cudaMemcpyDeviceToHost, st);
+	cudaFreeAsync(d_num, st);
+	cudaFreeAsync(temp, st);
+	if (ce == cudaSuccess)
+		ce = cudaStreamSynchronize(st);
+	if (ce != cudaSuccess)
+		return fail(YRTB_ERR_CUDA, std::string("histogram bin selection: ") +
+		                               cudaGetErrorString(ce));
+	*n_out = num;
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_em_step_histo3d_list(yrtb_projector* h, const float* d_image,
+                                      float* d_em, const float* d_meas,
+                                      const float* d_sens_histo,
+                                      const float* d_acf_histo,
+                                      const float* d_add_histo, int num_subsets,
+                                      int subset, const uint64_t* d_k, uint64_t n,
+                                      float global_scale, float denom_threshold,
+                                      yrtb_stream stream)
+{
+	if (!h || !h->h3)
+		return fail(YRTB_ERR_ARGUMENT, "projector has no Histogram3D (odd ring)");
+	if (!d_k && n > 0)
+		return fail(YRTB_ERR_ARGUMENT, "null bin list");
+	if (n == 0)
+		return YRTB_OK;
+	return dispatchHisto<true>(h, num_subsets, subset, d_image, d_em, d_meas,
+	                           d_sens_histo, d_acf_histo, d_add_histo, nullptr,
+	                           nullptr, global_scale, denom_threshold, stream, d_k, n);
 }
 
 yrtb_status yrtb_listmode_to_histo3d(yrtb_projector* h, const uint32_t* d1,

@@ -128,6 +128,11 @@ SIGNATURES = {
     "yrtb_em_step_histo3d": ([c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                               ctypes.c_int, ctypes.c_int, c_f, c_f, c_vp],
                              ctypes.c_int),
+    "yrtb_histo3d_subset_nonzero": ([c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_u64,
+                                     _P(c_u64), c_vp], ctypes.c_int),
+    "yrtb_em_step_histo3d_list": ([c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                   ctypes.c_int, ctypes.c_int, c_vp, c_u64, c_f, c_f,
+                                   c_vp], ctypes.c_int),
     "yrtb_listmode_to_histo3d": ([c_vp, c_vp, c_vp, c_vp, c_u64, c_vp,
                                   _P(c_u64), c_vp], ctypes.c_int),
     "yrtb_events_subset_order": ([c_vp, _P(yrtb_events), ctypes.c_int, c_vp,

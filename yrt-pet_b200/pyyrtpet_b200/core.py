@@ -842,13 +842,33 @@ class DeviceProjector:
 
     def em_step_histo3d(self, img, em, meas, num_subsets, subset,
                         sens_histo=None, acf_histo=None, additive_histo=None,
-                        global_scale=1.0, denom_threshold=1e-35):
+                        global_scale=1.0, denom_threshold=1e-35, bins=None):
+        """Histogram-mode EM pass over one subset; with bins (the list of
+        histo3d_subset_nonzero for this subset) only those bins are visited."""
+        if bins is not None:
+            L.check(L.lib().yrtb_em_step_histo3d_list(
+                self.h, img.data_ptr(), em.data_ptr(), meas.data_ptr(),
+                _ptr(sens_histo), _ptr(acf_histo), _ptr(additive_histo),
+                int(num_subsets), int(subset), bins.data_ptr(), bins.numel(),
+                float(global_scale), float(denom_threshold), _stream()))
+            return em
         L.check(L.lib().yrtb_em_step_histo3d(
             self.h, img.data_ptr(), em.data_ptr(), meas.data_ptr(),
             _ptr(sens_histo), _ptr(acf_histo), _ptr(additive_histo),
             int(num_subsets), int(subset), float(global_scale),
             float(denom_threshold), _stream()))
         return em
+
+    def histo3d_subset_nonzero(self, meas, num_subsets, subset, capacity):
+        """Subset-local indices (int64 tensor, increasing) of the bins of the
+        subset with a valid pair and a non-zero measurement; capacity >= the
+        subset's bin count."""
+        buf = torch.empty(int(capacity), dtype=torch.int64, device=meas.device)
+        n = ctypes.c_uint64()
+        L.check(L.lib().yrtb_histo3d_subset_nonzero(
+            self.h, meas.data_ptr(), int(num_subsets), int(subset), buf.data_ptr(),
+            int(capacity), ctypes.byref(n), _stream()))
+        return buf[:n.value].clone()
 
 
 _proj_cache = {}

@@ -402,6 +402,16 @@ class OSEM_GPU:
                                              1, 1, 0.0, 0.0, 0.0, 1.0, 0.0,
                                              _stream()))
         em = torch.empty(J, dtype=torch.float32, device="cuda")
+        # The bins each subset's EM pass does work for (valid pair, non-zero
+        # measurement), selected once per reconstruction: the passes then
+        # run full warps of such bins instead of skipping empty bins inside
+        # each warp.
+        S = self.num_OSEM_subsets
+        bins = []
+        for s in range(S):
+            nps = h.numPhi // S + (1 if s + (h.numPhi // S) * S < h.numPhi else 0)
+            bins.append(proj.histo3d_subset_nonzero(meas, S, s,
+                                                    h.numR * nps * h.numZBin))
         psf = self.imagePsf if self.flagImagePSF else None
         if psf is not None:
             # Project PSF x, apply PSF^H to the EM image
@@ -418,7 +428,8 @@ class OSEM_GPU:
                                      sens_histo=sh, acf_histo=acf,
                                      additive_histo=add,
                                      global_scale=self._global,
-                                     denom_threshold=self.denomThreshold)
+                                     denom_threshold=self.denomThreshold,
+                                     bins=bins[s])
                 if psf is not None:
                     psf.applyAH(em, em_psf, ip)
                 L.check(L.lib().yrtb_em_update(
