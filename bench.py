@@ -33,6 +33,8 @@ import torch  # noqa: E402
 
 METRIC = "events/s fwd+back TOF Siddon, batched vs plain on 1 GPU, rel err<1e-4 vs FP64"
 UNIT = "events/s"
+WORKLOAD = ("C2 list-mode TOF Siddon OSEM iteration (fused fwd+bwd), 80x672 scanner "
+            "R=410, 256x256x160 @2mm, 214 ps TOF 5 sigma, 10 subsets")
 NUM_EVENTS = 50_000_000
 SUBSETS = 10
 # OSEM iterations of one reconstruction of this workload (the end-to-end
@@ -219,10 +221,9 @@ def run_reference_arm(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * args.ref_sample * ITERATIONS / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded phantom events)",
+            "dtype": "f32", "data": "synthetic (seeded phantom events, C2 shapes)",
             "impl": "reference",
-            "config": {"workload": "C2 list-mode TOF Siddon OSEM, 80x672 scanner, "
-                                   "256x256x160 @2mm, 10 subsets",
+            "config": {"workload": WORKLOAD,
                        "sample_events": args.ref_sample, "subsets": SUBSETS},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads,
                              "kind": kind,
@@ -547,10 +548,7 @@ def main():
                 "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded phantom events, C2 shapes)",
-                "config": {"workload": "C2 list-mode TOF Siddon OSEM iteration "
-                                       "(fused fwd+bwd), 80x672 scanner R=410, "
-                                       "256x256x160 @2mm, 214 ps TOF 5 sigma, "
-                                       "10 subsets",
+                "config": {"workload": WORKLOAD,
                            "events_per_gpu": ev.count, "subsets": SUBSETS,
                            "precision": args.precision,
                            "deterministic": bool(args.deterministic),
