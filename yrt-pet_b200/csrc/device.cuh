@@ -625,19 +625,22 @@ struct MultiRay
 __device__ __forceinline__ float psfIntegral(const float* kernel,
                                              int kernelSize, float kernelStep,
                                              float x0, float x1,
-                                             const float* prefix = nullptr)
+                                             const float* prefix = nullptr,
+                                             float invStep = 0.f)
 {
 	const int halfSize = (kernelSize - 1) / 2;
 	if (x0 > (halfSize + 1) * kernelStep || x1 < -(halfSize + 1) * kernelStep ||
 	    x0 >= x1)
 		return 0.f;
-	const float x0_s = x0 / kernelStep;
+	// The prefix form (compensated precision) scales by the reciprocal of the
+	// step; the bin-by-bin form divides as the reference does.
+	const float x0_s = prefix ? x0 * invStep : x0 / kernelStep;
 	const int x0_i = static_cast<int>(floorf(x0_s + halfSize));
 	const float tau_0 = x0_s + -(-halfSize + x0_i);
 	const float v0_lo = (x0_i < 0 || x0_i >= kernelSize) ? 0.f : __ldg(kernel + x0_i);
 	const float v0_hi = (x0_i < -1 || x0_i >= kernelSize - 1) ? 0.f : __ldg(kernel + x0_i + 1);
 	const float v0 = v0_lo * (1 - tau_0) + v0_hi * tau_0;
-	const float x1_s = x1 / kernelStep;
+	const float x1_s = prefix ? x1 * invStep : x1 / kernelStep;
 	const int x1_i = static_cast<int>(floorf(x1_s + halfSize));
 	const float tau_1 = x1_s - (-halfSize + x1_i);
 	const float v1_lo = (x1_i < 0 || x1_i >= kernelSize) ? 0.f : __ldg(kernel + x1_i);
@@ -676,7 +679,11 @@ __device__ __forceinline__ float psfIntegral(const float* kernel,
 // Distance-driven footprint of one LOR.  d1, d2: crystal centres relative to
 // the image centre; n1, n2: crystal orientations.  visit(offset, weight).
 // FASTPSF: PSF integrals from the prefix sums (compensated precision).
-template <bool TOF, bool PSF, bool FASTPSF, typename Visit>
+// FAST (compensated precision): every division by a value that is constant
+// along the LOR or along a row becomes a product with its reciprocal, taken
+// once (at most 1 ulp more rounding per weight); otherwise the reference's
+// divisions in its order.
+template <bool TOF, bool PSF, bool FASTPSF, bool FAST = false, typename Visit>
 __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
                                        const float3 d2, const float3 n1,
                                        const float3 n2, float thickness_trans,
@@ -791,14 +798,25 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 	const float z_off = static_cast<float>(g.nz - 1) * 0.5f;
 	const float inv_dz = 1.0f / dz;
 	const float half_dyx = dyx * 0.5f;
+	// FAST: reciprocals of the denominators that are constant along the LOR.
+	const float r_xy_lo = FAST ? 1.0f / (d2_xy_hi - d1_xy_lo) : 0.f;
+	const float r_xy_hi = FAST ? 1.0f / (d2_xy_lo - d1_xy_hi) : 0.f;
+	const float r_z_lo = FAST ? 1.0f / (d2_z_lo_i - d1_z_lo_i) : 0.f;
+	const float r_z_hi = FAST ? 1.0f / (d2_z_hi_i - d1_z_hi_i) : 0.f;
+	const float r_i = (FAST && TOF) ? 1.0f / (d2_i - d1_i) : 0.f;
+	const float r_step = (FAST && PSF) ? 1.0f / psf.kSpacing : 0.f;
 
 	for (int xyi = xy_i_0; xyi <= xy_i_1; xyi++)
 	{
 		const float pix_xy = -0.5f * lxy + (static_cast<float>(xyi) + 0.5f) * dxy;
-		const float a_xy_lo = (pix_xy - d1_xy_lo) / (d2_xy_hi - d1_xy_lo);
-		const float a_xy_hi = (pix_xy - d1_xy_hi) / (d2_xy_lo - d1_xy_hi);
-		const float a_z_lo = (pix_xy - d1_z_lo_i) / (d2_z_lo_i - d1_z_lo_i);
-		const float a_z_hi = (pix_xy - d1_z_hi_i) / (d2_z_hi_i - d1_z_hi_i);
+		const float a_xy_lo = FAST ? (pix_xy - d1_xy_lo) * r_xy_lo
+		                           : (pix_xy - d1_xy_lo) / (d2_xy_hi - d1_xy_lo);
+		const float a_xy_hi = FAST ? (pix_xy - d1_xy_hi) * r_xy_hi
+		                           : (pix_xy - d1_xy_hi) / (d2_xy_lo - d1_xy_hi);
+		const float a_z_lo = FAST ? (pix_xy - d1_z_lo_i) * r_z_lo
+		                          : (pix_xy - d1_z_lo_i) / (d2_z_lo_i - d1_z_lo_i);
+		const float a_z_hi = FAST ? (pix_xy - d1_z_hi_i) * r_z_hi
+		                          : (pix_xy - d1_z_hi_i) / (d2_z_hi_i - d1_z_hi_i);
 		float r0 = d1_yx_lo + a_xy_lo * (d2_yx_hi - d1_yx_lo);
 		float r1 = d1_yx_hi + a_xy_hi * (d2_yx_lo - d1_yx_hi);
 		if (r0 > r1)
@@ -827,10 +845,16 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 		float tw = 1.f;
 		if constexpr (TOF)
 		{
-			const float a_lo = (pix_xy - d1_i - 0.5f * dxy) / (d2_i - d1_i);
-			const float a_hi = (pix_xy - d1_i + 0.5f * dxy) / (d2_i - d1_i);
+			const float a_lo = FAST ? (pix_xy - d1_i - 0.5f * dxy) * r_i
+			                        : (pix_xy - d1_i - 0.5f * dxy) / (d2_i - d1_i);
+			const float a_hi = FAST ? (pix_xy - d1_i + 0.5f * dxy) * r_i
+			                        : (pix_xy - d1_i + 0.5f * dxy) / (d2_i - d1_i);
 			tw = tofWeight(tp, d_norm, tofValue, a_lo * d_norm, a_hi * d_norm);
 		}
+		// FAST: per-row reciprocals of the footprint widths, and the
+		// row factor dxy/cos(theta) folded into the transverse weight.
+		const float r_wyx = FAST ? 1.0f / widthFrac_yx : 0.f;
+		const float r_wz = FAST ? 1.0f / widthFrac_z : 0.f;
 		for (int yxi = i0; yxi <= i1; yxi++)
 		{
 			const float pix_yx = -0.5f * lyx + (static_cast<float>(yxi) + 0.5f) * dyx;
@@ -846,13 +870,14 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 					wxy = 0.f;
 				else
 					wxy = psfIntegral(kern, psf.size, psf.kSpacing, xa, xb,
-					                  FASTPSF ? kpre : nullptr);
+					                  FASTPSF ? kpre : nullptr, r_step);
 			}
 			else
 			{
 				wxy = fminf(p1, r1_ov) - fmaxf(p0, r0_ov);
 			}
-			const float wxy_s = wxy / widthFrac_yx;
+			const float wxy_s = FAST ? wxy * r_wyx * dxy_cos_theta : wxy / widthFrac_yx;
+			const int oxy = flag_y ? g.nx * xyi + yxi : g.nx * yxi + xyi;
 			for (int zi = zi0; zi <= zi1; zi++)
 			{
 				const float pix_z = -0.5f * g.lz + (static_cast<float>(zi) + 0.5f) * g.vz;
@@ -860,9 +885,9 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 				if (zr1 >= zp0 && zr0 < zp1)
 				{
 					const float wz = fminf(zp1, zr1) - fmaxf(zp0, zr0);
-					const float wz_s = wz / widthFrac_z;
-					const int o = zi * nxy + (flag_y ? g.nx * xyi + yxi : g.nx * yxi + xyi);
-					float w = wxy_s * wz_s * dxy_cos_theta;
+					const int o = zi * nxy + oxy;
+					float w = FAST ? wxy_s * (wz * r_wz)
+					               : wxy_s * (wz / widthFrac_z) * dxy_cos_theta;
 					if constexpr (TOF)
 						w *= tw;
 					visit(o, w);

@@ -377,7 +377,7 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
 	}
 	else
 	{
-		ddWalk<TOF, KIND == K_DD_PSF, COMP && KIND == K_DD_PSF>(P.g, p1, p2, n1, n2, P.scan.crystalTrans,
+		ddWalk<TOF, KIND == K_DD_PSF, COMP && KIND == K_DD_PSF, COMP>(P.g, p1, p2, n1, n2, P.scan.crystalTrans,
 		                              P.scan.crystalZ, P.tof, tofv, P.psf,
 		                              forward, visit);
 		endRay();
@@ -2272,7 +2272,8 @@ yrtb_status checkEvents(const yrtb_projector* h, const yrtb_events* ev,
 
 // Calls fn(kind, tof, comp) with the projector's configuration as
 // std::integral_constant / bool_constant values (compensated arithmetic
-// exists for the Siddon projectors and, as prefix-sum PSF integrals, for
+// exists for the Siddon projectors and, as prefix-sum PSF integrals and
+// products with reciprocals of the LOR's and rows' constant denominators, for
 // distance-driven projection with a PSF).
 template <typename Fn>
 void withConfig(const yrtb_projector* h, Fn&& fn)
