@@ -2241,11 +2241,27 @@ Events toDev(const yrtb_events* ev)
 	return E;
 }
 
+// An event set with no events: its per-event arrays (and the caller's
+// per-event outputs) may be null, since empty buffers have no storage.
+bool emptyEvents(const yrtb_events* ev)
+{
+	return ev != nullptr && ev->count == 0;
+}
+
 yrtb_status checkEvents(const yrtb_projector* h, const yrtb_events* ev,
                         yrtb_range& r, bool needTof)
 {
 	if (!h || !ev)
 		return fail(YRTB_ERR_ARGUMENT, "null projector or events");
+	if (ev->count == 0)
+	{
+		// Nothing to project: accepted whatever arrays are given (an empty
+		// tensor has no storage), and the range is empty.
+		if (r.stride == 0)
+			r.stride = 1;
+		r.count = 0;
+		return YRTB_OK;
+	}
 	if (!ev->d1 && !ev->lor)
 		return fail(YRTB_ERR_ARGUMENT, "events need detector ids or LORs");
 	if ((ev->d1 == nullptr) != (ev->d2 == nullptr))
@@ -2936,8 +2952,8 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
                                      uint64_t* subset_offsets,
                                      yrtb_stream stream)
 {
-	if (!h || !ev || !d_perm || !subset_offsets || num_subsets <= 0 ||
-	    num_subsets > (ev && ev->frame ? 4095 : 65535))
+	if (!h || !ev || (!d_perm && ev->count > 0) || !subset_offsets || num_subsets <= 0 ||
+	    num_subsets > (ev->frame ? 4095 : 65535))
 		return fail(YRTB_ERR_ARGUMENT, "invalid subset-order arguments");
 	const uint64_t n = ev->count;
 	const uint64_t S = static_cast<uint64_t>(num_subsets);
@@ -2960,11 +2976,15 @@ namespace
 yrtb_status gatherEvents(const yrtb_events* in, const uint64_t* d_perm,
                          const yrtb_events* out, yrtb_stream stream, bool packable)
 {
-	if (!in || !out || !d_perm)
+	if (!in || !out)
 		return fail(YRTB_ERR_ARGUMENT, "invalid gather arguments");
 	const uint64_t n = in->count;
 	if (out->count != n)
 		return fail(YRTB_ERR_ARGUMENT, "gather needs equal event counts");
+	if (n == 0)
+		return YRTB_OK;
+	if (!d_perm)
+		return fail(YRTB_ERR_ARGUMENT, "invalid gather arguments");
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	const unsigned long long* perm = reinterpret_cast<const unsigned long long*>(d_perm);
 	auto g32 = [&](const void* a, const void* b, int w) -> yrtb_status
@@ -3059,7 +3079,7 @@ yrtb_status yrtb_forward(yrtb_projector* h, const float* d_image,
                          const yrtb_events* ev, yrtb_range range, float* d_out,
                          yrtb_stream stream)
 {
-	if (!d_image || !d_out)
+	if (!d_image || (!d_out && !emptyEvents(ev)))
 		return fail(YRTB_ERR_ARGUMENT, "null image or output");
 	return dispatchEvents<OP_FWD>(h, ev, range, d_image, d_out, 1.f, 0.f, stream);
 }
@@ -3068,7 +3088,7 @@ yrtb_status yrtb_backward(yrtb_projector* h, const float* d_values,
                           const yrtb_events* ev, yrtb_range range,
                           float* d_image, yrtb_stream stream)
 {
-	if (!d_image || !d_values)
+	if (!d_image || (!d_values && !emptyEvents(ev)))
 		return fail(YRTB_ERR_ARGUMENT, "null image or values");
 	return dispatchEvents<OP_BWD>(h, ev, range, d_values, d_image, 1.f, 0.f, stream);
 }
@@ -3088,7 +3108,7 @@ yrtb_status yrtb_count_crossings(yrtb_projector* h, const yrtb_events* ev,
                                  yrtb_range range, uint32_t* d_out,
                                  yrtb_stream stream)
 {
-	if (!d_out)
+	if (!d_out && !emptyEvents(ev))
 		return fail(YRTB_ERR_ARGUMENT, "null output");
 	return dispatchEvents<OP_COUNT>(h, ev, range, nullptr,
 	                                reinterpret_cast<float*>(d_out), 1.f, 0.f,
@@ -3100,7 +3120,7 @@ yrtb_status yrtb_attenuation_factors(yrtb_projector* h, const float* d_mu,
                                      const yrtb_events* ev, yrtb_range range,
                                      float* d_out, yrtb_stream stream)
 {
-	if (!d_mu || !d_out || !validImage(mu_params))
+	if (!d_mu || (!d_out && !emptyEvents(ev)) || !validImage(mu_params))
 		return fail(YRTB_ERR_ARGUMENT, "invalid attenuation image or output");
 	yrtb_status s = checkEvents(h, ev, range, false);
 	if (s != YRTB_OK)
@@ -3130,15 +3150,17 @@ yrtb_status yrtb_gather_histo3d(yrtb_projector* h, const float* d_histo,
                                 const yrtb_events* ev, yrtb_range range,
                                 int invert, float* d_out, yrtb_stream stream)
 {
-	if (!d_histo || !d_out)
+	if (!d_histo || (!d_out && !emptyEvents(ev)))
 		return fail(YRTB_ERR_ARGUMENT, "null histogram or output");
 	yrtb_status s = checkEvents(h, ev, range, false);
 	if (s != YRTB_OK)
 		return s;
-	if (!ev->d1 || !h->h3)
+	if (!h->h3)
 		return fail(YRTB_ERR_ARGUMENT, "histogram gather needs detector ids and an even ring");
 	if (range.count == 0)
 		return YRTB_OK;
+	if (!ev->d1)
+		return fail(YRTB_ERR_ARGUMENT, "histogram gather needs detector ids and an even ring");
 	YRTB_CUDA(cudaSetDevice(h->device));
 	k_gather_histo<<<gridAll(range.count), kBlock, 0,
 	                 reinterpret_cast<cudaStream_t>(stream)>>>(
