@@ -471,6 +471,39 @@ def test_histogram_em_over_nonzero_bin_list(projector, rays, det):
         p.histo3d_subset_nonzero(meas, S, 0, 10)
 
 
+def test_histogram_dd_psf_compensated_rows_split_over_threads():
+    # Compensated DD + PSF histogram EM runs 4 threads per bin, each on a share
+    # of the bin's rows, the forward partial sums added over the group.  Its
+    # image equals the single-thread compensated pass (deterministic mode,
+    # fixed-point sums) to 1e-6 and the mirror pass to 1e-5.
+    psf = gaussian_psf()
+    sc = yrt.Scanner("t", *SC_ARGS)
+    ip = yrt.ImageParams(*IP_ARGS)
+    h = yrt.Histogram3D(sc)
+    rng = np.random.default_rng(43)
+    m = np.where(rng.random(h.histoSize) < 0.05,
+                 rng.integers(1, 5, h.histoSize), 0).astype(np.float32)
+    meas = torch.from_numpy(m).cuda()
+    img = torch.from_numpy(rng.uniform(0.5, 1.5, ip.shape).astype(np.float32)).cuda()
+    out = {}
+    for name, prec, det in (("split", L.YRTB_COMPENSATED, False),
+                            ("single", L.YRTB_COMPENSATED, True),
+                            ("mirror", L.YRTB_MIRROR, False)):
+        pp = yrt.ProjectorParams(sc)
+        pp.setProjector("DD")
+        pp.setProjPsf(*psf)
+        pp.precision = prec
+        pp.deterministic = det
+        p = yrt.DeviceProjector(sc, ip, pp)
+        em = torch.zeros(ip.shape, device="cuda")
+        for s in range(3):
+            p.em_step_histo3d(img, em, meas, 3, s)
+        out[name] = em.cpu().numpy()
+    assert np.count_nonzero(out["split"]) > 0
+    assert rel_l2(out["split"], out["single"]) < 1e-6
+    assert rel_l2(out["split"], out["mirror"]) < 1e-5
+
+
 def test_graph_and_plain_osem_agree():
     sc, ip, evs = _small_c1_problem(n=30000, seed=23, tof=True)
     e = evs.numpy()

@@ -689,7 +689,8 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
                                        const float3 n2, float thickness_trans,
                                        float thickness_z, const TofP& tp,
                                        float tofValue, const Psf& psf,
-                                       bool forward, Visit& visit)
+                                       bool forward, Visit& visit,
+                                       int part = 0, int parts = 1)
 {
 	const float3 d12 = f3sub(d1, d2);
 	const bool flag_y = fabsf(d12.y) > fabsf(d12.x);
@@ -806,7 +807,16 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 	const float r_i = (FAST && TOF) ? 1.0f / (d2_i - d1_i) : 0.f;
 	const float r_step = (FAST && PSF) ? 1.0f / psf.kSpacing : 0.f;
 
-	for (int xyi = xy_i_0; xyi <= xy_i_1; xyi++)
+	// Piece `part` of `parts` (several threads per LOR): an even share of the
+	// main-axis rows, each row computed exactly as by a single thread.
+	int row_lo = xy_i_0, row_hi = xy_i_1;
+	if (parts > 1 && xy_i_1 >= xy_i_0)
+	{
+		const int nrows = xy_i_1 - xy_i_0 + 1;
+		row_lo = xy_i_0 + (nrows * part) / parts;
+		row_hi = xy_i_0 + (nrows * (part + 1)) / parts - 1;
+	}
+	for (int xyi = row_lo; xyi <= row_hi; xyi++)
 	{
 		const float pix_xy = -0.5f * lxy + (static_cast<float>(xyi) + 0.5f) * dxy;
 		const float a_xy_lo = FAST ? (pix_xy - d1_xy_lo) * r_xy_lo

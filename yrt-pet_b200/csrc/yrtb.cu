@@ -379,7 +379,7 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
 	{
 		ddWalk<TOF, KIND == K_DD_PSF, COMP && KIND == K_DD_PSF, COMP>(P.g, p1, p2, n1, n2, P.scan.crystalTrans,
 		                              P.scan.crystalZ, P.tof, tofv, P.psf,
-		                              forward, visit);
+		                              forward, visit, part, parts);
 		endRay();
 	}
 }
@@ -973,7 +973,7 @@ enum HistoMode
 	H_FIX = 2
 };
 
-template <int KIND, bool EM, int MODE = H_PLAIN, bool COMP = false>
+template <int KIND, bool EM, int MODE = H_PLAIN, bool COMP = false, int TPL = 1>
 __global__ void __launch_bounds__(kBlock)
     k_histo(KParams P, H3Dev H, uint64_t count, uint64_t numPhiSubset,
             uint64_t numSubsets, uint64_t subset, const float* __restrict__ img,
@@ -983,11 +983,17 @@ __global__ void __launch_bounds__(kBlock)
             const float* __restrict__ muImg, float globalScale, float denomThr,
             Fixed F, unsigned* maxBits, const uint64_t* __restrict__ list)
 {
-	// One item per thread: a warp's threads stay converged across items
+	static_assert(TPL == 1 || (KIND == K_DD_PSF && EM && MODE == H_PLAIN && COMP),
+	              "several threads per bin: compensated DD + PSF histogram EM");
+	// One item per TPL threads: a warp's threads stay converged across items
 	// (a grid-stride loop lets them drift apart between items).  With a list,
-	// thread t takes the subset-local bin index list[t] (count = list length),
-	// so that warps hold only the bins that do work.
-	const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	// item t is the subset-local bin index list[t] (count = list length), so
+	// that warps hold only the bins that do work.  TPL > 1: lane j of a group
+	// walks piece j of the bin's rows; the forward partial sums are added over
+	// the group, which then shares the EM ratio.
+	const uint64_t gt = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	const uint64_t t = gt / TPL;
+	const int part = static_cast<int>(gt % TPL);
 	float bound = 0.f;  // H_BOUND: |v| * max|w| of this bin
 	do
 	{
@@ -1032,7 +1038,8 @@ __global__ void __launch_bounds__(kBlock)
 				u = forwardEvent<KIND, false, COMP, true>(P, img, p1, p2, n1, n2,
 				                                          0.f, k, &mw);
 			else
-				u = forwardEvent<KIND, false, COMP>(P, img, p1, p2, n1, n2, 0.f, k);
+				u = groupSum<TPL>(forwardEvent<KIND, false, COMP>(
+				    P, img, p1, p2, n1, n2, 0.f, k, nullptr, part, TPL));
 			u *= s;
 			u *= a;
 			u *= globalScale;
@@ -1057,7 +1064,8 @@ __global__ void __launch_bounds__(kBlock)
 			backwardEvent<KIND, false, COMP, true>(P, nullptr, v, p1, p2, n1, n2,
 			                                       0.f, k, F.acc, fixedScale(F));
 		else
-			backwardEvent<KIND, false, COMP>(P, out, v, p1, p2, n1, n2, 0.f, k);
+			backwardEvent<KIND, false, COMP>(P, out, v, p1, p2, n1, n2, 0.f, k, nullptr,
+			                                 0.0, part, TPL);
 	} while (false);
 	if constexpr (MODE == H_BOUND)
 		warpMaxInto(maxBits, bound != bound ? __uint_as_float(0x7fffffffu) : bound);
@@ -2466,6 +2474,11 @@ yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
 	return YRTB_OK;
 }
 
+// Threads per bin of the compensated DD + PSF histogram EM pass (measured
+// on a 12-subset OSEM iteration of a 1.8M-bin histogram: 1 thread 84.6 ms,
+// 2: 80.0, 4: 76.8, 8: 78.5).
+constexpr int kHistoDDThreads = 4;
+
 // Bins of one subset that the histogram EM pass does work for: a valid
 // detector pair and a non-zero measurement (NaN included), exactly the bins
 // k_histo<EM> does not skip.
@@ -2529,6 +2542,15 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
 			    acfH, addH, mg, mu, gs, thr, F, h->d_fixMax, list);
 			k_histo<K, EM, H_FIX, C><<<grid, kBlock, 0, st>>>(
+			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
+			    acfH, addH, mg, mu, gs, thr, F, nullptr, list);
+		}
+		else if constexpr (EM && K == K_DD_PSF && C)
+		{
+			// Compensated DD + PSF EM: kHistoDDThreads threads per bin, each
+			// on an even share of the bin's rows.
+			constexpr int T = kHistoDDThreads;
+			k_histo<K, EM, H_PLAIN, C, T><<<gridAll(count * T), kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
 			    acfH, addH, mg, mu, gs, thr, F, nullptr, list);
 		}
