@@ -194,8 +194,8 @@ def run_c5(args):
     J = ip1.numVoxels
     sens_proj = yrt.DeviceProjector(sc, ip1, yrt.ProjectorParams(sc))
     sens = torch.zeros(J, device="cuda")
-    sens_proj.sensitivity_histo3d(sens, 20, 0)
-    sens.mul_(20.0)
+    for part in range(20):  # all bins of the histogram, in 20 parts
+        sens_proj.sensitivity_histo3d(sens, 20, part)
     s_ptr = _stream()
     lib = L.lib()
 
@@ -559,8 +559,8 @@ def run_lrem(args):
     J = ip1.numVoxels
     sens_proj = yrt.DeviceProjector(sc, ip1, yrt.ProjectorParams(sc))
     sens = torch.zeros(J, device="cuda")
-    sens_proj.sensitivity_histo3d(sens, 20, 0)
-    sens.mul_(20.0)
+    for part in range(20):  # all bins of the histogram, in 20 parts
+        sens_proj.sensitivity_histo3d(sens, 20, part)
     lib = L.lib()
     st = _stream()
     g = torch.Generator(device="cuda").manual_seed(20261203 + 61)
