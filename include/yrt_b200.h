@@ -274,6 +274,20 @@ yrtb_status yrtb_em_step(yrtb_projector* h, const float* d_image,
                          yrtb_range range, float global_scale,
                          float denom_threshold, yrtb_stream stream);
 
+/* yrtb_em_step that also writes each event's model value u (the corrected
+ * forward projection, the EM ratio's denominator; 0 for a skipped event)
+ * to d_model[e].  With unit measurements and no corrections the pass yields
+ * the list-mode Poisson log-likelihood's terms log u_e and the back
+ * projection A^T (1/u) of its gradient in one traversal per event, which the
+ * reference computes as separate forward and back projections
+ * (util::forwProject / util::backProject, src/utils/ReconstructionUtils.cpp:
+ * 1005-1061). */
+yrtb_status yrtb_em_step_model(yrtb_projector* h, const float* d_image,
+                               float* d_em, const yrtb_events* ev,
+                               yrtb_range range, float global_scale,
+                               float denom_threshold, float* d_model,
+                               yrtb_stream stream);
+
 /* Number of voxel crossings (Siddon) or footprint voxels (DD) of every event
  * of the range, summed over rays: d_out[e] (uint32).  Used to count the
  * algorithmic traffic of a projection; no counterpart in the reference. */

@@ -13,7 +13,7 @@ import pyoracle as po
 import pyyrtpet_b200 as yrt
 from pyyrtpet_b200 import _lib as L
 from pyyrtpet_b200 import synthetic as S
-from pyyrtpet_b200.autograd import SiddonProjectFn, poisson_nll
+from pyyrtpet_b200.autograd import SiddonProjectFn, poisson_nll, poisson_nll_fused
 
 pytestmark = pytest.mark.gpu
 needs_ref = pytest.mark.skipif(not po.ref_available(),
@@ -153,6 +153,34 @@ def test_autograd_batched_and_adjoint():
     # torch.autograd.gradcheck-style check of linearity: A(a x) = a A(x).
     y2 = SiddonProjectFn.apply(2.0 * xb.detach(), proj, ev)
     assert rel_l2(y2.cpu().numpy(), 2.0 * y.detach().cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [L.YRTB_MIRROR, L.YRTB_COMPENSATED])
+def test_fused_poisson_nll_matches_composed(precision):
+    # One fused pass per event set (yrtb_em_step_model) gives the same loss
+    # as forward projection + torch reductions (identical forward sums, FP64
+    # sums) and the same gradient as autograd through the adjoint kernel, up
+    # to the order of the FP32 atomic sums (1e-6 relative L2).
+    sc, ip, _, ev, e = _c1_setup(30000, 71)
+    pp = yrt.ProjectorParams(sc)
+    pp.addTOF(214.0, 5)
+    pp.precision = precision
+    proj = yrt.DeviceProjector(sc, ip, pp)
+    e2 = S.generate_events(sc, 30000, 73, tof_fwhm_ps=214.0).numpy()
+    ev2 = yrt.DeviceEvents.from_arrays(e2["d1"], e2["d2"], tof=e2["tof"])
+    rng = np.random.default_rng(72)
+    x0 = torch.from_numpy(rng.uniform(0.0, 1.0, (2,) + ip.shape).astype(np.float32)).cuda()
+    sens = torch.from_numpy(rng.uniform(0.5, 1.0, ip.shape).astype(np.float32)).cuda()
+    for x_init, evs in ((x0[0], ev), (x0, [ev, ev2])):
+        xa = x_init.clone().requires_grad_(True)
+        xb = x_init.clone().requires_grad_(True)
+        la = poisson_nll(xa, proj, evs, sens)
+        lb = poisson_nll_fused(xb, proj, evs, sens)
+        assert torch.equal(la, lb)
+        w = torch.arange(1, la.numel() + 1, dtype=la.dtype, device=la.device).reshape(la.shape)
+        (w * la).sum().backward()
+        (w * lb).sum().backward()
+        assert rel_l2(xb.grad.cpu().numpy(), xa.grad.cpu().numpy()) < 1e-6
 
 
 def test_compensated_mode_error_vs_fp64():

@@ -78,6 +78,10 @@ struct Events
 	const float* sens;
 	const float* att;
 	const float* add;
+	// EM step only: when not null, each event's model value (forward
+	// projection with its corrections, the denominator of the EM ratio) is
+	// written here; 0 for an event that is skipped.
+	float* model;
 };
 
 struct Range

@@ -686,6 +686,9 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 					atomicAdd(err, 1ULL);
 				if constexpr (OP == OP_FWD)
 					out[e] = 0.f;
+				if constexpr (OP == OP_EM)
+					if (E.model)
+						E.model[e] = 0.f;
 				if constexpr (OP == OP_COUNT)
 					reinterpret_cast<uint32_t*>(out)[e] = 0u;
 			}
@@ -727,7 +730,11 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 			const float s = E.sens ? __ldg(E.sens + e) : 1.0f;
 			const float a = E.att ? __ldg(E.att + e) : 1.0f;
 			if (m == 0.f || s == 0.f || a == 0.f)
+			{
+				if (E.model && part == 0)
+					E.model[e] = 0.f;
 				return;
+			}
 			float u = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			u *= s;
@@ -735,6 +742,8 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
 			u *= globalScale;
 			if (E.add)
 				u += __ldg(E.add + e);
+			if (E.model && part == 0)
+				E.model[e] = u;
 			if (fabsf(u) > denomThr)
 			{
 				u = m / u;
@@ -2421,7 +2430,8 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 template <int OP>
 yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
                            yrtb_range range, const float* in, float* out,
-                           float gs, float thr, yrtb_stream stream)
+                           float gs, float thr, yrtb_stream stream,
+                           float* model = nullptr)
 {
 	yrtb_status s = checkEvents(h, ev, range, true);
 	if (s != YRTB_OK)
@@ -2429,7 +2439,8 @@ yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
 	if (range.count == 0)
 		return YRTB_OK;
 	YRTB_CUDA(cudaSetDevice(h->device));
-	const Events E = toDev(ev);
+	Events E = toDev(ev);
+	E.model = model;
 	const Range R{range.start, range.stride, range.count};
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	constexpr bool kScatter = OP == OP_BWD || OP == OP_EM;
@@ -3124,6 +3135,17 @@ yrtb_status yrtb_em_step(yrtb_projector* h, const float* d_image, float* d_em,
 		return fail(YRTB_ERR_ARGUMENT, "null image or EM buffer");
 	return dispatchEvents<OP_EM>(h, ev, range, d_image, d_em, global_scale,
 	                             denom_threshold, stream);
+}
+
+yrtb_status yrtb_em_step_model(yrtb_projector* h, const float* d_image, float* d_em,
+                               const yrtb_events* ev, yrtb_range range,
+                               float global_scale, float denom_threshold,
+                               float* d_model, yrtb_stream stream)
+{
+	if (!d_image || !d_em || (!d_model && !emptyEvents(ev)))
+		return fail(YRTB_ERR_ARGUMENT, "null image, EM buffer or model output");
+	return dispatchEvents<OP_EM>(h, ev, range, d_image, d_em, global_scale,
+	                             denom_threshold, stream, d_model);
 }
 
 yrtb_status yrtb_count_crossings(yrtb_projector* h, const yrtb_events* ev,

@@ -115,6 +115,8 @@ SIGNATURES = {
                       ctypes.c_int),
     "yrtb_em_step": ([c_vp, c_vp, c_vp, _P(yrtb_events), yrtb_range, c_f, c_f,
                       c_vp], ctypes.c_int),
+    "yrtb_em_step_model": ([c_vp, c_vp, c_vp, _P(yrtb_events), yrtb_range, c_f, c_f,
+                            c_vp, c_vp], ctypes.c_int),
     "yrtb_count_crossings": ([c_vp, _P(yrtb_events), yrtb_range, c_vp, c_vp],
                              ctypes.c_int),
     "yrtb_attenuation_factors": ([c_vp, c_vp, _P(yrtb_image_params),

@@ -738,10 +738,20 @@ class DeviceProjector:
         return img
 
     def em_step(self, img, em, ev: DeviceEvents, rng=None, global_scale=1.0,
-                denom_threshold=1e-35):
+                denom_threshold=1e-35, model=None):
+        """Fused EM pass: em += A^T (m / u), u the corrected forward
+        projection; with model (a float32 tensor of ev.count), u is also
+        written there per event."""
         self._check_image(img)
         self._check_image(em)
         r = rng or L.yrtb_range(0, 1, 0)
+        if model is not None:
+            L.check(L.lib().yrtb_em_step_model(self.h, img.data_ptr(), em.data_ptr(),
+                                               ctypes.byref(ev.c()), r,
+                                               float(global_scale),
+                                               float(denom_threshold),
+                                               model.data_ptr(), _stream()))
+            return em
         L.check(L.lib().yrtb_em_step(self.h, img.data_ptr(), em.data_ptr(),
                                      ctypes.byref(ev.c()), r,
                                      float(global_scale),
