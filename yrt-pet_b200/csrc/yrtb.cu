@@ -906,19 +906,80 @@ __global__ void k_support_box(const float* __restrict__ img, Geom g, int* box)
 	}
 }
 
+// Moves the endpoints of fetchEvent (relative to the reconstruction grid) to
+// the attenuation grid and gives the ray's parametric window inside the
+// mu-map's non-zero bounding box: only voxels there contribute, so the walk
+// is limited to it.
+__device__ __forceinline__ void attWindow(const KParams& P, const Geom& mu,
+                                          const int* box, float3& p1, float3& p2,
+                                          float& wlo, float& whi)
+{
+	const float3 fix = make_float3(P.g.offx - mu.offx, P.g.offy - mu.offy,
+	                               P.g.offz - mu.offz);
+	p1 = make_float3(p1.x + fix.x, p1.y + fix.y, p1.z + fix.z);
+	p2 = make_float3(p2.x + fix.x, p2.y + fix.y, p2.z + fix.z);
+	boxWindow(mu, box, p1, p2, wlo, whi);
+}
+
+// Walk-length bucket of each item of the range for the attenuation walks:
+// an O(1) estimate of the voxel planes the ray crosses inside its window in
+// the mu-map's support box, in buckets of 4 (255 = 1020 or more), with the
+// item's index for the sort.  The events arrive in reconstruction order
+// (subset, TOF-window length, LOR), which says nothing about the length of
+// their full chords through the mu-map; a warp of such walks ran about 10 of
+// its 32 lanes.
+__global__ void k_att_keys(KParams P, Geom mu, Events E, Range R,
+                           const int* __restrict__ box, uint8_t* __restrict__ keys,
+                           uint32_t* __restrict__ idx)
+{
+	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	     i < R.count; i += nthreads)
+	{
+		const uint64_t e = R.start + i * R.stride;
+		float3 p1, p2, n1, n2;
+		unsigned c = 0;
+		if (fetchEvent(P, E, e, p1, p2, n1, n2))
+		{
+			float wlo, whi;
+			attWindow(P, mu, box, p1, p2, wlo, whi);
+			if (wlo < whi)
+			{
+				auto planes = [&](float p, float d, float q0, float dq) -> unsigned
+				{
+					if (d == 0.f)
+						return 0u;
+					const float u = floorf((p + wlo * d - q0) / dq);
+					const float v = floorf((p + whi * d - q0) / dq);
+					return static_cast<unsigned>(fminf(fabsf(v - u), 65536.f));
+				};
+				c = 1u + planes(p1.x, p2.x - p1.x, -0.5f * mu.lx, mu.vx) +
+				    planes(p1.y, p2.y - p1.y, -0.5f * mu.ly, mu.vy) +
+				    planes(p1.z, p2.z - p1.z, -0.5f * mu.lz, mu.vz);
+			}
+		}
+		keys[i] = static_cast<uint8_t>(min(c >> 2, 255u));
+		idx[i] = static_cast<uint32_t>(i);
+	}
+}
+
 // Attenuation factor per event: exp(-0.1 * line integral of mu), walked with
 // the projector's arithmetic (COMP: compensated walk).
 template <bool COMP>
 __global__ void __launch_bounds__(kBlock, 8)
     k_attenuation(KParams P, Geom mu, Events E, Range R,
                   const float* __restrict__ muImg, const int* __restrict__ box,
-                  float* __restrict__ out, unsigned long long* err)
+                  float* __restrict__ out, unsigned long long* err,
+                  const uint32_t* __restrict__ order)
 {
 	// One item per thread: a warp's threads stay converged across items
-	// (a grid-stride loop lets them drift apart between items).
-	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-	if (k < R.count)
+	// (a grid-stride loop lets them drift apart between items).  With order,
+	// thread i walks item order[i] (items grouped by walk length, see
+	// k_att_keys), so that the lanes of a warp walk similar lengths.
+	const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (i < R.count)
 	{
+		const uint64_t k = order ? __ldg(order + i) : i;
 		const uint64_t e = R.start + k * R.stride;
 		float3 p1, p2, n1, n2;
 		if (!fetchEvent(P, E, e, p1, p2, n1, n2))
@@ -927,16 +988,8 @@ __global__ void __launch_bounds__(kBlock, 8)
 			out[e] = 0.f;
 			return;
 		}
-		// fetchEvent subtracted the reconstruction grid offset; move to the
-		// attenuation grid instead.
-		const float3 fix = make_float3(P.g.offx - mu.offx, P.g.offy - mu.offy,
-		                               P.g.offz - mu.offz);
-		p1 = make_float3(p1.x + fix.x, p1.y + fix.y, p1.z + fix.z);
-		p2 = make_float3(p2.x + fix.x, p2.y + fix.y, p2.z + fix.z);
-		// Only voxels of the mu-map's non-zero bounding box contribute, so
-		// the walk is limited to the ray's window inside that box.
 		float wlo, whi;
-		boxWindow(mu, box, p1, p2, wlo, whi);
+		attWindow(P, mu, box, p1, p2, wlo, whi);
 		float acc = 0.f;
 		auto visit = [&](int o, float w) { acc += w * __ldg(muImg + o); };
 		if (wlo < whi)
@@ -3179,14 +3232,60 @@ yrtb_status yrtb_attenuation_factors(yrtb_projector* h, const float* d_mu,
 	k_box_init<<<1, 32, 0, st>>>(d_box);
 	k_support_box<<<gridFor(mg.nvox, 4), kBlock, 0, st>>>(d_mu, mg, d_box);
 	const Range R{range.start, range.stride, range.count};
+	const Events E = toDev(ev);
+	// Items grouped by walk length: one stable radix pass over an 8-bit
+	// bucket keeps the reconstruction order inside each bucket.  Every item's
+	// walk is unchanged, so the factors are the same in any order.
+	uint8_t *keys = nullptr, *keys2 = nullptr;
+	uint32_t *idx = nullptr, *order = nullptr;
+	void* temp = nullptr;
+	size_t tempBytes = 0;
+	const uint64_t n = range.count;
+	cudaError_t ce = cudaSuccess;
+	if (n < (1ULL << 32))
+	{
+		ce = poolAlloc(&keys, n, st);
+		if (ce == cudaSuccess)
+			ce = poolAlloc(&keys2, n, st);
+		if (ce == cudaSuccess)
+			ce = poolAlloc(&idx, n * sizeof(uint32_t), st);
+		if (ce == cudaSuccess)
+			ce = poolAlloc(&order, n * sizeof(uint32_t), st);
+		if (ce == cudaSuccess)
+			ce = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, idx, order,
+			                                     static_cast<int64_t>(n), 0, 8, st);
+		if (ce == cudaSuccess)
+			ce = poolAlloc(&temp, tempBytes, st);
+		if (ce == cudaSuccess)
+		{
+			k_att_keys<<<gridFor(n, 16), kBlock, 0, st>>>(h->P, mg, E, R, d_box, keys, idx);
+			ce = cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, idx, order,
+			                                     static_cast<int64_t>(n), 0, 8, st);
+		}
+	}
+	auto release = [&]
+	{
+		cudaFreeAsync(keys, st);
+		cudaFreeAsync(keys2, st);
+		cudaFreeAsync(idx, st);
+		cudaFreeAsync(order, st);
+		cudaFreeAsync(temp, st);
+		cudaFreeAsync(d_box, st);
+	};
+	if (ce != cudaSuccess)
+	{
+		release();
+		return fail(YRTB_ERR_CUDA, std::string("attenuation walk order: ") +
+		                               cudaGetErrorString(ce));
+	}
 	if (h->comp)
-		k_attenuation<true><<<gridAll(range.count), kBlock, 0, st>>>(
-		    h->P, mg, toDev(ev), R, d_mu, d_box, d_out, h->d_err);
+		k_attenuation<true><<<gridAll(n), kBlock, 0, st>>>(
+		    h->P, mg, E, R, d_mu, d_box, d_out, h->d_err, order);
 	else
-		k_attenuation<false><<<gridAll(range.count), kBlock, 0, st>>>(
-		    h->P, mg, toDev(ev), R, d_mu, d_box, d_out, h->d_err);
+		k_attenuation<false><<<gridAll(n), kBlock, 0, st>>>(
+		    h->P, mg, E, R, d_mu, d_box, d_out, h->d_err, order);
 	YRTB_LAUNCHED();
-	YRTB_CUDA(cudaFreeAsync(d_box, st));
+	release();
 	return YRTB_OK;
 }
 
