@@ -170,3 +170,31 @@ def test_all_zero_histogram_selects_no_bins():
     p.em_step_histo3d(img, em, meas, 4, 1, bins=bins)
     p.em_step_histo3d(img, em, meas, 4, 1)
     assert torch.count_nonzero(em) == 0
+
+
+@pytest.mark.parametrize("precision", [L.YRTB_MIRROR, L.YRTB_COMPENSATED])
+def test_attenuation_strided_range_matches_full_range(precision):
+    # The attenuation walks run grouped by their length through a
+    # permutation of the range's items: a strided range gives, event by
+    # event, the factors of the full range (bit for bit) and writes nothing
+    # else.
+    from pyyrtpet_b200 import synthetic as S
+    sc = S.scanner_c1()
+    ip = yrt.ImageParams(64, 64, 32, 256, 256, 128)
+    pp = yrt.ProjectorParams(sc)
+    pp.precision = precision
+    p = yrt.DeviceProjector(sc, ip, pp)
+    e = S.generate_events(sc, 20000, 93).numpy()
+    ev = yrt.DeviceEvents.from_arrays(e["d1"], e["d2"])
+    mu = S.Phantom(cyl_half_length=32).mu_image(ip, device="cuda").reshape(-1).contiguous()
+    full = p.attenuation_factors(mu, ip, ev).cpu().numpy()
+    out = torch.full((ev.count,), -1.0, device="cuda")
+    start, stride, count = 5, 3, 4000
+    p.attenuation_factors(mu, ip, ev, out=out, rng=L.yrtb_range(start, stride, count))
+    v = out.cpu().numpy()
+    idx = start + stride * np.arange(count)
+    assert np.array_equal(bits(v[idx]), bits(full[idx]))
+    mask = np.ones(ev.count, bool)
+    mask[idx] = False
+    assert np.all(v[mask] == -1.0)
+    assert np.any(full < 1.0)
