@@ -65,7 +65,7 @@ def parse():
                     help="write every autotuner candidate and its time (JSON)")
     ap.add_argument("--deterministic", action="store_true",
                     help="two-pass fixed-point back projection")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "psf", "lrem"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2mr", "c3", "c4", "c5", "psf", "lrem"],
                     help="c2 (default) is the headline workload; the others "
                          "run bench_configs.py")
     ap.add_argument("--cfg-events", type=int, default=0,

@@ -681,5 +681,116 @@ def _measured_peaks():
         return 6650.0
 
 
+# ------------------------------------------------------ C2 multi-ray ----
+def run_c2mr(args):
+    """The C2 TOF list-mode workload with 4-ray Siddon (rays after the first
+    offset across the crystal faces, curand stream per event): one OSEM
+    iteration x 10 subsets through yrtb_osem_listmode, beside the same
+    iteration with one ray, the reference CPU 4-ray OSEM on a sample, and
+    the 4-ray forward projections of a sample against the FP64 oracle with
+    the device's ray offsets."""
+    import bench
+    yrt, L, S, _stream = _yrt()
+    n = args.cfg_events or bench.NUM_EVENTS
+    sc, ip, ph, eff, evs, mu = bench.build_workload(n, "cuda", seed=bench.SEED)
+    mu_flat = mu.reshape(-1).contiguous()
+    J = ip.numVoxels
+    # Sensitivity image (set-up, not timed): all histogram bins, attenuation
+    # from the mu-map.
+    sens_proj = yrt.DeviceProjector(sc, ip, yrt.ProjectorParams(sc))
+    sens = torch.zeros(J, device="cuda")
+    for part in range(20):
+        sens_proj.sensitivity_histo3d(sens, 20, part, mu=mu_flat, mu_params=ip)
+    lib = L.lib()
+    n_rand_lors = float(sc.getNumDets()) ** 2 / 2 * 0.45
+    ms = {}
+    proj4 = None
+    for rays in (4, 1):
+        pp = yrt.ProjectorParams(sc)
+        pp.addTOF(bench.TOF_FWHM, bench.TOF_NSTD)
+        pp.numRays = rays
+        pp.precision = L.YRTB_COMPENSATED
+        proj = yrt.DeviceProjector(sc, ip, pp)
+        if rays == 4:
+            proj4 = proj
+        ev = yrt.DeviceEvents.from_arrays(evs.d1.to(torch.int32), evs.d2.to(torch.int32),
+                                          tof=evs.tof)
+        ev, offs = proj.order_events(ev, bench.SUBSETS)
+        ev.sens = (eff[ev.d1.long()] * eff[ev.d2.long()]).contiguous()
+        ev.att = proj.attenuation_factors(mu_flat, ip, ev)
+        ev.additive = torch.full((ev.count,), 0.2 * ev.count / n_rand_lors, device="cuda")
+        if rays > 1:
+            # Set-up, not timed: the offsets of every item index of a subset.
+            with Timer() as tt:
+                proj.multiray_table(int(np.max(np.diff(offs))))
+            table_ms = tt.ms
+        img = torch.empty(J, device="cuda")
+        work = torch.empty(2 * J, device="cuda")
+        p = L.yrtb_osem_params(1, bench.SUBSETS, 1.0, 1e-35, 1.19209e-07, 0, 0, None,
+                               offs.ctypes.data)
+
+        def one():
+            L.check(lib.yrtb_osem_listmode(proj.h, ctypes.byref(ev.c()), sens.data_ptr(),
+                                           img.data_ptr(), work.data_ptr(),
+                                           ctypes.byref(p), _stream()))
+        for _ in range(max(1, args.warmup)):
+            one()
+        times = []
+        for _ in range(args.steps):
+            with Timer() as t:
+                one()
+            times.append(t.ms)
+        ms[rays] = float(np.median(times))
+        del ev, img, work
+    out = _base("C2 list-mode TOF OSEM iteration with 4-ray Siddon, 80x672 scanner "
+                "R=410, 256x256x160 @2mm, 214 ps TOF 5 sigma, 10 subsets",
+                "events/s (4-ray fwd+back TOF Siddon, one OSEM iteration)",
+                n / (ms[4] * 1e-3), "events/s", args.steps, args.warmup, ms[4],
+                {"events": n, "rays": 4, "subsets": bench.SUBSETS,
+                 "precision": "compensated",
+                 "multi_ray_stream": "curand XORWOW, seed 13, subsequence = event "
+                                     "index in the call"})
+    out["single_ray"] = {"value": n / (ms[1] * 1e-3), "ms_per_step": ms[1]}
+    out["multiray_table_ms"] = table_ms
+    # FP64 parity of the 4-ray forward projections on a sample, with the
+    # offsets the device draws for it.
+    po = _po()
+    k = 20000
+    d1 = evs.d1[:k].to(torch.int32).cpu().numpy().view(np.uint32)
+    d2 = evs.d2[:k].to(torch.int32).cpu().numpy().view(np.uint32)
+    tof = evs.tof[:k].cpu().numpy()
+    g = torch.Generator(device="cuda").manual_seed(20261203 + 21)
+    x = (0.5 + torch.rand(ip.shape, generator=g, device="cuda")).contiguous()
+    v = proj4.forward(x, yrt.DeviceEvents.from_arrays(d1, d2, tof=tof)).cpu().numpy()
+    roffs = proj4.multiray_offsets(k).cpu().numpy()
+    lors, ori = po.lors_from_detpairs(po.scanner_lut(_po_scanner(po, sc)), d1, d2)
+    ref = po.project(_po_image(po, ip),
+                     po.Proj(num_rays=4, crystal_z=sc.crystalSize_z,
+                             crystal_trans=sc.crystalSize_trans,
+                             tof_fwhm_ps=bench.TOF_FWHM, tof_n_std=bench.TOF_NSTD),
+                     lors, image=x.cpu().numpy(), orients=ori, tof=tof, ray_offsets=roffs,
+                     precision="f64")
+    out["parity_vs_fp64"] = {"fwd_rel_l2": _rel_l2(v, ref), "sample_events": k}
+    if po.ref_available() and not args.no_cpu_baseline:
+        m = 200_000
+        osc = _po_scanner(po, sc)
+        oip = _po_image(po, ip)
+        _, sec = po.ref_osem_listmode(
+            osc, oip, np.ones((ip.nz, ip.ny, ip.nx), np.float32),
+            evs.d1[:m].cpu().numpy().astype(np.uint32),
+            evs.d2[:m].cpu().numpy().astype(np.uint32),
+            tof=evs.tof[:m].cpu().numpy().astype(np.float32),
+            randoms=np.full(m, 1e-3, np.float32), att_params=oip,
+            att_image=mu.cpu().numpy(), iterations=1, subsets=bench.SUBSETS,
+            tof_fwhm_ps=bench.TOF_FWHM, tof_n_std=bench.TOF_NSTD, num_rays=4,
+            threads=os.cpu_count() or 1)
+        out["cpu_baseline"] = {"value": m / sec, "unit": "events/s",
+                               "cores": os.cpu_count(), "kind": "reference",
+                               "sample": f"{m} events of the workload, one 4-ray OSEM "
+                                         "iteration x 10 subsets (includes the "
+                                         "reference's correction precompute)"}
+    return out
+
+
 RUNNERS = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5,
-           "psf": run_psf, "lrem": run_lrem}
+           "psf": run_psf, "lrem": run_lrem, "c2mr": run_c2mr}

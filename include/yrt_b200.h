@@ -250,6 +250,17 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 yrtb_status yrtb_multiray_offsets(yrtb_projector* h, uint64_t count,
                                   float* d_out, yrtb_stream stream);
 
+/* Builds (or grows to count item indices) a table of those offsets that the
+ * projector keeps: multi-ray projections of a range then read item k's
+ * offsets from it when k < count, instead of deriving the generator state
+ * for subsequence k per event and per walk (the reference device path calls
+ * curand_init per event, SiddonKernels.cuh:27-84).  Same values, so the same
+ * projections.  Allocates count * 16 * (num_rays - 1) bytes and synchronises
+ * the device when it grows; no-op for single-ray projectors or when the
+ * table already covers count.  Without a table the generator is used. */
+yrtb_status yrtb_multiray_table(yrtb_projector* h, uint64_t count,
+                                yrtb_stream stream);
+
 /* d_out[e] = (A x)_e for every event e of the range (entries of other events
  * untouched).  Replaces OperatorProjectorDevice::applyA
  * (src/operators/OperatorProjectorDevice.cu:442-544) with the kernels of

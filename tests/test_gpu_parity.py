@@ -240,6 +240,28 @@ def test_multiray_vs_oracle_with_device_offsets():
     assert rel_l2(b, bref) < 1e-5
 
 
+def test_multiray_table_gives_the_same_projections():
+    # yrtb_multiray_table: item indices below the table's size read their
+    # offsets from it, the others still derive them from the generator; the
+    # uniforms are the same, so the forward projections are bit-identical and
+    # the EM image equal up to the order of the FP32 atomics.
+    sc, ip, p = make(num_rays=4, tof=(214.0, 5))
+    _, _, q = make(num_rays=4, tof=(214.0, 5))
+    d1, d2 = random_events(SC_ARGS, 5000, 31)
+    rng = np.random.default_rng(32)
+    tof = rng.normal(0, 200, len(d1)).astype(np.float32)
+    img = torch.from_numpy(rng.random(ip.shape, dtype=np.float32)).cuda()
+    ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tof)
+    v0 = p.forward(img, ev)
+    e0 = p.em_step(img, torch.zeros(ip.shape, device="cuda"), ev)
+    q.multiray_table(3000)
+    assert torch.equal(q.forward(img, ev), v0)
+    e1 = q.em_step(img, torch.zeros(ip.shape, device="cuda"), ev)
+    assert rel_l2(e1.cpu().numpy(), e0.cpu().numpy()) < 1e-6
+    q.multiray_table(len(d1))
+    assert torch.equal(q.forward(img, ev), v0)
+
+
 # ---------------------------------------------------------------- DD ------
 @pytest.mark.parametrize("tof,psf,prec", [(None, False, L.YRTB_MIRROR),
                                           ((214.0, 5), False, L.YRTB_MIRROR),

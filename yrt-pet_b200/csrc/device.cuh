@@ -592,6 +592,12 @@ struct MultiRay
 	                                     float3 n2)
 	{
 		curand_init(13ULL, id, 0ULL, &state);
+		setDirs(n1, n2);
+	}
+	// Transverse offset directions of both crystals (without the generator,
+	// for offsets read from a table).
+	__device__ __forceinline__ void setDirs(float3 n1, float3 n2)
+	{
 		// cross(n, z) normalised with norm3df, as the reference device code.
 		t1 = make_float3(n1.y * 1.f - n1.z * 0.f, n1.z * 0.f - n1.x * 1.f,
 		                 n1.x * 0.f - n1.y * 0.f);

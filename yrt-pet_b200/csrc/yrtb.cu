@@ -282,6 +282,10 @@ struct KParams
 	Psf psf;
 	Scan scan;
 	int numRays;
+	// Multi-ray offsets of item indices 0 .. mrCount-1 (4 (numRays - 1)
+	// uniforms each, as MultiRay::next draws them), or null.
+	const float* mrTable;
+	uint64_t mrCount;
 };
 
 // Endpoints (relative to the image centre) and orientations of event e.
@@ -360,15 +364,34 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
 	}
 	else if constexpr (KIND == K_SIDDON_MR)
 	{
+		// The offsets come from the projector's table when it covers this
+		// item index (same values), else from the generator.
 		MultiRay mr;
-		mr.init(rid, n1, n2);
+		const bool tab = P.mrTable != nullptr && rid < P.mrCount;
+		if (tab)
+			mr.setDirs(n1, n2);
+		else
+			mr.init(rid, n1, n2);
+		const float* tu = tab ? P.mrTable + rid * 4 * static_cast<uint64_t>(P.numRays - 1)
+		                      : nullptr;
 		for (int k = 0; k < P.numRays; k++)
 		{
 			float3 a = p1, b = p2;
 			if (k > 0)
 			{
 				float u[4];
-				mr.next(u);
+				if (tab)
+				{
+					const float4 t = __ldg(reinterpret_cast<const float4*>(tu) + (k - 1));
+					u[0] = t.x;
+					u[1] = t.y;
+					u[2] = t.z;
+					u[3] = t.w;
+				}
+				else
+				{
+					mr.next(u);
+				}
 				mr.offset(u, P.scan.crystalZ, P.scan.crystalTrans, a, b);
 			}
 			siddonWalk<TOF, COMP>(P.g, a, b, P.tof, tofv, visit);
@@ -2233,6 +2256,9 @@ struct yrtb_projector
 	int32_t* d_ring = nullptr;
 	int2* d_z = nullptr;
 	unsigned long long* d_err = nullptr;
+	// Multi-ray offset table (yrtb_multiray_table): capacity in item indices.
+	float* d_mrTable = nullptr;
+	uint64_t mrCapacity = 0;
 	// Launch configuration of the single-ray Siddon event kernels.
 	yrtb_launch_config launch{256, 1, 3, YRTB_ORDER_LOR, 1, 2};
 	// Deterministic back projection: fixed-point image (nvox * nt) and bound.
@@ -2254,6 +2280,7 @@ struct yrtb_projector
 		cudaFree(d_ring);
 		cudaFree(d_z);
 		cudaFree(d_err);
+		cudaFree(d_mrTable);
 	}
 };
 
@@ -2880,6 +2907,8 @@ yrtb_status yrtb_projector_create(const yrtb_scanner* s, const float* lut,
 	P.scan.crystalZ = s->crystal_size_z;
 	P.scan.crystalTrans = s->crystal_size_trans;
 	P.numRays = pp->num_rays;
+	P.mrTable = nullptr;
+	P.mrCount = 0;
 	h->hasTof = pp->tof_fwhm_ps > 0.f;
 	if (h->hasTof)
 	{
@@ -3030,6 +3059,33 @@ yrtb_status yrtb_multiray_offsets(yrtb_projector* h, uint64_t count,
 	                     reinterpret_cast<cudaStream_t>(stream)>>>(
 	    count, h->P.numRays, d_out);
 	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_multiray_table(yrtb_projector* h, uint64_t count,
+                                yrtb_stream stream)
+{
+	if (!h)
+		return fail(YRTB_ERR_ARGUMENT, "null projector");
+	if (h->P.numRays < 2 || count <= h->mrCapacity)
+		return YRTB_OK;
+	YRTB_CUDA(cudaSetDevice(h->device));
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	// Launches already queued may still read the old table.
+	YRTB_CUDA(cudaDeviceSynchronize());
+	h->P.mrTable = nullptr;
+	h->P.mrCount = 0;
+	YRTB_CUDA(cudaFree(h->d_mrTable));
+	h->d_mrTable = nullptr;
+	h->mrCapacity = 0;
+	const uint64_t per = 4 * static_cast<uint64_t>(h->P.numRays - 1);
+	YRTB_CUDA(cudaMalloc(&h->d_mrTable, count * per * sizeof(float)));
+	k_multiray_offsets<<<gridAll(count), kBlock, 0, st>>>(count, h->P.numRays,
+	                                                       h->d_mrTable);
+	YRTB_LAUNCHED();
+	h->mrCapacity = count;
+	h->P.mrTable = h->d_mrTable;
+	h->P.mrCount = count;
 	return YRTB_OK;
 }
 

@@ -109,6 +109,7 @@ SIGNATURES = {
     "yrtb_autotune": ([c_vp, c_vp, _P(yrtb_events), ctypes.c_int, c_u64,
                        _P(yrtb_tune_report), c_vp], ctypes.c_int),
     "yrtb_multiray_offsets": ([c_vp, c_u64, c_vp, c_vp], ctypes.c_int),
+    "yrtb_multiray_table": ([c_vp, c_u64, c_vp], ctypes.c_int),
     "yrtb_forward": ([c_vp, c_vp, _P(yrtb_events), yrtb_range, c_vp, c_vp],
                      ctypes.c_int),
     "yrtb_backward": ([c_vp, c_vp, _P(yrtb_events), yrtb_range, c_vp, c_vp],

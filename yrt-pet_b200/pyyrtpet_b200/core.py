@@ -711,6 +711,12 @@ class DeviceProjector:
                                                   _stream()))
         return out
 
+    def multiray_table(self, count: int):
+        """Keep the multi-ray offsets of item indices 0..count-1 in a table
+        (yrtb_multiray_table): later projections read them instead of
+        re-deriving the generator per event; same values."""
+        L.check(L.lib().yrtb_multiray_table(self.h, int(count), _stream()))
+
     def take_event_errors(self) -> int:
         n = ctypes.c_uint64()
         L.check(L.lib().yrtb_projector_take_event_errors(self.h, ctypes.byref(n)))

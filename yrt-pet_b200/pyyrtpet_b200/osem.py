@@ -326,6 +326,11 @@ class OSEM_GPU:
         proj = DeviceProjector(self.scanner, ip, self.projectorParams)
         ev, offsets = self._listmode_events(
             proj, lm, self.num_OSEM_subsets if self.orderEvents else 0)
+        if self.projectorParams.numRays > 1:
+            # Multi-ray offsets of every item index a subset call uses, drawn
+            # once for the whole reconstruction.
+            S = self.num_OSEM_subsets
+            proj.multiray_table((ev.count + S - 1) // S)
         J = ip.numVoxels
         img = torch.empty(nt * J, dtype=torch.float32, device="cuda")
         init = 0
