@@ -69,7 +69,7 @@ def parse():
                     help="c2 (default) is the headline workload; the others "
                          "run bench_configs.py")
     ap.add_argument("--cfg-events", type=int, default=0,
-                    help="override the event count of --config c1/c3/c4/c5")
+                    help="override the event count of --config c1/c2mr/c3/c4/c5")
     return ap.parse_args()
 
 
