@@ -87,6 +87,25 @@ def test_histogram_maps_bitexact():
     assert np.array_equal(g1, o1) and np.array_equal(g2, o2)
 
 
+def test_histogram_maps_random_scanners_bitexact():
+    # The device maps equal the oracle's on every bin and on random detector
+    # pairs of the 25 random scanners whose properties (and agreement with the
+    # reference library) tests/test_histo3d_props.py checks.
+    from test_histo3d_props import SCANNERS, all_bins
+    for i, o in enumerate(SCANNERS):
+        sc = yrt.Scanner("r", o.axialFOV, o.crystalSize_z, o.crystalSize_trans,
+                         o.crystalDepth, o.scannerRadius, o.detsPerRing, o.numRings,
+                         o.numDOI, o.maxRingDiff, o.minAngDiff, o.detsPerBlock)
+        bins = all_bins(o)
+        g1, g2 = yrt.histo3d_detpairs(sc, bins)
+        o1, o2 = po.histo3d_detpairs(o, bins)
+        assert np.array_equal(g1, o1) and np.array_equal(g2, o2)
+        rng = np.random.default_rng(100 + i)
+        q1 = rng.integers(0, o.num_dets, 20000).astype(np.uint32)
+        q2 = rng.integers(0, o.num_dets, 20000).astype(np.uint32)
+        assert np.array_equal(yrt.histo3d_bins(sc, q1, q2), po.histo3d_bins(o, q1, q2))
+
+
 def test_listmode_to_histogram_bitexact():
     sc, ip, p = make()
     d1, d2 = random_events(SC_ARGS, 300000, 3)
