@@ -676,7 +676,8 @@ __device__ __forceinline__ float groupSum(float v)
 // deterministic back projection.
 template <int OP, int KIND, bool TOF, bool COMP, bool FIX = false,
           int BLOCK = kBlock, int TPL = 1, int VEC = 0>
-__global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK : 1)
+__global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK
+                                                         : (KIND == K_SIDDON_MR ? 768 / BLOCK : 1))
     k_events(KParams P, Events E, Range R, const float* __restrict__ in,
              float* __restrict__ out, float globalScale, float denomThr,
              unsigned long long* err, Fixed F)
