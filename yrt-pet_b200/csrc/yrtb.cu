@@ -990,7 +990,7 @@ __global__ void k_att_keys(KParams P, Geom mu, Events E, Range R,
 // Attenuation factor per event: exp(-0.1 * line integral of mu), walked with
 // the projector's arithmetic (COMP: compensated walk).
 template <bool COMP>
-__global__ void __launch_bounds__(kBlock, 8)
+__global__ void __launch_bounds__(kBlock, 6)
     k_attenuation(KParams P, Geom mu, Events E, Range R,
                   const float* __restrict__ muImg, const int* __restrict__ box,
                   float* __restrict__ out, unsigned long long* err,
