@@ -10,6 +10,13 @@ and to time the CPU baseline (``bench.py``):
   compiled from its own sources by ``oracle/ref.mk`` (present only where that
   recipe ran).
 
+and, on a machine with a GPU, the reference's own CUDA path:
+
+* ``_ref_cuda/libyrtref_gpu_harness.so`` -- the same harness built by
+  ``oracle/ref_cuda.mk`` against the reference compiled with BUILD_CUDA for
+  sm_100a; its OSEM and list-mode projection entry points run OSEM_GPU and
+  OperatorProjectorDevice (the functions below take ``gpu=True``).
+
 The product package never imports this module.
 """
 from __future__ import annotations
@@ -23,6 +30,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libyrtref_harness.so")
+REF_GPU_SO = os.path.join(HERE, "_ref_cuda", "libyrtref_gpu_harness.so")
 
 
 class ScannerDesc(ctypes.Structure):
@@ -131,6 +139,7 @@ def _c(a, dtype):
 
 _oracle = None
 _ref = None
+_ref_gpu = None
 
 
 def oracle_lib():
@@ -145,17 +154,32 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
-def ref_lib():
-    global _ref
+def _setup_ref(lib):
+    lib.ref_dd_overlap.restype = ctypes.c_float
+    lib.ref_dd_overlap.argtypes = [ctypes.c_float] * 4
+    lib.ref_last_error.restype = ctypes.c_char_p
+    lib.ref_tof.argtypes = [ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                            ctypes.c_float, ctypes.c_float,
+                            ctypes.c_float, ctypes.c_void_p]
+    return lib
+
+
+def ref_lib(gpu: bool = False):
+    """The reference harness: the CPU build, or with gpu=True the build whose
+    OSEM and list-mode projections run the reference's CUDA path."""
+    global _ref, _ref_gpu
+    if gpu:
+        if _ref_gpu is None:
+            _ref_gpu = _setup_ref(ctypes.CDLL(REF_GPU_SO))
+            assert _ref_gpu.ref_uses_gpu() == 1
+        return _ref_gpu
     if _ref is None:
-        _ref = ctypes.CDLL(REF_SO)
-        _ref.ref_dd_overlap.restype = ctypes.c_float
-        _ref.ref_dd_overlap.argtypes = [ctypes.c_float] * 4
-        _ref.ref_last_error.restype = ctypes.c_char_p
-        _ref.ref_tof.argtypes = [ctypes.c_float, ctypes.c_int, ctypes.c_float,
-                                 ctypes.c_float, ctypes.c_float,
-                                 ctypes.c_float, ctypes.c_void_p]
+        _ref = _setup_ref(ctypes.CDLL(REF_SO))
     return _ref
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
 
 
 class _StdoutToStderr:
@@ -185,9 +209,9 @@ def quiet():
     return _StdoutToStderr()
 
 
-def _ref_check(rc):
+def _ref_check(rc, gpu: bool = False):
     if rc != 0:
-        raise RuntimeError(ref_lib().ref_last_error().decode())
+        raise RuntimeError(ref_lib(gpu).ref_last_error().decode())
 
 
 @dataclass
@@ -492,7 +516,7 @@ def _osem_desc(projector="S", num_rays=1, tof_fwhm_ps=0.0, tof_n_std=0,
 
 def ref_sensitivity(sc: Scanner, ip: ImageParams, *, sens_histo=None,
                     att_params: ImageParams | None = None, att_image=None,
-                    psf_csv=None, **kw):
+                    psf_csv=None, gpu: bool = False, **kw):
     o = _osem_desc(**kw)
     nsub = 1 if o.listmode else o.subsets
     out = np.zeros((nsub, ip.nz, ip.ny, ip.nx), np.float32)
@@ -500,19 +524,19 @@ def ref_sensitivity(sc: Scanner, ip: ImageParams, *, sens_histo=None,
     sh = _c(sens_histo, np.float32)
     att = _c(att_image, np.float32)
     with quiet():
-        rc = ref_lib().ref_sensitivity(
+        rc = ref_lib(gpu).ref_sensitivity(
             ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
             _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
             _p(att), None if psf_csv is None else psf_csv.encode(), _p(out),
             ctypes.byref(sec))
-    _ref_check(rc)
+    _ref_check(rc, gpu)
     return out, sec.value
 
 
 def ref_osem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, *, tof=None,
                       randoms=None, sens_histo=None,
                       att_params: ImageParams | None = None, att_image=None,
-                      **kw):
+                      gpu: bool = False, **kw):
     o = _osem_desc(**kw)
     out = np.zeros(ip.shape, np.float32)
     sec = ctypes.c_double()
@@ -524,18 +548,18 @@ def ref_osem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, *, tof=None,
     att = _c(att_image, np.float32)
     s = _c(sens, np.float32)
     with quiet():
-        rc = ref_lib().ref_osem_listmode(
+        rc = ref_lib(gpu).ref_osem_listmode(
             ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
             _p(s), ctypes.c_uint64(len(d1)), _p(d1), _p(d2), _p(tof), _p(randoms),
             _p(sh), None if att_params is None else ctypes.byref(att_params.desc()),
             _p(att), _p(out), ctypes.byref(sec))
-    _ref_check(rc)
+    _ref_check(rc, gpu)
     return out, sec.value
 
 
 def ref_osem_listmode_dynamic(sc: Scanner, ip: ImageParams, sens, d1, d2,
                               timestamps, *, frame_ts=None, motion_starts=None,
-                              motion=None, tof=None, **kw):
+                              motion=None, tof=None, gpu: bool = False, **kw):
     """Reference OSEM with DynamicFraming and/or LORMotion; ip.nt must equal
     the number of dynamic frames (len(frame_ts) - 1)."""
     o = _osem_desc(**kw)
@@ -555,28 +579,55 @@ def ref_osem_listmode_dynamic(sc: Scanner, ip: ImageParams, sens, d1, d2,
                  None if ms is None else ms.ctypes.data,
                  None if mo is None else mo.ctypes.data)
     with quiet():
-        rc = ref_lib().ref_osem_listmode_ex(
+        rc = ref_lib(gpu).ref_osem_listmode_ex(
             ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
             _p(s), ctypes.c_uint64(len(d1)), _p(d1), _p(d2), _p(tof), None,
             None, None, None, ctypes.byref(ex), _p(out), ctypes.byref(sec))
-    _ref_check(rc)
+    _ref_check(rc, gpu)
     return out, sec.value
 
 
 def ref_osem_histo3d(sc: Scanner, ip: ImageParams, sens_images, histo, *,
-                     psf_csv=None, **kw):
+                     psf_csv=None, gpu: bool = False, **kw):
     o = _osem_desc(listmode=False, **kw)
     out = np.zeros((ip.nz, ip.ny, ip.nx), np.float32)
     sec = ctypes.c_double()
     s = _c(sens_images, np.float32)
     h = _c(histo, np.float32)
     with quiet():
-        rc = ref_lib().ref_osem_histo3d(
+        rc = ref_lib(gpu).ref_osem_histo3d(
             ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), ctypes.byref(o),
             _p(s), _p(h), None if psf_csv is None else psf_csv.encode(), _p(out),
             ctypes.byref(sec))
-    _ref_check(rc)
+    _ref_check(rc, gpu)
     return out, sec.value
+
+
+def ref_project_lm(sc: Scanner, ip: ImageParams, d1, d2, *, tof=None,
+                   image=None, values=None, fwd=True, psf_csv=None,
+                   gpu: bool = False, **kw):
+    """List-mode forward (values = A x) or back projection (image + A^T v)
+    through the reference's util::forwProject / util::backProject, on its CPU
+    projector or, with gpu=True, on OperatorProjectorDevice (its CUDA
+    kernels).  kw: projector ("S" / "DD"), num_rays, tof_fwhm_ps, tof_n_std,
+    threads."""
+    o = _osem_desc(**kw)
+    d1 = _c(d1, np.uint32)
+    d2 = _c(d2, np.uint32)
+    n = len(d1)
+    tof = _c(tof, np.float32)
+    img = (np.zeros(ip.shape, np.float32) if image is None
+           else np.ascontiguousarray(image, np.float32).copy())
+    vals = (np.zeros(n, np.float32) if values is None
+            else np.ascontiguousarray(values, np.float32).copy())
+    with quiet():
+        rc = ref_lib(gpu).ref_project_lm(
+            ctypes.byref(sc.desc()), ctypes.byref(ip.desc()), _p(img),
+            ctypes.c_uint64(n), _p(d1), _p(d2), _p(tof), ctypes.byref(o),
+            None if psf_csv is None else psf_csv.encode(), ctypes.c_int(int(fwd)),
+            _p(vals))
+    _ref_check(rc, gpu)
+    return vals if fwd else img
 
 
 # ------------------------------------------------------ image-space PSF ---

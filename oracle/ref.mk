@@ -2,13 +2,14 @@
 # g++, without its CMake project, into oracle/_ref/.  Test infrastructure only:
 # the outputs check results and give the timed CPU baseline, never the product.
 #
-#   make -f oracle/ref.mk -j8 REF=/root/reference/yrt-pet
+#   make -f oracle/ref.mk -j8 REF=<yrt-pet source tree> JSON_HPP=<nlohmann/json.hpp>
 #
 # Needs: g++ (C++20), zlib headers + libz, and the header-only nlohmann/json
-# (the copy that ships inside the image's cudnn_frontend wheel is used).
-REF      ?= /root/reference/yrt-pet
+# 3.11 (JSON_HPP; only read when oracle/_ref/include does not hold it yet).
+ifndef REF
+$(error REF=<path of the yrt-pet source tree> is required)
+endif
 OUT      ?= oracle/_ref
-JSON_HPP ?= $(firstword $(wildcard /opt/prime-rl/.venv/lib/python3.12/site-packages/include/cudnn_frontend/thirdparty/nlohmann/json.hpp))
 CXX      ?= g++
 # Same flags as the reference's Release build (-O3, no -march, C++20, -fPIC).
 CXXFLAGS := -O3 -std=c++20 -fPIC -DHAVE_ZLIB -w -I$(REF)/include -I$(OUT)/include
@@ -19,6 +20,9 @@ OBJS := $(patsubst $(REF)/src/%.cpp,$(OUT)/obj/%.o,$(SRCS))
 all: $(OUT)/libyrtref.a $(OUT)/libyrtref_harness.so
 
 $(OUT)/include/nlohmann/json.hpp:
+ifndef JSON_HPP
+	$(error JSON_HPP=<path of nlohmann/json.hpp 3.11> is required)
+endif
 	@mkdir -p $(OUT)/include/nlohmann $(OUT)/include/yrt-pet
 	cp $(JSON_HPP) $@
 	printf '#pragma once\n#include "json.hpp"\n' > $(OUT)/include/nlohmann/json_fwd.hpp

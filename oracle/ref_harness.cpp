@@ -1,10 +1,21 @@
 // Test infrastructure, not product code.
 //
 // C-ABI harness over the YRT-PET 2.0.7 reference library compiled from its own
-// sources by oracle/ref.mk.  Every entry point drives the reference's public
-// C++ API on plain arrays so that tests and the CPU-baseline leg of bench.py
-// can run the reference itself on the same inputs as the CUDA path.  Nothing
-// here is linked into or called by the product library.
+// sources.  Every entry point drives the reference's public C++ API on plain
+// arrays so that tests and the CPU-baseline leg of bench.py can run the
+// reference itself on the same inputs as the CUDA path.  Nothing here is
+// linked into or called by the product library.
+//
+// The file is built twice:
+//   oracle/ref.mk       -> oracle/_ref/libyrtref_harness.so, against the CPU
+//                          library (OSEM entry points create OSEM_CPU, the
+//                          list-mode projection runs OperatorProjector);
+//   oracle/ref_cuda.mk  -> oracle/_ref_cuda/libyrtref_gpu_harness.so, with
+//                          REF_HARNESS_GPU defined, against the library built
+//                          with BUILD_CUDA: the same OSEM and list-mode
+//                          projection entry points run the reference's GPU
+//                          path (OSEM_GPU, OperatorProjectorDevice and its
+//                          CUDA kernels).
 //
 // Reference interfaces exercised (paths inside the yrt-pet project):
 //   Scanner ctor + DetRegular LUT   src/datastruct/scanner/Scanner.cpp:102-127,
@@ -23,6 +34,7 @@
 #include "yrt-pet/datastruct/projection/LORMotion.hpp"
 #include "yrt-pet/datastruct/projection/Histogram3D.hpp"
 #include "yrt-pet/datastruct/projection/ListModeLUT.hpp"
+#include "yrt-pet/datastruct/projection/ProjectionList.hpp"
 #include "yrt-pet/datastruct/projection/UniformHistogram.hpp"
 #include "yrt-pet/datastruct/scanner/Scanner.hpp"
 #include "yrt-pet/operators/OperatorPsf.hpp"
@@ -46,6 +58,12 @@
 #include <vector>
 
 using namespace yrt;
+
+#ifdef REF_HARNESS_GPU
+constexpr bool kUseGPU = true;
+#else
+constexpr bool kUseGPU = false;
+#endif
 
 extern "C" {
 
@@ -507,7 +525,7 @@ int ref_sensitivity(const ref_scanner_desc* s, const ref_image_desc* d,
 	    {
 		    auto sc = makeScanner(s);
 		    globals::setNumThreads(o->threads);
-		    auto osem = util::createOSEM(*sc, false);
+		    auto osem = util::createOSEM(*sc, kUseGPU);
 		    osem->setImageParams(makeParams(d));
 		    osem->num_OSEM_subsets = o->subsets;
 		    osem->num_MLEM_iterations = o->iterations;
@@ -613,7 +631,7 @@ int ref_osem_listmode_ex(const ref_scanner_desc* s, const ref_image_desc* d,
 			    }
 			    lm.addLORMotion(mot);
 		    }
-		    auto osem = util::createOSEM(*sc, false);
+		    auto osem = util::createOSEM(*sc, kUseGPU);
 		    ImageParams ip = makeParams(d);
 		    osem->setImageParams(ip);
 		    osem->num_OSEM_subsets = o->subsets;
@@ -687,7 +705,7 @@ int ref_osem_histo3d(const ref_scanner_desc* s, const ref_image_desc* d,
 		    h.allocate();
 		    std::memcpy(h.getData().getRawPointer(), histo,
 		                h.count() * sizeof(float));
-		    auto osem = util::createOSEM(*sc, false);
+		    auto osem = util::createOSEM(*sc, kUseGPU);
 		    osem->setImageParams(makeParams(d));
 		    osem->num_OSEM_subsets = o->subsets;
 		    osem->num_MLEM_iterations = o->iterations;
@@ -717,6 +735,68 @@ int ref_osem_histo3d(const ref_scanner_desc* s, const ref_image_desc* d,
 		    if (seconds)
 			    *seconds = std::chrono::duration<double>(t1 - t0).count();
 		    std::memcpy(out, res->getRawPointer(), nv * sizeof(float));
+	    });
+}
+
+// 1 when this build runs the reference's GPU path.
+int ref_uses_gpu() { return kUseGPU ? 1 : 0; }
+
+// Forward (fwd=1: values[i] = A_i x) or back projection (fwd=0: image +=
+// A^T values) of n list-mode events (detector pairs, optional TOF in ps)
+// through util::forwProject / util::backProject
+// (src/utils/ReconstructionUtils.cpp:948-1061) with one subset: the
+// reference's OperatorProjector on the CPU build, OperatorProjectorDevice and
+// its CUDA kernels (projectSiddon_kernel, projectDD_kernel) on the GPU build.
+// o gives the projector (Siddon / DD), the number of rays, TOF and the host
+// threads; psf_csv (nullable) a projection-space PSF.  On the GPU path the
+// multi-ray offsets of event i are drawn with curand_init(13, i, 0)
+// (include/yrt-pet/operators/SiddonKernels.cuh:27-84, 502-574) when all
+// events fit one batch.
+int ref_project_lm(const ref_scanner_desc* s, const ref_image_desc* d,
+                   float* image, uint64_t n, const uint32_t* d1,
+                   const uint32_t* d2, const float* tof, const ref_osem_desc* o,
+                   const char* psf_csv, int fwd, float* values)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    globals::setNumThreads(o->threads);
+		    ListModeLUTOwned lm(*sc, tof != nullptr, false);
+		    lm.allocate(n);
+		    for (uint64_t i = 0; i < n; i++)
+		    {
+			    lm.setDetectorIdsOfEvent(i, d1[i], d2[i]);
+			    if (tof)
+				    lm.setTOFValueOfEvent(i, tof[i]);
+		    }
+		    ProjectionListOwned pl(&lm);
+		    pl.allocate();
+		    if (fwd)
+			    pl.clearProjections(0.0f);
+		    else
+			    std::memcpy(pl.getRawPointer(), values, n * sizeof(float));
+		    ProjectorParams pp(*sc);
+		    pp.projectorType =
+		        o->projector == 0 ? ProjectorType::SIDDON : ProjectorType::DD;
+		    pp.numRays = o->num_rays;
+		    if (o->tof_fwhm_ps > 0)
+			    pp.addTOF(o->tof_fwhm_ps, o->tof_n_std);
+		    if (psf_csv && psf_csv[0])
+			    pp.projPsf_fname = psf_csv;
+		    auto img = makeImage(d, image);
+		    const auto binIter = pl.getBinIter(1, 0);
+		    if (fwd)
+		    {
+			    util::forwProject(*img, pl, pp, *binIter, kUseGPU);
+			    std::memcpy(values, pl.getRawPointer(), n * sizeof(float));
+		    }
+		    else
+		    {
+			    util::backProject(*img, pl, pp, *binIter, kUseGPU);
+			    const size_t nv = d->nx * d->ny * d->nz * d->nt;
+			    std::memcpy(image, img->getRawPointer(), nv * sizeof(float));
+		    }
 	    });
 }
 
