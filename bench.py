@@ -12,6 +12,12 @@ reconstructions (3 iterations x 10 subsets) through the public OSEM API from
 pinned host event arrays (H2D of the events, event ordering, correction
 factors on device and D2H of the image inside the timed region).
 
+Beside the timed line, on one GPU: the reference's own GPU reconstruction
+(YRT-PET OSEM_GPU built for sm_100a from its sources) of the same 50M events
+(`plain_reference_gpu`), the reference CPU reconstruction of a sample
+(`cpu_baseline`), and the image error of this path against both
+(`parity_vs_reference`).
+
     python bench.py [--gpus N] [--steps K] [--warmup W]
     python bench.py --impl reference     # reference CPU OSEM on a sample
 """
@@ -54,7 +60,10 @@ def parse():
     ap.add_argument("--events", type=int, default=NUM_EVENTS)
     ap.add_argument("--ref-sample", type=int, default=1_000_000)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the parity and reference legs")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference OSEM_GPU leg")
     ap.add_argument("--precision", default="compensated",
                     choices=["mirror", "compensated"])
     ap.add_argument("--parity-sample", type=int, default=200_000)
@@ -74,10 +83,15 @@ def parse():
 
 
 # ----------------------------------------------------------------- workload --
-def build_workload(n_events, device, seed=SEED):
+def build_workload(n_events, device, seed=SEED, lut=None):
+    """C2 scanner, image, phantom, crystal efficiencies, events, mu-map.
+    lut (optional): the crystal LUT to use instead of this library's
+    DetRegular LUT (the reference arm passes the reference's own, so that it
+    never loads the product library; the two are bit-identical)."""
     from pyyrtpet_b200 import synthetic as S
-    import pyyrtpet_b200 as yrt
     sc = S.scanner_c2()
+    if lut is not None:
+        sc.setDetectorLUT(lut)
     ip = S.image_c2()
     ph = S.Phantom(cyl_half_length=sc.axialFOV / 2)
     eff = S.crystal_efficiencies(sc, seed + 1, device=device)
@@ -86,6 +100,54 @@ def build_workload(n_events, device, seed=SEED):
                            randoms_fraction=0.2, device=device)
     mu = ph.mu_image(ip, device=device)
     return sc, ip, ph, eff, ev, mu
+
+
+def additive_per_event(sc, n_events):
+    """Flat randoms estimate per event: 20 % of the prompts spread uniformly
+    over the LORs (about 45 % of all crystal pairs have a histogram bin)."""
+    n_rand_lors = float(sc.getNumDets()) ** 2 / 2 * 0.45
+    return 0.2 * n_events / n_rand_lors
+
+
+def common_config(world, n_events, sample_events):
+    """The workload as both arms state it (identical dicts)."""
+    return {"workload": WORKLOAD, "events_per_gpu": n_events,
+            "subsets": SUBSETS, "iterations_per_reconstruction": ITERATIONS,
+            "corrections": "LOR sensitivity eff1*eff2 (lognormal crystal "
+                           "efficiencies, sigma 0.1), attenuation from the "
+                           "water mu-map, flat 20 % randoms estimate per event",
+            "sensitivity_image": "all 1.44e9 Histogram3D bins, eff1*eff2 and "
+                                 "attenuation, hard threshold 1.0",
+            "sample_events": sample_events,
+            "l2": "event arrays (1.2 GB) larger than L2; image (42 MB) "
+                  "L2-resident by design",
+            "parallelism": f"dp{world} (events sharded, EM image all-reduced "
+                           "per subset)"}
+
+
+def ref_scanner(po, sc):
+    return po.Scanner(sc.axialFOV, sc.crystalSize_z, sc.crystalSize_trans,
+                      sc.crystalDepth, sc.scannerRadius, sc.detsPerRing,
+                      sc.numRings, sc.numDOI, sc.maxRingDiff, sc.minAngDiff,
+                      sc.detsPerBlock)
+
+
+def ref_image(po, ip):
+    return po.ImageParams(ip.nx, ip.ny, ip.nz, ip.length_x, ip.length_y,
+                          ip.length_z)
+
+
+def loaded_libraries():
+    """Shared libraries of this repository mapped into this process."""
+    out = set()
+    try:
+        for line in open("/proc/self/maps"):
+            path = line.split()[-1] if len(line.split()) >= 6 else ""
+            if path.endswith(".so") and path.startswith(ROOT):
+                out.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
 
 
 def clocks_sampler(path):
@@ -133,108 +195,255 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-# --------------------------------------------------------- reference (CPU) --
-def reference_rate(sc, ip, ev, mu, eff_np, n_sample, threads, iterations=1):
-    """Reference YRT-PET CPU OSEM (oracle/_ref) on a bounded sample of the
-    same workload; returns (events/s, kind, sample description)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as po
-    e = {"d1": ev.d1[:n_sample].cpu().numpy().astype(np.uint32),
-         "d2": ev.d2[:n_sample].cpu().numpy().astype(np.uint32),
-         "tof": ev.tof[:n_sample].cpu().numpy().astype(np.float32)}
-    n = len(e["d1"])
-    osc = po.Scanner(sc.axialFOV, sc.crystalSize_z, sc.crystalSize_trans,
-                     sc.crystalDepth, sc.scannerRadius, sc.detsPerRing,
-                     sc.numRings, sc.numDOI, sc.maxRingDiff, sc.minAngDiff,
-                     sc.detsPerBlock)
-    oip = po.ImageParams(ip.nx, ip.ny, ip.nz, ip.length_x, ip.length_y, ip.length_z)
-    sens = np.ones((ip.nz, ip.ny, ip.nx), np.float32)
-    randoms = np.full(n, 1e-3, np.float32)
-    if po.ref_available():
-        _, sec = po.ref_osem_listmode(
-            osc, oip, sens, e["d1"], e["d2"], tof=e["tof"], randoms=randoms,
-            att_params=oip, att_image=mu.cpu().numpy(), iterations=iterations,
-            subsets=SUBSETS, tof_fwhm_ps=TOF_FWHM, tof_n_std=TOF_NSTD,
-            threads=threads)
-        return n * iterations / sec, "reference", sec
-    # Fallback: the oracle's FP64 EM pass (a port, not the reference).
-    lut = po.scanner_lut(osc)
-    lors, _ = po.lors_from_detpairs(lut, e["d1"], e["d2"])
-    img = np.full((1, ip.nz, ip.ny, ip.nx), 0.125, np.float32)
-    t0 = time.perf_counter()
-    for s in range(SUBSETS):
-        sl = slice(s, n, SUBSETS)
-        po.em_step_f64(po.ImageParams(ip.nx, ip.ny, ip.nz, ip.length_x,
-                                      ip.length_y, ip.length_z),
-                       po.Proj(tof_fwhm_ps=TOF_FWHM, tof_n_std=TOF_NSTD,
-                               threads=threads),
-                       lors[sl], img, tof=e["tof"][sl], additive=randoms[sl])
-    sec = time.perf_counter() - t0
-    return n / sec, "port", sec
+# ------------------------------------------------------------ reference legs --
+def reference_osem(po, sc, ip, d1, d2, tof, additive, sens, sens_histo, mu_np,
+                   threads, gpu):
+    """One reconstruction (ITERATIONS x SUBSETS) of the given events with the
+    reference library: OSEM_CPU (oracle/_ref), or OSEM_GPU (oracle/_ref_cuda)
+    with gpu=True.  Returns (image, seconds of OSEM::reconstruct)."""
+    n = len(d1)
+    randoms = np.full(n, additive, np.float32)
+    oip = ref_image(po, ip)
+    return po.ref_osem_listmode(
+        ref_scanner(po, sc), oip, sens, d1, d2, tof=tof, randoms=randoms,
+        sens_histo=sens_histo, att_params=oip, att_image=mu_np,
+        iterations=ITERATIONS, subsets=SUBSETS, tof_fwhm_ps=TOF_FWHM,
+        tof_n_std=TOF_NSTD, threads=threads, gpu=gpu)
 
 
-def fp64_parity(sc, ip, proj, ev, n_sample, precision):
-    """rel-L2 of this path's forward projections vs the FP64 oracle on the
-    first n_sample events (non-zero random image)."""
+def our_osem(proj, ip, d1, d2, tof, additive, eff, mu_flat, sens):
+    """One reconstruction (ITERATIONS x SUBSETS) of the given device events
+    through the public C ABI, as the end-to-end step does: subset-major
+    ordering, device corrections, yrtb_osem_listmode."""
+    import ctypes
+    import pyyrtpet_b200 as yrt
+    from pyyrtpet_b200 import _lib as L
+    from pyyrtpet_b200.core import _stream
+    e = yrt.DeviceEvents(int(d1.numel()), d1, d2, tof=tof)
+    e.additive = torch.full((e.count,), additive, device="cuda")
+    e, offs = proj.order_events(e, SUBSETS)
+    e.sens = proj.gather_crystal_product(eff, e)
+    e.att = proj.attenuation_factors(mu_flat, ip, e)
+    J = ip.numVoxels
+    x = torch.empty(J, device="cuda")
+    work = torch.empty(2 * J, device="cuda")
+    p = L.yrtb_osem_params(ITERATIONS, SUBSETS, 1.0, 1e-35, 1.19209e-07, 0, 0,
+                           None, offs.ctypes.data)
+    L.check(L.lib().yrtb_osem_listmode(proj.h, ctypes.byref(e.c()),
+                                       sens.data_ptr(), x.data_ptr(),
+                                       work.data_ptr(), ctypes.byref(p),
+                                       _stream()))
+    return x.cpu().numpy().reshape(ip.nz, ip.ny, ip.nx)
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def reference_legs(args, proj, sc, ip, eff, mu, mu_flat, sens, ev_plain,
+                   additive, e2e_image):
+    """The reference library on this run's workload, with this run's
+    sensitivity image (the reference's sensitivity histogram eff1*eff2 is
+    filled through its own bin map):
+    * cpu_baseline: reference OSEM_CPU (oracle/_ref) on the first
+      ref_sample events, timed.  Its image is not compared: with 1M events
+      in 10 subsets most voxels of the 10.5M-voxel image get no crossing in
+      some subset, and 3 iterations take the whole image to 0, in the
+      reference and in this path alike;
+    * plain_reference_gpu: reference OSEM_GPU (oracle/_ref_cuda, built for
+      sm_100a) on all events, timed (OSEM::reconstruct), and the images of
+      the last end-to-end reconstruction (this run's precision) and of a
+      mirror-mode reconstruction of the same events against it;
+    * the reference GPU sensitivity image against this run's."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
     import pyyrtpet_b200 as yrt
+    from pyyrtpet_b200 import _lib as L
+    threads = os.cpu_count() or 1
+    cpu, gpu, par = None, None, {}
+    try:
+        osc = ref_scanner(po, sc)
+        h = po.ref_histo3d_crystal_product(osc, eff.cpu().numpy(), threads)
+        sens_np = sens.reshape(ip.nz, ip.ny, ip.nx).cpu().numpy()
+        mu_np = mu.cpu().numpy()
+        n = min(args.ref_sample, ev_plain.count)
+        to_np = lambda t: t.cpu().numpy()
+        _, sec = reference_osem(po, sc, ip, to_np(ev_plain.d1[:n]).view(np.uint32),
+                                to_np(ev_plain.d2[:n]).view(np.uint32),
+                                to_np(ev_plain.tof[:n]), additive, sens_np, h,
+                                mu_np, threads, gpu=False)
+        cpu = {"value": n * ITERATIONS / sec, "unit": UNIT, "cores": threads,
+               "kind": "reference",
+               "sample": f"the first {n} of the workload's events, one "
+                         f"reconstruction of {ITERATIONS} OSEM iterations x "
+                         f"{SUBSETS} subsets (event-iterations/s)"}
+        if po.ref_gpu_available() and not args.no_ref_gpu:
+            N = ev_plain.count
+            img_g, sec_g = reference_osem(
+                po, sc, ip, to_np(ev_plain.d1).view(np.uint32),
+                to_np(ev_plain.d2).view(np.uint32), to_np(ev_plain.tof),
+                additive, sens_np, h, mu_np, threads, gpu=True)
+            gpu = {"value": N * ITERATIONS / sec_g, "unit": UNIT,
+                   "s_per_reconstruction": sec_g,
+                   "what": f"reference OSEM_GPU (YRT-PET compiled for sm_100a "
+                           f"from its sources) on the same {N} events, "
+                           f"{ITERATIONS} iterations x {SUBSETS} subsets, same "
+                           "sensitivity image and corrections; "
+                           "OSEM::reconstruct time (its per-subset host "
+                           "precompute and copies included), event-iterations/s"}
+            par["events"] = N
+            if e2e_image is not None:
+                par["image_rel_l2_vs_reference_gpu"] = _rel(e2e_image, img_g)
+                par["image_precision"] = args.precision
+            pp = yrt.ProjectorParams(sc)
+            pp.addTOF(TOF_FWHM, TOF_NSTD)
+            pp.precision = L.YRTB_MIRROR
+            pm = yrt.DeviceProjector(sc, ip, pp)
+            mirror = our_osem(pm, ip, ev_plain.d1, ev_plain.d2, ev_plain.tof,
+                              additive, eff, mu_flat, sens)
+            par["mirror_image_rel_l2_vs_reference_gpu"] = _rel(mirror, img_g)
+            if e2e_image is not None:
+                par["image_rel_l2_vs_mirror"] = _rel(e2e_image, mirror)
+            del pm
+            sens_g, _ = po.ref_sensitivity(
+                osc, ref_image(po, ip), listmode=True, sens_histo=h,
+                att_params=ref_image(po, ip), att_image=mu_np, threads=threads,
+                gpu=True)
+            par["sensitivity_rel_l2_vs_reference_gpu"] = _rel(sens_np, sens_g[0])
+    except Exception as exc:  # reported, never silently replaced
+        par["error"] = str(exc)[:300]
+        if cpu is None:
+            cpu = {"value": None, "unit": UNIT, "cores": threads,
+                   "kind": "unavailable", "sample": str(exc)[:200]}
+    return cpu, gpu, par
+
+
+def fp64_parity(sc, ip, proj, ev, n_sample, precision, n_em):
+    """This path against the FP64 oracle on the workload's own events:
+    forward projections of the first n_sample events (random positive
+    image), and one fused EM pass (all corrections) over the first n_em
+    events with the initial image.  With the reference's CUDA library built,
+    also the reference GPU projector's forward projections of the same sample
+    against the same oracle (its own FP32 error)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    import pyyrtpet_b200 as yrt
+    threads = os.cpu_count() or 1
+    osc = ref_scanner(po, sc)
+    oip = ref_image(po, ip)
+    lut = po.scanner_lut(osc)
+    pr = po.Proj(tof_fwhm_ps=TOF_FWHM, tof_n_std=TOF_NSTD, threads=threads)
+    out = {"sample_events": 0, "precision": precision,
+           "oracle": "FP64 restatement (oracle/oracle.cpp)"}
     n = min(n_sample, ev.count)
     g = torch.Generator(device="cuda")
     g.manual_seed(5)
     img = torch.rand(ip.shape, generator=g, device="cuda") + 0.5
     sub = yrt.DeviceEvents(n, ev.d1[:n], ev.d2[:n], tof=ev.tof[:n])
     got = proj.forward(img, sub).double().cpu().numpy()
-    osc = po.Scanner(sc.axialFOV, sc.crystalSize_z, sc.crystalSize_trans,
-                     sc.crystalDepth, sc.scannerRadius, sc.detsPerRing,
-                     sc.numRings, sc.numDOI, sc.maxRingDiff, sc.minAngDiff,
-                     sc.detsPerBlock)
-    lut = po.scanner_lut(osc)
+    d1 = sub.d1.cpu().numpy().view(np.uint32)
+    d2 = sub.d2.cpu().numpy().view(np.uint32)
+    tof = sub.tof.cpu().numpy()
+    lors, _ = po.lors_from_detpairs(lut, d1, d2)
+    img_np = img.cpu().numpy()
+    ref = po.project(oip, pr, lors, image=img_np, tof=tof, precision="f64")
+    out["fwd_rel_l2"] = _rel(got, ref)
+    out["sample_events"] = n
+    if po.ref_gpu_available():
+        rg = po.ref_project_lm(osc, oip, d1, d2, tof=tof, image=img_np,
+                               tof_fwhm_ps=TOF_FWHM, tof_n_std=TOF_NSTD,
+                               threads=threads, gpu=True)
+        out["reference_gpu_fwd_rel_l2"] = _rel(rg, ref)
+    # One EM pass at config scale: the first n_em events (about one subset)
+    # with their sensitivity, attenuation and additive terms, image 0.125.
+    m = min(n_em, ev.count)
+    x = torch.full(ip.shape, 0.125, device="cuda")
+    em = torch.zeros(ip.shape, device="cuda")
+    sub = yrt.DeviceEvents(m, ev.d1[:m], ev.d2[:m], tof=ev.tof[:m])
+    sub.sens, sub.att, sub.additive = ev.sens[:m], ev.att[:m], ev.additive[:m]
+    proj.em_step(x, em, sub)
     d1 = sub.d1.cpu().numpy().view(np.uint32)
     d2 = sub.d2.cpu().numpy().view(np.uint32)
     lors, _ = po.lors_from_detpairs(lut, d1, d2)
-    oip = po.ImageParams(ip.nx, ip.ny, ip.nz, ip.length_x, ip.length_y,
-                         ip.length_z)
-    ref = po.project(oip, po.Proj(tof_fwhm_ps=TOF_FWHM, tof_n_std=TOF_NSTD,
-                                  threads=os.cpu_count() or 1),
-                     lors, image=img.cpu().numpy(), tof=sub.tof.cpu().numpy(),
-                     precision="f64")
-    err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-    return {"fwd_rel_l2": err, "sample_events": n, "precision": precision,
-            "oracle": "FP64 restatement (oracle/oracle.cpp)"}
+    ref_em = po.em_step_f64(oip, pr, lors, x.cpu().numpy(),
+                            tof=sub.tof.cpu().numpy(),
+                            sens=sub.sens.cpu().numpy(), att=sub.att.cpu().numpy(),
+                            additive=sub.additive.cpu().numpy())
+    out["em_pass_rel_l2"] = _rel(em.cpu().numpy(), ref_em)
+    out["em_pass_events"] = m
+    return out
 
 
 def run_reference_arm(args):
+    """The reference's own CPU OSEM (YRT-PET compiled from its sources,
+    oracle/_ref) on a sample of the workload, on all host threads.  The
+    product library is never loaded in this process: the crystal LUT, the
+    sensitivity histogram and the sensitivity image come from the reference
+    (the image from its OSEM_GPU::generateSensitivityImages when
+    oracle/_ref_cuda is built), and the events from the seeded generator
+    (torch only), identical to the B200 arm's."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from pyyrtpet_b200 import synthetic as S
     threads = os.cpu_count() or 1
-    sc, ip, ph, eff, ev, mu = build_workload(max(args.ref_sample, 1000), "cpu")
+    device = "cuda" if torch.cuda.is_available() else "cpu"
+    osc = ref_scanner(po, S.scanner_c2())
+    lut = po.ref_scanner_lut(osc)
+    sc, ip, ph, eff, evs, mu = build_workload(args.events, device, lut=lut)
+    n = min(args.ref_sample, args.events)
+    d1 = evs.d1[:n].cpu().numpy().astype(np.uint32)
+    d2 = evs.d2[:n].cpu().numpy().astype(np.uint32)
+    tof = evs.tof[:n].cpu().numpy().astype(np.float32)
+    del evs
+    mu_np = mu.cpu().numpy()
+    t0 = time.perf_counter()
+    h = po.ref_histo3d_crystal_product(osc, eff.cpu().numpy(), threads=threads)
+    if po.ref_gpu_available() and torch.cuda.is_available():
+        sens, _ = po.ref_sensitivity(osc, ref_image(po, ip), listmode=True,
+                                     sens_histo=h, att_params=ref_image(po, ip),
+                                     att_image=mu_np, threads=threads, gpu=True)
+        sens = sens[0]
+        sens_src = ("reference OSEM_GPU::generateSensitivityImages over all "
+                    "bins (eff1*eff2 histogram, attenuation)")
+    else:
+        sens = np.ones((ip.nz, ip.ny, ip.nx), np.float32)
+        sens_src = "ones (no reference CUDA library or no GPU here)"
+    setup_s = time.perf_counter() - t0
+    add = additive_per_event(sc, args.events)
     rates = []
     for i in range(args.warmup + args.steps):
-        r, kind, sec = reference_rate(sc, ip, ev, mu, None, args.ref_sample,
-                                      threads, ITERATIONS)
+        _, sec = reference_osem(po, sc, ip, d1, d2, tof, add, sens, h, mu_np,
+                                threads, gpu=False)
         if i >= args.warmup:
-            rates.append(r)
+            rates.append(n * ITERATIONS / sec)
     v = float(np.median(rates))
+    libs = loaded_libraries()
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * args.ref_sample * ITERATIONS / v,
+            "ms_per_step": 1e3 * n * ITERATIONS / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded phantom events, C2 shapes)",
             "impl": "reference",
-            "config": {"workload": WORKLOAD,
-                       "sample_events": args.ref_sample, "subsets": SUBSETS},
+            "config": common_config(world, args.events, n),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads,
-                             "kind": kind,
-                             "sample": f"{args.ref_sample} events of the workload, "
+                             "kind": "reference",
+                             "sample": f"the first {n} of the workload's events, "
                                        f"one reconstruction of {ITERATIONS} OSEM "
-                                       f"iterations x {SUBSETS} subsets, in "
-                                       "event-iterations/s (includes the "
+                                       f"iterations x {SUBSETS} subsets per step, "
+                                       "in event-iterations/s (includes the "
                                        "reference's per-reconstruction "
                                        "correction precompute)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "setup": {"sensitivity_image": sens_src, "setup_s": round(setup_s, 2)},
+            "libraries": libs}
+    assert not any("libyrtb" in x for x in libs), libs
     print(json.dumps(line), flush=True)
 
 
@@ -274,28 +483,32 @@ def main():
                     else L.YRTB_MIRROR)
     pp.deterministic = bool(args.deterministic)
     proj = yrt.DeviceProjector(sc, ip, pp)
-    # Correction factors per event, on device (sens = eff1*eff2 histogram
-    # gather is equivalent to the direct product here; ACF via Siddon
-    # through the mu-map; flat additive randoms estimate).
+    # Correction factors per event, on device: LOR sensitivity eff1*eff2
+    # gathered per crystal, ACF via Siddon through the mu-map, flat additive
+    # randoms estimate.
     ev = yrt.DeviceEvents.from_arrays(evs.d1.to(torch.int32), evs.d2.to(torch.int32),
                                       tof=evs.tof)
-    ev.sens = (eff[evs.d1] * eff[evs.d2]).float().contiguous()
+    ev.sens = proj.gather_crystal_product(eff, ev)
     mu_flat = mu.reshape(-1).contiguous()
     ev.att = proj.attenuation_factors(mu_flat, ip, ev)
-    n_rand_lors = float(sc.getNumDets()) ** 2 / 2 * 0.45
-    ev.additive = torch.full((ev.count,), 0.2 * ev.count / n_rand_lors,
-                             device="cuda")
+    additive = additive_per_event(sc, args.events)
+    ev.additive = torch.full((ev.count,), additive, device="cuda")
     torch.cuda.synchronize()
 
     # Sensitivity image (setup only, not timed): back projection of all
-    # 1.44e9 bins of the scanner's histogram, with the attenuation factor of
-    # each bin from the mu-map, in 20 phi-interleaved parts.
+    # 1.44e9 bins of the scanner's histogram, each with its LOR sensitivity
+    # eff1*eff2 and its attenuation factor from the mu-map, in 20
+    # phi-interleaved parts, then the reference's hard threshold (1.0).
     sens_pp = yrt.ProjectorParams(sc)
     sens_proj = yrt.DeviceProjector(sc, ip, sens_pp)
     sens = torch.zeros(ip.numVoxels, device="cuda")
     t_sens = time.perf_counter()
     for part in range(20):
-        sens_proj.sensitivity_histo3d(sens, 20, part, mu=mu_flat, mu_params=ip)
+        sens_proj.sensitivity_histo3d(sens, 20, part, mu=mu_flat, mu_params=ip,
+                                      crystal_eff=eff)
+    L.check(L.lib().yrtb_apply_threshold(sens.data_ptr(), sens.data_ptr(),
+                                         ip.numVoxels, 1, 1, 1.0, 0.0, 0.0,
+                                         1.0, 0.0, _stream()))
     torch.cuda.synchronize()
     sens_setup_s = time.perf_counter() - t_sens
     sens_sub = (sens / SUBSETS).contiguous()
@@ -423,11 +636,14 @@ def main():
     # step k computes (two device buffers); every step's copy is still inside
     # the timed region.
     e2e = None
+    e2e_image = None
     if not args.no_e2e:
         h_d1 = evs.d1.to(torch.int32).cpu().pin_memory()
         h_d2 = evs.d2.to(torch.int32).cpu().pin_memory()
         h_tof = evs.tof.cpu().pin_memory()
-        bufs = [tuple(torch.empty_like(h, device="cuda") for h in (h_d1, h_d2, h_tof))
+        h_add = ev_plain.additive.cpu().pin_memory()
+        host = (h_d1, h_d2, h_tof, h_add)
+        bufs = [tuple(torch.empty_like(h, device="cuda") for h in host)
                 for _ in range(2)]
         h_img = torch.empty(J, dtype=torch.float32).pin_memory()
         eff_d = eff
@@ -441,7 +657,7 @@ def main():
             b = bufs[k % 2]
             copy_stream.wait_event(released[k % 2])  # its previous step is done
             with torch.cuda.stream(copy_stream):
-                for dst, src in zip(b, (h_d1, h_d2, h_tof)):
+                for dst, src in zip(b, host):
                     dst.copy_(src, non_blocking=True)
             copied[k % 2].record(copy_stream)
 
@@ -449,14 +665,14 @@ def main():
             st.wait_event(copied[k % 2])
             if not last:
                 upload(k + 1)
-            d_d1, d_d2, d_tof = bufs[k % 2]
+            d_d1, d_d2, d_tof, d_add = bufs[k % 2]
             e = yrt.DeviceEvents(int(d_d1.numel()), d_d1, d_d2, tof=d_tof)
-            e.additive = ev_plain.additive
+            e.additive = d_add
             # Subset-major order first, then the corrections on the ordered
             # arrays (the attenuation walks run on grouped rays).
             e, offs = proj.order_events(e, SUBSETS)
             released[k % 2].record(st)  # the ordered copy no longer reads it
-            e.sens = (eff_d[e.d1.long()] * eff_d[e.d2.long()]).contiguous()
+            e.sens = proj.gather_crystal_product(eff_d, e)
             e.att = proj.attenuation_factors(mu_flat, ip, e)
             x = torch.full((J,), 0.125, device="cuda")
             if dist is None:
@@ -494,17 +710,20 @@ def main():
             tt = torch.tensor([e2e_ms], device="cuda")
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             e2e_ms = tt.item()
+        e2e_image = h_img.numpy().reshape(ip.nz, ip.ny, ip.nx).copy()
         e2e = {"value": total_events * ITERATIONS / (e2e_ms * 1e-3), "unit": UNIT,
-               "h2d_bytes_per_step": int(h_d1.numel() * 12),
+               "h2d_bytes_per_step": int(sum(h.numel() * h.element_size() for h in host)),
                "d2h_bytes_per_step": int(J * 4), "ms_per_step": e2e_ms,
                "iterations_per_step": ITERATIONS,
                "path": ("yrtb_osem_listmode (C ABI)" if dist is None else
                         "pyyrtpet_b200.distributed.osem_listmode (C ABI EM "
                         "passes, NCCL all-reduce per subset)") + " from pinned host events; "
-                       "per step: H2D events (double-buffered: the next "
-                       "step's copy overlaps this step's compute), event "
-                       "ordering, device corrections, one reconstruction of 3 "
-                       "OSEM iterations x 10 subsets, D2H image"}
+                       "per step: H2D events (detector pairs, TOF, randoms "
+                       "estimate; double-buffered: the next step's copy "
+                       "overlaps this step's compute), event ordering, device "
+                       "corrections (eff1*eff2 gather, attenuation walks), one "
+                       "reconstruction of 3 OSEM iterations x 10 subsets, D2H "
+                       "image"}
 
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes_iter / SUBSETS / (em_ms * 1e-3) / 1e9
@@ -524,26 +743,20 @@ def main():
 
     cpu = None
     parity = None
+    plain_ref_gpu = None
+    par_ref = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        # CPU leg: forward projections of a sample of the workload's events in
-        # this run's precision mode against the FP64 oracle.
+        # Parity and baseline legs (not timed): forward projections of a
+        # sample against the FP64 oracle; then the reference library itself
+        # on the same events with the same sensitivity image and corrections.
         try:
             parity = fp64_parity(sc, ip, proj, ev_plain, args.parity_sample,
-                                 args.precision)
+                                 args.precision, ev_plain.count // SUBSETS)
         except Exception as exc:
             parity = {"error": str(exc)[:200]}
-        try:
-            r, kind, sec = reference_rate(sc, ip, evs, mu, None,
-                                          min(args.ref_sample, ev.count),
-                                          os.cpu_count() or 1, ITERATIONS)
-            cpu = {"value": r, "unit": UNIT, "cores": os.cpu_count(),
-                   "kind": kind,
-                   "sample": f"{min(args.ref_sample, ev.count)} events of this "
-                             f"workload, one reconstruction of {ITERATIONS} OSEM "
-                             f"iterations x {SUBSETS} subsets (event-iterations/s)"}
-        except Exception as exc:  # reported, never silently replaced
-            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
-                   "kind": "unavailable", "sample": str(exc)[:200]}
+        cpu, plain_ref_gpu, par_ref = reference_legs(
+            args, proj, sc, ip, eff, mu, mu_flat, sens, ev_plain, additive,
+            e2e_image)
 
     if rank == 0:
         clocks = summarize_clocks(clk_path, local) if sampler else None
@@ -552,27 +765,21 @@ def main():
                 "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded phantom events, C2 shapes)",
-                "config": {"workload": WORKLOAD,
-                           "events_per_gpu": ev.count, "subsets": SUBSETS,
-                           "precision": args.precision,
-                           "deterministic": bool(args.deterministic),
-                           "launch": launch,
-                           "autotune": None if tune is None else {
-                               "sample_events": tune["sample_events"],
-                               "candidates": len(tune["tried"]),
-                               "best_ms": min(ms for _, ms in tune["tried"]) if tune["tried"] else None,
-                               "default_ms": next((ms for c, ms in tune["tried"]
-                                                   if c == {"block": 256, "threads_per_lor": 1,
-                                                            "bucket_shift": 3, "order": 0,
-                                                            "tile_shift": 1,
-                                                            "vector_groups": 2}), None)},
-                           "sensitivity": {"bins": "all 1.44e9 histogram bins, "
-                                                   "attenuation from the mu-map",
-                                           "setup_s": round(sens_setup_s, 3)},
-                           "l2": "event arrays (1.2 GB) larger than L2; "
-                                 "image (42 MB) L2-resident by design",
-                           "parallelism": f"dp{world} (events sharded, EM image "
-                                          "all-reduced per subset)"},
+                "config": common_config(world, args.events,
+                                        min(args.ref_sample, args.events)),
+                "mode": {"precision": args.precision,
+                         "deterministic": bool(args.deterministic),
+                         "launch": launch,
+                         "autotune": None if tune is None else {
+                             "sample_events": tune["sample_events"],
+                             "candidates": len(tune["tried"]),
+                             "best_ms": min(ms for _, ms in tune["tried"]) if tune["tried"] else None,
+                             "default_ms": next((ms for c, ms in tune["tried"]
+                                                 if c == {"block": 256, "threads_per_lor": 1,
+                                                          "bucket_shift": 3, "order": 0,
+                                                          "tile_shift": 1,
+                                                          "vector_groups": 2}), None)},
+                         "sensitivity_setup_s": round(sens_setup_s, 3)},
                 "gpu_launches": timed_launches,
                 "plain": {"value": total_events / (plain_ms * 1e-3),
                           "ms_per_step": plain_ms,
@@ -581,7 +788,12 @@ def main():
                                   "single-frame batching)"},
                 "osem_s_per_iteration": ms * 1e-3,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "plain_reference_gpu": plain_ref_gpu,
+                "batched_vs_plain_reference_gpu": (
+                    e2e["value"] / plain_ref_gpu["value"]
+                    if e2e and plain_ref_gpu and plain_ref_gpu.get("value") else None),
                 "parity_vs_fp64": parity,
+                "parity_vs_reference": par_ref,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -322,6 +322,19 @@ yrtb_status yrtb_gather_histo3d(yrtb_projector* h, const float* d_histo,
                                 const yrtb_events* ev, yrtb_range range,
                                 int invert, float* d_out, yrtb_stream stream);
 
+/* Per-event LOR sensitivity from per-crystal factors: d_out[e] =
+ * eff[d1] * eff[d2] (FP32), the value a sensitivity Histogram3D filled with
+ * eff[d1] * eff[d2] gives through yrtb_gather_histo3d, without building the
+ * histogram (1.44e9 bins, 5.8 GB on an 80-ring x 672-crystal scanner).  The
+ * reference reads it per bin from its sensitivity histogram
+ * (Corrector::getMultiplicativeCorrectionFactor,
+ * src/recon/Corrector_CPU.cpp:17-45; Corrector.cpp:294-306).  Detector ids
+ * outside the scanner give 0 and are counted in the error counter. */
+yrtb_status yrtb_gather_crystal_product(yrtb_projector* h,
+                                        const float* d_crystal_eff,
+                                        const yrtb_events* ev, yrtb_range range,
+                                        float* d_out, yrtb_stream stream);
+
 /* ------------------------------------------------------- event ordering --- */
 /* Permutation that groups events by OSEM subset (event index mod
  * num_subsets, the reference's chronological interleaving) and, inside a
@@ -362,6 +375,20 @@ yrtb_status yrtb_sensitivity_histo3d(yrtb_projector* h, float* d_sens,
                                      const yrtb_image_params* mu_params,
                                      int num_subsets, int subset,
                                      yrtb_stream stream);
+
+/* The same sensitivity image with each bin's LOR sensitivity formed in the
+ * kernel as d_crystal_eff[d1] * d_crystal_eff[d2] (FP32, bit-identical to a
+ * sensitivity histogram holding those products): the reference's
+ * generateSensImage_kernel over a Histogram3D sensitivity
+ * (src/recon/OSEM_GPU.cu:1048-1157, Corrector_CPU.cpp:17-45) without the
+ * histogram in memory. */
+yrtb_status yrtb_sensitivity_histo3d_crystal(yrtb_projector* h, float* d_sens,
+                                             const float* d_crystal_eff,
+                                             const float* d_acf_histo,
+                                             const float* d_mu,
+                                             const yrtb_image_params* mu_params,
+                                             int num_subsets, int subset,
+                                             yrtb_stream stream);
 
 /* Histogram-mode EM pass over one subset of bins: bins with zero measurement
  * are skipped (OSEM_GPU.cu:1224-1225).  Optional per-bin histograms: sens,

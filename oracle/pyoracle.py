@@ -411,6 +411,17 @@ def ref_histo3d_detpairs(sc: Scanner, bins):
     return d1, d2
 
 
+def ref_histo3d_crystal_product(sc: Scanner, eff, threads=8, gpu=False):
+    """Sensitivity histogram eff[d1] * eff[d2] over every bin, through the
+    reference's Histogram3D bin -> detector-pair map."""
+    nz, nphi, nr = ref_histo3d_dims(sc)
+    out = np.empty(int(nz) * int(nphi) * int(nr), np.float32)
+    e = _c(eff, np.float32)
+    _ref_check(ref_lib(gpu).ref_histo3d_crystal_product(
+        ctypes.byref(sc.desc()), _p(e), ctypes.c_int(threads), _p(out)), gpu)
+    return out
+
+
 def ref_tof(fwhm, nstd, lor_norm, tof, lo, hi):
     out = np.zeros(6, np.float32)
     ref_lib().ref_tof(fwhm, nstd, lor_norm, tof, lo, hi, _p(out))

@@ -237,6 +237,27 @@ int ref_histo3d_detpairs(const ref_scanner_desc* s, uint64_t n,
 	    });
 }
 
+// Sensitivity histogram of a normalisation made of crystal factors:
+// out[bin] = eff[d1] * eff[d2] (FP32) for every bin of the scanner's
+// Histogram3D, through the reference's own bin -> detector-pair map
+// (Histogram3D::getDetPairFromBinId), on `threads` host threads.
+int ref_histo3d_crystal_product(const ref_scanner_desc* s, const float* eff,
+                                int threads, float* out)
+{
+	return guarded(
+	    [&]
+	    {
+		    auto sc = makeScanner(s);
+		    Histogram3DOwned h(*sc);
+		    parallelFor(h.count(), threads,
+		                [&](size_t b, int)
+		                {
+			                const det_pair_t p = h.getDetPairFromBinId(b);
+			                out[b] = eff[p.d1] * eff[p.d2];
+		                });
+	    });
+}
+
 int ref_tof(float fwhm_ps, int n_std, float lorNorm, float tof_ps, float lo,
             float hi, float* out /* weight, amin, amax, sigma, trunc, norm */)
 {

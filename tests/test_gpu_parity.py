@@ -565,6 +565,42 @@ def test_graph_and_plain_osem_agree():
     assert rel_l2(outs[0], outs[1]) < 1e-5
 
 
+@needs_ref
+def test_crystal_factor_sensitivity_and_gather_equal_histogram_forms():
+    # LOR sensitivity formed in the kernel as eff[d1] * eff[d2] against a
+    # sensitivity histogram holding those products (filled through the
+    # reference's own bin -> detector-pair map): the per-event gather is
+    # bit-identical, and so is the sensitivity image in deterministic mode;
+    # the image also matches the reference's sensitivity image (1e-5).
+    from pyyrtpet_b200 import synthetic as S
+    sc = S.scanner_c1()
+    ip = yrt.ImageParams(32, 32, 16, 256, 256, 128)
+    osc = po.Scanner(*SC_ARGS)
+    eff = S.crystal_efficiencies(sc, 23)
+    h = po.ref_histo3d_crystal_product(osc, eff.numpy())
+    a, b = yrt.histo3d_detpairs(sc, np.arange(len(h), dtype=np.uint64))
+    assert np.array_equal(bits(h), bits(eff.numpy()[a] * eff.numpy()[b]))
+    pp = yrt.ProjectorParams(sc)
+    pp.deterministic = True
+    p = yrt.DeviceProjector(sc, ip, pp)
+    eff_d, h_d = eff.cuda(), torch.from_numpy(h).cuda()
+    s_eff = p.sensitivity_histo3d(torch.zeros(ip.shape, device="cuda"),
+                                  crystal_eff=eff_d)
+    s_hist = p.sensitivity_histo3d(torch.zeros(ip.shape, device="cuda"),
+                                   sens_histo=h_d)
+    assert torch.equal(s_eff, s_hist)
+    rs, _ = po.ref_sensitivity(osc, po.ImageParams(32, 32, 16, 256, 256, 128),
+                               listmode=True, sens_histo=h)
+    got = s_eff.cpu().numpy()
+    got[got <= 1.0] = 0.0  # the reference's hard threshold (1.0)
+    assert rel_l2(got, rs[0]) < 1e-5
+    d1, d2 = random_events(SC_ARGS, 20000, 24)
+    ev = yrt.DeviceEvents.from_arrays(d1, d2)
+    g_eff = p.gather_crystal_product(eff_d, ev)
+    g_hist = p.gather_histo3d(h_d, ev)
+    assert torch.equal(g_eff, g_hist)
+
+
 def test_em_update_variants_vs_numpy():
     rng = np.random.default_rng(24)
     J, nt = 1000, 3

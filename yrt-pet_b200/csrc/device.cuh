@@ -270,31 +270,28 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	    (inv_z >= 0.0f && p1.z > z1) || (inv_z < 0.0f && p1.z < z0))
 		return;
 
-	// First plane crossing at or beyond the entry point, per axis.
-	float ax_next = flat_x ? 3.402823466e+38f : ax_min;
-	if (!flat_x)
+	// First plane crossing at or beyond the entry point, per axis: the plane
+	// index is ceil of the entry position's distance from the walk's start
+	// plane in voxels, in FP32 as the reference computes it, or in FP64
+	// (COMP) so that an entry within float rounding of a plane cannot skip
+	// that plane.
+	auto firstPlane = [&](float q1, float q2, float inv, int dir, float d,
+	                      float& cur) -> float
 	{
-		const long long kx = static_cast<long long>(
-		    ceilf(static_cast<float>(dir_x) * (a_cur * (p2.x - p1.x) - x_cur + p1.x) / dx));
-		x_cur += static_cast<float>(kx * dir_x) * dx;
-		ax_next = (x_cur - p1.x) * inv_x;
-	}
-	float ay_next = flat_y ? 3.402823466e+38f : ay_min;
-	if (!flat_y)
-	{
-		const long long ky = static_cast<long long>(
-		    ceilf(static_cast<float>(dir_y) * (a_cur * (p2.y - p1.y) - y_cur + p1.y) / dy));
-		y_cur += static_cast<float>(ky * dir_y) * dy;
-		ay_next = (y_cur - p1.y) * inv_y;
-	}
-	float az_next = flat_z ? 3.402823466e+38f : az_min;
-	if (!flat_z)
-	{
-		const long long kz = static_cast<long long>(
-		    ceilf(static_cast<float>(dir_z) * (a_cur * (p2.z - p1.z) - z_cur + p1.z) / dz));
-		z_cur += static_cast<float>(kz * dir_z) * dz;
-		az_next = (z_cur - p1.z) * inv_z;
-	}
+		long long k;
+		if constexpr (COMP)
+			k = static_cast<long long>(
+			    ceil(double(dir) * (double(a_cur) * (double(q2) - double(q1)) -
+			                        double(cur) + double(q1)) * (1.0 / double(d))));
+		else
+			k = static_cast<long long>(
+			    ceilf(static_cast<float>(dir) * (a_cur * (q2 - q1) - cur + q1) / d));
+		cur += static_cast<float>(k * dir) * d;
+		return (cur - q1) * inv;
+	};
+	float ax_next = flat_x ? 3.402823466e+38f : firstPlane(p1.x, p2.x, inv_x, dir_x, dx, x_cur);
+	float ay_next = flat_y ? 3.402823466e+38f : firstPlane(p1.y, p2.y, inv_y, dir_y, dy, y_cur);
+	float az_next = flat_z ? 3.402823466e+38f : firstPlane(p1.z, p2.z, inv_z, dir_z, dz, z_cur);
 
 	int vx, vy, vz;
 	int dir_prev = 0;
@@ -385,36 +382,32 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 	step++;
 	if constexpr (COMP)
 	{
-		// Entry voxel in FP64: a ray lying within float rounding of a voxel
-		// boundary (e.g. an LOR between opposite crystals on an image axis)
-		// is placed on the side the exact geometry gives, not where the FP32
-		// sum with l/2 rounds it.
-		const double am = 0.5 * (static_cast<double>(a_cur) + static_cast<double>(a_next));
-		vx = static_cast<int>((double(p1.x) + am * (double(p2.x) - double(p1.x)) + 0.5 * double(g.lx)) / double(dx));
-		vy = static_cast<int>((double(p1.y) + am * (double(p2.y) - double(p1.y)) + 0.5 * double(g.ly)) / double(dy));
-		vz = static_cast<int>((double(p1.z) + am * (double(p2.z) - double(p1.z)) + 0.5 * double(g.lz)) / double(dz));
-		if (part > 0)
+		// Entry voxel from the walk's own plane bookkeeping: the first
+		// segment lies just before the next plane of each axis (the plane at
+		// a_next for the axes stepped last), so the voxel and the planes the
+		// walk steps by can never disagree.  A voxel taken from the segment's
+		// midpoint instead is off by one for the whole walk when the first
+		// segment is tiny (a TOF window or a piece that starts right before a
+		// plane) and the midpoint rounds across that plane.  With the first
+		// plane chosen in FP64, a ray within float rounding of a plane (e.g.
+		// an LOR between opposite crystals on an image axis) is placed on the
+		// side the exact geometry gives.  An axis the ray runs parallel to
+		// takes its voxel from the (constant) coordinate in FP64.
+		auto fromPlanes = [](bool flat, bool stepped, float cur, float fd,
+		                     float q0, float d, int dir, float q1, int& v)
 		{
-			// A piece that starts at a cut inside the ray: its first segment
-			// can be arbitrarily short (a plane of another axis right after
-			// the cut, e.g. at a voxel corner), and an exact midpoint may then
-			// fall on the other side of a plane than the FP32 crossings the
-			// walk steps by.  Take the voxel from the walk's own crossings:
-			// the segment lies just before the next plane of each stepping
-			// axis (the plane at a_next for the axes stepped last).
-			auto fromPlanes = [](bool flat, bool stepped, float cur, float fd,
-			                     float q0, float d, int dir, int& v)
+			if (flat)
 			{
-				if (flat)
-					return;
-				const float pre = stepped ? cur - fd : cur;
-				const int ip = static_cast<int>(rintf((pre - q0) / d));
-				v = dir > 0 ? ip - 1 : ip;
-			};
-			fromPlanes(flat_x, sx, x_cur, fdx, x0, dx, dir_x, vx);
-			fromPlanes(flat_y, sy, y_cur, fdy, y0, dy, dir_y, vy);
-			fromPlanes(flat_z, sz, z_cur, fdz, z0, dz, dir_z, vz);
-		}
+				v = static_cast<int>(floor((double(q1) - double(q0)) * (1.0 / double(d))));
+				return;
+			}
+			const float pre = stepped ? cur - fd : cur;
+			const int ip = static_cast<int>(rintf((pre - q0) / d));
+			v = dir > 0 ? ip - 1 : ip;
+		};
+		fromPlanes(flat_x, sx, x_cur, fdx, x0, dx, dir_x, p1.x, vx);
+		fromPlanes(flat_y, sy, y_cur, fdy, y0, dy, dir_y, p1.y, vy);
+		fromPlanes(flat_z, sz, z_cur, fdz, z0, dz, dir_z, p1.z, vz);
 	}
 	else
 	{

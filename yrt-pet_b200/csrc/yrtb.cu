@@ -1049,6 +1049,29 @@ __global__ void __launch_bounds__(kBlock)
 	}
 }
 
+// Per-event product of crystal factors eff[d1] * eff[d2]: the LOR
+// sensitivity of a normalisation made of per-crystal efficiencies (the value a
+// Histogram3D filled with eff[d1] * eff[d2] holds for the event's bin).
+// Detector ids outside the scanner give 0 and are counted.
+__global__ void __launch_bounds__(kBlock)
+    k_gather_crystal(uint32_t numDets, Events E, Range R,
+                     const float* __restrict__ eff, float* __restrict__ out,
+                     unsigned long long* err)
+{
+	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (k < R.count)
+	{
+		const uint64_t e = R.start + k * R.stride;
+		const uint32_t a = __ldg(E.d1 + e), b = __ldg(E.d2 + e);
+		float v = 0.f;
+		if (a < numDets && b < numDets)
+			v = __ldg(eff + a) * __ldg(eff + b);
+		else
+			atomicAdd(err, 1ULL);
+		out[e] = v;
+	}
+}
+
 // Histogram-bin kernels: sensitivity back projection and histogram EM.
 // MODE H_BOUND is pass 1 and H_FIX pass 2 of the deterministic back
 // projection (see Fixed); H_PLAIN scatters floats.
@@ -1067,7 +1090,8 @@ __global__ void __launch_bounds__(kBlock)
             const float* __restrict__ sensH, const float* __restrict__ acfH,
             const float* __restrict__ addH, Geom mu,
             const float* __restrict__ muImg, float globalScale, float denomThr,
-            Fixed F, unsigned* maxBits, const uint64_t* __restrict__ list)
+            Fixed F, unsigned* maxBits, const uint64_t* __restrict__ list,
+            const float* __restrict__ crystalEff)
 {
 	static_assert(TPL == 1 || (KIND == K_DD_PSF && EM && MODE == H_PLAIN && COMP),
 	              "several threads per bin: compensated DD + PSF histogram EM");
@@ -1094,7 +1118,10 @@ __global__ void __launch_bounds__(kBlock)
 		const float m = EM ? __ldg(meas + bin) : 1.0f;
 		if (EM && m == 0.f)
 			break;
-		const float s = sensH ? __ldg(sensH + bin) : 1.0f;
+		// LOR sensitivity: a histogram value, or the product of the two
+		// crystals' factors (the same FP32 product a histogram of them holds).
+		const float s = sensH ? __ldg(sensH + bin) :
+		                (crystalEff ? __ldg(crystalEff + d1) * __ldg(crystalEff + d2) : 1.0f);
 		const float4 pa = __ldg(P.scan.pos + d1), pb = __ldg(P.scan.pos + d2);
 		const float4 oa = __ldg(P.scan.ori + d1), ob = __ldg(P.scan.ori + d2);
 		float3 p1 = make_float3(pa.x, pa.y, pa.z), p2 = make_float3(pb.x, pb.y, pb.z);
@@ -2597,7 +2624,8 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
                           const float* addH, const float* mu,
                           const yrtb_image_params* muParams, float gs,
                           float thr, yrtb_stream stream,
-                          const uint64_t* list = nullptr, uint64_t listCount = 0)
+                          const uint64_t* list = nullptr, uint64_t listCount = 0,
+                          const float* crystalEff = nullptr)
 {
 	if (!h || !out || numSubsets <= 0 || subset < 0 || subset >= numSubsets)
 		return fail(YRTB_ERR_ARGUMENT, "invalid histogram subset or buffers");
@@ -2632,10 +2660,10 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 		{
 			k_histo<K, EM, H_BOUND, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
-			    acfH, addH, mg, mu, gs, thr, F, h->d_fixMax, list);
+			    acfH, addH, mg, mu, gs, thr, F, h->d_fixMax, list, crystalEff);
 			k_histo<K, EM, H_FIX, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
-			    acfH, addH, mg, mu, gs, thr, F, nullptr, list);
+			    acfH, addH, mg, mu, gs, thr, F, nullptr, list, crystalEff);
 		}
 		else if constexpr (EM && K == K_DD_PSF && C)
 		{
@@ -2644,13 +2672,13 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 			constexpr int T = kHistoDDThreads;
 			k_histo<K, EM, H_PLAIN, C, T><<<gridAll(count * T), kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
-			    acfH, addH, mg, mu, gs, thr, F, nullptr, list);
+			    acfH, addH, mg, mu, gs, thr, F, nullptr, list, crystalEff);
 		}
 		else
 		{
 			k_histo<K, EM, H_PLAIN, C><<<grid, kBlock, 0, st>>>(
 			    h->P, h->h3d, count, nps, numSubsets, subset, img, out, meas, sensH,
-			    acfH, addH, mg, mu, gs, thr, F, nullptr, list);
+			    acfH, addH, mg, mu, gs, thr, F, nullptr, list, crystalEff);
 		}
 	};
 	// Histogram mode honours the precision for single-ray Siddon and DD + PSF.
@@ -3383,6 +3411,46 @@ yrtb_status yrtb_sensitivity_histo3d(yrtb_projector* h, float* d_sens,
 	return dispatchHisto<false>(h, num_subsets, subset, nullptr, d_sens, nullptr,
 	                            d_sens_histo, d_acf_histo, nullptr, d_mu,
 	                            mu_params, 1.f, 0.f, stream);
+}
+
+yrtb_status yrtb_sensitivity_histo3d_crystal(yrtb_projector* h, float* d_sens,
+                                             const float* d_crystal_eff,
+                                             const float* d_acf_histo,
+                                             const float* d_mu,
+                                             const yrtb_image_params* mu_params,
+                                             int num_subsets, int subset,
+                                             yrtb_stream stream)
+{
+	if (!h || !h->h3)
+		return fail(YRTB_ERR_ARGUMENT, "projector has no Histogram3D (odd ring)");
+	if (!d_crystal_eff)
+		return fail(YRTB_ERR_ARGUMENT, "null crystal factors");
+	return dispatchHisto<false>(h, num_subsets, subset, nullptr, d_sens, nullptr,
+	                            nullptr, d_acf_histo, nullptr, d_mu, mu_params,
+	                            1.f, 0.f, stream, nullptr, 0, d_crystal_eff);
+}
+
+yrtb_status yrtb_gather_crystal_product(yrtb_projector* h,
+                                        const float* d_crystal_eff,
+                                        const yrtb_events* ev, yrtb_range range,
+                                        float* d_out, yrtb_stream stream)
+{
+	if (!d_crystal_eff || (!d_out && !emptyEvents(ev)))
+		return fail(YRTB_ERR_ARGUMENT, "null crystal factors or output");
+	yrtb_status s = checkEvents(h, ev, range, false);
+	if (s != YRTB_OK)
+		return s;
+	if (range.count == 0)
+		return YRTB_OK;
+	if (!ev->d1)
+		return fail(YRTB_ERR_ARGUMENT, "crystal factors need detector ids");
+	YRTB_CUDA(cudaSetDevice(h->device));
+	k_gather_crystal<<<gridAll(range.count), kBlock, 0,
+	                   reinterpret_cast<cudaStream_t>(stream)>>>(
+	    h->P.scan.numDets, toDev(ev), Range{range.start, range.stride, range.count},
+	    d_crystal_eff, d_out, h->d_err);
+	YRTB_LAUNCHED();
+	return YRTB_OK;
 }
 
 yrtb_status yrtb_em_step_histo3d(yrtb_projector* h, const float* d_image,

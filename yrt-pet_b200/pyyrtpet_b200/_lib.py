@@ -128,6 +128,11 @@ SIGNATURES = {
     "yrtb_sensitivity_histo3d": ([c_vp, c_vp, c_vp, c_vp, c_vp,
                                   _P(yrtb_image_params), ctypes.c_int,
                                   ctypes.c_int, c_vp], ctypes.c_int),
+    "yrtb_sensitivity_histo3d_crystal": ([c_vp, c_vp, c_vp, c_vp, c_vp,
+                                          _P(yrtb_image_params), ctypes.c_int,
+                                          ctypes.c_int, c_vp], ctypes.c_int),
+    "yrtb_gather_crystal_product": ([c_vp, c_vp, _P(yrtb_events), yrtb_range,
+                                     c_vp, c_vp], ctypes.c_int),
     "yrtb_em_step_histo3d": ([c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                               ctypes.c_int, ctypes.c_int, c_f, c_f, c_vp],
                              ctypes.c_int),

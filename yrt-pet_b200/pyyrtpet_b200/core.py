@@ -846,14 +846,38 @@ class DeviceProjector:
                                             _stream()))
         return out
 
+    def gather_crystal_product(self, crystal_eff: torch.Tensor,
+                               ev: DeviceEvents, out=None, rng=None):
+        """Per-event eff[d1] * eff[d2] (LOR sensitivity from crystal factors)."""
+        if out is None:
+            out = torch.zeros(ev.count, dtype=torch.float32,
+                              device=crystal_eff.device)
+        r = rng or L.yrtb_range(0, 1, 0)
+        L.check(L.lib().yrtb_gather_crystal_product(
+            self.h, crystal_eff.data_ptr(), ctypes.byref(ev.c()), r,
+            out.data_ptr(), _stream()))
+        return out
+
     def sensitivity_histo3d(self, sens_img, num_subsets=1, subset=0,
                             sens_histo=None, acf_histo=None, mu=None,
-                            mu_params: Optional[ImageParams] = None):
+                            mu_params: Optional[ImageParams] = None,
+                            crystal_eff=None):
+        """Back projection of a subset of all histogram bins; the LOR
+        sensitivity is sens_histo[bin], or crystal_eff[d1] * crystal_eff[d2]."""
         self._check_image(sens_img, nt=1)
+        mp = None if mu_params is None else ctypes.byref(mu_params._c())
+        if crystal_eff is not None:
+            if sens_histo is not None:
+                raise RuntimeError("give a sensitivity histogram or crystal "
+                                   "factors, not both")
+            L.check(L.lib().yrtb_sensitivity_histo3d_crystal(
+                self.h, sens_img.data_ptr(), crystal_eff.data_ptr(),
+                _ptr(acf_histo), _ptr(mu), mp, int(num_subsets), int(subset),
+                _stream()))
+            return sens_img
         L.check(L.lib().yrtb_sensitivity_histo3d(
             self.h, sens_img.data_ptr(), _ptr(sens_histo), _ptr(acf_histo),
-            _ptr(mu), None if mu_params is None else ctypes.byref(mu_params._c()),
-            int(num_subsets), int(subset), _stream()))
+            _ptr(mu), mp, int(num_subsets), int(subset), _stream()))
         return sens_img
 
     def em_step_histo3d(self, img, em, meas, num_subsets, subset,
