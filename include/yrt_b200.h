@@ -94,7 +94,9 @@ typedef struct
 
 /* Events (list-mode) in structure-of-arrays form, device pointers.  Either
  * (d1, d2) detector ids or lor (6 floats per event: p1 xyz, p2 xyz) must be
- * given.  All other arrays are optional (NULL):
+ * given; with lor, distance-driven and multi-ray projection also need orient
+ * (6 floats per event: the two crystals' orientations n1 xyz, n2 xyz; the
+ * reference's DET_ORIENT property).  All other arrays are optional (NULL):
  *   tof_ps        TOF value in ps (needs a TOF projector)
  *   frame         dynamic frame; events with frame < 0 are skipped, frames
  *                 >= nt are counted as invalid and skipped
@@ -124,6 +126,7 @@ typedef struct
 	const float* att;
 	const float* additive;
 	uint64_t count;
+	const float* orient;
 } yrtb_events;
 
 /* Events start + k*stride for k < count: one OSEM subset of the reference
@@ -353,6 +356,43 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
                                      int num_subsets, uint64_t* d_perm,
                                      uint64_t* subset_offsets,
                                      yrtb_stream stream);
+
+/* Byte layout of one event row of the reference's device batches: the
+ * projection-property rows of PropStructManager<ProjectionPropertyType>
+ * (include/yrt-pet/datastruct/projection/ProjectionProperties.hpp:59-140,
+ * src/datastruct/projection/ProjectionProperties.cpp:40-81), which
+ * ProjectionListDevice / LORsDevice and OSEM_GPU keep on the device (one row
+ * per event, the properties packed in enum order).  Each field is the
+ * property's byte offset in the row (PropStructManager::getOffset), -1 when
+ * the row does not hold it. */
+typedef struct
+{
+	uint32_t row_bytes;   /* PropStructManager::getElementSize */
+	int32_t lor;          /* LOR: 6 floats */
+	int32_t det_orient;   /* DET_ORIENT: 6 floats */
+	int32_t tof;          /* TOF: float, ps */
+	int32_t dynamic_frame;/* DYNAMIC_FRAME: int32 */
+	int32_t measurement;  /* MEASUREMENT: float */
+	int32_t sensitivity;  /* SENSITIVITY: float */
+	int32_t attenuation;  /* ATTENUATION: float */
+	int32_t randoms;      /* RANDOMS_ESTIMATE: float */
+	int32_t scatter;      /* SCATTER_ESTIMATE: float */
+} yrtb_row_layout;
+
+/* Unpacks count rows (device memory, 4-byte aligned, layout->row_bytes
+ * apart) into the structure of arrays of `out`: out->lor (6 floats per
+ * event) must be given, and every other array of `out` that is not NULL
+ * receives its property (orient, tof_ps, frame, measurement, sens, att;
+ * additive = randoms + scatter, either may be absent); an array whose
+ * property the row does not hold is an error.  This is how the reference's
+ * own batches (OperatorProjectorDevice::applyAOnLoadedBatch,
+ * OSEM_GPU::computeEMUpdateImageForLoadedBatch,
+ * src/recon/OSEM_GPU.cu:877-982) reach the projection kernels, which read
+ * each field per event from the rows instead
+ * (OSEM_GPU.cu:1172-1265, SiddonKernels.cuh:502-574). */
+yrtb_status yrtb_events_from_rows(const void* d_rows, uint64_t count,
+                                  const yrtb_row_layout* layout,
+                                  const yrtb_events* out, yrtb_stream stream);
 
 /* out->X[i] = in->X[d_perm[i]] for every array present in `in` (output
  * buffers allocated by the caller; out->count == in->count).  d_perm must be

@@ -31,6 +31,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libyrtref_harness.so")
 REF_GPU_SO = os.path.join(HERE, "_ref_cuda", "libyrtref_gpu_harness.so")
+REF_B200_SO = os.path.join(HERE, "_ref_cuda", "libyrtref_b200_harness.so")
 
 
 class ScannerDesc(ctypes.Structure):
@@ -140,6 +141,7 @@ def _c(a, dtype):
 _oracle = None
 _ref = None
 _ref_gpu = None
+_ref_b200 = None
 
 
 def oracle_lib():
@@ -164,10 +166,18 @@ def _setup_ref(lib):
     return lib
 
 
-def ref_lib(gpu: bool = False):
-    """The reference harness: the CPU build, or with gpu=True the build whose
-    OSEM and list-mode projections run the reference's CUDA path."""
-    global _ref, _ref_gpu
+def ref_lib(gpu=False):
+    """The reference harness: the CPU build; with gpu=True the build whose
+    OSEM and list-mode projections run the reference's CUDA path; with
+    gpu="b200" the build whose OSEM and list-mode projections run the
+    reference's drivers on the product's binding classes (OSEM_GPU_B200,
+    OperatorProjectorB200 over libyrtb)."""
+    global _ref, _ref_gpu, _ref_b200
+    if gpu == "b200":
+        if _ref_b200 is None:
+            _ref_b200 = _setup_ref(ctypes.CDLL(REF_B200_SO))
+            assert _ref_b200.ref_uses_gpu() == 2
+        return _ref_b200
     if gpu:
         if _ref_gpu is None:
             _ref_gpu = _setup_ref(ctypes.CDLL(REF_GPU_SO))
@@ -180,6 +190,15 @@ def ref_lib(gpu: bool = False):
 
 def ref_gpu_available() -> bool:
     return os.path.exists(REF_GPU_SO)
+
+
+def ref_b200_available() -> bool:
+    return os.path.exists(REF_B200_SO)
+
+
+def ref_set_b200_precision(precision: int):
+    """0: mirror, 1: compensated arithmetic for the binding's projections."""
+    ref_lib("b200").ref_set_b200_precision(ctypes.c_int(precision))
 
 
 class _StdoutToStderr:
@@ -209,7 +228,7 @@ def quiet():
     return _StdoutToStderr()
 
 
-def _ref_check(rc, gpu: bool = False):
+def _ref_check(rc, gpu=False):
     if rc != 0:
         raise RuntimeError(ref_lib(gpu).ref_last_error().decode())
 
@@ -527,7 +546,7 @@ def _osem_desc(projector="S", num_rays=1, tof_fwhm_ps=0.0, tof_n_std=0,
 
 def ref_sensitivity(sc: Scanner, ip: ImageParams, *, sens_histo=None,
                     att_params: ImageParams | None = None, att_image=None,
-                    psf_csv=None, gpu: bool = False, **kw):
+                    psf_csv=None, gpu=False, **kw):
     o = _osem_desc(**kw)
     nsub = 1 if o.listmode else o.subsets
     out = np.zeros((nsub, ip.nz, ip.ny, ip.nx), np.float32)
@@ -547,7 +566,7 @@ def ref_sensitivity(sc: Scanner, ip: ImageParams, *, sens_histo=None,
 def ref_osem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, *, tof=None,
                       randoms=None, sens_histo=None,
                       att_params: ImageParams | None = None, att_image=None,
-                      gpu: bool = False, **kw):
+                      gpu=False, **kw):
     o = _osem_desc(**kw)
     out = np.zeros(ip.shape, np.float32)
     sec = ctypes.c_double()
@@ -570,7 +589,7 @@ def ref_osem_listmode(sc: Scanner, ip: ImageParams, sens, d1, d2, *, tof=None,
 
 def ref_osem_listmode_dynamic(sc: Scanner, ip: ImageParams, sens, d1, d2,
                               timestamps, *, frame_ts=None, motion_starts=None,
-                              motion=None, tof=None, gpu: bool = False, **kw):
+                              motion=None, tof=None, gpu=False, **kw):
     """Reference OSEM with DynamicFraming and/or LORMotion; ip.nt must equal
     the number of dynamic frames (len(frame_ts) - 1)."""
     o = _osem_desc(**kw)
@@ -599,7 +618,7 @@ def ref_osem_listmode_dynamic(sc: Scanner, ip: ImageParams, sens, d1, d2,
 
 
 def ref_osem_histo3d(sc: Scanner, ip: ImageParams, sens_images, histo, *,
-                     psf_csv=None, gpu: bool = False, **kw):
+                     psf_csv=None, gpu=False, **kw):
     o = _osem_desc(listmode=False, **kw)
     out = np.zeros((ip.nz, ip.ny, ip.nx), np.float32)
     sec = ctypes.c_double()
@@ -616,7 +635,7 @@ def ref_osem_histo3d(sc: Scanner, ip: ImageParams, sens_images, histo, *,
 
 def ref_project_lm(sc: Scanner, ip: ImageParams, d1, d2, *, tof=None,
                    image=None, values=None, fwd=True, psf_csv=None,
-                   gpu: bool = False, **kw):
+                   gpu=False, **kw):
     """List-mode forward (values = A x) or back projection (image + A^T v)
     through the reference's util::forwProject / util::backProject, on its CPU
     projector or, with gpu=True, on OperatorProjectorDevice (its CUDA

@@ -33,7 +33,7 @@ CU_SRCS  := $(shell find $(REF)/src -name '*.cu' | sort)
 OBJS     := $(patsubst $(REF)/src/%.cpp,$(OUT)/obj/%.o,$(CPP_SRCS)) \
             $(patsubst $(REF)/src/%.cu,$(OUT)/obj/%.cu.o,$(CU_SRCS))
 
-all: $(OUT)/libyrtref_cuda.a $(OUT)/libyrtref_gpu_harness.so
+all: $(OUT)/libyrtref_cuda.a $(OUT)/libyrtref_gpu_harness.so $(OUT)/libyrtref_b200_harness.so
 
 $(OUT)/include/nlohmann/json.hpp:
 ifndef JSON_HPP
@@ -62,5 +62,24 @@ $(OUT)/libyrtref_cuda.a: $(OBJS)
 # the CUDA runtime linked statically.
 $(OUT)/libyrtref_gpu_harness.so: oracle/ref_harness.cpp $(OUT)/libyrtref_cuda.a
 	$(CXX) $(CXXFLAGS) -DREF_HARNESS_GPU -shared $< -o $@ -Wl,--whole-archive $(OUT)/libyrtref_cuda.a -Wl,--no-whole-archive -L$(CUDA_DIR)/lib64 -lcudart_static -lz -lpthread -ldl -lrt -Wl,-Bsymbolic -Wl,--exclude-libs,ALL
+
+# The reference's drivers on the product's binding (REF_HARNESS_B200):
+# OSEM_GPU_B200 / OperatorProjectorB200 (yrt-pet_b200/binding, compiled by its
+# own recipe) over libyrtb.so, found at run time next to this tree's copy.
+B200_OBJ := yrt-pet_b200/lib/yrtb_yrtpet.o
+LIBYRTB  := yrt-pet_b200/lib/libyrtb.so
+
+$(B200_OBJ): yrt-pet_b200/binding/yrtb_yrtpet.cu yrt-pet_b200/binding/yrtb_yrtpet.cuh include/yrt_b200.h $(OUT)/include/nlohmann/json.hpp
+	$(MAKE) -f yrt-pet_b200/binding/binding.mk REF=$(REF) INC="-I$(OUT)/include" NVCC=$(NVCC)
+
+$(OUT)/obj/ref_harness_b200.o: oracle/ref_harness.cpp yrt-pet_b200/binding/yrtb_yrtpet.cuh include/yrt_b200.h $(OUT)/include/nlohmann/json.hpp
+	@mkdir -p $(dir $@)
+	$(NVCC) $(NVFLAGS) -Iinclude -Iyrt-pet_b200/binding -DREF_HARNESS_GPU -DREF_HARNESS_B200 -x cu -c $< -o $@
+
+$(OUT)/libyrtref_b200_harness.so: $(OUT)/obj/ref_harness_b200.o $(OUT)/libyrtref_cuda.a $(B200_OBJ) $(LIBYRTB)
+	$(CXX) -shared $(OUT)/obj/ref_harness_b200.o $(B200_OBJ) -o $@ \
+	    -Wl,--whole-archive $(OUT)/libyrtref_cuda.a -Wl,--no-whole-archive \
+	    -Lyrt-pet_b200/lib -lyrtb -L$(CUDA_DIR)/lib64 -lcudart_static -lz -lpthread -ldl -lrt \
+	    -Wl,-rpath,'$$ORIGIN/../../yrt-pet_b200/lib' -Wl,-Bsymbolic -Wl,--exclude-libs,ALL
 
 .PHONY: all

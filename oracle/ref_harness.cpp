@@ -15,7 +15,13 @@
 //                          with BUILD_CUDA: the same OSEM and list-mode
 //                          projection entry points run the reference's GPU
 //                          path (OSEM_GPU, OperatorProjectorDevice and its
-//                          CUDA kernels).
+//                          CUDA kernels);
+//   oracle/ref_cuda.mk  -> oracle/_ref_cuda/libyrtref_b200_harness.so, with
+//                          REF_HARNESS_B200 defined as well: the reference's
+//                          drivers run on the product's binding classes
+//                          (yrt-pet_b200/binding: OSEM_GPU_B200 and
+//                          OperatorProjectorB200 over libyrtb), which is how
+//                          the tests check that binding end to end.
 //
 // Reference interfaces exercised (paths inside the yrt-pet project):
 //   Scanner ctor + DetRegular LUT   src/datastruct/scanner/Scanner.cpp:102-127,
@@ -64,6 +70,24 @@ constexpr bool kUseGPU = true;
 #else
 constexpr bool kUseGPU = false;
 #endif
+
+#ifdef REF_HARNESS_B200
+#include "yrtb_yrtpet.cuh"
+static int g_b200_precision = YRTB_MIRROR;
+#endif
+
+namespace
+{
+// The OSEM driver of this build: OSEM_CPU, OSEM_GPU, or OSEM_GPU_B200.
+std::unique_ptr<OSEM> createDriver(const Scanner& sc)
+{
+#ifdef REF_HARNESS_B200
+	return b200::createOSEM(sc, g_b200_precision);
+#else
+	return util::createOSEM(sc, kUseGPU);
+#endif
+}
+}  // namespace
 
 extern "C" {
 
@@ -546,7 +570,7 @@ int ref_sensitivity(const ref_scanner_desc* s, const ref_image_desc* d,
 	    {
 		    auto sc = makeScanner(s);
 		    globals::setNumThreads(o->threads);
-		    auto osem = util::createOSEM(*sc, kUseGPU);
+		    auto osem = createDriver(*sc);
 		    osem->setImageParams(makeParams(d));
 		    osem->num_OSEM_subsets = o->subsets;
 		    osem->num_MLEM_iterations = o->iterations;
@@ -652,7 +676,7 @@ int ref_osem_listmode_ex(const ref_scanner_desc* s, const ref_image_desc* d,
 			    }
 			    lm.addLORMotion(mot);
 		    }
-		    auto osem = util::createOSEM(*sc, kUseGPU);
+		    auto osem = createDriver(*sc);
 		    ImageParams ip = makeParams(d);
 		    osem->setImageParams(ip);
 		    osem->num_OSEM_subsets = o->subsets;
@@ -726,7 +750,7 @@ int ref_osem_histo3d(const ref_scanner_desc* s, const ref_image_desc* d,
 		    h.allocate();
 		    std::memcpy(h.getData().getRawPointer(), histo,
 		                h.count() * sizeof(float));
-		    auto osem = util::createOSEM(*sc, kUseGPU);
+		    auto osem = createDriver(*sc);
 		    osem->setImageParams(makeParams(d));
 		    osem->num_OSEM_subsets = o->subsets;
 		    osem->num_MLEM_iterations = o->iterations;
@@ -759,8 +783,26 @@ int ref_osem_histo3d(const ref_scanner_desc* s, const ref_image_desc* d,
 	    });
 }
 
-// 1 when this build runs the reference's GPU path.
-int ref_uses_gpu() { return kUseGPU ? 1 : 0; }
+// 1 when this build runs the reference's GPU path, 2 when it runs the
+// reference's drivers on the libyrtb binding.
+int ref_uses_gpu()
+{
+#ifdef REF_HARNESS_B200
+	return 2;
+#else
+	return kUseGPU ? 1 : 0;
+#endif
+}
+
+// Arithmetic of the libyrtb binding (YRTB_MIRROR or YRTB_COMPENSATED);
+// other builds ignore it.
+int ref_set_b200_precision(int precision)
+{
+#ifdef REF_HARNESS_B200
+	g_b200_precision = precision;
+#endif
+	return 0;
+}
 
 // Forward (fwd=1: values[i] = A_i x) or back projection (fwd=0: image +=
 // A^T values) of n list-mode events (detector pairs, optional TOF in ps)
@@ -807,14 +849,33 @@ int ref_project_lm(const ref_scanner_desc* s, const ref_image_desc* d,
 			    pp.projPsf_fname = psf_csv;
 		    auto img = makeImage(d, image);
 		    const auto binIter = pl.getBinIter(1, 0);
+#ifdef REF_HARNESS_B200
+		    // The reference's operator contract on the binding's projector:
+		    // OperatorProjectorDevice::applyA / applyAH stage the host data,
+		    // batch it and call OperatorProjectorB200 per loaded batch.
+		    std::vector<std::unique_ptr<Constraint>> cons;
+		    sc->collectConstraints(cons);
+		    std::vector<Constraint*> consPtr;
+		    for (auto& c : cons)
+			    consPtr.push_back(c.get());
+		    auto op = b200::createOperatorProjectorDevice(
+		        pp, binIter.get(), consPtr, nullptr, nullptr, g_b200_precision);
+		    if (fwd)
+			    op->applyA(img.get(), &pl);
+		    else
+			    op->applyAH(&pl, img.get());
+#else
+		    if (fwd)
+			    util::forwProject(*img, pl, pp, *binIter, kUseGPU);
+		    else
+			    util::backProject(*img, pl, pp, *binIter, kUseGPU);
+#endif
 		    if (fwd)
 		    {
-			    util::forwProject(*img, pl, pp, *binIter, kUseGPU);
 			    std::memcpy(values, pl.getRawPointer(), n * sizeof(float));
 		    }
 		    else
 		    {
-			    util::backProject(*img, pl, pp, *binIter, kUseGPU);
 			    const size_t nv = d->nx * d->ny * d->nz * d->nt;
 			    std::memcpy(image, img->getRawPointer(), nv * sizeof(float));
 		    }

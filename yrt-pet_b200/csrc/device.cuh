@@ -82,6 +82,8 @@ struct Events
 	// projection with its corrections, the denominator of the EM ratio) is
 	// written here; 0 for an event that is skipped.
 	float* model;
+	// With lor: crystal orientations n1, n2 (6 floats per event), or null.
+	const float* orient;
 };
 
 struct Range

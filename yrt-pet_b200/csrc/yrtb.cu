@@ -311,8 +311,17 @@ __device__ __forceinline__ bool fetchEvent(const KParams& P, const Events& E,
 		const float* l = E.lor + e * 6;
 		p1 = make_float3(__ldg(l + 0), __ldg(l + 1), __ldg(l + 2));
 		p2 = make_float3(__ldg(l + 3), __ldg(l + 4), __ldg(l + 5));
-		n1 = make_float3(0.f, 0.f, 0.f);
-		n2 = n1;
+		if (E.orient != nullptr)
+		{
+			const float* o = E.orient + e * 6;
+			n1 = make_float3(__ldg(o + 0), __ldg(o + 1), __ldg(o + 2));
+			n2 = make_float3(__ldg(o + 3), __ldg(o + 4), __ldg(o + 5));
+		}
+		else
+		{
+			n1 = make_float3(0.f, 0.f, 0.f);
+			n2 = n1;
+		}
 	}
 	if (E.mframe != nullptr)
 	{
@@ -934,14 +943,20 @@ __global__ void k_support_box(const float* __restrict__ img, Geom g, int* box)
 // the attenuation grid and gives the ray's parametric window inside the
 // mu-map's non-zero bounding box: only voxels there contribute, so the walk
 // is limited to it.
-__device__ __forceinline__ void attWindow(const KParams& P, const Geom& mu,
-                                          const int* box, float3& p1, float3& p2,
-                                          float& wlo, float& whi)
+__device__ __forceinline__ void attShift(const KParams& P, const Geom& mu,
+                                         float3& p1, float3& p2)
 {
 	const float3 fix = make_float3(P.g.offx - mu.offx, P.g.offy - mu.offy,
 	                               P.g.offz - mu.offz);
 	p1 = make_float3(p1.x + fix.x, p1.y + fix.y, p1.z + fix.z);
 	p2 = make_float3(p2.x + fix.x, p2.y + fix.y, p2.z + fix.z);
+}
+
+__device__ __forceinline__ void attWindow(const KParams& P, const Geom& mu,
+                                          const int* box, float3& p1, float3& p2,
+                                          float& wlo, float& whi)
+{
+	attShift(P, mu, p1, p2);
 	boxWindow(mu, box, p1, p2, wlo, whi);
 }
 
@@ -1012,8 +1027,21 @@ __global__ void __launch_bounds__(kBlock, 6)
 			out[e] = 0.f;
 			return;
 		}
-		float wlo, whi;
-		attWindow(P, mu, box, p1, p2, wlo, whi);
+		float wlo = 0.f, whi = 1.f;
+		if constexpr (COMP)
+		{
+			attWindow(P, mu, box, p1, p2, wlo, whi);
+		}
+		else
+		{
+			// Mirror arithmetic walks the whole chord, as the reference's
+			// Siddon projection of the mu-map does
+			// (Corrector::getAttenuationFactorFromAttenuationImage,
+			// src/recon/Corrector.cpp:601-611): a walk that starts at the
+			// support box places its first voxel from a different first
+			// segment, which in FP32 can round onto the other side of a plane.
+			attShift(P, mu, p1, p2);
+		}
 		float acc = 0.f;
 		auto visit = [&](int o, float w) { acc += w * __ldg(muImg + o); };
 		if (wlo < whi)
@@ -2363,6 +2391,7 @@ Events toDev(const yrtb_events* ev)
 	E.sens = ev->sens;
 	E.att = ev->att;
 	E.add = ev->additive;
+	E.orient = ev->orient;
 	return E;
 }
 
@@ -2393,12 +2422,10 @@ yrtb_status checkEvents(const yrtb_projector* h, const yrtb_events* ev,
 		return fail(YRTB_ERR_ARGUMENT, "d1 and d2 must both be given");
 	if (ev->motion_frame && (!ev->motion || ev->num_motion_frames == 0))
 		return fail(YRTB_ERR_ARGUMENT, "motion frames given without transforms");
-	if (h->kind != K_SIDDON && h->kind != K_SIDDON_MR && !ev->d1)
+	if (h->kind != K_SIDDON && !ev->d1 && !ev->orient)
 		return fail(YRTB_ERR_ARGUMENT,
 		            "distance-driven and multi-ray projection need detector ids "
-		            "(crystal orientations)");
-	if (h->kind == K_SIDDON_MR && !ev->d1)
-		return fail(YRTB_ERR_ARGUMENT, "multi-ray projection needs detector ids");
+		            "or, with LORs, crystal orientations");
 	if (needTof && h->hasTof && !ev->tof_ps)
 		return fail(YRTB_ERR_ARGUMENT, "TOF projector requires per-event TOF values");
 	if (r.stride == 0)
@@ -3187,7 +3214,8 @@ yrtb_status gatherEvents(const yrtb_events* in, const uint64_t* d_perm,
 	    (r = add(in->motion_frame, out->motion_frame)) ||
 	    (r = add(in->measurement, out->measurement)) ||
 	    (r = add(in->sens, out->sens)) || (r = add(in->att, out->att)) ||
-	    (r = add(in->additive, out->additive)) || (r = g32(in->lor, out->lor, 6)))
+	    (r = add(in->additive, out->additive)) || (r = g32(in->lor, out->lor, 6)) ||
+	    (r = g32(in->orient, out->orient, 6)))
 		return r;
 	if (G.count == 1)
 	{
@@ -3227,6 +3255,107 @@ yrtb_status gatherEvents(const yrtb_events* in, const uint64_t* d_perm,
 }  // namespace
 
 extern "C" {
+
+// Byte offsets of the properties of one row (-1: absent), as yrtb_row_layout.
+struct RowLayout
+{
+	uint32_t bytes;
+	int lor, orient, tof, frame, meas, sens, att, rnd, sct;
+};
+
+// One event per thread: its row's properties into the structure of arrays.
+// Rows are packed 4-byte words, so every field is read as 32-bit words.
+__global__ void __launch_bounds__(kBlock)
+    k_events_from_rows(const uint8_t* __restrict__ rows, uint64_t n, RowLayout L,
+                       float* lor, float* orient, float* tof, int32_t* frame,
+                       float* meas, float* sens, float* att, float* add)
+{
+	const uint64_t e = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (e >= n)
+		return;
+	const uint8_t* r = rows + e * L.bytes;
+	auto f = [&](int off) { return __ldg(reinterpret_cast<const float*>(r + off)); };
+	for (int k = 0; k < 6; k++)
+		lor[e * 6 + k] = f(L.lor + 4 * k);
+	if (orient)
+		for (int k = 0; k < 6; k++)
+			orient[e * 6 + k] = f(L.orient + 4 * k);
+	if (tof)
+		tof[e] = f(L.tof);
+	if (frame)
+		frame[e] = __ldg(reinterpret_cast<const int32_t*>(r + L.frame));
+	if (meas)
+		meas[e] = f(L.meas);
+	if (sens)
+		sens[e] = f(L.sens);
+	if (att)
+		att[e] = f(L.att);
+	if (add)
+	{
+		// randoms + scatter: the reference adds them to the model one after
+		// the other (OSEM_GPU.cu:1283-1295); one sum here, at most one
+		// rounding apart.
+		float a = 0.f;
+		if (L.rnd >= 0)
+			a = f(L.rnd);
+		if (L.sct >= 0)
+			a = (L.rnd >= 0) ? a + f(L.sct) : f(L.sct);
+		add[e] = a;
+	}
+}
+
+yrtb_status yrtb_events_from_rows(const void* d_rows, uint64_t count,
+                                  const yrtb_row_layout* layout,
+                                  const yrtb_events* out, yrtb_stream stream)
+{
+	if (!layout || !out)
+		return fail(YRTB_ERR_ARGUMENT, "null row layout or events");
+	if (count == 0)
+		return YRTB_OK;
+	if (!d_rows || !out->lor)
+		return fail(YRTB_ERR_ARGUMENT, "rows and an LOR output are required");
+	const yrtb_row_layout& l = *layout;
+	if (l.row_bytes == 0 || l.row_bytes % 4 != 0 ||
+	    reinterpret_cast<uintptr_t>(d_rows) % 4 != 0)
+		return fail(YRTB_ERR_ARGUMENT, "rows must be 4-byte aligned and a "
+		                               "multiple of 4 bytes long");
+	auto bad = [&](int32_t off, uint32_t words) {
+		return off < 0 || off % 4 != 0 ||
+		       static_cast<uint64_t>(off) + 4u * words > l.row_bytes;
+	};
+	if (bad(l.lor, 6))
+		return fail(YRTB_ERR_ARGUMENT, "rows hold no LOR");
+	struct Want
+	{
+		const void* out;
+		int32_t off;
+		uint32_t words;
+		const char* name;
+	} want[] = {{out->orient, l.det_orient, 6, "DET_ORIENT"},
+	            {out->tof_ps, l.tof, 1, "TOF"},
+	            {out->frame, l.dynamic_frame, 1, "DYNAMIC_FRAME"},
+	            {out->measurement, l.measurement, 1, "MEASUREMENT"},
+	            {out->sens, l.sensitivity, 1, "SENSITIVITY"},
+	            {out->att, l.attenuation, 1, "ATTENUATION"}};
+	for (const Want& w : want)
+		if (w.out && bad(w.off, w.words))
+			return fail(YRTB_ERR_ARGUMENT,
+			            std::string("rows hold no ") + w.name + " property");
+	if (out->additive && bad(l.randoms, 1) && bad(l.scatter, 1))
+		return fail(YRTB_ERR_ARGUMENT, "rows hold no randoms or scatter estimate");
+	RowLayout L{l.row_bytes, l.lor, l.det_orient, l.tof, l.dynamic_frame,
+	            l.measurement, l.sensitivity, l.attenuation,
+	            bad(l.randoms, 1) ? -1 : l.randoms, bad(l.scatter, 1) ? -1 : l.scatter};
+	k_events_from_rows<<<gridAll(count), kBlock, 0,
+	                     reinterpret_cast<cudaStream_t>(stream)>>>(
+	    static_cast<const uint8_t*>(d_rows), count, L, const_cast<float*>(out->lor),
+	    const_cast<float*>(out->orient), const_cast<float*>(out->tof_ps),
+	    const_cast<int32_t*>(out->frame), const_cast<float*>(out->measurement),
+	    const_cast<float*>(out->sens), const_cast<float*>(out->att),
+	    const_cast<float*>(out->additive));
+	YRTB_LAUNCHED();
+	return YRTB_OK;
+}
 
 yrtb_status yrtb_events_gather(const yrtb_events* in, const uint64_t* d_perm,
                                const yrtb_events* out, yrtb_stream stream)
@@ -4275,6 +4404,7 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	twin(ev->d1, 4, reinterpret_cast<const void**>(&A.d1), reinterpret_cast<const void**>(&B.d1));
 	twin(ev->d2, 4, reinterpret_cast<const void**>(&A.d2), reinterpret_cast<const void**>(&B.d2));
 	twin(ev->lor, 24, reinterpret_cast<const void**>(&A.lor), reinterpret_cast<const void**>(&B.lor));
+	twin(ev->orient, 24, reinterpret_cast<const void**>(&A.orient), reinterpret_cast<const void**>(&B.orient));
 	twin(ev->tof_ps, 4, reinterpret_cast<const void**>(&A.tof_ps), reinterpret_cast<const void**>(&B.tof_ps));
 	twin(ev->frame, 4, reinterpret_cast<const void**>(&A.frame), reinterpret_cast<const void**>(&B.frame));
 	twin(ev->motion_frame, 4, reinterpret_cast<const void**>(&A.motion_frame), reinterpret_cast<const void**>(&B.motion_frame));

@@ -60,7 +60,14 @@ class yrtb_events(ctypes.Structure):
     _fields_ = [("d1", c_vp), ("d2", c_vp), ("lor", c_vp), ("tof_ps", c_vp),
                 ("frame", c_vp), ("motion_frame", c_vp), ("motion", c_vp),
                 ("num_motion_frames", c_u64), ("measurement", c_vp), ("sens", c_vp), ("att", c_vp),
-                ("additive", c_vp), ("count", c_u64)]
+                ("additive", c_vp), ("count", c_u64), ("orient", c_vp)]
+
+
+class yrtb_row_layout(ctypes.Structure):
+    _fields_ = [("row_bytes", ctypes.c_uint32)] + \
+               [(n, ctypes.c_int32) for n in
+                ("lor", "det_orient", "tof", "dynamic_frame", "measurement",
+                 "sensitivity", "attenuation", "randoms", "scatter")]
 
 
 class yrtb_range(ctypes.Structure):
@@ -147,6 +154,8 @@ SIGNATURES = {
                                   c_vp, c_vp], ctypes.c_int),
     "yrtb_events_gather": ([_P(yrtb_events), c_vp, _P(yrtb_events), c_vp],
                            ctypes.c_int),
+    "yrtb_events_from_rows": ([c_vp, c_u64, _P(yrtb_row_layout), _P(yrtb_events),
+                               c_vp], ctypes.c_int),
     "yrtb_unpack_listmode": ([c_vp, c_u64, ctypes.c_int, ctypes.c_int,
                               ctypes.c_uint32, c_vp, c_vp, c_vp, c_vp, c_vp,
                               c_vp], ctypes.c_int),

@@ -625,12 +625,16 @@ class DeviceEvents:
     att: Optional[torch.Tensor] = None
     additive: Optional[torch.Tensor] = None
     perm: Optional[torch.Tensor] = None
+    orient: Optional[torch.Tensor] = None
     _c_cache: object = field(default=None, repr=False)
 
     @staticmethod
     def from_arrays(d1=None, d2=None, *, lor=None, tof=None, frame=None,
                     motion_frame=None, motion=None, measurement=None,
-                    sens=None, att=None, additive=None, device="cuda"):
+                    sens=None, att=None, additive=None, orient=None,
+                    device="cuda"):
+        """orient (with lor): crystal orientations n1, n2, 6 floats per
+        event, for distance-driven and multi-ray projection."""
         n = len(d1) if d1 is not None else len(lor)
         return DeviceEvents(
             n, _dev(d1, torch.int32, device), _dev(d2, torch.int32, device),
@@ -640,7 +644,8 @@ class DeviceEvents:
             _dev(motion, torch.float32, device),
             _dev(measurement, torch.float32, device),
             _dev(sens, torch.float32, device), _dev(att, torch.float32, device),
-            _dev(additive, torch.float32, device))
+            _dev(additive, torch.float32, device),
+            orient=_dev(orient, torch.float32, device))
 
     @staticmethod
     def from_listmode(lm: ListModeLUT) -> "DeviceEvents":
@@ -655,7 +660,8 @@ class DeviceEvents:
                              _ptr(self.tof), _ptr(self.frame),
                              _ptr(self.motion_frame), _ptr(self.motion), nm,
                              _ptr(self.measurement), _ptr(self.sens),
-                             _ptr(self.att), _ptr(self.additive), self.count)
+                             _ptr(self.att), _ptr(self.additive), self.count,
+                             _ptr(self.orient))
 
 
 # ---------------------------------------------------------------- projector --
@@ -812,7 +818,7 @@ class DeviceProjector:
         out = DeviceEvents(n, like(ev.d1), like(ev.d2), like(ev.lor),
                            like(ev.tof), like(ev.frame), like(ev.motion_frame),
                            ev.motion, like(ev.measurement), like(ev.sens),
-                           like(ev.att), like(ev.additive))
+                           like(ev.att), like(ev.additive), orient=like(ev.orient))
         L.check(L.lib().yrtb_events_gather(ctypes.byref(ev.c()), perm.data_ptr(),
                                            ctypes.byref(out.c()), _stream()))
         out.perm = perm
