@@ -674,15 +674,18 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
  * hosts own every byte of device memory through their own pool, or run
  * inside a real-time loop where cudaMalloc / cudaFree (which synchronise the
  * device) are not allowed after start-up; they still have to reconstruct.
- * The scratch (EM image and scaled sensitivity, (nt + 1) x voxels floats)
- * lives in one static device array of YRTB_OSEM_STATIC_MAX_FLOATS floats
- * (16 MiB) that every GPU loading the library holds until exit; larger images
- * are rejected with YRTB_ERR_ARGUMENT.  use_graph must be 0.  The first call
- * on a device looks up the array's device address (with that device
- * current); make that first call before any stream capture.  All calls share
- * the one array: calls that overlap on the GPU (other streams, other host
- * threads, same device) race and must be serialised by the caller.  No
- * counterpart in the reference. */
+ * The scratch (EM image and scaled sensitivity: (nt + 1) x voxels floats;
+ * with an image-space PSF also the blurred image and the PSF's temporary:
+ * (3 nt + 1) x voxels floats) lives in one static device array of
+ * YRTB_OSEM_STATIC_MAX_FLOATS floats (16 MiB) that every GPU loading the
+ * library holds until exit; larger images are rejected with
+ * YRTB_ERR_ARGUMENT.  use_graph must be 0.  Every call looks up the array's
+ * device address with the projector's device current; the first call on a
+ * device may load the library's device code, which is when the array is
+ * allocated, so make it during start-up, before any stream capture.  All
+ * calls share the one array: calls that overlap on the GPU (other streams,
+ * other host threads, same device) race and must be serialised by the
+ * caller.  No counterpart in the reference. */
 #define YRTB_OSEM_STATIC_MAX_FLOATS (4u * 1024u * 1024u)
 yrtb_status yrtb_osem_listmode_static(yrtb_projector* h, const yrtb_events* ev,
                                       const float* d_sens, float* d_image,

@@ -72,6 +72,59 @@ def test_static_osem_matches_work_buffer_osem_twice():
         assert rel_l2(img, ref) < 1e-5
 
 
+def test_static_osem_allocates_nothing():
+    # The property the entry point exists for: once the library's device
+    # code is loaded (first call), a call changes neither the device's free
+    # memory (cudaMemGetInfo: no cudaMalloc, no memory-pool growth) nor
+    # torch's reserved memory.
+    ip, proj, ev, sens = _problem(48, 48, 24)
+    evc = ev.c()
+    p = _params()
+    img = torch.empty(ip.numVoxels, device="cuda")
+
+    def call():
+        L.check(L.lib().yrtb_osem_listmode_static(
+            proj.h, ctypes.byref(evc), sens.data_ptr(), img.data_ptr(),
+            ctypes.byref(p), _stream()))
+        torch.cuda.synchronize()
+
+    call()
+    free0 = torch.cuda.mem_get_info()[0]
+    reserved0 = torch.cuda.memory_reserved()
+    call()
+    call()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_reserved() == reserved0
+    assert torch.isfinite(img).all()
+
+
+def test_static_osem_with_image_psf_matches_work_buffer_osem():
+    # With an image-space PSF the scratch also holds the blurred image and
+    # the PSF's temporary ((3 nt + 1) x voxels): same image as the work-buffer
+    # driver given a (3 nt + 1) x voxels buffer, on two calls in a row.
+    from pyyrtpet_b200 import OperatorPsfDevice
+    ip, proj, ev, sens = _problem()
+    J = ip.numVoxels
+    k = np.array([0.25, 0.5, 0.25], np.float32)
+    psf = OperatorPsfDevice(k, k, k)
+    evc = ev.c()
+    p = L.yrtb_osem_params(2, 3, 1.0, 1e-35, 1.19209e-07, 0, 0, None, None,
+                           psf.handle, None)
+    ref = torch.empty(J, device="cuda")
+    work = torch.empty(4 * J, device="cuda")
+    L.check(L.lib().yrtb_osem_listmode(proj.h, ctypes.byref(evc), sens.data_ptr(),
+                                       ref.data_ptr(), work.data_ptr(),
+                                       ctypes.byref(p), _stream()))
+    for _ in range(2):
+        img = torch.empty(J, device="cuda")
+        L.check(L.lib().yrtb_osem_listmode_static(
+            proj.h, ctypes.byref(evc), sens.data_ptr(), img.data_ptr(),
+            ctypes.byref(p), _stream()))
+        torch.cuda.synchronize()
+        assert torch.isfinite(img).all()
+        assert rel_l2(img, ref) < 1e-5
+
+
 def test_static_osem_rejects_oversized_images_and_graphs():
     sc = S.scanner_c1()
     big = yrt.ImageParams(256, 256, 64, 256, 256, 128)   # 2 x 4.19M floats > 4M
@@ -86,6 +139,7 @@ def test_static_osem_rejects_oversized_images_and_graphs():
                                            ctypes.byref(p), _stream())
     assert rc == L.YRTB_ERR_ARGUMENT
     assert b"too large" in L.lib().yrtb_last_error()
+    assert b"(3nt+1) x voxels with one" in L.lib().yrtb_last_error()
     small = yrt.ImageParams(16, 16, 8, 256, 256, 128)
     proj2 = yrt.DeviceProjector(sc, small, yrt.ProjectorParams(sc))
     pg = _params(use_graph=1)

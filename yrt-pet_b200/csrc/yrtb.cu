@@ -4538,28 +4538,20 @@ static __device__ __align__(256) float g_osemStaticScratch[YRTB_OSEM_STATIC_MAX_
 
 namespace
 {
-// Device address of g_osemStaticScratch per device.  In host code the array's
-// name is only a host-side stand-in, so the address is looked up once per
-// device with that device current.
-yrtb_status osemStaticScratch(int device, float** out)
+// Device address of g_osemStaticScratch on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// with the device current, on every call: the lookup allocates nothing once
+// the module is loaded, and an address kept from before a device reset would
+// point into a context that no longer exists.
+yrtb_status osemStaticScratch(float** out)
 {
-	constexpr int kMaxDevices = 64;
-	static std::mutex lock;
-	static float* addr[kMaxDevices] = {};
-	if (device < 0 || device >= kMaxDevices)
-		return fail(YRTB_ERR_ARGUMENT, "device index out of range");
-	std::lock_guard<std::mutex> guard(lock);
-	if (addr[device] == nullptr)
-	{
-		void* p = nullptr;
-		const cudaError_t e = cudaGetSymbolAddress(&p, g_osemStaticScratch);
-		if (e != cudaSuccess || p == nullptr)
-			return fail(YRTB_ERR_CUDA,
-			            std::string("cudaGetSymbolAddress(osem static scratch): ") +
-			                cudaGetErrorString(e));
-		addr[device] = static_cast<float*>(p);
-	}
-	*out = addr[device];
+	void* p = nullptr;
+	const cudaError_t e = cudaGetSymbolAddress(&p, g_osemStaticScratch);
+	if (e != cudaSuccess || p == nullptr)
+		return fail(YRTB_ERR_CUDA,
+		            std::string("cudaGetSymbolAddress(osem static scratch): ") +
+		                cudaGetErrorString(e));
+	*out = static_cast<float*>(p);
 	return YRTB_OK;
 }
 }  // namespace
@@ -4583,13 +4575,14 @@ extern "C" yrtb_status yrtb_osem_listmode_static(yrtb_projector* h,
 	if (need > YRTB_OSEM_STATIC_MAX_FLOATS)
 		return fail(YRTB_ERR_ARGUMENT,
 		            "image too large for yrtb_osem_listmode_static: needs " +
-		                std::to_string(need) + " floats of scratch ((nt+1) x voxels), "
+		                std::to_string(need) + " floats of scratch ((nt+1) x voxels "
+		                "without an image-space PSF, (3nt+1) x voxels with one), "
 		                "the static buffer holds " +
 		                std::to_string(static_cast<uint64_t>(YRTB_OSEM_STATIC_MAX_FLOATS)) +
 		                "; use yrtb_osem_listmode with a caller-provided work buffer");
 	YRTB_CUDA(cudaSetDevice(h->device));
 	float* scratch = nullptr;
-	const yrtb_status st = osemStaticScratch(h->device, &scratch);
+	const yrtb_status st = osemStaticScratch(&scratch);
 	if (st != YRTB_OK)
 		return st;
 	// The shared driver overwrites the sensitivity part and clears the EM
