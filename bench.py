@@ -94,7 +94,9 @@ def build_workload(n_events, device, seed=SEED, lut=None):
         sc.setDetectorLUT(lut)
     ip = S.image_c2()
     ph = S.Phantom(cyl_half_length=sc.axialFOV / 2)
-    eff = S.crystal_efficiencies(sc, seed + 1, device=device)
+    # One scanner for every shard: the efficiencies do not depend on the
+    # events' seed.
+    eff = S.crystal_efficiencies(sc, SEED + 1, device=device)
     ev = S.generate_events(sc, n_events, seed, phantom=ph, tof_fwhm_ps=TOF_FWHM,
                            mu_per_mm=0.0096, crystal_eff=eff,
                            randoms_fraction=0.2, device=device)
@@ -462,6 +464,7 @@ def main():
     import pyyrtpet_b200 as yrt
     from pyyrtpet_b200 import _lib as L
     from pyyrtpet_b200.core import _stream
+    from pyyrtpet_b200.distributed import local_subset_range
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -474,7 +477,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
+    # Rank r holds events [r * n_local, (r + 1) * n_local) of one stream
+    # (weak scaling: n_local per GPU); an event's OSEM subset is its global
+    # index mod SUBSETS, as the reference's interleaved subsets of the whole
+    # stream.
     n_local = args.events
+    first_global = rank * n_local
     sc, ip, ph, eff, evs, mu = build_workload(n_local, "cuda",
                                               seed=SEED + 7919 * rank)
     pp = yrt.ProjectorParams(sc)
@@ -491,7 +499,7 @@ def main():
     ev.sens = proj.gather_crystal_product(eff, ev)
     mu_flat = mu.reshape(-1).contiguous()
     ev.att = proj.attenuation_factors(mu_flat, ip, ev)
-    additive = additive_per_event(sc, args.events)
+    additive = additive_per_event(sc, args.events * world)
     ev.additive = torch.full((ev.count,), additive, device="cuda")
     torch.cuda.synchronize()
 
@@ -503,9 +511,9 @@ def main():
     sens_proj = yrt.DeviceProjector(sc, ip, sens_pp)
     sens = torch.zeros(ip.numVoxels, device="cuda")
     t_sens = time.perf_counter()
-    for part in range(20):
-        sens_proj.sensitivity_histo3d(sens, 20, part, mu=mu_flat, mu_params=ip,
-                                      crystal_eff=eff)
+    # Each rank back-projects its share of the 20 parts; one all-reduce.
+    from pyyrtpet_b200.distributed import sensitivity_histo3d as sharded_sens
+    sharded_sens(sens_proj, sens, 20, mu=mu_flat, mu_params=ip, crystal_eff=eff)
     L.check(L.lib().yrtb_apply_threshold(sens.data_ptr(), sens.data_ptr(),
                                          ip.numVoxels, 1, 1, 1.0, 0.0, 0.0,
                                          1.0, 0.0, _stream()))
@@ -531,7 +539,8 @@ def main():
     # Plain form: events in file order, subset = interleaved stride (the
     # reference's batching).  Ordered form: subset-major, LOR-sorted copy.
     ev_plain = ev
-    ev, offsets = proj.order_events(ev_plain, SUBSETS)
+    ev, offsets = proj.order_events(ev_plain, SUBSETS,
+                                    first_global_index=first_global)
     torch.cuda.synchronize()
 
     # Algorithmic traffic of the fused EM kernel: per event 24 B of event data
@@ -554,7 +563,8 @@ def main():
         for s in range(SUBSETS):
             L.check(lib.yrtb_fill(em.data_ptr(), J, 0.0, s_ptr))
             if plain:
-                r = L.yrtb_range(s, SUBSETS, 0)
+                r = L.yrtb_range(*local_subset_range(ev_plain.count, first_global,
+                                                     SUBSETS, s))
             else:
                 r = L.yrtb_range(int(offsets[s]), 1,
                                  int(offsets[s + 1] - offsets[s]))
@@ -670,7 +680,7 @@ def main():
             e.additive = d_add
             # Subset-major order first, then the corrections on the ordered
             # arrays (the attenuation walks run on grouped rays).
-            e, offs = proj.order_events(e, SUBSETS)
+            e, offs = proj.order_events(e, SUBSETS, first_global_index=first_global)
             released[k % 2].record(st)  # the ordered copy no longer reads it
             e.sens = proj.gather_crystal_product(eff_d, e)
             e.att = proj.attenuation_factors(mu_flat, ip, e)
@@ -687,7 +697,8 @@ def main():
                 # Sharded reconstruction: the EM image is summed over ranks
                 # once per subset (NCCL) between the EM pass and the update.
                 from pyyrtpet_b200.distributed import osem_listmode
-                osem_listmode(proj, e, offs, sens, x, ITERATIONS, SUBSETS)
+                osem_listmode(proj, e, offs, sens, x, ITERATIONS, SUBSETS,
+                              first_global_index=first_global)
             h_img.copy_(x, non_blocking=True)
 
         def run_steps(n, a=None):

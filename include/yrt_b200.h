@@ -357,6 +357,18 @@ yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
                                      uint64_t* subset_offsets,
                                      yrtb_stream stream);
 
+/* The same for one shard of a longer event stream: local event e is the
+ * stream's event first_global_index + e, and belongs to subset
+ * (first_global_index + e) mod num_subsets, so that shards cut anywhere keep
+ * the reference's subsets of the whole stream (BinIteratorChronological
+ * Interleaved, src/datastruct/projection/BinIterator.cpp:261-265).
+ * yrtb_events_subset_order is this with first_global_index = 0. */
+yrtb_status yrtb_events_subset_order_from(yrtb_projector* h, const yrtb_events* ev,
+                                          int num_subsets,
+                                          uint64_t first_global_index,
+                                          uint64_t* d_perm, uint64_t* subset_offsets,
+                                          yrtb_stream stream);
+
 /* Byte layout of one event row of the reference's device batches: the
  * projection-property rows of PropStructManager<ProjectionPropertyType>
  * (include/yrt-pet/datastruct/projection/ProjectionProperties.hpp:59-140,

@@ -75,3 +75,38 @@ def test_projection_oper_subsets_and_adjoint(kind, projector, tof, rays):
         assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
     if rays == 1:
         assert np.array_equal(Ax_sub, Ax)
+
+
+@pytest.mark.parametrize("kind", ["listmode", "histogram"])
+def test_operator_projector_device_reference_signatures(kind):
+    # OperatorProjectorDevice with the reference's pybind signatures
+    # (src/operators/OperatorProjectorDevice.cu:26-90): applyA(img, proj)
+    # writes into a ProjectionList (entries of other subsets untouched),
+    # applyAH(proj, img) adds into img; same values as ProjectionOper.
+    sc, data = _data(kind, False)
+    ip = yrt.ImageParams(*IP_ARGS)
+    pp = yrt.ProjectorParams(sc)
+    it = data.getBinIter(3, 1)
+    op = yrt.OperatorProjectorDevice.create(pp, it, img_params=ip)
+    rng = np.random.default_rng(62)
+    x = torch.from_numpy(rng.random(ip.shape, dtype=np.float32)).cuda()
+    pl = yrt.ProjectionListOwned(data)
+    pl.allocate()
+    pl.clearProjections(-1.0)
+    op.applyA(x, pl)
+    A = yrt.ProjectionOper(sc, ip, data, idx_subset=1, num_subsets=3)
+    ref = A.A(x.cpu().numpy())
+    idx = np.asarray(it.indices()) if kind == "histogram" else np.arange(1, data.count(), 3)
+    got = pl.getProjectionsArray()
+    assert np.array_equal(got[idx], ref[idx])
+    outside = np.setdiff1d(np.arange(data.count()), idx)
+    assert np.all(got[outside] == -1.0)
+    y = yrt.ProjectionListOwned(data)
+    y.allocate()
+    y.values.copy_(torch.from_numpy(rng.random(data.count(), dtype=np.float32)))
+    img = torch.zeros(ip.shape, device="cuda")
+    op.applyAH(y, img)
+    bp = A.At(y.getProjectionsArray())
+    assert np.allclose(img.cpu().numpy(), bp, rtol=1e-5, atol=1e-6)
+    with pytest.raises(RuntimeError):
+        op.applyA(x, data)          # a ProjectionList receives the values

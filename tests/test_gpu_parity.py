@@ -717,6 +717,37 @@ def test_event_ordering_is_subset_major_permutation():
     assert rel_l2(em_b.cpu().numpy(), em_a.cpu().numpy()) < 1e-5
 
 
+@pytest.mark.parametrize("first", [0, 3, 10**9 + 5])
+def test_event_ordering_of_a_shard_keeps_global_subsets(first):
+    # A shard whose first event has global index `first`: local event e is
+    # in subset (first + e) mod S; the subset-major order and its offsets
+    # follow that rule, and a shard's EM pass over a subset equals the pass
+    # over the same events of the whole stream.
+    from pyyrtpet_b200.distributed import local_subset_range
+    sc, ip, p = make(tof=(214.0, 5))
+    d1, d2 = random_events(SC_ARGS, 30003, 27)
+    rng = np.random.default_rng(28)
+    tv = rng.normal(0, 300, len(d1)).astype(np.float32)
+    ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv)
+    S = 7
+    out, offs = p.order_events(ev, S, first_global_index=first)
+    perm = out.perm.cpu().numpy()
+    n = len(d1)
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    img = torch.from_numpy(rng.uniform(0.5, 1.5, ip.shape).astype(np.float32)).cuda()
+    for s in range(S):
+        src = perm[offs[s]:offs[s + 1]]
+        assert np.all((first + src) % S == s)
+        start, stride, count = local_subset_range(n, first, S, s)
+        assert count == len(src)
+        if s == 2:
+            em_a = torch.zeros(ip.shape, device="cuda")
+            em_b = torch.zeros(ip.shape, device="cuda")
+            p.em_step(img, em_a, ev, rng=L.yrtb_range(start, stride, count))
+            p.em_step(img, em_b, out, rng=L.yrtb_range(int(offs[s]), 1, count))
+            assert rel_l2(em_b.cpu().numpy(), em_a.cpu().numpy()) < 1e-5
+
+
 @needs_ref
 @pytest.mark.parametrize("grid", [(32, 32, 16, 256, 256, 128), (64, 64, 32, 256, 256, 128)])
 def test_attenuation_factors_mirror_equal_reference_fp32(grid):

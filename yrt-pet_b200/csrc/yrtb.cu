@@ -1265,7 +1265,8 @@ __device__ __forceinline__ uint64_t spatialKey(const KParams& P, float3 p1, floa
 // of similar length keeps the threads of a warp iterating together; the LOR
 // key keeps neighbouring rays together.
 __global__ void k_order_keys(KParams P, H3Dev H, bool hasH3, Events E, uint64_t n,
-                             uint64_t numSubsets, const uint32_t* __restrict__ counts,
+                             uint64_t numSubsets, uint64_t first,
+                             const uint32_t* __restrict__ counts,
                              int bucketShift, int lorShift, int spatial, float cell,
                              unsigned long long* __restrict__ keys,
                              unsigned long long* __restrict__ vals)
@@ -1305,12 +1306,12 @@ __global__ void k_order_keys(KParams P, H3Dev H, bool hasH3, Events E, uint64_t 
 			// is traced at a time and stays L2 resident.
 			const int f = __ldg(E.frame + e);
 			const uint64_t fk = f < 0 ? 255u : static_cast<uint64_t>(min(f, 254));
-			keys[e] = ((e % numSubsets) << 52) | (fk << 44) | (bucket << 37) |
+			keys[e] = (((first + e) % numSubsets) << 52) | (fk << 44) | (bucket << 37) |
 			          ((lorKey & 0x1FFFFFFFULL) << 8) | q;
 		}
 		else
 		{
-			keys[e] = ((e % numSubsets) << 48) | (bucket << 41) |
+			keys[e] = (((first + e) % numSubsets) << 48) | (bucket << 41) |
 			          ((lorKey & 0x1FFFFFFFFULL) << 8) | q;
 		}
 		vals[e] = e;
@@ -2736,7 +2737,7 @@ yrtb_status dispatchHisto(yrtb_projector* h, int numSubsets, int subset,
 // with the ordering parameters of cfg.
 yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
                         const yrtb_launch_config& cfg, uint64_t* d_perm,
-                        cudaStream_t st)
+                        cudaStream_t st, uint64_t first = 0)
 {
 	const uint64_t n = ev->count;
 	if (n == 0)
@@ -2786,8 +2787,8 @@ yrtb_status orderEvents(yrtb_projector* h, const yrtb_events* ev, uint64_t S,
 	const float voxel = std::max(h->P.g.vx, std::max(h->P.g.vy, h->P.g.vz));
 	const float cell = voxel * static_cast<float>(1 << cfg.tile_shift);
 	k_order_keys<<<gridFor(n, 16), kBlock, 0, st>>>(
-	    h->P, h->h3d, h->h3 != nullptr, toDev(ev), n, S, counts, cfg.bucket_shift,
-	    lorShift, cfg.order, cell, keys, vals);
+	    h->P, h->h3d, h->h3 != nullptr, toDev(ev), n, S, first % S, counts,
+	    cfg.bucket_shift, lorShift, cfg.order, cell, keys, vals);
 	// Only the key bits in use are sorted: the subset field ends at bit
 	// (frames ? 52 : 48) + bits(S - 1).
 	int sBits = 0;
@@ -3145,21 +3146,37 @@ yrtb_status yrtb_multiray_table(yrtb_projector* h, uint64_t count,
 	return YRTB_OK;
 }
 
-yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
-                                     int num_subsets, uint64_t* d_perm,
-                                     uint64_t* subset_offsets,
-                                     yrtb_stream stream)
+yrtb_status yrtb_events_subset_order_from(yrtb_projector* h, const yrtb_events* ev,
+                                          int num_subsets,
+                                          uint64_t first_global_index,
+                                          uint64_t* d_perm, uint64_t* subset_offsets,
+                                          yrtb_stream stream)
 {
 	if (!h || !ev || (!d_perm && ev->count > 0) || !subset_offsets || num_subsets <= 0 ||
 	    num_subsets > (ev->frame ? 4095 : 65535))
 		return fail(YRTB_ERR_ARGUMENT, "invalid subset-order arguments");
 	const uint64_t n = ev->count;
 	const uint64_t S = static_cast<uint64_t>(num_subsets);
+	const uint64_t r = first_global_index % S;
+	// Subset s holds the local events e with (r + e) mod S == s: the first
+	// is e = (s - r) mod S, then every S-th.
 	subset_offsets[0] = 0;
 	for (uint64_t s = 0; s < S; s++)
-		subset_offsets[s + 1] = subset_offsets[s] + (n > s ? (n - s + S - 1) / S : 0);
+	{
+		const uint64_t k = (s + S - r) % S;
+		subset_offsets[s + 1] = subset_offsets[s] + (n > k ? (n - k + S - 1) / S : 0);
+	}
 	return orderEvents(h, ev, S, h->launch, d_perm,
-	                   reinterpret_cast<cudaStream_t>(stream));
+	                   reinterpret_cast<cudaStream_t>(stream), first_global_index);
+}
+
+yrtb_status yrtb_events_subset_order(yrtb_projector* h, const yrtb_events* ev,
+                                     int num_subsets, uint64_t* d_perm,
+                                     uint64_t* subset_offsets,
+                                     yrtb_stream stream)
+{
+	return yrtb_events_subset_order_from(h, ev, num_subsets, 0, d_perm,
+	                                     subset_offsets, stream);
 }
 
 }  // extern "C"

@@ -8,7 +8,8 @@ from ._lib import YrtbError, lib  # noqa: F401
 from .core import (BinIteratorChronologicalInterleaved,  # noqa: F401
                    BinIteratorRangeHistogram3D, DeviceEvents, DeviceProjector,
                    Histogram3D, ImageParams, ListModeLUT,
-                   OperatorProjectorDevice, ProjectionOper, ProjectorParams,
+                   OperatorProjectorDevice, ProjectionList,
+                   ProjectionListOwned, ProjectionOper, ProjectorParams,
                    Scanner, UniformHistogram, convertToHistogram3D,
                    histo3d_bins, histo3d_detpairs, read_psf_csv,
                    release_cached_memory, write_psf_csv)

@@ -152,6 +152,8 @@ SIGNATURES = {
                                   _P(c_u64), c_vp], ctypes.c_int),
     "yrtb_events_subset_order": ([c_vp, _P(yrtb_events), ctypes.c_int, c_vp,
                                   c_vp, c_vp], ctypes.c_int),
+    "yrtb_events_subset_order_from": ([c_vp, _P(yrtb_events), ctypes.c_int, c_u64,
+                                       c_vp, c_vp, c_vp], ctypes.c_int),
     "yrtb_events_gather": ([_P(yrtb_events), c_vp, _P(yrtb_events), c_vp],
                            ctypes.c_int),
     "yrtb_events_from_rows": ([c_vp, c_u64, _P(yrtb_row_layout), _P(yrtb_events),

@@ -805,15 +805,20 @@ class DeviceProjector:
                 "tried": [(cfg(rep.tried[i]), float(rep.ms[i]))
                           for i in range(rep.num_tried)]}
 
-    def order_events(self, ev: DeviceEvents, num_subsets: int):
-        """Subset-major, LOR-sorted copy of the events (yrtb_events_subset_order
-        + yrtb_events_gather).  Returns (events, subset offsets)."""
+    def order_events(self, ev: DeviceEvents, num_subsets: int,
+                     first_global_index: int = 0):
+        """Subset-major, LOR-sorted copy of the events (yrtb_events_subset_
+        order_from + yrtb_events_gather); event e belongs to subset
+        (first_global_index + e) mod num_subsets (a shard of a longer stream
+        starts at its first event's global index).  Returns (events, subset
+        offsets)."""
         n = ev.count
         perm = torch.empty(n, dtype=torch.int64, device="cuda")
         offs = np.zeros(num_subsets + 1, np.uint64)
-        L.check(L.lib().yrtb_events_subset_order(
-            self.h, ctypes.byref(ev.c()), int(num_subsets), perm.data_ptr(),
-            offs.ctypes.data, _stream()))
+        L.check(L.lib().yrtb_events_subset_order_from(
+            self.h, ctypes.byref(ev.c()), int(num_subsets),
+            int(first_global_index), perm.data_ptr(), offs.ctypes.data,
+            _stream()))
         like = lambda t: None if t is None else torch.empty_like(t)
         out = DeviceEvents(n, like(ev.d1), like(ev.d2), like(ev.lor),
                            like(ev.tof), like(ev.frame), like(ev.motion_frame),
@@ -969,28 +974,102 @@ def convertToHistogram3D(lm: ListModeLUT, values=None) -> Histogram3D:
 
 
 # --------------------------------------------------- OperatorProjectorDevice --
+class ProjectionList:
+    """Projection values over the bins of a projection data object, on the
+    GPU: the reference's ProjectionListOwned
+    (include/yrt-pet/datastruct/projection/ProjectionList.hpp:21-84), one
+    float per list-mode event or histogram bin, that
+    OperatorProjectorDevice.applyA writes and applyAH reads."""
+
+    def __init__(self, reference):
+        self.reference = reference
+        self.values: Optional[torch.Tensor] = None
+
+    def allocate(self):
+        self.values = torch.zeros(self.reference.count(), dtype=torch.float32,
+                                  device="cuda")
+
+    def count(self) -> int:
+        return self.reference.count()
+
+    def getBinIter(self, numSubsets: int, idxSubset: int):
+        return self.reference.getBinIter(numSubsets, idxSubset)
+
+    def _require(self):
+        if self.values is None:
+            raise RuntimeError("ProjectionList memory is not allocated")
+        return self.values
+
+    def getProjectionValue(self, i: int) -> float:
+        return float(self._require()[i])
+
+    def setProjectionValue(self, i: int, v: float):
+        self._require()[i] = float(v)
+
+    def clearProjections(self, v: float = 0.0):
+        self._require().fill_(float(v))
+
+    def getProjectionsArray(self) -> np.ndarray:
+        return self._require().cpu().numpy()
+
+
+ProjectionListOwned = ProjectionList
+
+
 class OperatorProjectorDevice:
     """Projection operator A (applyA) and its adjoint (applyAH) over the bins
-    of one BinIterator, on the GPU."""
+    of one BinIterator, on the GPU, with the reference's pybind signatures
+    (src/operators/OperatorProjectorDevice.cu:26-90): applyA(img, proj)
+    writes A img into the ProjectionList proj (its entries outside the bin
+    iterator untouched), applyAH(proj, img) adds A^T proj to img.  Images are
+    float32 CUDA tensors of the operator's image parameters (create(...,
+    img_params=...) or setImageParams)."""
 
-    def __init__(self, proj_params: ProjectorParams, bin_iter, img_params=None):
+    def __init__(self, proj_params: ProjectorParams, bin_iter=None,
+                 img_params: Optional[ImageParams] = None):
         self.proj_params = proj_params
         self.bin_iter = bin_iter
         self.img_params = img_params
         self._proj = None
 
     @staticmethod
-    def create(proj_params: ProjectorParams, bin_iter, constraints=None,
-               mem_available: int = 0, img_params: ImageParams | None = None):
+    def create(proj_params: ProjectorParams, bin_iter, constraints=(),
+               mem_available: int = 0, img_params: Optional[ImageParams] = None):
+        """OperatorProjectorDevice::create (OperatorProjectorDevice.cuh:27-31).
+        Detector constraints and a memory budget are not supported: events
+        stay resident on the device instead of being loaded in batches, and
+        constraints would have to filter them first; both raise."""
+        if constraints:
+            raise RuntimeError("libyrtb projectors take no detector constraints: "
+                               "filter the events before projecting them")
+        if mem_available:
+            raise RuntimeError("libyrtb projectors keep the events resident on "
+                               "the device and take no memory budget "
+                               "(mem_available must be 0)")
         return OperatorProjectorDevice(proj_params, bin_iter, img_params)
 
-    def _projector(self, img_params: ImageParams) -> DeviceProjector:
-        if self._proj is None or self._proj.img_params is not img_params:
-            self._proj = DeviceProjector(self.proj_params.scanner, img_params,
+    def setImageParams(self, img_params: ImageParams):
+        self.img_params = img_params
+
+    def getBinIter(self):
+        return self.bin_iter
+
+    def setBinIter(self, bin_iter):
+        self.bin_iter = bin_iter
+
+    def _projector(self, img_params: Optional[ImageParams] = None) -> DeviceProjector:
+        ip = img_params or self.img_params
+        if ip is None:
+            raise RuntimeError("The operator has no image parameters (give "
+                               "img_params to create() or setImageParams)")
+        if self._proj is None or self._proj.img_params is not ip:
+            self._proj = DeviceProjector(self.proj_params.scanner, ip,
                                          self.proj_params)
         return self._proj
 
     def _events(self, projData):
+        if isinstance(projData, ProjectionList):
+            projData = projData.reference
         if isinstance(projData, ListModeLUT):
             return projData.device_events(), self.bin_iter._range()
         if isinstance(projData, Histogram3D):
@@ -998,32 +1077,47 @@ class OperatorProjectorDevice:
             d1, d2 = histo3d_detpairs(projData.scanner, bins)
             ev = DeviceEvents.from_arrays(d1, d2)
             return ev, None
-        raise RuntimeError("unsupported projection data type")
+        raise RuntimeError("The Projection Data provided is not a "
+                           "ProjectionList, ListModeLUT nor Histogram3D")
 
-    def applyA(self, img: torch.Tensor, projData, img_params: ImageParams):
-        """Returns the projection values of every bin of projData (entries
-        outside the bin iterator stay zero)."""
-        p = self._projector(img_params)
-        ev, rng = self._events(projData)
-        if isinstance(projData, Histogram3D):
-            out_sub = p.forward(img.contiguous(), DeviceEvents(
-                ev.count, ev.d1, ev.d2, tof=None))
-            out = torch.zeros(projData.count(), dtype=torch.float32,
-                              device=img.device)
-            idx = torch.from_numpy(self.bin_iter.indices()).to(img.device)
-            out[idx] = out_sub
-            return out
-        out = torch.zeros(ev.count, dtype=torch.float32, device=img.device)
-        return p.forward(img.contiguous(), ev, out=out, rng=rng)
+    def _check_image(self, img: torch.Tensor, p: DeviceProjector):
+        if not isinstance(img, torch.Tensor) or not img.is_cuda:
+            raise RuntimeError("The image provided is not a CUDA tensor")
+        if img.numel() != p.img_params.nt * p.img_params.numVoxels:
+            raise RuntimeError("The image does not match the operator's image "
+                               "parameters")
 
-    def applyAH(self, values: torch.Tensor, projData, img_params: ImageParams,
-                img: torch.Tensor | None = None):
-        p = self._projector(img_params)
-        ev, rng = self._events(projData)
-        if isinstance(projData, Histogram3D):
-            idx = torch.from_numpy(self.bin_iter.indices()).to(values.device)
-            return p.backward(values[idx].contiguous(), ev, img=img)
-        return p.backward(values.contiguous(), ev, img=img, rng=rng)
+    def applyA(self, img: torch.Tensor, proj: ProjectionList):
+        """proj.values[bins of the iterator] = A img."""
+        if not isinstance(proj, ProjectionList):
+            raise RuntimeError("applyA writes into a ProjectionList "
+                               "(ProjectionListOwned(data).allocate())")
+        p = self._projector()
+        self._check_image(img, p)
+        vals = proj._require()
+        ev, rng = self._events(proj)
+        x = img.contiguous()
+        if isinstance(proj.reference, Histogram3D):
+            idx = torch.from_numpy(self.bin_iter.indices().astype(np.int64)).to(img.device)
+            vals[idx] = p.forward(x, ev)
+            return proj
+        p.forward(x, ev, out=vals, rng=rng)
+        return proj
+
+    def applyAH(self, proj: ProjectionList, img: torch.Tensor):
+        """img += A^T proj.values over the bins of the iterator."""
+        if not isinstance(proj, ProjectionList):
+            raise RuntimeError("applyAH reads a ProjectionList")
+        p = self._projector()
+        self._check_image(img, p)
+        vals = proj._require()
+        ev, rng = self._events(proj)
+        if isinstance(proj.reference, Histogram3D):
+            idx = torch.from_numpy(self.bin_iter.indices().astype(np.int64)).to(vals.device)
+            p.backward(vals[idx].contiguous(), ev, img=img)
+            return img
+        p.backward(vals, ev, img=img, rng=rng)
+        return img
 
 
 class ProjectionOper:
@@ -1048,7 +1142,8 @@ class ProjectionOper:
         pp.projPsf_fname = proj_psf_fname or ""
         pp.numRays = num_rays
         self._proj_params = pp
-        self._oper = OperatorProjectorDevice.create(pp, self._binIter)
+        self._oper = OperatorProjectorDevice.create(pp, self._binIter,
+                                                    img_params=img_params)
         self._image_shape = img_params.shape
         self._lr = None
         if updater_type == "LR":
@@ -1078,8 +1173,10 @@ class ProjectionOper:
             ev, rng = self._oper._events(self._projData)
             out = torch.zeros(ev.count, dtype=torch.float32, device="cuda")
             return self._lr_projector().forward(xx, ev, out=out, rng=rng).cpu().numpy()
-        y = self._oper.applyA(xx, self._projData, self._img_params)
-        return y.cpu().numpy()
+        pl = ProjectionList(self._projData)
+        pl.allocate()
+        self._oper.applyA(xx, pl)
+        return pl.values.cpu().numpy()
 
     def At(self, y, W=None):
         """Back projection.  With the LR updater: onto W (rank images), or,
@@ -1096,5 +1193,8 @@ class ProjectionOper:
                     self._image_shape).cuda()
                 return lrp.backward_h(yy, Wt, ev, rng=rng).cpu().numpy()
             return lrp.backward(yy, ev, rng=rng).cpu().numpy()
-        x = self._oper.applyAH(yy, self._projData, self._img_params)
+        pl = ProjectionList(self._projData)
+        pl.values = yy.reshape(-1).contiguous()
+        x = torch.zeros(self._img_params.shape, dtype=torch.float32, device="cuda")
+        self._oper.applyAH(pl, x)
         return x.cpu().numpy()
