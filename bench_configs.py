@@ -198,6 +198,9 @@ def run_c5(args):
         sens_proj.sensitivity_histo3d(sens, 20, part)
     s_ptr = _stream()
     lib = L.lib()
+    # The reference's hard threshold (1.0) on the sensitivity image.
+    L.check(lib.yrtb_apply_threshold(sens.data_ptr(), sens.data_ptr(), J, 1, 1,
+                                     1.0, 0.0, 0.0, 1.0, 0.0, s_ptr))
 
     # Batched: one event set for all frames, subset-major / frame ordering,
     # one CUDA graph per subset replayed by yrtb_osem_listmode; launch
@@ -273,6 +276,76 @@ def run_c5(args):
                             "frame, file order, interleaved subsets)"}
     out["batched_over_plain"] = ms_p / ms_b
     out["frame_events"] = [int(c) for c in counts]
+    if not args.no_cpu_baseline:
+        out.update(_c5_reference(args, sc, ip1, nt, subsets, counts, d1, d2, ev.tof,
+                                 motion, sens, n / (ms_b * 1e-3)))
+    return out
+
+
+def _c5_reference(args, sc, ip1, nt, subsets, counts, d1, d2, tof, motion, sens,
+                  batched_value):
+    """The reference on the C5 workload (events/s of one OSEM iteration):
+    its CPU OSEM with DynamicFraming and LORMotion on a 2M-event sample
+    (frame shares kept), and its GPU OSEM_GPU (built for sm_100a) on all
+    events, both as one 4-D reconstruction and frame by frame (24 separate
+    single-frame reconstructions: the plain single-frame GPU form)."""
+    po = _po()
+    threads = os.cpu_count() or 1
+    out = {}
+    osc = _po_scanner(po, sc)
+    J = ip1.numVoxels
+    sens_np = sens.reshape(ip1.nz, ip1.ny, ip1.nx).cpu().numpy()
+    h1 = d1.cpu().numpy().view(np.uint32)
+    h2 = d2.cpu().numpy().view(np.uint32)
+    ht = tof.cpu().numpy()
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    frame_ts = (np.arange(nt + 1) * 1000).astype(np.uint32)
+    motion_starts = (np.arange(nt) * 1000).astype(np.uint32)
+    kw = dict(tof_fwhm_ps=214.0, tof_n_std=5, iterations=1, subsets=subsets,
+              threads=threads)
+    if po.ref_available():
+        # Sample: the first events of every frame, in the frames' proportions.
+        share = 2_000_000 / float(counts.sum())
+        take = np.maximum(1, np.round(counts * share)).astype(np.int64)
+        idx = np.concatenate([np.arange(starts[f], starts[f] + take[f]) for f in range(nt)])
+        ts = (np.repeat(np.arange(nt), take) * 1000 + 500).astype(np.uint32)
+        _, sec = po.ref_osem_listmode_dynamic(
+            osc, _po_image(po, ip1, nt=nt), sens_np, h1[idx], h2[idx], ts,
+            frame_ts=frame_ts, motion_starts=motion_starts, motion=motion,
+            tof=ht[idx], gpu=False, **kw)
+        out["cpu_baseline"] = {"value": len(idx) / sec, "unit": "events/s",
+                               "cores": threads, "kind": "reference",
+                               "sample": f"{len(idx)} events (every frame's first "
+                                         "events, frame shares kept), one OSEM "
+                                         f"iteration x {subsets} subsets with "
+                                         "DynamicFraming and LORMotion"}
+    if po.ref_gpu_available():
+        ts_all = (np.repeat(np.arange(nt), counts) * 1000 + 500).astype(np.uint32)
+        _, sec4 = po.ref_osem_listmode_dynamic(
+            osc, _po_image(po, ip1, nt=nt), sens_np, h1, h2, ts_all,
+            frame_ts=frame_ts, motion_starts=motion_starts, motion=motion,
+            tof=ht, gpu=True, **kw)
+        total = 0.0
+        for f in range(nt):
+            a, b = int(starts[f]), int(starts[f + 1])
+            _, secf = po.ref_osem_listmode_dynamic(
+                osc, _po_image(po, ip1, nt=1), sens_np, h1[a:b], h2[a:b],
+                np.full(b - a, 500, np.uint32),
+                frame_ts=np.array([0, 1000], np.uint32),
+                motion_starts=np.array([0], np.uint32), motion=motion[f:f + 1],
+                tof=ht[a:b], gpu=True, **kw)
+            total += secf
+        n = int(counts.sum())
+        out["plain_reference_gpu"] = {
+            "value": n / total, "unit": "events/s", "s_per_iteration": total,
+            "what": "reference OSEM_GPU (YRT-PET built for sm_100a) frame by "
+                    "frame: 24 single-frame reconstructions of one iteration, "
+                    "OSEM::reconstruct time summed"}
+        out["reference_gpu_4d"] = {
+            "value": n / sec4, "unit": "events/s", "s_per_iteration": sec4,
+            "what": "reference OSEM_GPU, one 4-D reconstruction of all frames "
+                    "(DynamicFraming + LORMotion), one iteration"}
+        out["batched_vs_plain_reference_gpu"] = batched_value / (n / total)
     return out
 
 
@@ -435,6 +508,31 @@ def run_c4(args):
     out["composed"] = {"value": per * 8 / (ms_c * 1e-3), "ms_per_step": ms_c,
                        "what": "SiddonProjectFn forward kernel + torch FP64 reductions + "
                                "adjoint kernel in backward"}
+    po = _po()
+    if po.ref_available() and not args.no_cpu_baseline:
+        # The reference CPU forward + back projection (util::forwProject /
+        # util::backProject) of the first phantom's first 1M events, TOF.
+        m = min(per, 1_000_000)
+        osc = _po_scanner(po, sc)
+        oip = _po_image(po, ip)
+        e0 = evs[0]
+        a = e0.d1[:m].cpu().numpy().view(np.uint32)
+        b = e0.d2[:m].cpu().numpy().view(np.uint32)
+        tv = e0.tof[:m].cpu().numpy()
+        xv = x[0].detach().cpu().numpy()
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        yv = po.ref_project_lm(osc, oip, a, b, tof=tv, image=xv, tof_fwhm_ps=214.0,
+                               tof_n_std=5, threads=threads)
+        w = np.where(yv > 1e-12, 1.0 / np.maximum(yv, 1e-12), 0.0).astype(np.float32)
+        po.ref_project_lm(osc, oip, a, b, tof=tv, values=w, fwd=False,
+                          tof_fwhm_ps=214.0, tof_n_std=5, threads=threads)
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": m / sec, "unit": "events/s",
+                               "cores": threads, "kind": "reference",
+                               "sample": f"{m} events of phantom 0: forward "
+                                         "projection, 1/y, back projection "
+                                         "(util::forwProject + util::backProject)"}
     return out
 
 
