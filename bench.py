@@ -64,6 +64,8 @@ def parse():
                     help="skip the parity and reference legs")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the reference OSEM_GPU leg")
+    ap.add_argument("--no-l2-peak", action="store_true",
+                    help="skip the live L2 request-throughput measurement")
     ap.add_argument("--precision", default="compensated",
                     choices=["mirror", "compensated"])
     ap.add_argument("--parity-sample", type=int, default=200_000)
@@ -195,6 +197,52 @@ def measured_peak_hbm():
         return float(json.load(open(p))["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+L2_MODES = {0: "red.f32", 1: "red.v4.f32", 2: "ld.cg.f32",
+            3: "ld.cg.f32 + red.v4.f32 (every warp)",
+            4: "ld.cg.f32 + red.v4.f32 (reading warps beside reducing warps)"}
+
+
+def measured_l2_request_rates(n_floats, reps=5):
+    """L2 request throughput of this GPU (requests/s), measured live with
+    libyrtb_l2bench.so: uniformly random aligned float groups inside two
+    L2-resident buffers of n_floats each (the sizes of the image read and of
+    the EM image reduced into), per request kind (L2_MODES), median of reps
+    launches timed with CUDA events after warm-up."""
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(ROOT, "yrt-pet_b200", "lib", "libyrtb_l2bench.so"))
+    lib.yrtb_l2bench_launch.restype = ctypes.c_int
+    lib.yrtb_l2bench_launch.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_uint, ctypes.c_void_p,
+                                        ctypes.c_void_p]
+    lib.yrtb_l2bench_requests.restype = ctypes.c_uint64
+    lib.yrtb_l2bench_requests.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint]
+    n = 2 * ((int(n_floats) // 4) * 4)
+    buf = torch.zeros(n, dtype=torch.float32, device="cuda")
+    sink = torch.zeros(1, dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream()
+    blocks = torch.cuda.get_device_properties(0).multi_processor_count * 8
+    iters = 96
+    out = {}
+    for mode in L2_MODES:
+        times = []
+        for r in range(reps + 2):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            rc = lib.yrtb_l2bench_launch(buf.data_ptr(), n, mode, iters, blocks,
+                                         sink.data_ptr(), st.cuda_stream)
+            b.record(st)
+            if rc != 0:
+                raise RuntimeError(f"yrtb_l2bench_launch: error {rc}")
+            torch.cuda.synchronize()
+            if r >= 2:
+                times.append(a.elapsed_time(b))
+        ms = sorted(times)[len(times) // 2]
+        out[L2_MODES[mode]] = lib.yrtb_l2bench_requests(mode, iters, blocks) / (ms * 1e-3)
+    del buf, sink
+    return out
 
 
 # ------------------------------------------------------------ reference legs --
@@ -751,6 +799,34 @@ def main():
             roofline["traffic"] = json.load(open(prof))["dram_bytes_per_launch"]
         except Exception:
             pass
+    # The kernel's L2 ceiling: its L2 requests per event (reads of the image
+    # by the forward walk, float4 reductions by the back projection; ncu
+    # counts for the same launch configuration) at the measured L2 request
+    # rate of the same mix on this GPU.
+    l2prof = os.path.join(ROOT, "profiles", "em_siddon_tof_c2_l2.json")
+    if not args.no_l2_peak and os.path.exists(l2prof):
+        rates = measured_l2_request_rates(J)
+        l2 = {"peak_requests_per_s": rates,
+              "peak_source": "measured live (libyrtb_l2bench.so: random aligned groups "
+                             "in an L2-resident buffer of the image's size)"}
+        cnt = json.load(open(l2prof))
+        launch = proj.get_launch()
+        if all(launch.get(k) == v for k, v in cnt["launch"].items()):
+            reqs = (cnt["red_requests_per_event"] + cnt["read_requests_per_event"]) \
+                * ev.count / SUBSETS
+            l2["requests_per_launch"] = reqs
+            l2["requests_source"] = cnt["source"]
+            l2["achieved_requests_per_s"] = reqs / (em_ms * 1e-3)
+            # The ceiling of a 1:1 mix of reads and reductions: the faster of
+            # the two ways of mixing them.
+            mix = max(rates[L2_MODES[3]], rates[L2_MODES[4]])
+            l2["peak_mix_requests_per_s"] = mix
+            roofline["l2_frac"] = l2["achieved_requests_per_s"] / mix
+        else:
+            l2["requests_per_launch"] = None
+            l2["requests_source"] = ("ncu counts were taken with launch "
+                                     f"{cnt['launch']}, this run chose {launch}")
+        roofline["l2"] = l2
 
     cpu = None
     parity = None

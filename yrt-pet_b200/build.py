@@ -1,8 +1,10 @@
-"""Builds libyrtb.so (the sm_100a kernels + C ABI) in-tree with nvcc.
+"""Builds libyrtb.so (the sm_100a kernels + C ABI) in-tree with nvcc, and
+libyrtb_l2bench.so (the L2 request-throughput measurement the benchmark's
+roofline uses).
 
     python yrt-pet_b200/build.py
 
-The library lands in yrt-pet_b200/lib/ and is what pyyrtpet_b200 loads.
+The libraries land in yrt-pet_b200/lib/; pyyrtpet_b200 loads libyrtb.so.
 """
 from __future__ import annotations
 
@@ -14,6 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc", "yrtb.cu")
 OUT = os.path.join(HERE, "lib", "libyrtb.so")
+L2_SRC = os.path.join(HERE, "csrc", "l2_bench.cu")
+L2_OUT = os.path.join(HERE, "lib", "libyrtb_l2bench.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 # -fmad=false: the FP32 "mirror" arithmetic must not be contracted into FMAs
@@ -23,17 +27,21 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
          "-I" + os.path.join(ROOT, "include")]
 
 
-def build(verbose: bool = False) -> str:
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    deps = [SRC, os.path.join(HERE, "csrc", "device.cuh"),
-            os.path.join(ROOT, "include", "yrt_b200.h")]
-    if os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(d)
+def _compile(src, out, deps, verbose):
+    if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d)
                                    for d in deps):
-        return OUT
-    cmd = [NVCC, *FLAGS, SRC, "-o", OUT]
+        return
+    cmd = [NVCC, *FLAGS, src, "-o", out]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
+
+
+def build(verbose: bool = False) -> str:
+    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+    _compile(SRC, OUT, [SRC, os.path.join(HERE, "csrc", "device.cuh"),
+                        os.path.join(ROOT, "include", "yrt_b200.h")], verbose)
+    _compile(L2_SRC, L2_OUT, [L2_SRC], verbose)
     return OUT
 
 

@@ -166,154 +166,41 @@ __device__ __forceinline__ void slabAlpha(R r0, R r1, R p1, R p2, R inv,
 // ------------------------------------------------------------ Siddon ----
 // Walks one ray through the image grid and calls visit(offset, weight) for
 // each voxel crossing, in order.  p1, p2: endpoints relative to the image
-// centre.  COMP places the entry voxel with FP64 arithmetic (see below); the
-// parametric set-up and the walk are FP32 in both modes.
-template <bool TOF, bool COMP, typename Visit>
-__device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
-                                           const float3 p2, const TofP& tp,
-                                           float tofValue, Visit& visit,
-                                           float wlo = 0.f, float whi = 1.f,
-                                           int part = 0, int parts = 1)
+// centre.  COMP chooses the first planes in FP64 and takes the entry voxel
+// from the walk's plane bookkeeping (see begin); the parametric set-up and
+// the walk are FP32 in both modes.
+//
+// The walk is a state machine: begin() sets up the ray and finds its first
+// non-empty segment, emitFirst() visits it, next() takes one step.
+// siddonWalk() runs it to the end on one thread; siddonWalkWarp() runs the
+// rays of a whole warp in lock step.
+template <bool TOF, bool COMP>
+struct SiddonWalker
 {
-	// 1. Clip to the FOV cylinder.
-	float t0, t1;
-	{
-		const float A = (p2.x - p1.x) * (p2.x - p1.x) + (p2.y - p1.y) * (p2.y - p1.y);
-		const float B = 2.0f * ((p2.x - p1.x) * p1.x + (p2.y - p1.y) * p1.y);
-		const float C = p1.x * p1.x + p1.y * p1.y - g.fovRadius * g.fovRadius;
-		const float Delta = B * B - 4.0f * A * C;
-		if (A != 0.0f)
-		{
-			if (Delta <= 0.0f)
-				return;
-			const float sq = sqrtf(Delta);
-			t0 = (-B - sq) / (2.0f * A);
-			t1 = (-B + sq) / (2.0f * A);
-		}
-		else
-		{
-			t0 = 0.f;
-			t1 = 1.f;
-		}
-	}
-	const float3 d12 = f3sub(p1, p2);
-	const float d_norm = sqrtf(d12.x * d12.x + d12.y * d12.y + d12.z * d12.z);
-	const bool flat_x = (p1.x == p2.x);
-	const bool flat_y = (p1.y == p2.y);
-	const bool flat_z = (p1.z == p2.z);
-	const float inv_x = flat_x ? 0.0f : 1.0f / (p2.x - p1.x);
-	const float inv_y = flat_y ? 0.0f : 1.0f / (p2.y - p1.y);
-	const float inv_z = flat_z ? 0.0f : 1.0f / (p2.z - p1.z);
-	const int dir_x = (inv_x >= 0.0f) ? 1 : -1;
-	const int dir_y = (inv_y >= 0.0f) ? 1 : -1;
-	const int dir_z = (inv_z >= 0.0f) ? 1 : -1;
+	float3 p1, p2;
+	float inv_x, inv_y, inv_z;
+	float fdx, fdy, fdz;
+	int dir_x, dir_y, dir_z;
+	float d_norm, amax;
+	float a_cur, a_next;
+	float x_cur, y_cur, z_cur, ax_next, ay_next, az_next;
+	bool sx, sy, sz;
+	int step, maxSteps;
+	// COMP: linear voxel index moved by a per-step delta.
+	int lin, dprev, dny, dnz;
+	unsigned nvox;
+	// Mirror: voxel coordinates and row offset, as the reference keeps them.
+	int vx, vy, vz, off, dir_prev, nx, ny, nz, nxy;
+	// TOF weight constants.
+	float pc, sigma, norm, hs, pcs, dnn;
 
-	// 2. Intersection with the volume.
-	const float dx = g.vx, dy = g.vy, dz = g.vz;
-	const float inv_dx = 1.0f / dx, inv_dy = 1.0f / dy, inv_dz = 1.0f / dz;
-	const float x0 = -g.lx * 0.5f, x1 = g.lx * 0.5f;
-	const float y0 = -g.ly * 0.5f, y1 = g.ly * 0.5f;
-	const float z0 = -g.lz * 0.5f, z1 = g.lz * 0.5f;
-	float amin, amax;
-	float ax_min, ay_min, az_min;
-	{
-		float ax_max, ay_max, az_max;
-		slabAlpha<float>(-0.5f * g.lx, 0.5f * g.lx, p1.x, p2.x, inv_x, ax_min, ax_max);
-		slabAlpha<float>(-0.5f * g.ly, 0.5f * g.ly, p1.y, p2.y, inv_y, ay_min, ay_max);
-		slabAlpha<float>(-0.5f * g.lz, 0.5f * g.lz, p1.z, p2.z, inv_z, az_min, az_max);
-		// max/min over {0|1, t, ax, ay, az} in the reference's order.
-		amin = fmaxf(fmaxf(fmaxf(fmaxf(0.0f, t0), ax_min), ay_min), az_min);
-		amax = fminf(fminf(fminf(fminf(1.0f, t1), ax_max), ay_max), az_max);
-	}
-	if constexpr (TOF)
-	{
-		float a0, a1;
-		tofAlphaRange(tp, d_norm, tofValue, a0, a1);
-		amin = fmaxf(amin, a0);
-		amax = fminf(amax, a1);
-	}
-	// Optional extra window [wlo, whi] (defaults leave amin, amax unchanged).
-	amin = fmaxf(amin, wlo);
-	amax = fminf(amax, whi);
-	if (parts > 1)
-	{
-		// Piece `part` of `parts` (several threads per LOR).  The cuts sit on
-		// voxel planes of the axis the ray crosses most often, so every
-		// segment of the walk stays whole and keeps the TOF weight of its
-		// midpoint; neighbouring pieces compute the same cut bit for bit.
-		const float cx = flat_x ? -1.f : fabsf(p2.x - p1.x) * inv_dx;
-		const float cy = flat_y ? -1.f : fabsf(p2.y - p1.y) * inv_dy;
-		const float cz = flat_z ? -1.f : fabsf(p2.z - p1.z) * inv_dz;
-		const int ax = (cx >= cy && cx >= cz) ? 0 : (cy >= cz ? 1 : 2);
-		const float q1 = ax == 0 ? p1.x : (ax == 1 ? p1.y : p1.z);
-		const float q2 = ax == 0 ? p2.x : (ax == 1 ? p2.y : p2.z);
-		const float qi = ax == 0 ? inv_x : (ax == 1 ? inv_y : inv_z);
-		const float q0 = ax == 0 ? x0 : (ax == 1 ? y0 : z0);
-		const float dq = ax == 0 ? dx : (ax == 1 ? dy : dz);
-		const float lo = amin, span = amax - amin;
-		auto cut = [&](int j) -> float
-		{
-			const float at = lo + (static_cast<float>(j) / static_cast<float>(parts)) * span;
-			const float plane = q0 + rintf((q1 + at * (q2 - q1) - q0) / dq) * dq;
-			return fminf(fmaxf((plane - q1) * qi, lo), lo + span);
-		};
-		const float hi = amax;
-		amin = part == 0 ? lo : cut(part);
-		amax = part == parts - 1 ? hi : cut(part + 1);
-	}
-
-	float a_cur = amin;
-	float a_next = -1.0f;
-	float x_cur = (inv_x > 0.0f) ? x0 : x1;
-	float y_cur = (inv_y > 0.0f) ? y0 : y1;
-	float z_cur = (inv_z > 0.0f) ? z0 : z1;
-	if ((inv_x >= 0.0f && p1.x > x1) || (inv_x < 0.0f && p1.x < x0) ||
-	    (inv_y >= 0.0f && p1.y > y1) || (inv_y < 0.0f && p1.y < y0) ||
-	    (inv_z >= 0.0f && p1.z > z1) || (inv_z < 0.0f && p1.z < z0))
-		return;
-
-	// First plane crossing at or beyond the entry point, per axis: the plane
-	// index is ceil of the entry position's distance from the walk's start
-	// plane in voxels, in FP32 as the reference computes it, or in FP64
-	// (COMP) so that an entry within float rounding of a plane cannot skip
-	// that plane.
-	auto firstPlane = [&](float q1, float q2, float inv, int dir, float d,
-	                      float& cur) -> float
-	{
-		long long k;
-		if constexpr (COMP)
-			k = static_cast<long long>(
-			    ceil(double(dir) * (double(a_cur) * (double(q2) - double(q1)) -
-			                        double(cur) + double(q1)) * (1.0 / double(d))));
-		else
-			k = static_cast<long long>(
-			    ceilf(static_cast<float>(dir) * (a_cur * (q2 - q1) - cur + q1) / d));
-		cur += static_cast<float>(k * dir) * d;
-		return (cur - q1) * inv;
-	};
-	float ax_next = flat_x ? 3.402823466e+38f : firstPlane(p1.x, p2.x, inv_x, dir_x, dx, x_cur);
-	float ay_next = flat_y ? 3.402823466e+38f : firstPlane(p1.y, p2.y, inv_y, dir_y, dy, y_cur);
-	float az_next = flat_z ? 3.402823466e+38f : firstPlane(p1.z, p2.z, inv_z, dir_z, dz, z_cur);
-
-	int vx, vy, vz;
-	int dir_prev = 0;
-	const int nx = g.nx, ny = g.ny, nz = g.nz;
-	const int nxy = nx * ny;
-	int off;
-	const float fdx = static_cast<float>(dir_x) * dx;
-	const float fdy = static_cast<float>(dir_y) * dy;
-	const float fdz = static_cast<float>(dir_z) * dz;
-
-	// 3. Incremental walk: step to the nearest crossing; ties step together
-	// (<= on the crossing values from the start of the step, i.e. every axis
-	// whose crossing equals the minimum).  Written with selects instead of
-	// branches so that the threads of a warp, whose rays step along different
-	// axes, stay converged; every value is the one the branchy formulation
-	// computes.  Every segment moves the voxel along at least one axis, always
-	// the same way, so the walk leaves the grid after at most nx+ny+nz
-	// segments; the step cap bounds the zero-length steps in between.
-	const int maxSteps = 2 * (nx + ny + nz) + 16;
-	auto advance = [&](bool& sx, bool& sy, bool& sz)
+	// Advances to the nearest crossing; ties step together (<= on the
+	// crossing values from the start of the step, i.e. every axis whose
+	// crossing equals the minimum).  Written with selects instead of
+	// branches so that the threads of a warp, whose rays step along
+	// different axes, stay converged; every value is the one the branchy
+	// formulation computes.
+	__device__ __forceinline__ void advance()
 	{
 		const float ax = ax_next, ay = ay_next, az = az_next;
 		const float m = fminf(fminf(ax, ay), az);
@@ -331,25 +218,20 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		ay_next = sy ? ayn : ay_next;
 		az_next = sz ? azn : az_next;
 		a_next = fminf(m, amax);
-	};
-	// TOF kernel centre along the LOR (mm from p1), loop invariant.
-	const float pc = TOF ? tofCenter(d_norm, tofValue) : 0.f;
-	const float inv_sigma = TOF ? 1.0f / tp.sigma : 0.f;
-	// Compensated TOF weight, per segment [a, b]:
-	//   (b - a) * L * norm * 2^(-y^2),  y = x sqrt(log2(e) / 2),
-	//   x = ((a + b) L/2 - pc) / sigma
-	// with y = (a + b) * hs - pcs in one fused multiply-add (the constant
-	// folded into hs and pcs) and the hardware base-2 exponential (relative
-	// error below 2^-21).
-	constexpr float kHalfLog2e = 0.84932180028801904f;  // sqrt(log2(e) / 2)
-	const float hs = 0.5f * d_norm * inv_sigma * kHalfLog2e;
-	const float pcs = pc * inv_sigma * kHalfLog2e;
-	const float dnn = d_norm * tp.norm;
-	auto emit = [&](int o)
+	}
+
+	template <typename Visit>
+	__device__ __forceinline__ void emit(int o, Visit& visit)
 	{
 		float w;
 		if constexpr (TOF && COMP)
 		{
+			// Compensated TOF weight, per segment [a, b]:
+			//   (b - a) * L * norm * 2^(-y^2),  y = x sqrt(log2(e) / 2),
+			//   x = ((a + b) L/2 - pc) / sigma
+			// with y = (a + b) * hs - pcs in one fused multiply-add (the
+			// constant folded into hs and pcs) and the hardware base-2
+			// exponential (relative error below 2^-21).
 			const float y = __fmaf_rn(a_cur + a_next, hs, -pcs);
 			float g2;
 			asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(g2) : "f"(-(y * y)));
@@ -363,107 +245,273 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 		{
 			// The reference's expression order (TimeOfFlight.hpp:74-84).
 			const float lo = a_cur * d_norm, hi = a_next * d_norm;
-			const float xc = (0.5f * (lo + hi) - pc) / tp.sigma;
-			w *= expf(-0.5f * xc * xc) * tp.norm;
+			const float xc = (0.5f * (lo + hi) - pc) / sigma;
+			w *= expf(-0.5f * xc * xc) * norm;
 		}
 		visit(o, w);
 		a_cur = a_next;
-	};
-
-	// First non-empty segment: its voxel comes from the segment midpoint.
-	int step = 0;
-	bool sx = false, sy = false, sz = false;
-	for (;; step++)
-	{
-		if (!(a_cur < amax) || step >= maxSteps)
-			return;
-		advance(sx, sy, sz);
-		if (a_cur < a_next)
-			break;
 	}
-	step++;
-	if constexpr (COMP)
+
+	// Sets up the ray and finds its first non-empty segment; false if the
+	// ray has nothing to visit.
+	__device__ __forceinline__ bool begin(const Geom& g, const float3 q1,
+	                                      const float3 q2, const TofP& tp,
+	                                      float tofValue, float wlo, float whi,
+	                                      int part, int parts)
 	{
-		// Entry voxel from the walk's own plane bookkeeping: the first
-		// segment lies just before the next plane of each axis (the plane at
-		// a_next for the axes stepped last), so the voxel and the planes the
-		// walk steps by can never disagree.  A voxel taken from the segment's
-		// midpoint instead is off by one for the whole walk when the first
-		// segment is tiny (a TOF window or a piece that starts right before a
-		// plane) and the midpoint rounds across that plane.  With the first
-		// plane chosen in FP64, a ray within float rounding of a plane (e.g.
-		// an LOR between opposite crystals on an image axis) is placed on the
-		// side the exact geometry gives.  An axis the ray runs parallel to
-		// takes its voxel from the (constant) coordinate in FP64.
-		auto fromPlanes = [](bool flat, bool stepped, float cur, float fd,
-		                     float q0, float d, int dir, float q1, int& v)
+		p1 = q1;
+		p2 = q2;
+		// 1. Clip to the FOV cylinder.
+		float t0, t1;
 		{
-			if (flat)
+			const float A = (p2.x - p1.x) * (p2.x - p1.x) + (p2.y - p1.y) * (p2.y - p1.y);
+			const float B = 2.0f * ((p2.x - p1.x) * p1.x + (p2.y - p1.y) * p1.y);
+			const float C = p1.x * p1.x + p1.y * p1.y - g.fovRadius * g.fovRadius;
+			const float Delta = B * B - 4.0f * A * C;
+			if (A != 0.0f)
 			{
-				v = static_cast<int>(floor((double(q1) - double(q0)) * (1.0 / double(d))));
-				return;
+				if (Delta <= 0.0f)
+					return false;
+				const float sq = sqrtf(Delta);
+				t0 = (-B - sq) / (2.0f * A);
+				t1 = (-B + sq) / (2.0f * A);
 			}
-			const float pre = stepped ? cur - fd : cur;
-			const int ip = static_cast<int>(rintf((pre - q0) / d));
-			v = dir > 0 ? ip - 1 : ip;
+			else
+			{
+				t0 = 0.f;
+				t1 = 1.f;
+			}
+		}
+		const float3 d12 = f3sub(p1, p2);
+		d_norm = sqrtf(d12.x * d12.x + d12.y * d12.y + d12.z * d12.z);
+		const bool flat_x = (p1.x == p2.x);
+		const bool flat_y = (p1.y == p2.y);
+		const bool flat_z = (p1.z == p2.z);
+		inv_x = flat_x ? 0.0f : 1.0f / (p2.x - p1.x);
+		inv_y = flat_y ? 0.0f : 1.0f / (p2.y - p1.y);
+		inv_z = flat_z ? 0.0f : 1.0f / (p2.z - p1.z);
+		dir_x = (inv_x >= 0.0f) ? 1 : -1;
+		dir_y = (inv_y >= 0.0f) ? 1 : -1;
+		dir_z = (inv_z >= 0.0f) ? 1 : -1;
+
+		// 2. Intersection with the volume.
+		const float dx = g.vx, dy = g.vy, dz = g.vz;
+		const float inv_dx = 1.0f / dx, inv_dy = 1.0f / dy, inv_dz = 1.0f / dz;
+		const float x0 = -g.lx * 0.5f, x1 = g.lx * 0.5f;
+		const float y0 = -g.ly * 0.5f, y1 = g.ly * 0.5f;
+		const float z0 = -g.lz * 0.5f, z1 = g.lz * 0.5f;
+		float amin;
+		{
+			float ax_min, ay_min, az_min, ax_max, ay_max, az_max;
+			slabAlpha<float>(-0.5f * g.lx, 0.5f * g.lx, p1.x, p2.x, inv_x, ax_min, ax_max);
+			slabAlpha<float>(-0.5f * g.ly, 0.5f * g.ly, p1.y, p2.y, inv_y, ay_min, ay_max);
+			slabAlpha<float>(-0.5f * g.lz, 0.5f * g.lz, p1.z, p2.z, inv_z, az_min, az_max);
+			// max/min over {0|1, t, ax, ay, az} in the reference's order.
+			amin = fmaxf(fmaxf(fmaxf(fmaxf(0.0f, t0), ax_min), ay_min), az_min);
+			amax = fminf(fminf(fminf(fminf(1.0f, t1), ax_max), ay_max), az_max);
+		}
+		if constexpr (TOF)
+		{
+			float a0, a1;
+			tofAlphaRange(tp, d_norm, tofValue, a0, a1);
+			amin = fmaxf(amin, a0);
+			amax = fminf(amax, a1);
+		}
+		// Optional extra window [wlo, whi] (defaults leave amin, amax unchanged).
+		amin = fmaxf(amin, wlo);
+		amax = fminf(amax, whi);
+		if (parts > 1)
+		{
+			// Piece `part` of `parts` (several threads per LOR).  The cuts sit
+			// on voxel planes of the axis the ray crosses most often, so every
+			// segment of the walk stays whole and keeps the TOF weight of its
+			// midpoint; neighbouring pieces compute the same cut bit for bit.
+			const float cx = flat_x ? -1.f : fabsf(p2.x - p1.x) * inv_dx;
+			const float cy = flat_y ? -1.f : fabsf(p2.y - p1.y) * inv_dy;
+			const float cz = flat_z ? -1.f : fabsf(p2.z - p1.z) * inv_dz;
+			const int ax = (cx >= cy && cx >= cz) ? 0 : (cy >= cz ? 1 : 2);
+			const float q1a = ax == 0 ? p1.x : (ax == 1 ? p1.y : p1.z);
+			const float q2a = ax == 0 ? p2.x : (ax == 1 ? p2.y : p2.z);
+			const float qi = ax == 0 ? inv_x : (ax == 1 ? inv_y : inv_z);
+			const float q0 = ax == 0 ? x0 : (ax == 1 ? y0 : z0);
+			const float dq = ax == 0 ? dx : (ax == 1 ? dy : dz);
+			const float lo = amin, span = amax - amin;
+			auto cut = [&](int j) -> float
+			{
+				const float at = lo + (static_cast<float>(j) / static_cast<float>(parts)) * span;
+				const float plane = q0 + rintf((q1a + at * (q2a - q1a) - q0) / dq) * dq;
+				return fminf(fmaxf((plane - q1a) * qi, lo), lo + span);
+			};
+			const float hi = amax;
+			amin = part == 0 ? lo : cut(part);
+			amax = part == parts - 1 ? hi : cut(part + 1);
+		}
+
+		a_cur = amin;
+		a_next = -1.0f;
+		x_cur = (inv_x > 0.0f) ? x0 : x1;
+		y_cur = (inv_y > 0.0f) ? y0 : y1;
+		z_cur = (inv_z > 0.0f) ? z0 : z1;
+		if ((inv_x >= 0.0f && p1.x > x1) || (inv_x < 0.0f && p1.x < x0) ||
+		    (inv_y >= 0.0f && p1.y > y1) || (inv_y < 0.0f && p1.y < y0) ||
+		    (inv_z >= 0.0f && p1.z > z1) || (inv_z < 0.0f && p1.z < z0))
+			return false;
+
+		// First plane crossing at or beyond the entry point, per axis: the
+		// plane index is ceil of the entry position's distance from the
+		// walk's start plane in voxels, in FP32 as the reference computes it,
+		// or in FP64 (COMP) so that an entry within float rounding of a plane
+		// cannot skip that plane.
+		auto firstPlane = [&](float q1a, float q2a, float inv, int dir, float d,
+		                      float& cur) -> float
+		{
+			long long k;
+			if constexpr (COMP)
+				k = static_cast<long long>(
+				    ceil(double(dir) * (double(a_cur) * (double(q2a) - double(q1a)) -
+				                        double(cur) + double(q1a)) * (1.0 / double(d))));
+			else
+				k = static_cast<long long>(
+				    ceilf(static_cast<float>(dir) * (a_cur * (q2a - q1a) - cur + q1a) / d));
+			cur += static_cast<float>(k * dir) * d;
+			return (cur - q1a) * inv;
 		};
-		fromPlanes(flat_x, sx, x_cur, fdx, x0, dx, dir_x, p1.x, vx);
-		fromPlanes(flat_y, sy, y_cur, fdy, y0, dy, dir_y, p1.y, vy);
-		fromPlanes(flat_z, sz, z_cur, fdz, z0, dz, dir_z, p1.z, vz);
-	}
-	else
-	{
-		const float a_mid = 0.5f * (a_cur + a_next);
-		vx = static_cast<int>((p1.x + a_mid * (p2.x - p1.x) + g.lx / 2.0f) * inv_dx);
-		vy = static_cast<int>((p1.y + a_mid * (p2.y - p1.y) + g.ly / 2.0f) * inv_dy);
-		vz = static_cast<int>((p1.z + a_mid * (p2.z - p1.z) + g.lz / 2.0f) * inv_dz);
-	}
-	if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
-		return;
+		ax_next = flat_x ? 3.402823466e+38f : firstPlane(p1.x, p2.x, inv_x, dir_x, dx, x_cur);
+		ay_next = flat_y ? 3.402823466e+38f : firstPlane(p1.y, p2.y, inv_y, dir_y, dy, y_cur);
+		az_next = flat_z ? 3.402823466e+38f : firstPlane(p1.z, p2.z, inv_z, dir_z, dz, z_cur);
 
-	// Following segments: move the voxel along the axes stepped last time.
-	if constexpr (COMP)
-	{
-		// Linear voxel index moved by a per-step delta.  The walk ends at the
-		// grid exit (amax); only a rounding-sized last segment can step past
-		// a face, and the index check keeps every access inside the image
-		// (such a segment adds a weight of ~1e-4 mm to a neighbouring voxel
-		// where the mirror walk stops).
-		const int dny = dir_y * nx, dnz = dir_z * nxy;
-		const unsigned nvox = static_cast<unsigned>(nxy * nz);
-		int lin = vz * nxy + vy * nx + vx;
-		int dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
-		emit(lin);
-		while (a_cur < amax)
+		nx = g.nx;
+		ny = g.ny;
+		nz = g.nz;
+		nxy = nx * ny;
+		fdx = static_cast<float>(dir_x) * dx;
+		fdy = static_cast<float>(dir_y) * dy;
+		fdz = static_cast<float>(dir_z) * dz;
+		// Every segment moves the voxel along at least one axis, always the
+		// same way, so the walk leaves the grid after at most nx+ny+nz
+		// segments; the step cap bounds the zero-length steps in between.
+		maxSteps = 2 * (nx + ny + nz) + 16;
+		if constexpr (TOF)
 		{
-			advance(sx, sy, sz);
-			if (a_cur >= a_next)
+			// TOF kernel centre along the LOR (mm from p1), loop invariant.
+			pc = tofCenter(d_norm, tofValue);
+			sigma = tp.sigma;
+			norm = tp.norm;
+			const float inv_sigma = 1.0f / tp.sigma;
+			constexpr float kHalfLog2e = 0.84932180028801904f;  // sqrt(log2(e) / 2)
+			hs = 0.5f * d_norm * inv_sigma * kHalfLog2e;
+			pcs = pc * inv_sigma * kHalfLog2e;
+			dnn = d_norm * tp.norm;
+		}
+
+		// First non-empty segment.
+		step = 0;
+		sx = sy = sz = false;
+		bool found = false;
+		for (; step < maxSteps && a_cur < amax; step++)
+		{
+			advance();
+			if (a_cur < a_next)
 			{
-				if (++step >= maxSteps)
-					break;
-				continue;
+				found = true;
+				break;
 			}
+		}
+		if (!found)
+			return false;
+		step++;
+		if constexpr (COMP)
+		{
+			// Entry voxel from the walk's own plane bookkeeping: the first
+			// segment lies just before the next plane of each axis (the plane
+			// at a_next for the axes stepped last), so the voxel and the
+			// planes the walk steps by can never disagree.  A voxel taken from
+			// the segment's midpoint instead is off by one for the whole walk
+			// when the first segment is tiny (a TOF window or a piece that
+			// starts right before a plane) and the midpoint rounds across that
+			// plane.  With the first plane chosen in FP64, a ray within float
+			// rounding of a plane (e.g. an LOR between opposite crystals on an
+			// image axis) is placed on the side the exact geometry gives.  An
+			// axis the ray runs parallel to takes its voxel from the
+			// (constant) coordinate in FP64.
+			auto fromPlanes = [](bool flat, bool stepped, float cur, float fd,
+			                     float q0, float d, int dir, float q1a, int& v)
+			{
+				if (flat)
+				{
+					v = static_cast<int>(floor((double(q1a) - double(q0)) * (1.0 / double(d))));
+					return;
+				}
+				const float pre = stepped ? cur - fd : cur;
+				const int ip = static_cast<int>(rintf((pre - q0) / d));
+				v = dir > 0 ? ip - 1 : ip;
+			};
+			fromPlanes(flat_x, sx, x_cur, fdx, x0, dx, dir_x, p1.x, vx);
+			fromPlanes(flat_y, sy, y_cur, fdy, y0, dy, dir_y, p1.y, vy);
+			fromPlanes(flat_z, sz, z_cur, fdz, z0, dz, dir_z, p1.z, vz);
+		}
+		else
+		{
+			const float a_mid = 0.5f * (a_cur + a_next);
+			vx = static_cast<int>((p1.x + a_mid * (p2.x - p1.x) + g.lx / 2.0f) * inv_dx);
+			vy = static_cast<int>((p1.y + a_mid * (p2.y - p1.y) + g.ly / 2.0f) * inv_dy);
+			vz = static_cast<int>((p1.z + a_mid * (p2.z - p1.z) + g.lz / 2.0f) * inv_dz);
+		}
+		if (vx < 0 || vx >= nx || vy < 0 || vy >= ny || vz < 0 || vz >= nz)
+			return false;
+		if constexpr (COMP)
+		{
+			// Linear voxel index moved by a per-step delta.  The walk ends at
+			// the grid exit (amax); only a rounding-sized last segment can
+			// step past a face, and the index check keeps every access inside
+			// the image (such a segment adds a weight of ~1e-4 mm to a
+			// neighbouring voxel where the mirror walk stops).
+			dny = dir_y * nx;
+			dnz = dir_z * nxy;
+			nvox = static_cast<unsigned>(nxy * nz);
+			lin = vz * nxy + vy * nx + vx;
+			dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
+		}
+		else
+		{
+			off = vz * nxy + vy * nx;
+			dir_prev = (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
+		}
+		return true;
+	}
+
+	// Visits the first segment (after a successful begin).
+	template <typename Visit>
+	__device__ __forceinline__ void emitFirst(Visit& visit)
+	{
+		if constexpr (COMP)
+			emit(lin, visit);
+		else
+			emit(vx + off, visit);
+	}
+
+	// One step of the walk: the next crossing, its voxel and its visit;
+	// false when the walk has ended.
+	template <typename Visit>
+	__device__ __forceinline__ bool next(Visit& visit)
+	{
+		if (!(a_cur < amax))
+			return false;
+		advance();
+		if (a_cur >= a_next)
+			return ++step < maxSteps;
+		if constexpr (COMP)
+		{
+			// Following segments: move the voxel along the axes stepped last
+			// time.
 			lin += dprev;
 			if (static_cast<unsigned>(lin) >= nvox)
-				break;
+				return false;
 			dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
-			emit(lin);
+			emit(lin, visit);
 		}
-	}
-	else
-	{
-		off = vz * nxy + vy * nx;
-		dir_prev = (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
-		emit(vx + off);
-		while (a_cur < amax)
+		else
 		{
-			advance(sx, sy, sz);
-			if (a_cur >= a_next)
-			{
-				if (++step >= maxSteps)
-					break;
-				continue;
-			}
 			const int mx = dir_prev & 1, my = (dir_prev >> 1) & 1, mz = (dir_prev >> 2) & 1;
 			vx += mx * dir_x;
 			vy += my * dir_y;
@@ -472,10 +520,97 @@ __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
 			if (static_cast<unsigned>(vx) >= static_cast<unsigned>(nx) ||
 			    static_cast<unsigned>(vy) >= static_cast<unsigned>(ny) ||
 			    static_cast<unsigned>(vz) >= static_cast<unsigned>(nz))
-				break;
+				return false;
 			dir_prev = (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
-			emit(vx + off);
+			emit(vx + off, visit);
 		}
+		return true;
+	}
+};
+
+template <bool TOF, bool COMP, typename Visit>
+__device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
+                                           const float3 p2, const TofP& tp,
+                                           float tofValue, Visit& visit,
+                                           float wlo = 0.f, float whi = 1.f,
+                                           int part = 0, int parts = 1)
+{
+	SiddonWalker<TOF, COMP> w;
+	if (!w.begin(g, p1, p2, tp, tofValue, wlo, whi, part, parts))
+		return;
+	w.emitFirst(visit);
+	while (w.next(visit))
+	{
+	}
+}
+
+// The same walk for the 32 rays of a warp in lock step: every lane takes one
+// step per round and the rounds continue while any lane's ray has steps
+// left.  The lanes of a warp whose rays step along different axes otherwise
+// drift into separate groups that each run the loop with a part of the warp
+// (measured on the attenuation walks: 16.5 of 32 threads per instruction).
+// Every lane of the warp must call it (alive = false for a lane without a
+// ray); each lane's walk is the one siddonWalk makes, step for step.
+template <bool TOF, bool COMP, typename Visit>
+__device__ __forceinline__ void siddonWalkWarp(bool alive, const Geom& g,
+                                               const float3 p1, const float3 p2,
+                                               const TofP& tp, float tofValue,
+                                               Visit& visit, float wlo = 0.f,
+                                               float whi = 1.f)
+{
+	SiddonWalker<TOF, COMP> w;
+	if (alive)
+		alive = w.begin(g, p1, p2, tp, tofValue, wlo, whi, 0, 1);
+	if (alive)
+		w.emitFirst(visit);
+	while (__any_sync(0xffffffffu, alive))
+	{
+		if (alive)
+			alive = w.next(visit);
+	}
+}
+
+// siddonWalkWarp in batches of B crossings: each round every lane takes up
+// to B steps, recording the crossings' voxels and weights (o[k] = -1 for a
+// step without a crossing or after the walk's end), then hands the batch to
+// consume(o, w), which can issue all B image reads before it uses the first
+// one.  The crossings reach consume in walk order.
+template <bool TOF, bool COMP, int B, typename Consume>
+__device__ __forceinline__ void siddonWalkWarpBatched(bool alive, const Geom& g,
+                                                      const float3 p1, const float3 p2,
+                                                      const TofP& tp, float tofValue,
+                                                      Consume& consume, float wlo = 0.f,
+                                                      float whi = 1.f)
+{
+	SiddonWalker<TOF, COMP> w;
+	if (alive)
+		alive = w.begin(g, p1, p2, tp, tofValue, wlo, whi, 0, 1);
+	bool first = alive;
+	while (__any_sync(0xffffffffu, alive))
+	{
+		int o[B];
+		float wt[B];
+#pragma unroll
+		for (int k = 0; k < B; k++)
+		{
+			o[k] = -1;
+			wt[k] = 0.f;
+			auto put = [&](int oo, float ww)
+			{
+				o[k] = oo;
+				wt[k] = ww;
+			};
+			if (k == 0 && first)
+			{
+				w.emitFirst(put);
+				first = false;
+			}
+			else if (alive)
+			{
+				alive = w.next(put);
+			}
+		}
+		consume(o, wt);
 	}
 }
 

@@ -1004,8 +1004,10 @@ __global__ void k_att_keys(KParams P, Geom mu, Events E, Range R,
 
 // Attenuation factor per event: exp(-0.1 * line integral of mu), walked with
 // the projector's arithmetic (COMP: compensated walk).
+constexpr int kAttBatch = 4;
+constexpr int kAttBlocksPerSM = 4;
 template <bool COMP>
-__global__ void __launch_bounds__(kBlock, 6)
+__global__ void __launch_bounds__(kBlock, kAttBlocksPerSM)
     k_attenuation(KParams P, Geom mu, Events E, Range R,
                   const float* __restrict__ muImg, const int* __restrict__ box,
                   float* __restrict__ out, unsigned long long* err,
@@ -1014,20 +1016,27 @@ __global__ void __launch_bounds__(kBlock, 6)
 	// One item per thread: a warp's threads stay converged across items
 	// (a grid-stride loop lets them drift apart between items).  With order,
 	// thread i walks item order[i] (items grouped by walk length, see
-	// k_att_keys), so that the lanes of a warp walk similar lengths.
+	// k_att_keys), so that the lanes of a warp walk similar lengths, and the
+	// warp walks its rays in lock step (siddonWalkWarp): every lane of the
+	// warp reaches the walk, lanes without a ray as idle participants.
 	const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	uint64_t e = 0;
+	float3 p1 = make_float3(0.f, 0.f, 0.f), p2 = p1, n1, n2;
+	bool ok = false;
 	if (i < R.count)
 	{
 		const uint64_t k = order ? __ldg(order + i) : i;
-		const uint64_t e = R.start + k * R.stride;
-		float3 p1, p2, n1, n2;
-		if (!fetchEvent(P, E, e, p1, p2, n1, n2))
+		e = R.start + k * R.stride;
+		ok = fetchEvent(P, E, e, p1, p2, n1, n2);
+		if (!ok)
 		{
 			atomicAdd(err, 1ULL);
 			out[e] = 0.f;
-			return;
 		}
-		float wlo = 0.f, whi = 1.f;
+	}
+	float wlo = 0.f, whi = 1.f;
+	if (ok)
+	{
 		if constexpr (COMP)
 		{
 			attWindow(P, mu, box, p1, p2, wlo, whi);
@@ -1042,12 +1051,26 @@ __global__ void __launch_bounds__(kBlock, 6)
 			// segment, which in FP32 can round onto the other side of a plane.
 			attShift(P, mu, p1, p2);
 		}
-		float acc = 0.f;
-		auto visit = [&](int o, float w) { acc += w * __ldg(muImg + o); };
-		if (wlo < whi)
-			siddonWalk<false, COMP>(mu, p1, p2, P.tof, 0.f, visit, wlo, whi);
-		out[e] = expf(-acc * 0.1f);
 	}
+	// Batches of kAttBatch crossings: their mu reads are all in flight before
+	// the first is added (the walk itself needs none of them), and the sum
+	// still runs in walk order.
+	float acc = 0.f;
+	auto consume = [&](const int (&o)[kAttBatch], const float (&w)[kAttBatch])
+	{
+		float m[kAttBatch];
+#pragma unroll
+		for (int k = 0; k < kAttBatch; k++)
+			m[k] = o[k] >= 0 ? __ldg(muImg + o[k]) : 0.f;
+#pragma unroll
+		for (int k = 0; k < kAttBatch; k++)
+			if (o[k] >= 0)
+				acc += w[k] * m[k];
+	};
+	siddonWalkWarpBatched<false, COMP, kAttBatch>(ok && wlo < whi, mu, p1, p2, P.tof,
+	                                              0.f, consume, wlo, whi);
+	if (ok)
+		out[e] = expf(-acc * 0.1f);
 }
 
 __global__ void __launch_bounds__(kBlock)
