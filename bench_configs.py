@@ -803,13 +803,19 @@ def run_c2mr(args):
     n_rand_lors = float(sc.getNumDets()) ** 2 / 2 * 0.45
     ms = {}
     proj4 = None
-    for rays in (4, 1):
+    # 4 rays with one lane per ray (the default), 4 rays with one thread
+    # walking them in turn, and one ray.
+    for rays, lanes in ((4, 4), (4, 1), (1, 1)):
         pp = yrt.ProjectorParams(sc)
         pp.addTOF(bench.TOF_FWHM, bench.TOF_NSTD)
         pp.numRays = rays
         pp.precision = L.YRTB_COMPENSATED
         proj = yrt.DeviceProjector(sc, ip, pp)
         if rays == 4:
+            cfg = proj.get_launch()
+            cfg["threads_per_lor"] = lanes
+            proj.set_launch(**cfg)
+        if rays == 4 and lanes == 4:
             proj4 = proj
         ev = yrt.DeviceEvents.from_arrays(evs.d1.to(torch.int32), evs.d2.to(torch.int32),
                                           tof=evs.tof)
@@ -838,17 +844,22 @@ def run_c2mr(args):
             with Timer() as t:
                 one()
             times.append(t.ms)
-        ms[rays] = float(np.median(times))
+        ms[(rays, lanes)] = float(np.median(times))
         del ev, img, work
     out = _base("C2 list-mode TOF OSEM iteration with 4-ray Siddon, 80x672 scanner "
                 "R=410, 256x256x160 @2mm, 214 ps TOF 5 sigma, 10 subsets",
                 "events/s (4-ray fwd+back TOF Siddon, one OSEM iteration)",
-                n / (ms[4] * 1e-3), "events/s", args.steps, args.warmup, ms[4],
+                n / (ms[(4, 4)] * 1e-3), "events/s", args.steps, args.warmup, ms[(4, 4)],
                 {"events": n, "rays": 4, "subsets": bench.SUBSETS,
                  "precision": "compensated",
                  "multi_ray_stream": "curand XORWOW, seed 13, subsequence = event "
                                      "index in the call"})
-    out["single_ray"] = {"value": n / (ms[1] * 1e-3), "ms_per_step": ms[1]}
+    out["single_ray"] = {"value": n / (ms[(1, 1)] * 1e-3), "ms_per_step": ms[(1, 1)]}
+    out["one_thread_per_event"] = {"value": n / (ms[(4, 1)] * 1e-3),
+                                   "ms_per_step": ms[(4, 1)],
+                                   "what": "4 rays walked in turn by one thread per event"}
+    out["cost_vs_single_ray"] = ms[(4, 4)] / ms[(1, 1)]
+    out["launch"] = proj4.get_launch()
     out["multiray_table_ms"] = table_ms
     # FP64 parity of the 4-ray forward projections on a sample, with the
     # offsets the device draws for it.

@@ -186,11 +186,16 @@ void yrtb_projector_destroy(yrtb_projector* h);
 typedef struct
 {
 	int block;            /* threads per block: 128 or 256 */
-	int threads_per_lor;  /* 1, 2 or 4 threads walk one LOR, each a piece cut
-	                         at voxel planes, the forward sum reduced over the
-	                         group; > 1 needs YRTB_COMPENSATED precision (the
-	                         pieces' sums round differently from one walk) and
-	                         is not used by deterministic back projections */
+	int threads_per_lor;  /* single-ray Siddon: 1, 2 or 4 threads walk one LOR,
+	                         each a piece cut at voxel planes, the forward sum
+	                         reduced over the group; > 1 needs YRTB_COMPENSATED
+	                         precision (the pieces' sums round differently from
+	                         one walk).  Multi-ray Siddon: 1 (one thread walks
+	                         the rays in turn) or the number of rays rounded up
+	                         to a power of two, at most 8 (one lane per ray, the
+	                         rays' forward sums added in ray order: the same
+	                         bits as one thread; the default up to 8 rays).  Not
+	                         used by deterministic back projections */
 	int bucket_shift;     /* yrtb_events_subset_order groups rays by
 	                         (voxel crossings >> bucket_shift), 0..7 */
 	int order;            /* YRTB_ORDER_LOR, YRTB_ORDER_SPATIAL or YRTB_ORDER_SPATIAL_FINE */

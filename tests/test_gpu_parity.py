@@ -281,6 +281,45 @@ def test_multiray_table_gives_the_same_projections():
     assert torch.equal(q.forward(img, ev), v0)
 
 
+@pytest.mark.parametrize("tof,prec,rays", [(None, L.YRTB_MIRROR, 4),
+                                           ((214.0, 5), L.YRTB_MIRROR, 4),
+                                           ((214.0, 5), L.YRTB_COMPENSATED, 4),
+                                           ((214.0, 5), L.YRTB_COMPENSATED, 3),
+                                           (None, L.YRTB_COMPENSATED, 8)])
+def test_multiray_one_lane_per_ray_matches_one_thread(tof, prec, rays):
+    # One lane per ray (threads_per_lor = rays rounded up to a power of two,
+    # the default with a table of offsets) adds the rays' forward sums in ray
+    # order, as one thread walking the rays in turn does: the forward
+    # projections are bit-identical; back projection and EM image equal up
+    # to the order of the FP32 atomics.  Without a table covering the call,
+    # the projector falls back to one thread per event.
+    sc, ip, p = make(num_rays=rays, tof=tof, precision=prec)
+    d1, d2 = random_events(SC_ARGS, 6000, 33)
+    rng = np.random.default_rng(34)
+    tv = rng.normal(0, 200, len(d1)).astype(np.float32) if tof else None
+    img = torch.from_numpy(rng.random(ip.shape, dtype=np.float32)).cuda()
+    y = torch.from_numpy(rng.uniform(0.1, 1.0, len(d1)).astype(np.float32)).cuda()
+    ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv)
+    lanes = 1 << (rays - 1).bit_length()
+    assert p.get_launch()["threads_per_lor"] == lanes
+    v_gen = p.forward(img, ev)                 # no table yet: one thread per event
+    p.multiray_table(len(d1))
+    cfg = p.get_launch()
+    out = {}
+    for tpl in (1, lanes):
+        cfg["threads_per_lor"] = tpl
+        p.set_launch(**cfg)
+        out[tpl] = (p.forward(img, ev), p.backward(y, ev),
+                    p.em_step(img, torch.zeros(ip.shape, device="cuda"), ev))
+    assert torch.equal(out[1][0], v_gen)
+    assert torch.equal(out[lanes][0], out[1][0])
+    assert rel_l2(out[lanes][1].cpu().numpy(), out[1][1].cpu().numpy()) < 1e-6
+    assert rel_l2(out[lanes][2].cpu().numpy(), out[1][2].cpu().numpy()) < 1e-6
+    with pytest.raises(RuntimeError):
+        cfg["threads_per_lor"] = 2 * lanes
+        p.set_launch(**cfg)
+
+
 # ---------------------------------------------------------------- DD ------
 @pytest.mark.parametrize("tof,psf,prec", [(None, False, L.YRTB_MIRROR),
                                           ((214.0, 5), False, L.YRTB_MIRROR),

@@ -375,6 +375,29 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
 	{
 		// The offsets come from the projector's table when it covers this
 		// item index (same values), else from the generator.
+		if (parts > 1)
+		{
+			// One lane per ray: this lane walks ray `part` only (none if part
+			// >= numRays), its offsets read from the table, which the host
+			// makes sure covers every item of the launch.  (parts is a
+			// constant of the kernel, so the generator's code and state stay
+			// out of these kernels.)
+			if (part >= P.numRays)
+				return;
+			float3 a = p1, b = p2;
+			if (part > 0)
+			{
+				MultiRay mr;
+				mr.setDirs(n1, n2);
+				const float4 t = __ldg(reinterpret_cast<const float4*>(P.mrTable) +
+				                       rid * static_cast<uint64_t>(P.numRays - 1) + (part - 1));
+				const float u[4] = {t.x, t.y, t.z, t.w};
+				mr.offset(u, P.scan.crystalZ, P.scan.crystalTrans, a, b);
+			}
+			siddonWalk<TOF, COMP>(P.g, a, b, P.tof, tofv, visit);
+			endRay();
+			return;
+		}
 		MultiRay mr;
 		const bool tab = P.mrTable != nullptr && rid < P.mrCount;
 		if (tab)
@@ -477,8 +500,11 @@ __device__ __forceinline__ float forwardEvent(const KParams& P,
 	};
 	projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, true, visit,
 	                              endRay, part, parts);
+	// One lane per ray (parts > 1): the caller adds the rays' sums in ray
+	// order and divides (rayGroupMean).
 	if constexpr (KIND == K_SIDDON_MR)
-		acc = acc / static_cast<float>(P.numRays);
+		if (parts == 1)
+			acc = acc / static_cast<float>(P.numRays);
 	if constexpr (TRACK)
 		*maxw = mw;
 	return acc;
@@ -583,7 +609,9 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 	}
 	else if constexpr (VEC == 2)
 	{
-		static_assert(KIND == K_SIDDON, "slots hold one value per voxel of one ray");
+		// Multi-ray: flush ends every ray, so a group never spans two rays.
+		static_assert(KIND == K_SIDDON || KIND == K_SIDDON_MR,
+		              "slots hold one value per voxel of one ray");
 		int gb = -1;
 		auto send = [&]
 		{
@@ -617,7 +645,8 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 	}
 	else if constexpr (VEC == 1)
 	{
-		static_assert(KIND == K_SIDDON, "lanes hold one value per voxel of one ray");
+		static_assert(KIND == K_SIDDON || KIND == K_SIDDON_MR,
+		              "lanes hold one value per voxel of one ray");
 		int gb = -1;
 		float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
 		auto visit = [&](int o, float w)
@@ -677,22 +706,57 @@ __device__ __forceinline__ float groupSum(float v)
 	return v;
 }
 
-// One event per TPL threads (TPL > 1: single-ray Siddon, compensated
-// arithmetic; lane j of the group walks piece j of the ray and the forward
-// sum is reduced over the group).  Siddon: 1024 threads per SM (64 registers
-// per thread, 32 warps) whatever the block size; the other projectors keep
-// the compiler's register choice.  FIX (OP_BWD, OP_EM): pass 2 of the
-// deterministic back projection.
+// Multi-ray event held by TPL lanes, lane r with the sum of ray r: the rays'
+// sums added in ray order from 0 and divided by the number of rays, as one
+// thread walking the rays one after the other computes them (same bits, in
+// every lane of the group).
+template <int TPL>
+__device__ __forceinline__ float rayGroupMean(float ray, int numRays)
+{
+	const unsigned lane = threadIdx.x & 31u;
+	const unsigned base = lane & ~static_cast<unsigned>(TPL - 1);
+	const unsigned mask = (TPL == 32 ? 0xffffffffu : ((1u << TPL) - 1u)) << base;
+	float acc = 0.f;
+#pragma unroll
+	for (int r = 0; r < TPL; r++)
+	{
+		const float x = __shfl_sync(mask, ray, base + r);
+		if (r < numRays)
+			acc += x;
+	}
+	return acc / static_cast<float>(numRays);
+}
+
+// One event per TPL threads.  TPL > 1, single-ray Siddon (compensated
+// arithmetic): lane j of the group walks piece j of the ray and the forward
+// sum is reduced over the group.  TPL > 1, multi-ray Siddon: lane r walks
+// ray r, the forward sums are added in ray order (rayGroupMean), the same
+// bits as one thread walking the rays in turn.  Siddon, and multi-ray with
+// one lane per ray: 1024 threads per SM (64 registers per thread, 32 warps)
+// whatever the block size; multi-ray with one thread per event: 768; the
+// other projectors keep the compiler's register choice.  FIX (OP_BWD,
+// OP_EM): pass 2 of the deterministic back projection.
 template <int OP, int KIND, bool TOF, bool COMP, bool FIX = false,
           int BLOCK = kBlock, int TPL = 1, int VEC = 0>
-__global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK
-                                                         : (KIND == K_SIDDON_MR ? 768 / BLOCK : 1))
+__global__ void __launch_bounds__(BLOCK, (KIND == K_SIDDON || (KIND == K_SIDDON_MR && TPL > 1))
+                                             ? 1024 / BLOCK
+                                             : (KIND == K_SIDDON_MR ? 768 / BLOCK : 1))
     k_events(KParams P, Events E, Range R, const float* __restrict__ in,
              float* __restrict__ out, float globalScale, float denomThr,
              unsigned long long* err, Fixed F)
 {
-	static_assert(TPL == 1 || (KIND == K_SIDDON && COMP && !FIX && OP != OP_COUNT),
-	              "several threads per LOR: single-ray Siddon, compensated");
+	static_assert(TPL == 1 || (KIND == K_SIDDON && COMP && !FIX && OP != OP_COUNT) ||
+	                  (KIND == K_SIDDON_MR && !FIX && OP != OP_COUNT),
+	              "several threads per LOR: single-ray Siddon (compensated) or one "
+	              "lane per ray of a multi-ray Siddon");
+	// Forward sum of the event from the TPL lanes' partial sums.
+	auto eventSum = [&](float v) -> float
+	{
+		if constexpr (KIND == K_SIDDON_MR && TPL > 1)
+			return rayGroupMean<TPL>(v, P.numRays);
+		else
+			return groupSum<TPL>(v);
+	};
 	// One item per thread group: a warp's threads stay converged across items
 	// (a grid-stride loop lets them drift apart between items).
 	const uint64_t gt = static_cast<uint64_t>(blockIdx.x) * BLOCK + threadIdx.x;
@@ -740,7 +804,7 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK
 		}
 		else if constexpr (OP == OP_FWD)
 		{
-			const float v = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
+			const float v = eventSum(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			if (part == 0)
 				out[e] = v;
@@ -768,7 +832,7 @@ __global__ void __launch_bounds__(BLOCK, KIND == K_SIDDON ? 1024 / BLOCK
 					E.model[e] = 0.f;
 				return;
 			}
-			float u = groupSum<TPL>(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
+			float u = eventSum(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			u *= s;
 			u *= a;
@@ -2520,8 +2584,9 @@ void fixedEnd(yrtb_projector* h, const Fixed& F, float* out, cudaStream_t st)
 	k_fixed_finish<<<gridFor(J, 8), kBlock, 0, st>>>(h->d_fix, J, F, out);
 }
 
-// Single-ray Siddon event kernel with block size B and the projector's
-// threads per LOR (compensated arithmetic only; 1 otherwise).
+// Siddon event kernel with block size B and the projector's threads per LOR:
+// pieces of a single ray (compensated arithmetic only; 1 otherwise), or one
+// lane per ray of a multi-ray projector.
 template <int OP, int K, bool T, bool C, int B>
 void launchTuned(const yrtb_projector* h, const Events& E, Range R,
                  const float* in, float* out, float gs, float thr,
@@ -2538,12 +2603,14 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 		constexpr int TPL = decltype(tplc)::value;
 		const uint64_t threads = R.count * TPL;
 		const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, (threads + B - 1) / B));
-		if constexpr (TPL == 1)
+		if constexpr (TPL == 1 || K == K_SIDDON_MR)
 		{
 			// Bit 0: float4 gathers (forward); bit 1: float4 reductions summed
 			// in registers, bit 2: staged in shared memory (back projection,
-			// bit 2 wins).  Each op instantiates only the modes it uses.
-			constexpr int kUse = OP == OP_FWD ? 1 : (OP == OP_BWD ? 6 : 7);
+			// bit 2 wins).  Each op instantiates only the modes it uses;
+			// multi-ray walks use the register reductions only.
+			constexpr int kUse = K == K_SIDDON_MR ? (OP == OP_FWD ? 0 : 2)
+			                                      : (OP == OP_FWD ? 1 : (OP == OP_BWD ? 6 : 7));
 			int vg = aligned ? (h->launch.vector_groups & kUse) : 0;
 			if (vg & 4)
 				vg &= ~2;
@@ -2553,7 +2620,7 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 				{
 					constexpr int V = decltype(vc)::value;
 					if constexpr ((V & kUse) == V)
-						k_events<OP, K, T, C, false, B, 1, V><<<grid, B, 0, st>>>(
+						k_events<OP, K, T, C, false, B, TPL, V><<<grid, B, 0, st>>>(
 						    h->P, E, R, in, out, gs, thr, h->d_err, F);
 				};
 				switch (vg)
@@ -2570,8 +2637,23 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 		k_events<OP, K, T, C, false, B, TPL><<<grid, B, 0, st>>>(h->P, E, R, in, out, gs,
 		                                                        thr, h->d_err, F);
 	};
-	const int tpl = h->launch.threads_per_lor;
-	if constexpr (C)
+	int tpl = h->launch.threads_per_lor;
+	if constexpr (K == K_SIDDON_MR)
+	{
+		// One lane per ray reads its offsets from the table only: without a
+		// table that covers the launch's items, one thread walks the rays.
+		if (!(h->P.mrTable != nullptr && R.count <= h->P.mrCount))
+			tpl = 1;
+		if (tpl == 8)
+			go(std::integral_constant<int, 8>{});
+		else if (tpl == 4)
+			go(std::integral_constant<int, 4>{});
+		else if (tpl == 2)
+			go(std::integral_constant<int, 2>{});
+		else
+			go(std::integral_constant<int, 1>{});
+	}
+	else if constexpr (C)
 	{
 		if (tpl == 4)
 			go(std::integral_constant<int, 4>{});
@@ -2584,6 +2666,16 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 	{
 		go(std::integral_constant<int, 1>{});
 	}
+}
+
+// Lanes of the one-lane-per-ray multi-ray walk: the number of rays rounded
+// up to a power of two; 0 above 8 rays (one thread then walks them all).
+inline int rayLanes(int numRays)
+{
+	int l = 1;
+	while (l < numRays)
+		l <<= 1;
+	return l <= 8 ? l : 0;
 }
 
 template <int OP>
@@ -2621,6 +2713,14 @@ yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
 					launchTuned<OP, K, T, C, 128>(h, E, R, in, out, gs, thr, st, F);
 				else
 					launchTuned<OP, K, T, C, 256>(h, E, R, in, out, gs, thr, st, F);
+				return;
+			}
+		}
+		if constexpr (K == K_SIDDON_MR && OP != OP_COUNT)
+		{
+			if (!(kScatter && h->det))
+			{
+				launchTuned<OP, K, T, C, kBlock>(h, E, R, in, out, gs, thr, st, F);
 				return;
 			}
 		}
@@ -3010,6 +3110,9 @@ yrtb_status yrtb_projector_create(const yrtb_scanner* s, const float* lut,
 		h->kind = pp->num_rays > 1 ? K_SIDDON_MR : K_SIDDON;
 	else
 		h->kind = pp->psf_num_s > 0 ? K_DD_PSF : K_DD;
+	// Multi-ray Siddon walks one ray per lane by default (up to 8 rays).
+	if (h->kind == K_SIDDON_MR && rayLanes(pp->num_rays) > 0)
+		h->launch.threads_per_lor = rayLanes(pp->num_rays);
 	if (pp->psf_num_s > 0)
 	{
 		const size_t n = static_cast<size_t>(pp->psf_num_s) * pp->psf_size;
@@ -3098,12 +3201,22 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 		return fail(YRTB_ERR_ARGUMENT, "null argument");
 	if (c->block != 128 && c->block != 256)
 		return fail(YRTB_ERR_ARGUMENT, "block must be 128 or 256");
-	if (c->threads_per_lor != 1 && c->threads_per_lor != 2 && c->threads_per_lor != 4)
-		return fail(YRTB_ERR_ARGUMENT, "threads_per_lor must be 1, 2 or 4");
-	if (c->threads_per_lor > 1 && !(h->kind == K_SIDDON && h->comp))
-		return fail(YRTB_ERR_ARGUMENT,
-		            "threads_per_lor > 1 needs a single-ray Siddon projector in "
-		            "YRTB_COMPENSATED precision");
+	if (h->kind == K_SIDDON_MR)
+	{
+		if (c->threads_per_lor != 1 && c->threads_per_lor != rayLanes(h->P.numRays))
+			return fail(YRTB_ERR_ARGUMENT,
+			            "threads_per_lor of a multi-ray Siddon projector must be 1 or "
+			            "the number of rays rounded up to a power of two (at most 8)");
+	}
+	else
+	{
+		if (c->threads_per_lor != 1 && c->threads_per_lor != 2 && c->threads_per_lor != 4)
+			return fail(YRTB_ERR_ARGUMENT, "threads_per_lor must be 1, 2 or 4");
+		if (c->threads_per_lor > 1 && !(h->kind == K_SIDDON && h->comp))
+			return fail(YRTB_ERR_ARGUMENT,
+			            "threads_per_lor > 1 needs a single-ray Siddon projector in "
+			            "YRTB_COMPENSATED precision, or a multi-ray one");
+	}
 	if (c->bucket_shift < 0 || c->bucket_shift > 7)
 		return fail(YRTB_ERR_ARGUMENT, "bucket_shift must be in 0..7");
 	if (c->order != YRTB_ORDER_LOR && c->order != YRTB_ORDER_SPATIAL &&
@@ -4397,8 +4510,9 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 		return fail(YRTB_ERR_ARGUMENT, "invalid autotune arguments");
 	*report = yrtb_tune_report{};
 	report->best = h->launch;
-	if (h->kind != K_SIDDON)
+	if (h->kind != K_SIDDON && h->kind != K_SIDDON_MR)
 		return YRTB_OK;
+	const bool multiRay = h->kind == K_SIDDON_MR;
 	yrtb_range all{0, 1, 0};
 	yrtb_status s = checkEvents(h, ev, all, true);
 	if (s != YRTB_OK)
@@ -4520,15 +4634,19 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 		return YRTB_OK;
 	};
 	// Stage 1: event orders x vector groups, with the current block size and
-	// threads per LOR (one thread per LOR when the projector splits none).
+	// threads per LOR (one thread per LOR when the projector splits none; a
+	// multi-ray projector keeps its lanes per event and tries the register
+	// float4 reductions, the only vector mode its walks use).
 	const int orders[3][2] = {{YRTB_ORDER_LOR, 1}, {YRTB_ORDER_SPATIAL, 1},
 	                          {YRTB_ORDER_SPATIAL, 2}};
 	for (int shift : {3, 4, 5})
 		for (const auto& ot : orders)
 			for (int vec : {2, 4, 1, 0})
 			{
+				if (multiRay && (vec == 4 || vec == 1))
+					continue;
 				yrtb_launch_config c = saved;
-				c.threads_per_lor = 1;
+				c.threads_per_lor = multiRay ? saved.threads_per_lor : 1;
 				c.bucket_shift = shift;
 				c.order = ot[0];
 				c.tile_shift = ot[1];
@@ -4541,10 +4659,19 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	{
 		const yrtb_launch_config o = report->tried[bestIdx];
 		const bool split = h->comp && !h->det;
+		const int lanes = rayLanes(h->P.numRays);
 		for (int block : {128, 256})
-			for (int tpl : {1, 2, 4})
+			for (int tpl : {1, 2, 4, 8})
 			{
-				if ((tpl > 1 && !split) || (h->det && (block != 256 || tpl != 1)))
+				if (multiRay)
+				{
+					// Multi-ray: 256-thread blocks; one thread per event or one
+					// lane per ray.
+					if (block != 256 || h->det || (tpl != 1 && tpl != lanes))
+						continue;
+				}
+				else if (tpl == 8 || (tpl > 1 && !split) ||
+				         (h->det && (block != 256 || tpl != 1)))
 					continue;
 				if (block == o.block && tpl == o.threads_per_lor)
 					continue;
