@@ -1005,6 +1005,29 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 		// row factor dxy/cos(theta) folded into the transverse weight.
 		const float r_wyx = FAST ? 1.0f / widthFrac_yx : 0.f;
 		const float r_wz = FAST ? 1.0f / widthFrac_z : 0.f;
+		// The z overlaps of the row's footprint are the same for every
+		// transverse voxel of the row: up to kDDZ of them are computed once
+		// per row (zq[j] = the factor of voxel zi0 + j, zmask its bit when the
+		// voxel overlaps); wider footprints take the per-visit loop.  Same
+		// values and visit order either way.
+		constexpr int kDDZ = 4;
+		float zq[kDDZ];
+		unsigned zmask = 0u;
+		const bool zfit = zi1 - zi0 < kDDZ;
+		if (zfit)
+		{
+#pragma unroll
+			for (int j = 0; j < kDDZ; j++)
+			{
+				const int zi = zi0 + j;
+				const float pix_z = -0.5f * g.lz + (static_cast<float>(zi) + 0.5f) * g.vz;
+				const float zp0 = pix_z - g.vz * 0.5f, zp1 = pix_z + g.vz * 0.5f;
+				const float wz = fminf(zp1, zr1) - fmaxf(zp0, zr0);
+				zq[j] = FAST ? wz * r_wz : wz / widthFrac_z;
+				if (zi <= zi1 && zr1 >= zp0 && zr0 < zp1)
+					zmask |= 1u << j;
+			}
+		}
 		for (int yxi = i0; yxi <= i1; yxi++)
 		{
 			const float pix_yx = -0.5f * lyx + (static_cast<float>(yxi) + 0.5f) * dyx;
@@ -1028,6 +1051,22 @@ __device__ __forceinline__ void ddWalk(const Geom& g, const float3 d1,
 			}
 			const float wxy_s = FAST ? wxy * r_wyx * dxy_cos_theta : wxy / widthFrac_yx;
 			const int oxy = flag_y ? g.nx * xyi + yxi : g.nx * yxi + xyi;
+			if (zfit)
+			{
+#pragma unroll
+				for (int j = 0; j < kDDZ; j++)
+				{
+					if (zmask & (1u << j))
+					{
+						const int o = (zi0 + j) * nxy + oxy;
+						float w = FAST ? wxy_s * zq[j] : wxy_s * zq[j] * dxy_cos_theta;
+						if constexpr (TOF)
+							w *= tw;
+						visit(o, w);
+					}
+				}
+				continue;
+			}
 			for (int zi = zi0; zi <= zi1; zi++)
 			{
 				const float pix_z = -0.5f * g.lz + (static_cast<float>(zi) + 0.5f) * g.vz;

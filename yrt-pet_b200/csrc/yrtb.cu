@@ -1197,8 +1197,11 @@ enum HistoMode
 	H_FIX = 2
 };
 
+// Blocks per SM of the compensated DD + PSF histogram EM kernel (several
+// threads per bin).
+constexpr int kDDPsfBlocksPerSM = 2;
 template <int KIND, bool EM, int MODE = H_PLAIN, bool COMP = false, int TPL = 1>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, (KIND == K_DD_PSF && TPL > 1) ? kDDPsfBlocksPerSM : 1)
     k_histo(KParams P, H3Dev H, uint64_t count, uint64_t numPhiSubset,
             uint64_t numSubsets, uint64_t subset, const float* __restrict__ img,
             float* __restrict__ out, const float* __restrict__ meas,

@@ -18,6 +18,7 @@ from .psf import (ConvolutionKernel, ConvolutionKernelGaussian,  # noqa: F401
                   ConvolutionKernelGaussianMixture, OperatorPsfDevice,
                   OperatorVarPsfDevice, write_image_psf_csv)
 from .lrem import LREM_GPU, LowRankProjector  # noqa: F401
+from .ranges import RangeList  # noqa: F401
 
 ListModeLUTOwned = ListModeLUT
 ListModeLUTAlias = ListModeLUT

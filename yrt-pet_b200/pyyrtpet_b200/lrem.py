@@ -244,7 +244,7 @@ class LREM_GPU(OSEM_GPU):
         Wn = None if update_h else torch.empty(R * J, dtype=torch.float32, device="cuda")
         Hn = torch.empty((R, T), dtype=torch.float64, device="cuda") if update_h else None
         evc = ev.c()
-        for _ in range(self.num_MLEM_iterations):
+        for it in range(self.num_MLEM_iterations):
             for s in range(nsub):
                 if offsets is None:
                     r = L.yrtb_range(s, nsub, 0)
@@ -264,6 +264,8 @@ class LREM_GPU(OSEM_GPU):
                     L.check(lib.yrtb_em_update(W.data_ptr(), Wn.data_ptr(),
                                                sens_sub.data_ptr(), J, R, 1,
                                                self.EPS_FLT, c.data_ptr(), st))
+            # The MLEM image of the low-rank updater is W (R basis images).
+            self._save_iteration(it, W, self.imageParams.withFrames(R).shape)
         if update_h:
             Hh[...] = H.cpu().numpy()
         self._last_events = ev

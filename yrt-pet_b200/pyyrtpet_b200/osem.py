@@ -23,6 +23,7 @@ from . import _lib as L
 from .core import (DeviceEvents, DeviceProjector, Histogram3D, ImageParams,
                    ListModeLUT, ProjectorParams, Scanner, _dev, _ptr, _stream)
 from .psf import OperatorPsfDevice, OperatorVarPsfDevice
+from .ranges import RangeList, iteration_filename
 
 
 class OSEM_GPU:
@@ -69,6 +70,9 @@ class OSEM_GPU:
         self._frame_scale = None
         self.imagePsf = None
         self.flagImagePSF = False
+        self.saveIterRanges = RangeList()
+        self.saveIterPath = ""
+        self._save_writer = None
 
     # ----------------------------------------------------------- setters --
     def setImageParams(self, p: ImageParams):
@@ -83,6 +87,34 @@ class OSEM_GPU:
 
     def getDataInput(self):
         return self._data
+
+    def setSaveIterRanges(self, range_list, path: str, writer=None):
+        """Save the image after the iterations in range_list (a RangeList or
+        its string form, 1-based) to path with "_iterationNN" inserted before
+        the extension (OSEM::setSaveIterRanges, src/recon/OSEM.cpp:651-655,
+        813-821).  writer(fname, image) writes one image (a CPU float32
+        array shaped like the reconstruction); by default .npy paths get
+        numpy's format and any other path the raw float32 voxels (NIfTI
+        writing is not part of this package: pass a writer for it)."""
+        self.saveIterRanges = (range_list if isinstance(range_list, RangeList)
+                               else RangeList(str(range_list)))
+        self.saveIterPath = path
+        self._save_writer = writer
+
+    def _save_iteration(self, iteration: int, img: torch.Tensor, shape):
+        """After MLEM iteration `iteration` (0-based): write the image when
+        the iteration is in saveIterRanges (OSEM.cpp:345-348)."""
+        if self.saveIterRanges.empty() or not self.saveIterRanges.isIn(iteration + 1):
+            return
+        fname = iteration_filename(self.saveIterPath, iteration,
+                                   self.num_MLEM_iterations)
+        arr = img.reshape(shape).detach().cpu().numpy()
+        if self._save_writer is not None:
+            self._save_writer(fname, arr)
+        elif fname.endswith(".npy"):
+            np.save(fname, arr)
+        else:
+            arr.astype(np.float32).tofile(fname)
 
     def setListModeEnabled(self, enabled: bool):
         self.usingListModeInput = bool(enabled)
@@ -369,10 +401,24 @@ class OSEM_GPU:
                     img.data_ptr(), mask_src.data_ptr(), J, nt, 1, 0.0, 0.0,
                     0.0, 1.0, 0.0, _stream()))
                 p.init_from_image = 1
-            L.check(L.lib().yrtb_osem_listmode(proj.h, ctypes.byref(ev.c()),
-                                               sens.data_ptr(), img.data_ptr(),
-                                               work.data_ptr(), ctypes.byref(p),
-                                               _stream()))
+            if self.saveIterRanges.empty():
+                L.check(L.lib().yrtb_osem_listmode(proj.h, ctypes.byref(ev.c()),
+                                                   sens.data_ptr(), img.data_ptr(),
+                                                   work.data_ptr(), ctypes.byref(p),
+                                                   _stream()))
+            else:
+                # One call per iteration, each continuing from the image of
+                # the last (the same passes: the mask is idempotent and the
+                # subset sensitivity is rebuilt the same way), so that the
+                # chosen iterations can be saved.
+                p.iterations = 1
+                for it in range(self.num_MLEM_iterations):
+                    L.check(L.lib().yrtb_osem_listmode(proj.h, ctypes.byref(ev.c()),
+                                                       sens.data_ptr(), img.data_ptr(),
+                                                       work.data_ptr(), ctypes.byref(p),
+                                                       _stream()))
+                    p.init_from_image = 1
+                    self._save_iteration(it, img, ip.shape)
         if use_side:
             stream.wait_stream(s)
         self._last_events = ev
@@ -423,7 +469,7 @@ class OSEM_GPU:
             # (OSEM_GPU::computeEMUpdateImage, OSEM_GPU.cu:456-509).
             xpsf = torch.empty_like(img)
             em_psf = torch.empty_like(em)
-        for _ in range(self.num_MLEM_iterations):
+        for it in range(self.num_MLEM_iterations):
             for s in range(self.num_OSEM_subsets):
                 em.zero_()
                 if psf is not None:
@@ -441,6 +487,7 @@ class OSEM_GPU:
                     img.data_ptr(), (em if psf is None else em_psf).data_ptr(),
                     self._sens_images[s].data_ptr(), J, 1, 1, self.EPS_FLT,
                     None, _stream()))
+            self._save_iteration(it, img, ip.shape)
         return img.reshape(ip.shape)
 
 
