@@ -76,6 +76,9 @@ def parse():
                     help="write every autotuner candidate and its time (JSON)")
     ap.add_argument("--deterministic", action="store_true",
                     help="two-pass fixed-point back projection")
+    ap.add_argument("--layout", default="tile", choices=["tile", "row"],
+                    help="image layout of the timed EM passes: 4x2 tiles "
+                         "(YRTB_LAYOUT_TILE_4X2) or the reference's row-major")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2mr", "c3", "c4", "c5", "psf", "lrem"],
                     help="c2 (default) is the headline workload; the others "
                          "run bench_configs.py")
@@ -572,6 +575,13 @@ def main():
     img = torch.full((J,), 0.125, device="cuda")
     img.mul_((sens > 0).float())
     em = torch.zeros(J, device="cuda")
+    # Image layout of the timed EM passes (set-up: the image and the subset
+    # sensitivity converted once; the EM update is elementwise).
+    tiled = args.layout == "tile" and not args.deterministic
+    if tiled:
+        proj.set_image_layout(L.YRTB_LAYOUT_TILE_4X2)
+        img = proj.to_layout(img, ip, L.YRTB_LAYOUT_TILE_4X2)
+        sens_sub = proj.to_layout(sens_sub, ip, L.YRTB_LAYOUT_TILE_4X2)
 
     # Launch configuration: timed on a sample of subset 0 (setup, not timed;
     # a calibration done once per projector, like a library's algorithm
@@ -670,7 +680,11 @@ def main():
 
     # Plain (file-order) form on the same GPU, for the batched-vs-plain ratio,
     # with the reference's launch shape (one thread per event, 256-thread
-    # blocks).
+    # blocks) and image layout (row-major).
+    if tiled:
+        img = proj.to_layout(img, ip, L.YRTB_LAYOUT_ROW_MAJOR)
+        sens_sub = proj.to_layout(sens_sub, ip, L.YRTB_LAYOUT_ROW_MAJOR)
+        proj.set_image_layout(L.YRTB_LAYOUT_ROW_MAJOR)
     proj.set_launch(256, 1, launch["bucket_shift"], launch["order"],
                     launch["tile_shift"], 0)
     for _ in range(1):
@@ -810,7 +824,8 @@ def main():
               "peak_source": "measured live (libyrtb_l2bench.so: random aligned groups "
                              "in an L2-resident buffer of the image's size)"}
         cnt = json.load(open(l2prof))
-        launch = proj.get_launch()
+        launch = dict(proj.get_launch(), image_layout=(L.YRTB_LAYOUT_TILE_4X2 if tiled
+                                                       else L.YRTB_LAYOUT_ROW_MAJOR))
         if all(launch.get(k) == v for k, v in cnt["launch"].items()):
             reqs = (cnt["red_requests_per_event"] + cnt["read_requests_per_event"]) \
                 * ev.count / SUBSETS
@@ -856,6 +871,7 @@ def main():
                                         min(args.ref_sample, args.events)),
                 "mode": {"precision": args.precision,
                          "deterministic": bool(args.deterministic),
+                         "image_layout": "tile_4x2" if tiled else "row_major",
                          "launch": launch,
                          "autotune": None if tune is None else {
                              "sample_events": tune["sample_events"],

@@ -214,6 +214,34 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 yrtb_status yrtb_projector_get_launch(const yrtb_projector* h,
                                       yrtb_launch_config* cfg);
 
+/* Image layouts.  ROW_MAJOR is the reference's (x fastest, then y, z, frame).
+ * TILE_4X2 stores each z plane as tiles of 4 x 2 voxels (x, y), 8 floats per
+ * tile (one 32-byte sector: voxel (x, y) of a tile at (x & 1) + 2 (y & 1) +
+ * 4 ((x >> 1) & 1)), tiles in row-major order inside the plane, planes and
+ * frames as in ROW_MAJOR; it needs nx % 4 == 0 and ny % 2 == 0.  An aligned
+ * group of 4 floats is then a 2 x 2 square, which a ray crosses in more
+ * steps than 4 voxels of a row, so the walks send fewer L2 requests.  No
+ * reference counterpart. */
+#define YRTB_LAYOUT_ROW_MAJOR 0
+#define YRTB_LAYOUT_TILE_4X2 1
+
+/* Layout of the images given to this projector's list-mode projections
+ * (yrtb_forward, yrtb_backward, yrtb_em_step, yrtb_em_step_model).  TILE_4X2
+ * needs a single-ray Siddon projector without deterministic back projection
+ * and image dimensions as above.  Every other call (histogram mode,
+ * sensitivity images, attenuation images, the image-space PSF, the OSEM
+ * drivers' arguments) takes ROW_MAJOR images whatever this setting.  No
+ * reference counterpart. */
+yrtb_status yrtb_projector_set_image_layout(yrtb_projector* h, int layout);
+yrtb_status yrtb_projector_get_image_layout(const yrtb_projector* h, int* layout);
+
+/* Converts nt frames of an image between layouts (d_src and d_dst distinct
+ * device buffers of ip->nx * ny * nz * nt floats).  to_layout: the layout of
+ * d_dst; d_src is in the other one.  No reference counterpart. */
+yrtb_status yrtb_image_convert_layout(const float* d_src, float* d_dst,
+                                      const yrtb_image_params* ip, int to_layout,
+                                      yrtb_stream stream);
+
 /* Temporaries of yrtb_events_subset_order, yrtb_attenuation_factors and
  * yrtb_autotune come from a stream-ordered memory pool per device that keeps
  * freed blocks for later calls (ordering 50M events holds about 3.6 GB).

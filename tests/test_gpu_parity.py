@@ -320,6 +320,101 @@ def test_multiray_one_lane_per_ray_matches_one_thread(tof, prec, rays):
         p.set_launch(**cfg)
 
 
+# ------------------------------------------------------- tiled images ------
+@pytest.mark.parametrize("tof,prec", [(None, L.YRTB_MIRROR), ((214.0, 5), L.YRTB_MIRROR),
+                                      (None, L.YRTB_COMPENSATED),
+                                      ((214.0, 5), L.YRTB_COMPENSATED)])
+def test_tiled_image_layout_gives_the_same_projections(tof, prec):
+    # YRTB_LAYOUT_TILE_4X2 changes only where each voxel is stored: the walks
+    # visit the same voxels with the same weights in the same order, so the
+    # forward projections are bit-identical to the row-major ones in every
+    # vector mode; back projections and EM images agree up to the order of
+    # the FP32 atomics.  Images with an offset and nt = 2 frames.
+    ip_args = (32, 24, 16, 128, 96, 64, 1.5, -2.0, 3.0)
+    sc, ip, p = make(ip_args=ip_args, tof=tof, precision=prec, nt=2)
+    _, _, q = make(ip_args=ip_args, tof=tof, precision=prec, nt=2)
+    d1, d2 = random_events(SC_ARGS, 8000, 41)
+    rng = np.random.default_rng(42)
+    tv = rng.normal(0, 200, len(d1)).astype(np.float32) if tof else None
+    fr = rng.integers(0, 2, len(d1)).astype(np.int32)
+    ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv, frame=torch.from_numpy(fr).cuda())
+    img = torch.from_numpy(rng.random(ip.shape, dtype=np.float32)).cuda()
+    y = torch.from_numpy(rng.uniform(0.1, 1.0, len(d1)).astype(np.float32)).cuda()
+    T, R = L.YRTB_LAYOUT_TILE_4X2, L.YRTB_LAYOUT_ROW_MAJOR
+    timg = q.to_layout(img, ip, T)
+    assert torch.equal(q.to_layout(timg, ip, R), img.reshape(-1))
+    assert not torch.equal(timg, img.reshape(-1))
+    q.set_image_layout(T)
+    assert q.get_image_layout() == T
+    for vg in (0, 1, 2, 4):
+        for h in (p, q):
+            cfg = h.get_launch()
+            cfg["vector_groups"] = vg
+            h.set_launch(**cfg)
+        f_row = p.forward(img, ev)
+        f_tile = q.forward(timg.reshape(ip.shape), ev)
+        assert torch.equal(f_row, f_tile), vg
+        b_row = p.backward(y, ev)
+        b_tile = q.to_layout(q.backward(y, ev), ip, R)
+        assert rel_l2(b_tile.cpu().numpy(), b_row.cpu().numpy()) < 1e-6
+        e_row = p.em_step(img, torch.zeros(ip.shape, device="cuda"), ev)
+        e_tile = q.to_layout(q.em_step(timg.reshape(ip.shape),
+                                       torch.zeros(ip.shape, device="cuda"), ev), ip, R)
+        assert rel_l2(e_tile.cpu().numpy(), e_row.cpu().numpy()) < 1e-6
+
+
+def test_tiled_image_layout_rejections():
+    T = L.YRTB_LAYOUT_TILE_4X2
+    for kw in (dict(projector="DD"), dict(num_rays=4),
+               dict(ip_args=(30, 32, 16, 120, 128, 64)),
+               dict(ip_args=(32, 31, 16, 128, 124, 64))):
+        _, _, p = make(**kw)
+        with pytest.raises(RuntimeError):
+            p.set_image_layout(T)
+    sc = yrt.Scanner("t", *SC_ARGS)
+    pp = yrt.ProjectorParams(sc)
+    pp.deterministic = True
+    p = yrt.DeviceProjector(sc, yrt.ImageParams(*IP_ARGS), pp)
+    with pytest.raises(RuntimeError):
+        p.set_image_layout(T)
+    with pytest.raises(RuntimeError):
+        p.set_image_layout(7)
+
+
+def test_osem_driver_tiles_internally_same_image():
+    # yrtb_osem_listmode walks 4 x 2 tiles internally for a single-ray
+    # Siddon projector; its arguments and result stay row-major.  The same
+    # OSEM driven subset by subset in row-major from Python must agree
+    # (rel-L2 <= 1e-5: FP32 atomics order over 2 x 3 subset updates).
+    import ctypes
+    from pyyrtpet_b200.core import _stream
+    sc, ip, p = make(tof=(214.0, 5), precision=L.YRTB_COMPENSATED)
+    d1, d2 = random_events(SC_ARGS, 30000, 43)
+    rng = np.random.default_rng(44)
+    tv = rng.normal(0, 200, len(d1)).astype(np.float32)
+    ev = yrt.DeviceEvents.from_arrays(d1, d2, tof=tv)
+    sens = torch.from_numpy(rng.uniform(0.5, 2.0, ip.numVoxels).astype(np.float32)).cuda()
+    sens[:100] = 0.0
+    J, S = ip.numVoxels, 3
+    x = torch.empty(J, device="cuda")
+    work = torch.empty(2 * J, device="cuda")
+    prm = L.yrtb_osem_params(2, S, 1.0, 1e-35, 1.19209e-07, 0, 0, None, None)
+    L.check(L.lib().yrtb_osem_listmode(p.h, ctypes.byref(ev.c()), sens.data_ptr(),
+                                       x.data_ptr(), work.data_ptr(), ctypes.byref(prm),
+                                       _stream()))
+    ref = torch.where(sens > 0, torch.full_like(sens, 0.125), torch.zeros_like(sens))
+    sens_sub = (sens / S).contiguous()
+    em = torch.empty(J, device="cuda")
+    for _ in range(2):
+        for s in range(S):
+            em.zero_()
+            p.em_step(ref, em, ev, rng=L.yrtb_range(s, S, 0))
+            L.check(L.lib().yrtb_em_update(ref.data_ptr(), em.data_ptr(), sens_sub.data_ptr(),
+                                           J, 1, 1, 1.19209e-07, None, _stream()))
+    assert float(x.abs().sum()) > 0
+    assert rel_l2(x.cpu().numpy(), ref.cpu().numpy()) < 1e-5
+
+
 # ---------------------------------------------------------------- DD ------
 @pytest.mark.parametrize("tof,psf,prec", [(None, False, L.YRTB_MIRROR),
                                           ((214.0, 5), False, L.YRTB_MIRROR),

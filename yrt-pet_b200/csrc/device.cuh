@@ -174,7 +174,21 @@ __device__ __forceinline__ void slabAlpha(R r0, R r1, R p1, R p2, R inv,
 // non-empty segment, emitFirst() visits it, next() takes one step.
 // siddonWalk() runs it to the end on one thread; siddonWalkWarp() runs the
 // rays of a whole warp in lock step.
-template <bool TOF, bool COMP>
+//
+// TILE: the image is stored in tiles of 4 x 2 voxels (x, y) of one z plane,
+// 8 floats (one 32-byte sector) per tile, tiles in row-major order inside a
+// plane and planes in z order (tileOffset); nx a multiple of 4, ny of 2.  An
+// aligned group of four floats is then a 2 x 2 square instead of 4 voxels of
+// one row, so that a ray crossing the plane in any direction stays longer in
+// one group and one sector.  Same voxels, weights and order: only the
+// offsets change.
+__device__ __forceinline__ int tileOffset(int vx, int vy, int vz, int nx, int nxy)
+{
+	return vz * nxy + (vy >> 1) * (2 * nx) + ((vx >> 2) << 3) + (((vx >> 1) & 1) << 2) +
+	       ((vy & 1) << 1) + (vx & 1);
+}
+
+template <bool TOF, bool COMP, bool TILE = false>
 struct SiddonWalker
 {
 	float3 p1, p2;
@@ -189,6 +203,9 @@ struct SiddonWalker
 	// COMP: linear voxel index moved by a per-step delta.
 	int lin, dprev, dny, dnz;
 	unsigned nvox;
+	// COMP and TILE: parity of the voxel's x and y, and the offset deltas of
+	// one x / y step from an odd or an even coordinate in the ray's direction.
+	int px, py, dxo, dxe, dyo, dye;
 	// Mirror: voxel coordinates and row offset, as the reference keeps them.
 	int vx, vy, vz, off, dir_prev, nx, ny, nz, nxy;
 	// TOF weight constants.
@@ -469,8 +486,25 @@ struct SiddonWalker
 			dny = dir_y * nx;
 			dnz = dir_z * nxy;
 			nvox = static_cast<unsigned>(nxy * nz);
-			lin = vz * nxy + vy * nx + vx;
-			dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
+			if constexpr (TILE)
+			{
+				// x: +1 from even, +3 from odd (into the next 2-wide half or
+				// tile); -1 from odd, -3 from even.  y: +2 inside a tile
+				// row, 2 nx - 2 into the next; mirrored backwards.
+				lin = tileOffset(vx, vy, vz, nx, nxy);
+				px = vx & 1;
+				py = vy & 1;
+				dxo = dir_x > 0 ? 3 : -1;
+				dxe = dir_x > 0 ? 1 : -3;
+				dyo = dir_y > 0 ? 2 * nx - 2 : -2;
+				dye = dir_y > 0 ? 2 : -(2 * nx - 2);
+				stepDelta();
+			}
+			else
+			{
+				lin = vz * nxy + vy * nx + vx;
+				dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
+			}
 		}
 		else
 		{
@@ -481,13 +515,31 @@ struct SiddonWalker
 	}
 
 	// Visits the first segment (after a successful begin).
+	// TILE, COMP: the offset delta of the axes stepped at the end of this
+	// segment, from the current voxel's parities, which then flip.
+	__device__ __forceinline__ void stepDelta()
+	{
+		dprev = (sx ? (px ? dxo : dxe) : 0) + (sy ? (py ? dyo : dye) : 0) + (sz ? dnz : 0);
+		px ^= static_cast<int>(sx);
+		py ^= static_cast<int>(sy);
+	}
+
+	// Offset of the mirror walk's voxel.
+	__device__ __forceinline__ int mirrorOffset() const
+	{
+		if constexpr (TILE)
+			return tileOffset(vx, vy, vz, nx, nxy);
+		else
+			return vx + off;
+	}
+
 	template <typename Visit>
 	__device__ __forceinline__ void emitFirst(Visit& visit)
 	{
 		if constexpr (COMP)
 			emit(lin, visit);
 		else
-			emit(vx + off, visit);
+			emit(mirrorOffset(), visit);
 	}
 
 	// One step of the walk: the next crossing, its voxel and its visit;
@@ -507,7 +559,10 @@ struct SiddonWalker
 			lin += dprev;
 			if (static_cast<unsigned>(lin) >= nvox)
 				return false;
-			dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
+			if constexpr (TILE)
+				stepDelta();
+			else
+				dprev = (sx ? dir_x : 0) + (sy ? dny : 0) + (sz ? dnz : 0);
 			emit(lin, visit);
 		}
 		else
@@ -522,20 +577,20 @@ struct SiddonWalker
 			    static_cast<unsigned>(vz) >= static_cast<unsigned>(nz))
 				return false;
 			dir_prev = (sx ? 1 : 0) | (sy ? 2 : 0) | (sz ? 4 : 0);
-			emit(vx + off, visit);
+			emit(mirrorOffset(), visit);
 		}
 		return true;
 	}
 };
 
-template <bool TOF, bool COMP, typename Visit>
+template <bool TOF, bool COMP, bool TILE = false, typename Visit>
 __device__ __forceinline__ void siddonWalk(const Geom& g, const float3 p1,
                                            const float3 p2, const TofP& tp,
                                            float tofValue, Visit& visit,
                                            float wlo = 0.f, float whi = 1.f,
                                            int part = 0, int parts = 1)
 {
-	SiddonWalker<TOF, COMP> w;
+	SiddonWalker<TOF, COMP, TILE> w;
 	if (!w.begin(g, p1, p2, tp, tofValue, wlo, whi, part, parts))
 		return;
 	w.emitFirst(visit);

@@ -357,7 +357,8 @@ __device__ __forceinline__ bool fetchEvent(const KParams& P, const Events& E,
 }
 
 // Runs the configured projector over one event; endRay() after each ray.
-template <int KIND, bool TOF, bool COMP, typename Visit, typename EndRay>
+// TILE: the image is in 4 x 2 tiles (tileOffset; single-ray Siddon only).
+template <int KIND, bool TOF, bool COMP, bool TILE = false, typename Visit, typename EndRay>
 __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
                                              float3 p2, float3 n1, float3 n2,
                                              float tofv, uint64_t rid,
@@ -365,10 +366,11 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
                                              EndRay& endRay, int part = 0,
                                              int parts = 1)
 {
+	static_assert(!TILE || KIND == K_SIDDON, "tiled images: single-ray Siddon");
 	if constexpr (KIND == K_SIDDON)
 	{
-		siddonWalk<TOF, COMP>(P.g, p1, p2, P.tof, tofv, visit, 0.f, 1.f, part,
-		                      parts);
+		siddonWalk<TOF, COMP, TILE>(P.g, p1, p2, P.tof, tofv, visit, 0.f, 1.f, part,
+		                            parts);
 		endRay();
 	}
 	else if constexpr (KIND == K_SIDDON_MR)
@@ -446,7 +448,8 @@ __device__ __forceinline__ void projectEvent(const KParams& P, float3 p1,
 // computed exactly as without TRACK).
 // VEC: the image is read as aligned float4 groups, and consecutive
 // crossings inside one group (x steps) reuse the group held in registers.
-template <int KIND, bool TOF, bool COMP, bool TRACK = false, bool VEC = false>
+template <int KIND, bool TOF, bool COMP, bool TRACK = false, bool VEC = false,
+          bool TILE = false>
 __device__ __forceinline__ float forwardEvent(const KParams& P,
                                               const float* __restrict__ img,
                                               float3 p1, float3 p2, float3 n1,
@@ -498,8 +501,8 @@ __device__ __forceinline__ float forwardEvent(const KParams& P,
 		ray = 0.f;
 		comp = 0.f;
 	};
-	projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, true, visit,
-	                              endRay, part, parts);
+	projectEvent<KIND, TOF, COMP, TILE>(P, p1, p2, n1, n2, tofv, rid, true, visit,
+	                                    endRay, part, parts);
 	// One lane per ray (parts > 1): the caller adds the rays' sums in ray
 	// order and divides (rayGroupMean).
 	if constexpr (KIND == K_SIDDON_MR)
@@ -581,7 +584,8 @@ __device__ __forceinline__ void redV4(float* p, float4 v)
 // are staged in this thread's shared-memory slots (vslot[l * vstride]; a
 // single-ray walk visits each voxel once, so a slot is written at most once
 // per group) and read back only to send the group.
-template <int KIND, bool TOF, bool COMP, bool FIX = false, int VEC = 0>
+template <int KIND, bool TOF, bool COMP, bool FIX = false, int VEC = 0,
+          bool TILE = false>
 __device__ __forceinline__ void backwardEvent(const KParams& P,
                                               float* __restrict__ img,
                                               float v, float3 p1, float3 p2,
@@ -640,8 +644,8 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 				send();
 			gb = -1;
 		};
-		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
-		                              flush, part, parts);
+		projectEvent<KIND, TOF, COMP, TILE>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+		                                    flush, part, parts);
 	}
 	else if constexpr (VEC == 1)
 	{
@@ -671,14 +675,14 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 				redV4(img + gb, a4);
 			gb = -1;
 		};
-		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
-		                              flush, part, parts);
+		projectEvent<KIND, TOF, COMP, TILE>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+		                                    flush, part, parts);
 	}
 	else
 	{
 		auto visit = [&](int o, float w) { atomicAdd(img + o, v * w); };
-		projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, rid, false, visit,
-		                              endRay, part, parts);
+		projectEvent<KIND, TOF, COMP, TILE>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+		                                    endRay, part, parts);
 	}
 }
 
@@ -735,9 +739,10 @@ __device__ __forceinline__ float rayGroupMean(float ray, int numRays)
 // one lane per ray: 1024 threads per SM (64 registers per thread, 32 warps)
 // whatever the block size; multi-ray with one thread per event: 768; the
 // other projectors keep the compiler's register choice.  FIX (OP_BWD,
-// OP_EM): pass 2 of the deterministic back projection.
+// OP_EM): pass 2 of the deterministic back projection.  TILE: the images
+// are in 4 x 2 tiles (tileOffset).
 template <int OP, int KIND, bool TOF, bool COMP, bool FIX = false,
-          int BLOCK = kBlock, int TPL = 1, int VEC = 0>
+          int BLOCK = kBlock, int TPL = 1, int VEC = 0, bool TILE = false>
 __global__ void __launch_bounds__(BLOCK, (KIND == K_SIDDON || (KIND == K_SIDDON_MR && TPL > 1))
                                              ? 1024 / BLOCK
                                              : (KIND == K_SIDDON_MR ? 768 / BLOCK : 1))
@@ -749,6 +754,8 @@ __global__ void __launch_bounds__(BLOCK, (KIND == K_SIDDON || (KIND == K_SIDDON_
 	                  (KIND == K_SIDDON_MR && !FIX && OP != OP_COUNT),
 	              "several threads per LOR: single-ray Siddon (compensated) or one "
 	              "lane per ray of a multi-ray Siddon");
+	static_assert(!TILE || (KIND == K_SIDDON && TPL == 1 && !FIX && OP != OP_COUNT),
+	              "tiled images: single-ray Siddon, one thread per LOR, float scatter");
 	// Forward sum of the event from the TPL lanes' partial sums.
 	auto eventSum = [&](float v) -> float
 	{
@@ -804,7 +811,7 @@ __global__ void __launch_bounds__(BLOCK, (KIND == K_SIDDON || (KIND == K_SIDDON_
 		}
 		else if constexpr (OP == OP_FWD)
 		{
-			const float v = eventSum(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
+			const float v = eventSum(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0, TILE>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			if (part == 0)
 				out[e] = v;
@@ -816,10 +823,9 @@ __global__ void __launch_bounds__(BLOCK, (KIND == K_SIDDON || (KIND == K_SIDDON_
 				                                     p2, n1, n2, tofv, k,
 				                                     F.acc + fo, fixedScale(F));
 			else
-				backwardEvent<KIND, TOF, COMP, false, kRedMode>(P, out + fo, __ldg(in + e),
-				                                                p1, p2, n1, n2, tofv, k,
-				                                                nullptr, 0.0, part, TPL,
-				                                                vslot, BLOCK);
+				backwardEvent<KIND, TOF, COMP, false, kRedMode, TILE>(
+				    P, out + fo, __ldg(in + e), p1, p2, n1, n2, tofv, k, nullptr, 0.0,
+				    part, TPL, vslot, BLOCK);
 		}
 		else
 		{
@@ -832,7 +838,7 @@ __global__ void __launch_bounds__(BLOCK, (KIND == K_SIDDON || (KIND == K_SIDDON_
 					E.model[e] = 0.f;
 				return;
 			}
-			float u = eventSum(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0>(
+			float u = eventSum(forwardEvent<KIND, TOF, COMP, false, (VEC & 1) != 0, TILE>(
 			    P, in + fo, p1, p2, n1, n2, tofv, k, nullptr, part, TPL));
 			u *= s;
 			u *= a;
@@ -852,7 +858,7 @@ __global__ void __launch_bounds__(BLOCK, (KIND == K_SIDDON || (KIND == K_SIDDON_
 					                                     n2, tofv, k, F.acc + fo,
 					                                     fixedScale(F));
 				else
-					backwardEvent<KIND, TOF, COMP, false, kRedMode>(P, out + fo, u, p1, p2,
+					backwardEvent<KIND, TOF, COMP, false, kRedMode, TILE>(P, out + fo, u, p1, p2,
 					                                                n1, n2, tofv, k, nullptr,
 					                                                0.0, part, TPL, vslot,
 					                                                BLOCK);
@@ -1750,6 +1756,31 @@ __global__ void __launch_bounds__(kBlock)
 	}
 }
 
+// Row-major <-> 4 x 2 tiles (tileOffset), one voxel per thread in row-major
+// order: the row-major side is read or written coalesced, the tiled side
+// within the same 32-byte sectors.
+template <bool TO_TILES>
+__global__ void k_convert_layout(const float* __restrict__ src, float* __restrict__ dst,
+                                 int nx, int ny, int nz, uint64_t total)
+{
+	const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (i >= total)
+		return;
+	const int nxy = nx * ny;
+	const uint64_t nvox = static_cast<uint64_t>(nxy) * nz;
+	const uint64_t frame = i / nvox;
+	const int r = static_cast<int>(i - frame * nvox);
+	const int z = r / nxy;
+	const int xy = r - z * nxy;
+	const int y = xy / nx;
+	const int x = xy - y * nx;
+	const uint64_t t = frame * nvox + static_cast<uint64_t>(tileOffset(x, y, z, nx, nxy));
+	if constexpr (TO_TILES)
+		dst[t] = __ldg(src + i);
+	else
+		dst[i] = __ldg(src + t);
+}
+
 __global__ void k_fill(float* __restrict__ x, uint64_t n, float v)
 {
 	const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -2408,6 +2439,8 @@ struct yrtb_projector
 	uint64_t mrCapacity = 0;
 	// Launch configuration of the single-ray Siddon event kernels.
 	yrtb_launch_config launch{256, 1, 3, YRTB_ORDER_LOR, 1, 2};
+	// Layout of the images of the list-mode projections (YRTB_LAYOUT_*).
+	int layout = YRTB_LAYOUT_ROW_MAJOR;
 	// Deterministic back projection: fixed-point image (nvox * nt) and bound.
 	bool det = false;
 	unsigned long long* d_fix = nullptr;
@@ -2590,7 +2623,7 @@ void fixedEnd(yrtb_projector* h, const Fixed& F, float* out, cudaStream_t st)
 // Siddon event kernel with block size B and the projector's threads per LOR:
 // pieces of a single ray (compensated arithmetic only; 1 otherwise), or one
 // lane per ray of a multi-ray projector.
-template <int OP, int K, bool T, bool C, int B>
+template <int OP, int K, bool T, bool C, int B, bool TILE = false>
 void launchTuned(const yrtb_projector* h, const Events& E, Range R,
                  const float* in, float* out, float gs, float thr,
                  cudaStream_t st, const Fixed& F)
@@ -2623,7 +2656,7 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 				{
 					constexpr int V = decltype(vc)::value;
 					if constexpr ((V & kUse) == V)
-						k_events<OP, K, T, C, false, B, TPL, V><<<grid, B, 0, st>>>(
+						k_events<OP, K, T, C, false, B, TPL, V, TILE><<<grid, B, 0, st>>>(
 						    h->P, E, R, in, out, gs, thr, h->d_err, F);
 				};
 				switch (vg)
@@ -2637,7 +2670,7 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 				return;
 			}
 		}
-		k_events<OP, K, T, C, false, B, TPL><<<grid, B, 0, st>>>(h->P, E, R, in, out, gs,
+		k_events<OP, K, T, C, false, B, TPL, 0, TILE><<<grid, B, 0, st>>>(h->P, E, R, in, out, gs,
 		                                                        thr, h->d_err, F);
 	};
 	int tpl = h->launch.threads_per_lor;
@@ -2656,7 +2689,7 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 		else
 			go(std::integral_constant<int, 1>{});
 	}
-	else if constexpr (C)
+	else if constexpr (C && !TILE)
 	{
 		if (tpl == 4)
 			go(std::integral_constant<int, 4>{});
@@ -2667,6 +2700,7 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 	}
 	else
 	{
+		// Tiled images: one thread per LOR.
 		go(std::integral_constant<int, 1>{});
 	}
 }
@@ -2681,15 +2715,20 @@ inline int rayLanes(int numRays)
 	return l <= 8 ? l : 0;
 }
 
+// layout: the images' layout (YRTB_LAYOUT_*), -1 for the projector's.
 template <int OP>
 yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
                            yrtb_range range, const float* in, float* out,
                            float gs, float thr, yrtb_stream stream,
-                           float* model = nullptr)
+                           float* model = nullptr, int layout = -1)
 {
 	yrtb_status s = checkEvents(h, ev, range, true);
 	if (s != YRTB_OK)
 		return s;
+	const bool tiled = OP != OP_COUNT && (layout < 0 ? h->layout : layout) == YRTB_LAYOUT_TILE_4X2;
+	if (tiled && (h->kind != K_SIDDON || h->det))
+		return fail(YRTB_ERR_ARGUMENT, "tiled images need a single-ray Siddon projector "
+		                               "without deterministic back projection");
 	if (range.count == 0)
 		return YRTB_OK;
 	YRTB_CUDA(cudaSetDevice(h->device));
@@ -2712,7 +2751,14 @@ yrtb_status dispatchEvents(yrtb_projector* h, const yrtb_events* ev,
 		{
 			if (!(kScatter && h->det))
 			{
-				if (h->launch.block == 128)
+				if (tiled)
+				{
+					if (h->launch.block == 128)
+						launchTuned<OP, K, T, C, 128, true>(h, E, R, in, out, gs, thr, st, F);
+					else
+						launchTuned<OP, K, T, C, 256, true>(h, E, R, in, out, gs, thr, st, F);
+				}
+				else if (h->launch.block == 128)
 					launchTuned<OP, K, T, C, 128>(h, E, R, in, out, gs, thr, st, F);
 				else
 					launchTuned<OP, K, T, C, 256>(h, E, R, in, out, gs, thr, st, F);
@@ -3240,6 +3286,53 @@ yrtb_status yrtb_projector_get_launch(const yrtb_projector* h,
 	if (!h || !c)
 		return fail(YRTB_ERR_ARGUMENT, "null argument");
 	*c = h->launch;
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_projector_set_image_layout(yrtb_projector* h, int layout)
+{
+	if (!h)
+		return fail(YRTB_ERR_ARGUMENT, "null projector");
+	if (layout != YRTB_LAYOUT_ROW_MAJOR && layout != YRTB_LAYOUT_TILE_4X2)
+		return fail(YRTB_ERR_ARGUMENT, "unknown image layout");
+	if (layout == YRTB_LAYOUT_TILE_4X2)
+	{
+		if (h->kind != K_SIDDON || h->det)
+			return fail(YRTB_ERR_ARGUMENT, "tiled images need a single-ray Siddon "
+			                               "projector without deterministic back projection");
+		if (h->ip.nx % 4 != 0 || h->ip.ny % 2 != 0)
+			return fail(YRTB_ERR_ARGUMENT, "tiled images need nx % 4 == 0 and ny % 2 == 0");
+	}
+	h->layout = layout;
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_projector_get_image_layout(const yrtb_projector* h, int* layout)
+{
+	if (!h || !layout)
+		return fail(YRTB_ERR_ARGUMENT, "null argument");
+	*layout = h->layout;
+	return YRTB_OK;
+}
+
+yrtb_status yrtb_image_convert_layout(const float* d_src, float* d_dst,
+                                      const yrtb_image_params* ip, int to_layout,
+                                      yrtb_stream stream)
+{
+	if (!d_src || !d_dst || d_src == d_dst || !validImage(ip))
+		return fail(YRTB_ERR_ARGUMENT, "invalid layout conversion arguments");
+	if (to_layout != YRTB_LAYOUT_ROW_MAJOR && to_layout != YRTB_LAYOUT_TILE_4X2)
+		return fail(YRTB_ERR_ARGUMENT, "unknown image layout");
+	if (ip->nx % 4 != 0 || ip->ny % 2 != 0)
+		return fail(YRTB_ERR_ARGUMENT, "tiled images need nx % 4 == 0 and ny % 2 == 0");
+	const uint64_t total = static_cast<uint64_t>(ip->nx) * ip->ny * ip->nz * ip->nt;
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	const unsigned grid = static_cast<unsigned>((total + kBlock - 1) / kBlock);
+	if (to_layout == YRTB_LAYOUT_TILE_4X2)
+		k_convert_layout<true><<<grid, kBlock, 0, st>>>(d_src, d_dst, ip->nx, ip->ny, ip->nz, total);
+	else
+		k_convert_layout<false><<<grid, kBlock, 0, st>>>(d_src, d_dst, ip->nx, ip->ny, ip->nz, total);
+	YRTB_LAUNCHED();
 	return YRTB_OK;
 }
 
@@ -4385,12 +4478,29 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 	// after the pass) and the PSF's temporary follow.
 	float* xpsf = sens + J;
 	float* ptmp = xpsf + J * nt;
+	// Without an image-space PSF, a single-ray Siddon projector walks the
+	// images in 4 x 2 tiles (YRTB_LAYOUT_TILE_4X2: fewer L2 requests per
+	// crossing; the same sums): the image and the sensitivity are converted
+	// on entry and the image back on exit, through the EM buffer.
+	const bool tile = h->kind == K_SIDDON && !h->det && !p->psf && !p->varpsf &&
+	                  h->ip.nx % 4 == 0 && h->ip.ny % 2 == 0;
+	const int layout = tile ? YRTB_LAYOUT_TILE_4X2 : YRTB_LAYOUT_ROW_MAJOR;
+	yrtb_image_params ip1 = h->ip;
+	ip1.nt = 1;
 	// List-mode sensitivity is shared by all subsets and divided by their
 	// number (OSEM::initializeSensImageBuffer, OSEM.cpp:1007-1035).
-	YRTB_CUDA(cudaMemcpyAsync(sens, d_sens, J * sizeof(float),
-	                          cudaMemcpyDeviceToDevice,
-	                          reinterpret_cast<cudaStream_t>(stream)));
 	yrtb_status s = YRTB_OK;
+	if (tile)
+	{
+		if ((s = yrtb_image_convert_layout(d_sens, sens, &ip1, layout, stream)) != YRTB_OK)
+			return s;
+	}
+	else
+	{
+		YRTB_CUDA(cudaMemcpyAsync(sens, d_sens, J * sizeof(float),
+		                          cudaMemcpyDeviceToDevice,
+		                          reinterpret_cast<cudaStream_t>(stream)));
+	}
 	if (p->subsets != 1)
 		s = yrtb_scale(sens, J, 1.0f / static_cast<float>(p->subsets), stream);
 	if (s != YRTB_OK)
@@ -4402,6 +4512,19 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 			return s;
 	if ((s = yrtb_apply_threshold(d_image, d_sens, J, nt, 1, 0.f, 0.f, 0.f, 1.f,
 	                              0.f, stream)) != YRTB_OK)
+		return s;
+	// Converts d_image in place to `to` through the EM buffer.
+	auto convertImage = [&](int to) -> yrtb_status
+	{
+		yrtb_status r = yrtb_image_convert_layout(d_image, em, &h->ip, to, stream);
+		if (r != YRTB_OK)
+			return r;
+		YRTB_CUDA(cudaMemcpyAsync(d_image, em, J * nt * sizeof(float),
+		                          cudaMemcpyDeviceToDevice,
+		                          reinterpret_cast<cudaStream_t>(stream)));
+		return YRTB_OK;
+	};
+	if (tile && (s = convertImage(YRTB_LAYOUT_TILE_4X2)) != YRTB_OK)
 		return s;
 
 	auto subsetOps = [&](int sub) -> yrtb_status
@@ -4438,8 +4561,8 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 			return yrtb_em_update(d_image, xpsf, sens, J, nt, 1, p->em_threshold,
 			                      p->d_frame_scale, stream);
 		}
-		if ((r = yrtb_em_step(h, d_image, em, ev, range, p->global_scale,
-		                      p->denom_threshold, stream)) != YRTB_OK)
+		if ((r = dispatchEvents<OP_EM>(h, ev, range, d_image, em, p->global_scale,
+		                               p->denom_threshold, stream, nullptr, layout)) != YRTB_OK)
 			return r;
 		return yrtb_em_update(d_image, em, sens, J, nt, 1, p->em_threshold,
 		                      p->d_frame_scale, stream);
@@ -4452,7 +4575,7 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 			for (int sub = 0; sub < p->subsets; sub++)
 				if ((s = subsetOps(sub)) != YRTB_OK)
 					return s;
-		return YRTB_OK;
+		return tile ? convertImage(YRTB_LAYOUT_ROW_MAJOR) : YRTB_OK;
 	}
 	// One graph per subset, captured once and replayed every iteration.
 	if (st == nullptr)
@@ -4501,7 +4624,7 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 			}
 		}
 	cleanup();
-	return YRTB_OK;
+	return tile ? convertImage(YRTB_LAYOUT_ROW_MAJOR) : YRTB_OK;
 }
 
 yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,

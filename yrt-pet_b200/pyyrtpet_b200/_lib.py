@@ -23,6 +23,8 @@ YRTB_OSEM_STATIC_MAX_FLOATS = 4 * 1024 * 1024
 YRTB_MIRROR = 0
 YRTB_COMPENSATED = 1
 YRTB_ORDER_LOR = 0
+YRTB_LAYOUT_ROW_MAJOR = 0
+YRTB_LAYOUT_TILE_4X2 = 1
 YRTB_ORDER_SPATIAL = 1
 YRTB_ORDER_SPATIAL_FINE = 2
 
@@ -112,6 +114,10 @@ SIGNATURES = {
     "yrtb_projector_destroy": ([c_vp], None),
     "yrtb_projector_set_launch": ([c_vp, _P(yrtb_launch_config)], ctypes.c_int),
     "yrtb_projector_get_launch": ([c_vp, _P(yrtb_launch_config)], ctypes.c_int),
+    "yrtb_projector_set_image_layout": ([c_vp, ctypes.c_int], ctypes.c_int),
+    "yrtb_projector_get_image_layout": ([c_vp, _P(ctypes.c_int)], ctypes.c_int),
+    "yrtb_image_convert_layout": ([c_vp, c_vp, _P(yrtb_image_params), ctypes.c_int, c_vp],
+                                  ctypes.c_int),
     "yrtb_release_cached_memory": ([], ctypes.c_int),
     "yrtb_autotune": ([c_vp, c_vp, _P(yrtb_events), ctypes.c_int, c_u64,
                        _P(yrtb_tune_report), c_vp], ctypes.c_int),

@@ -789,6 +789,33 @@ class DeviceProjector:
         L.check(L.lib().yrtb_projector_get_launch(self.h, ctypes.byref(c)))
         return self._launch_dict(c)
 
+    # --------------------------------------------------------- image layout --
+    def set_image_layout(self, layout: int):
+        """Layout of the images given to forward / backward / em_step
+        (L.YRTB_LAYOUT_ROW_MAJOR or L.YRTB_LAYOUT_TILE_4X2, see
+        yrtb_projector_set_image_layout); convert images with to_layout."""
+        L.check(L.lib().yrtb_projector_set_image_layout(self.h, int(layout)))
+
+    def get_image_layout(self) -> int:
+        v = ctypes.c_int()
+        L.check(L.lib().yrtb_projector_get_image_layout(self.h, ctypes.byref(v)))
+        return v.value
+
+    @staticmethod
+    def to_layout(img: torch.Tensor, img_params: ImageParams, layout: int,
+                  out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """img (nt frames, in the other layout) converted to `layout`."""
+        src = img.contiguous().reshape(-1)
+        if src.numel() != img_params.numVoxels * img_params.nt or \
+                src.dtype != torch.float32 or not src.is_cuda:
+            raise RuntimeError("image does not match the image parameters")
+        if out is None:
+            out = torch.empty_like(src)
+        L.check(L.lib().yrtb_image_convert_layout(src.data_ptr(), out.data_ptr(),
+                                                  ctypes.byref(img_params._c()),
+                                                  int(layout), _stream()))
+        return out
+
     def autotune(self, img, ev: DeviceEvents, num_subsets: int = 1,
                  max_sample: int = 2_000_000) -> dict:
         """Time the fused EM step over a sample of the events for every launch
