@@ -76,7 +76,7 @@ def parse():
                     help="write every autotuner candidate and its time (JSON)")
     ap.add_argument("--deterministic", action="store_true",
                     help="two-pass fixed-point back projection")
-    ap.add_argument("--layout", default="tile", choices=["tile", "row"],
+    ap.add_argument("--layout", default="row", choices=["tile", "row"],
                     help="image layout of the timed EM passes: 4x2 tiles "
                          "(YRTB_LAYOUT_TILE_4X2) or the reference's row-major")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2mr", "c3", "c4", "c5", "psf", "lrem"],

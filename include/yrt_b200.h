@@ -228,10 +228,14 @@ yrtb_status yrtb_projector_get_launch(const yrtb_projector* h,
 /* Layout of the images given to this projector's list-mode projections
  * (yrtb_forward, yrtb_backward, yrtb_em_step, yrtb_em_step_model).  TILE_4X2
  * needs a single-ray Siddon projector without deterministic back projection
- * and image dimensions as above.  Every other call (histogram mode,
- * sensitivity images, attenuation images, the image-space PSF, the OSEM
- * drivers' arguments) takes ROW_MAJOR images whatever this setting.  No
- * reference counterpart. */
+ * and image dimensions as above, and its walks run one thread per LOR
+ * whatever threads_per_lor says; yrtb_osem_listmode then also walks tiles
+ * internally (without an image-space PSF).  Every other call (histogram
+ * mode, sensitivity images, attenuation images, the image-space PSF, the
+ * OSEM drivers' arguments) takes ROW_MAJOR images whatever this setting.
+ * On the C2 TOF workload TILE_4X2 sends 22 % fewer L2 requests but runs
+ * 5 % slower (the parity bookkeeping adds instructions to an issue-bound
+ * walk), so ROW_MAJOR is the default.  No reference counterpart. */
 yrtb_status yrtb_projector_set_image_layout(yrtb_projector* h, int layout);
 yrtb_status yrtb_projector_get_image_layout(const yrtb_projector* h, int* layout);
 

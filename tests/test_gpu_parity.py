@@ -383,12 +383,15 @@ def test_tiled_image_layout_rejections():
 
 def test_osem_driver_tiles_internally_same_image():
     # yrtb_osem_listmode walks 4 x 2 tiles internally for a single-ray
-    # Siddon projector; its arguments and result stay row-major.  The same
-    # OSEM driven subset by subset in row-major from Python must agree
-    # (rel-L2 <= 1e-5: FP32 atomics order over 2 x 3 subset updates).
+    # Siddon projector set to that layout; its arguments and result stay
+    # row-major.  The same OSEM driven subset by subset in row-major from
+    # Python must agree (rel-L2 <= 1e-5: FP32 atomics order over 2 x 3
+    # subset updates).
     import ctypes
     from pyyrtpet_b200.core import _stream
-    sc, ip, p = make(tof=(214.0, 5), precision=L.YRTB_COMPENSATED)
+    sc, ip, q = make(tof=(214.0, 5), precision=L.YRTB_COMPENSATED)
+    _, _, p = make(tof=(214.0, 5), precision=L.YRTB_COMPENSATED)
+    q.set_image_layout(L.YRTB_LAYOUT_TILE_4X2)
     d1, d2 = random_events(SC_ARGS, 30000, 43)
     rng = np.random.default_rng(44)
     tv = rng.normal(0, 200, len(d1)).astype(np.float32)
@@ -399,7 +402,7 @@ def test_osem_driver_tiles_internally_same_image():
     x = torch.empty(J, device="cuda")
     work = torch.empty(2 * J, device="cuda")
     prm = L.yrtb_osem_params(2, S, 1.0, 1e-35, 1.19209e-07, 0, 0, None, None)
-    L.check(L.lib().yrtb_osem_listmode(p.h, ctypes.byref(ev.c()), sens.data_ptr(),
+    L.check(L.lib().yrtb_osem_listmode(q.h, ctypes.byref(ev.c()), sens.data_ptr(),
                                        x.data_ptr(), work.data_ptr(), ctypes.byref(prm),
                                        _stream()))
     ref = torch.where(sens > 0, torch.full_like(sens, 0.125), torch.zeros_like(sens))

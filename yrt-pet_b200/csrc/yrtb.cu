@@ -4478,12 +4478,11 @@ yrtb_status yrtb_osem_listmode(yrtb_projector* h, const yrtb_events* ev,
 	// after the pass) and the PSF's temporary follow.
 	float* xpsf = sens + J;
 	float* ptmp = xpsf + J * nt;
-	// Without an image-space PSF, a single-ray Siddon projector walks the
-	// images in 4 x 2 tiles (YRTB_LAYOUT_TILE_4X2: fewer L2 requests per
-	// crossing; the same sums): the image and the sensitivity are converted
-	// on entry and the image back on exit, through the EM buffer.
-	const bool tile = h->kind == K_SIDDON && !h->det && !p->psf && !p->varpsf &&
-	                  h->ip.nx % 4 == 0 && h->ip.ny % 2 == 0;
+	// A projector set to YRTB_LAYOUT_TILE_4X2 walks 4 x 2 tiles here too
+	// (without an image-space PSF): the image and the sensitivity, given
+	// row-major, are converted on entry and the image back on exit, through
+	// the EM buffer.
+	const bool tile = h->layout == YRTB_LAYOUT_TILE_4X2 && !p->psf && !p->varpsf;
 	const int layout = tile ? YRTB_LAYOUT_TILE_4X2 : YRTB_LAYOUT_ROW_MAJOR;
 	yrtb_image_params ip1 = h->ip;
 	ip1.nt = 1;
@@ -4796,7 +4795,7 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 					if (block != 256 || h->det || (tpl != 1 && tpl != lanes))
 						continue;
 				}
-				else if (tpl == 8 || (tpl > 1 && !split) ||
+				else if (tpl == 8 || (tpl > 1 && (!split || h->layout == YRTB_LAYOUT_TILE_4X2)) ||
 				         (h->det && (block != 256 || tpl != 1)))
 					continue;
 				if (block == o.block && tpl == o.threads_per_lor)
