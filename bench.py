@@ -79,11 +79,11 @@ def parse():
     ap.add_argument("--layout", default="row", choices=["tile", "row"],
                     help="image layout of the timed EM passes: 4x2 tiles "
                          "(YRTB_LAYOUT_TILE_4X2) or the reference's row-major")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2mr", "c3", "c4", "c5", "psf", "lrem"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2mr", "c3", "c4", "c5", "psf", "lrem", "walks"],
                     help="c2 (default) is the headline workload; the others "
                          "run bench_configs.py")
     ap.add_argument("--cfg-events", type=int, default=0,
-                    help="override the event count of --config c1/c2mr/c3/c4/c5")
+                    help="override the event count of --config c1/c2mr/c3/c4/c5/walks")
     return ap.parse_args()
 
 

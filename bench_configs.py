@@ -901,5 +901,52 @@ def run_c2mr(args):
     return out
 
 
+# ------------------------------------------------------- walk sequences ----
+def run_walks(args):
+    """Voxel index sequences of the single-ray Siddon walks on the first
+    events of the C2 workload (yrtb_trace_walks, LOR input), against the CPU
+    restatement's FP32 and FP64 walks (orc_siddon_trace_f32/_f64): the
+    number of rays whose offset sequences differ, per precision mode, without
+    and with TOF.  A parity measurement, not a timing."""
+    import bench
+    yrt, L, S, _stream = _yrt()
+    po = _po()
+    n = args.cfg_events or 20000
+    sc, ip, ph, eff, evs, mu = bench.build_workload(n, "cuda")
+    d1 = evs.d1.cpu().numpy().astype(np.uint32)
+    d2 = evs.d2.cpu().numpy().astype(np.uint32)
+    tof = evs.tof.cpu().numpy()
+    lors, _ = po.lors_from_detpairs(po.scanner_lut(bench.ref_scanner(po, sc)), d1, d2)
+    oip = _po_image(po, ip)
+    out = {"metric": "voxel index sequences of the Siddon walks vs the CPU restatement",
+           "config": {"workload": "C2 scanner and image, the first events of the bench "
+                                  "workload", "events": n}}
+    for tof_on in (False, True):
+        pr = po.Proj(tof_fwhm_ps=bench.TOF_FWHM if tof_on else 0.0,
+                     tof_n_std=bench.TOF_NSTD if tof_on else 0)
+        ev = yrt.DeviceEvents.from_arrays(lor=lors, tof=tof if tof_on else None)
+        seq = {}
+        for prec in (L.YRTB_MIRROR, L.YRTB_COMPENSATED):
+            pp = yrt.ProjectorParams(sc)
+            if tof_on:
+                pp.addTOF(bench.TOF_FWHM, bench.TOF_NSTD)
+            pp.precision = prec
+            o, w, c = yrt.DeviceProjector(sc, ip, pp).trace_walks(ev, 1024)
+            o, c = o.cpu().numpy(), c.cpu().numpy()
+            seq[prec] = [o[k, :c[k]] for k in range(n)]
+        f32 = [po.siddon_trace(oip, pr, lors[k], float(tof[k]))[0] for k in range(n)]
+        f64 = [po.siddon_trace_f64(oip, pr, lors[k], float(tof[k]))[0] for k in range(n)]
+
+        def differ(a, b):
+            return int(sum(not np.array_equal(x, y) for x, y in zip(a, b)))
+        m, cmp = seq[L.YRTB_MIRROR], seq[L.YRTB_COMPENSATED]
+        out["tof" if tof_on else "non_tof"] = {
+            "rays": n, "mirror_vs_fp32_restatement": differ(m, f32),
+            "mirror_vs_fp64": differ(m, f64), "compensated_vs_fp64": differ(cmp, f64),
+            "compensated_vs_mirror": differ(cmp, m),
+            "mean_crossings": float(np.mean([len(x) for x in m]))}
+    return out
+
+
 RUNNERS = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5,
-           "psf": run_psf, "lrem": run_lrem, "c2mr": run_c2mr}
+           "psf": run_psf, "lrem": run_lrem, "c2mr": run_c2mr, "walks": run_walks}

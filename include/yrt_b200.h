@@ -346,6 +346,19 @@ yrtb_status yrtb_count_crossings(yrtb_projector* h, const yrtb_events* ev,
                                  yrtb_range range, uint32_t* d_out,
                                  yrtb_stream stream);
 
+/* Diagnostics: the walk of every event of the range as the projector's
+ * forward projection visits it, in visit order: for item k (k = 0 ..
+ * count-1 of the range) at most cap (voxel offset within the event's
+ * frame, weight) pairs at d_offsets / d_weights[k * cap ...], and the number
+ * of visits (which may exceed cap) in d_counts[k].  Multi-ray walks list
+ * their rays one after the other.  Offsets are row-major whatever the
+ * projector's image layout.  Pins the voxel index sequence of the walks
+ * against a CPU restatement; no counterpart in the reference. */
+yrtb_status yrtb_trace_walks(yrtb_projector* h, const yrtb_events* ev,
+                             yrtb_range range, uint32_t cap, int32_t* d_offsets,
+                             float* d_weights, uint32_t* d_counts,
+                             yrtb_stream stream);
+
 /* Per-event attenuation factors exp(-0.1 * Siddon(mu-image)).  Replaces the
  * Corrector's ACF precompute (src/recon/Corrector.cpp:601-612,
  * include/yrt-pet/utils/Tools.hpp:98-102). */

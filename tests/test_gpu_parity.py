@@ -199,6 +199,79 @@ def test_siddon_random_vs_oracle(tof):
     assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
 
 
+def _walk_sequences(p, ev, n, cap=512):
+    offs, wts, cnt = p.trace_walks(ev, cap)
+    offs, wts, cnt = offs.cpu().numpy(), wts.cpu().numpy(), cnt.cpu().numpy()
+    assert cnt.max() <= cap
+    return [(offs[k, :cnt[k]], wts[k, :cnt[k]]) for k in range(n)]
+
+
+@pytest.mark.parametrize("tof", [None, (214.0, 5)])
+def test_walk_voxel_sequences_vs_oracle(tof):
+    # The voxel index sequence of every walk, compared directly
+    # (yrtb_trace_walks) with the CPU restatement's (orc_siddon_trace_f32 /
+    # _f64).  Mirror arithmetic: the same sequence as the FP32 walk on every
+    # ray, the non-TOF weights bit-identical, the TOF weights within 2e-6
+    # (device expf).  Compensated arithmetic aims at the FP64 walk: it may
+    # differ from it on no more rays than the mirror walk does, and on the
+    # rays whose sequence matches, each interior weight (a difference of two
+    # FP32 plane-crossing alphas times the LOR length L) is within 8 FP32
+    # ulps of alpha times L (times the TOF kernel's peak with TOF) of FP64,
+    # plus 1e-5 relative.  The first and last segments start or end where
+    # the ray meets the FOV cylinder, a root of a quadratic that the FP32
+    # set-up (the reference's) computes with cancellation near tangency:
+    # they are held to 1e-4 L.  Random LORs plus LORs between opposite
+    # crystals, which run on or near voxel planes.
+    sc_args = SC_ARGS
+    ip_args = (64, 64, 32, 128, 128, 64)
+    osc = po.Scanner(*sc_args)
+    d1, d2 = random_events(sc_args, 3000, 51)
+    opp = np.arange(0, osc.num_dets, 7, dtype=np.uint32)
+    d1 = np.concatenate([d1, opp])
+    d2 = np.concatenate([d2, ((opp // 256) * 256 + (opp % 256 + 128) % 256).astype(np.uint32)])
+    lors, _ = po.lors_from_detpairs(po.scanner_lut(osc), d1, d2)
+    rng = np.random.default_rng(52)
+    tv = rng.normal(0, 300, len(lors)).astype(np.float32) if tof else None
+    oip = po.ImageParams(*ip_args)
+    pr = po.Proj(tof_fwhm_ps=tof[0] if tof else 0.0, tof_n_std=tof[1] if tof else 0)
+    n = len(lors)
+    ev = yrt.DeviceEvents.from_arrays(lor=lors, tof=tv)
+    seqs = {}
+    for prec in (L.YRTB_MIRROR, L.YRTB_COMPENSATED):
+        _, _, p = make(sc_args, ip_args, tof=tof, precision=prec)
+        seqs[prec] = _walk_sequences(p, ev, n)
+    f32 = [po.siddon_trace(oip, pr, lors[k], 0.0 if tv is None else float(tv[k]))
+           for k in range(n)]
+    f64 = [po.siddon_trace_f64(oip, pr, lors[k], 0.0 if tv is None else float(tv[k]))
+           for k in range(n)]
+    for k in range(n):
+        o, w = seqs[L.YRTB_MIRROR][k]
+        assert np.array_equal(o, f32[k][0]), k
+        if tof:
+            np.testing.assert_allclose(w, f32[k][1], rtol=2e-6, atol=0)
+        else:
+            assert np.array_equal(bits(w), bits(f32[k][1])), k
+    differ = {prec: sum(1 for k in range(n) if not np.array_equal(seqs[prec][k][0], f64[k][0]))
+              for prec in seqs}
+    print(f"walks differing from the FP64 walk's sequence ({n} rays, tof={tof}): "
+          f"mirror {differ[L.YRTB_MIRROR]}, compensated {differ[L.YRTB_COMPENSATED]}")
+    assert differ[L.YRTB_COMPENSATED] <= differ[L.YRTB_MIRROR]
+    peak = 1.0
+    if tof:
+        sigma = tof[0] * 0.299792458 / 2 / (2 * np.sqrt(2 * np.log(2)))
+        peak = 1.0 / (np.sqrt(2 * np.pi) * sigma)
+    for k in range(n):
+        o, w = seqs[L.YRTB_COMPENSATED][k]
+        if np.array_equal(o, f64[k][0]) and len(o):
+            length = float(np.linalg.norm(lors[k, 3:].astype(np.float64) -
+                                          lors[k, :3].astype(np.float64)))
+            err = np.abs(w.astype(np.float64) - f64[k][1])
+            bound = 8 * 2.0 ** -24 * length * peak + 1e-5 * np.abs(f64[k][1])
+            bound[[0, -1]] = 1e-4 * length * peak
+            j = int(np.argmax(err - bound))
+            assert err[j] <= bound[j], (k, j, len(o), float(err[j]), float(bound[j]))
+
+
 def test_siddon_image_offset_and_motion_and_frames():
     ip_args = (48, 40, 20, 120, 100, 80)
     sc = yrt.Scanner("t", *SC_ARGS)

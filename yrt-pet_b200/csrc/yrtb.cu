@@ -867,6 +867,46 @@ __global__ void __launch_bounds__(BLOCK, (KIND == K_SIDDON || (KIND == K_SIDDON_
 	}
 }
 
+// Diagnostics: the (offset, weight) visits of each event's walk in walk
+// order, item k of the range at offs/wts[k * cap ...] (at most cap of them),
+// the number of visits in counts[k]; offsets within the event's frame.
+template <int KIND, bool TOF, bool COMP>
+__global__ void __launch_bounds__(kBlock)
+    k_trace(KParams P, Events E, Range R, uint32_t cap, int32_t* __restrict__ offs,
+            float* __restrict__ wts, uint32_t* __restrict__ counts,
+            unsigned long long* err)
+{
+	const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (k >= R.count)
+		return;
+	const uint64_t e = R.start + k * R.stride;
+	const int frame = E.frame ? __ldg(E.frame + e) : 0;
+	float3 p1, p2, n1, n2;
+	if (frame < 0 || frame >= P.g.nt || !fetchEvent(P, E, e, p1, p2, n1, n2))
+	{
+		if (frame >= 0)
+			atomicAdd(err, 1ULL);
+		counts[k] = 0u;
+		return;
+	}
+	const float tofv = TOF ? __ldg(E.tof + e) : 0.f;
+	int32_t* o = offs + k * cap;
+	float* w = wts + k * cap;
+	uint32_t c = 0;
+	auto visit = [&](int off, float wt)
+	{
+		if (c < cap)
+		{
+			o[c] = off;
+			w[c] = wt;
+		}
+		c++;
+	};
+	auto endRay = [] {};
+	projectEvent<KIND, TOF, COMP>(P, p1, p2, n1, n2, tofv, k, true, visit, endRay);
+	counts[k] = c;
+}
+
 // Pass 1 of the deterministic back projection of k_events<OP_BWD / OP_EM>:
 // folds |v_e| * max|w| of every event that pass 2 back-projects into
 // *maxBits.  The EM value v_e is computed exactly as in k_events (same
@@ -3673,6 +3713,33 @@ yrtb_status yrtb_count_crossings(yrtb_projector* h, const yrtb_events* ev,
 	return dispatchEvents<OP_COUNT>(h, ev, range, nullptr,
 	                                reinterpret_cast<float*>(d_out), 1.f, 0.f,
 	                                stream);
+}
+
+yrtb_status yrtb_trace_walks(yrtb_projector* h, const yrtb_events* ev,
+                             yrtb_range range, uint32_t cap, int32_t* d_offsets,
+                             float* d_weights, uint32_t* d_counts,
+                             yrtb_stream stream)
+{
+	yrtb_status s = checkEvents(h, ev, range, true);
+	if (s != YRTB_OK)
+		return s;
+	if (range.count == 0)
+		return YRTB_OK;
+	if (!d_counts || (cap > 0 && (!d_offsets || !d_weights)))
+		return fail(YRTB_ERR_ARGUMENT, "null trace output");
+	YRTB_CUDA(cudaSetDevice(h->device));
+	const Events E = toDev(ev);
+	const Range R{range.start, range.stride, range.count};
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	withConfig(h, [&](auto kind, auto tof, auto comp)
+	{
+		constexpr int K = decltype(kind)::value;
+		k_trace<K, decltype(tof)::value, decltype(comp)::value>
+		    <<<gridAll(R.count), kBlock, 0, st>>>(h->P, E, R, cap, d_offsets, d_weights,
+		                                          d_counts, h->d_err);
+	});
+	YRTB_LAUNCHED();
+	return YRTB_OK;
 }
 
 yrtb_status yrtb_attenuation_factors(yrtb_projector* h, const float* d_mu,

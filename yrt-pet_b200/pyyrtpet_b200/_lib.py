@@ -115,6 +115,8 @@ SIGNATURES = {
     "yrtb_projector_set_launch": ([c_vp, _P(yrtb_launch_config)], ctypes.c_int),
     "yrtb_projector_get_launch": ([c_vp, _P(yrtb_launch_config)], ctypes.c_int),
     "yrtb_projector_set_image_layout": ([c_vp, ctypes.c_int], ctypes.c_int),
+    "yrtb_trace_walks": ([c_vp, _P(yrtb_events), yrtb_range, ctypes.c_uint32, c_vp, c_vp,
+                          c_vp, c_vp], ctypes.c_int),
     "yrtb_projector_get_image_layout": ([c_vp, _P(ctypes.c_int)], ctypes.c_int),
     "yrtb_image_convert_layout": ([c_vp, c_vp, _P(yrtb_image_params), ctypes.c_int, c_vp],
                                   ctypes.c_int),

@@ -863,6 +863,21 @@ class DeviceProjector:
                                              out.data_ptr(), _stream()))
         return out
 
+    def trace_walks(self, ev: DeviceEvents, cap: int = 1024, rng=None):
+        """Visits of each event's forward walk (yrtb_trace_walks): (offsets
+        int32 [n, cap], weights float32 [n, cap], counts int32 [n]); row k
+        holds the first counts[k] (at most cap) visits of item k in visit
+        order."""
+        r = rng or L.yrtb_range(0, 1, 0)
+        n = ev.count if r.count == 0 else int(r.count)
+        offs = torch.zeros((n, cap), dtype=torch.int32, device="cuda")
+        wts = torch.zeros((n, cap), dtype=torch.float32, device="cuda")
+        cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
+        L.check(L.lib().yrtb_trace_walks(self.h, ctypes.byref(ev.c()), r, int(cap),
+                                         offs.data_ptr(), wts.data_ptr(), cnt.data_ptr(),
+                                         _stream()))
+        return offs, wts, cnt
+
     def attenuation_factors(self, mu: torch.Tensor, mu_params: ImageParams,
                             ev: DeviceEvents, out=None, rng=None):
         if out is None:
