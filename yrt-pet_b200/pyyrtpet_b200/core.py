@@ -869,7 +869,8 @@ class DeviceProjector:
         holds the first counts[k] (at most cap) visits of item k in visit
         order."""
         r = rng or L.yrtb_range(0, 1, 0)
-        n = ev.count if r.count == 0 else int(r.count)
+        stride = max(1, int(r.stride))
+        n = int(r.count) if r.count else max(0, (ev.count - int(r.start) + stride - 1) // stride)
         offs = torch.zeros((n, cap), dtype=torch.int32, device="cuda")
         wts = torch.zeros((n, cap), dtype=torch.float32, device="cuda")
         cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
