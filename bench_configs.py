@@ -92,6 +92,44 @@ def _rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+def _roofline(launch, alg_bytes, kernel, per_unit, reps=5):
+    """Roofline of the dominant kernel of a configuration: its algorithmic
+    bytes per launch (alg_bytes, stated by the caller from the per-unit
+    figures in per_unit) over its CUDA-event time on the launching stream
+    (median of reps launches after two warm-up launches), against the HBM
+    peak (measured, else the fallback, as bench.py)."""
+    import bench
+    for _ in range(2):
+        launch()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    ts = []
+    for _ in range(reps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        launch()
+        b.record(st)
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    ms = float(np.median(ts))
+    peak, kind = bench.measured_peak_hbm()
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": kind, "traffic": None,
+            "kernel": kernel, "alg_bytes_per_launch": float(alg_bytes),
+            "alg_bytes_per_unit": per_unit, "kernel_ms_per_launch": ms}
+
+
+def _visits(proj, ev, rng=None):
+    """Voxel visits (crossings or footprint voxels, all rays) of the events
+    of rng, and the number of those events."""
+    c = proj.count_crossings(ev, rng).double()
+    if rng is None or rng.count == 0:
+        return float(c.sum().item()), int(ev.count)
+    return float(c.sum().item()), int(rng.count)
+
+
 def _base(cfg, metric, value, unit, steps, warmup, ms, config):
     return {"metric": metric, "value": value, "unit": unit, "n_gpus": 1,
             "steps": steps, "warmup": warmup, "ms_per_step": ms,
@@ -145,6 +183,22 @@ def run_c1(args):
                  "launch": osem.launchConfig})
     out["sens_image_ms"] = ts.ms
     out["sens_bins"] = int(yrt.Histogram3D(sc).count())
+    # Roofline of the fused EM kernel over subset 0 (the reconstruction's own
+    # projector parameters, launch configuration and event order).
+    rp = yrt.DeviceProjector(sc, ip, osem.projectorParams)
+    rp.set_launch(**osem.launchConfig)
+    dev = yrt.DeviceEvents.from_arrays(torch.from_numpy(e["d1"].view(np.int32)).cuda(),
+                                       torch.from_numpy(e["d2"].view(np.int32)).cuda())
+    dev, offs = rp.order_events(dev, 5)
+    r0 = L.yrtb_range(int(offs[0]), 1, int(offs[1] - offs[0]))
+    nv, ne = _visits(rp, dev, r0)
+    x0 = torch.full((ip.numVoxels,), 0.125, device="cuda")
+    em0 = torch.zeros_like(x0)
+    out["roofline"] = _roofline(
+        lambda: rp.em_step(x0, em0, dev, rng=r0), 8 * ne + 12 * nv,
+        "k_events<OP_EM, K_SIDDON, mirror> (fused fwd->ratio->bwd, subset 0)",
+        {"per_event": "8 B (d1, d2)", "per_crossing": "12 B (4 B gather, 8 B reduction)",
+         "events": ne, "crossings": nv})
     po = _po()
     if po.ref_available() and not args.no_cpu_baseline:
         osc = _po_scanner(po, sc)
@@ -276,6 +330,17 @@ def run_c5(args):
                             "frame, file order, interleaved subsets)"}
     out["batched_over_plain"] = ms_p / ms_b
     out["frame_events"] = [int(c) for c in counts]
+    # Roofline of the batched EM kernel over subset 0 (all frames' events).
+    r0 = L.yrtb_range(int(offs[0]), 1, int(offs[1] - offs[0]))
+    nv, ne = _visits(proj, ordered, r0)
+    x0 = torch.full((nt * J,), 0.125, device="cuda")
+    em0 = torch.zeros_like(x0)
+    out["roofline"] = _roofline(
+        lambda: proj.em_step(x0, em0, ordered, rng=r0), 20 * ne + 12 * nv,
+        "k_events<OP_EM, K_SIDDON, TOF, compensated> over all 24 frames (subset 0)",
+        {"per_event": "20 B (d1, d2, TOF, frame, motion frame)",
+         "per_crossing": "12 B (4 B gather, 8 B reduction)", "events": ne,
+         "crossings": nv})
     if not args.no_cpu_baseline:
         out.update(_c5_reference(args, sc, ip1, nt, subsets, counts, d1, d2, ev.tof,
                                  motion, sens, n / (ms_b * 1e-3)))
@@ -425,6 +490,22 @@ def run_c3(args):
     out["binning"] = {"events_per_s": total / (bin_ms * 1e-3), "ms": bin_ms}
     out["sens_images_ms"] = ts.ms
     out["osem_s_per_iteration"] = ms * 1e-3
+    # Roofline of the histogram EM kernel over subset 0's list of non-zero
+    # bins (the reconstruction's projector parameters).
+    rp = yrt.DeviceProjector(sc, ip, osem.projectorParams)
+    it = yrt.BinIteratorRangeHistogram3D(h.numZBin, h.numPhi, h.numR, 12, 0)
+    bins0 = rp.histo3d_subset_nonzero(hist, 12, 0, it.size())
+    glob = it.indices()[bins0.cpu().numpy()].astype(np.uint64)
+    pa, pb = yrt.histo3d_detpairs(sc, glob)
+    nv, nb = _visits(rp, yrt.DeviceEvents.from_arrays(pa, pb))
+    x0 = torch.full((ip.numVoxels,), 0.125, device="cuda")
+    em0 = torch.zeros_like(x0)
+    out["roofline"] = _roofline(
+        lambda: rp.em_step_histo3d(x0, em0, hist, 12, 0, bins=bins0), 12 * nb + 12 * nv,
+        "k_histo<K_DD_PSF, EM, compensated, 4 threads per bin> (subset 0's non-zero bins)",
+        {"per_bin": "12 B (measurement, list entry)",
+         "per_footprint_voxel": "12 B (4 B gather, 8 B reduction)", "bins": nb,
+         "footprint_voxels": nv})
     po = _po()
     if po.ref_available() and not args.no_cpu_baseline:
         osc = _po_scanner(po, sc)
@@ -508,6 +589,18 @@ def run_c4(args):
     out["composed"] = {"value": per * 8 / (ms_c * 1e-3), "ms_per_step": ms_c,
                        "what": "SiddonProjectFn forward kernel + torch FP64 reductions + "
                                "adjoint kernel in backward"}
+    # Roofline of the fused pass of one phantom (loss terms and gradient).
+    ev0 = evs[0]
+    x0 = x[0].detach().contiguous()
+    em0 = torch.zeros_like(x0)
+    model = torch.empty(ev0.count, device="cuda")
+    nv, ne = _visits(proj, ev0)
+    out["roofline"] = _roofline(
+        lambda: proj.em_step(x0, em0, ev0, model=model), 16 * ne + 12 * nv,
+        "k_events<OP_EM, K_SIDDON, TOF, compensated> writing the model (one phantom)",
+        {"per_event": "16 B (d1, d2, TOF, model value)",
+         "per_crossing": "12 B (4 B gather, 8 B reduction)", "events": ne,
+         "crossings": nv})
     po = _po()
     if po.ref_available() and not args.no_cpu_baseline:
         # The reference CPU forward + back projection (util::forwProject /
@@ -845,6 +938,19 @@ def run_c2mr(args):
                 one()
             times.append(t.ms)
         ms[(rays, lanes)] = float(np.median(times))
+        if rays == 4 and lanes == 4:
+            # Roofline of the 4-ray EM kernel over subset 0.
+            r0 = L.yrtb_range(int(offs[0]), 1, int(offs[1] - offs[0]))
+            nv, ne = _visits(proj, ev, r0)
+            x0 = torch.full((J,), 0.125, device="cuda")
+            em0 = torch.zeros_like(x0)
+            roof = _roofline(
+                lambda: proj.em_step(x0, em0, ev, rng=r0), 24 * ne + 12 * nv,
+                "k_events<OP_EM, K_SIDDON_MR, TOF, compensated, one lane per ray> (subset 0)",
+                {"per_event": "24 B (d1, d2, TOF, sens, att, additive)",
+                 "per_crossing": "12 B (4 B gather, 8 B reduction), 4 rays",
+                 "events": ne, "crossings": nv})
+            del x0, em0
         del ev, img, work
     out = _base("C2 list-mode TOF OSEM iteration with 4-ray Siddon, 80x672 scanner "
                 "R=410, 256x256x160 @2mm, 214 ps TOF 5 sigma, 10 subsets",
@@ -859,6 +965,7 @@ def run_c2mr(args):
                                    "ms_per_step": ms[(4, 1)],
                                    "what": "4 rays walked in turn by one thread per event"}
     out["cost_vs_single_ray"] = ms[(4, 4)] / ms[(1, 1)]
+    out["roofline"] = roof
     out["launch"] = proj4.get_launch()
     out["multiray_table_ms"] = table_ms
     # FP64 parity of the 4-ray forward projections on a sample, with the
