@@ -76,6 +76,9 @@ def parse():
                     help="write every autotuner candidate and its time (JSON)")
     ap.add_argument("--deterministic", action="store_true",
                     help="two-pass fixed-point back projection")
+    ap.add_argument("--vector-groups", type=int, default=-1,
+                    help="force the launch's vector_groups after autotuning "
+                         "(default: the autotuner's choice)")
     ap.add_argument("--layout", default="row", choices=["tile", "row"],
                     help="image layout of the timed EM passes: 4x2 tiles "
                          "(YRTB_LAYOUT_TILE_4X2) or the reference's row-major")
@@ -592,6 +595,8 @@ def main():
         if args.tune_report and rank == 0:
             with open(args.tune_report, "w") as f:
                 json.dump(tune, f, indent=1)
+    if args.vector_groups >= 0:
+        proj.set_launch(**dict(proj.get_launch(), vector_groups=args.vector_groups))
     launch = proj.get_launch()
 
     # Plain form: events in file order, subset = interleaved stride (the
@@ -825,10 +830,14 @@ def main():
         l2 = {"peak_requests_per_s": rates,
               "peak_source": "measured live (libyrtb_l2bench.so: random aligned groups "
                              "in an L2-resident buffer of the image's size)"}
-        cnt = json.load(open(l2prof))
+        # ncu request counts per event, one entry per launch configuration
+        # they were taken with; the first entry that matches this run's.
+        entries = json.load(open(l2prof))["entries"]
         launch = dict(proj.get_launch(), image_layout=(L.YRTB_LAYOUT_TILE_4X2 if tiled
                                                        else L.YRTB_LAYOUT_ROW_MAJOR))
-        if all(launch.get(k) == v for k, v in cnt["launch"].items()):
+        cnt = next((c for c in entries
+                    if all(launch.get(k) == v for k, v in c["launch"].items())), None)
+        if cnt is not None:
             reqs = (cnt["red_requests_per_event"] + cnt["read_requests_per_event"]) \
                 * ev.count / SUBSETS
             l2["requests_per_launch"] = reqs
@@ -841,8 +850,9 @@ def main():
             roofline["l2_frac"] = l2["achieved_requests_per_s"] / mix
         else:
             l2["requests_per_launch"] = None
-            l2["requests_source"] = ("ncu counts were taken with launch "
-                                     f"{cnt['launch']}, this run chose {launch}")
+            l2["requests_source"] = ("ncu counts were taken with launches "
+                                     f"{[c['launch'] for c in entries]}, this run "
+                                     f"chose {launch}")
         roofline["l2"] = l2
 
     cpu = None

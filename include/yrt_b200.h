@@ -204,9 +204,10 @@ typedef struct
 	                         float4 groups (consecutive x steps reuse the group held in
 	                         registers); bit 1: they send the contributions to one group as a
 	                         single red.global.add.v4.f32, summed in registers; bit 2: the
-	                         same with the group staged in shared memory (wins over bit 1).
-	                         Images must be 16-byte aligned with a multiple of 4 voxels per
-	                         frame, else scalar accesses are used */
+	                         same with the group staged in shared memory (wins over bit 1);
+	                         bit 3: pairs of voxels sent as one red.global.add.v2.f32 (bits 1
+	                         and 2 win over it).  Images must be 16-byte aligned with a
+	                         multiple of 4 voxels per frame, else scalar accesses are used */
 } yrtb_launch_config;
 
 yrtb_status yrtb_projector_set_launch(yrtb_projector* h,

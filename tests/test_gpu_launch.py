@@ -47,7 +47,8 @@ def random_events(n, seed):
     return d1[ok][:n], d2[ok][:n]
 
 
-CONFIGS = [(b, t, v) for b in (128, 256) for t in (1, 2, 4) for v in (3, 2, 1, 0, 4, 5)
+CONFIGS = [(b, t, v) for b in (128, 256) for t in (1, 2, 4)
+           for v in (3, 2, 1, 0, 4, 5, 8, 9)
            if not (t > 1 and v != 0)]
 
 
@@ -76,6 +77,12 @@ def test_every_launch_config_vs_oracle(tof):
                                   "vector_groups": vec}
         v = p.forward(gimg, ev).cpu().numpy()
         b = p.backward(gy, ev).cpu().numpy()
+        # The fused EM pass in every vector mode (float4 gathers, float4 or
+        # float2 reductions): the same image up to the FP32 atomics' order.
+        em = p.em_step(gimg, torch.zeros(ip.shape, device="cuda"), ev).cpu().numpy()
+        if base is None:
+            em0 = em
+        assert rel_l2(em, em0) < 1e-5, (block, tpl, vec)
         assert rel_l2(v, f64) < 1e-5, (block, tpl)
         assert rel_l2(b, b64) < 1e-4, (block, tpl)
         lhs = float(np.dot(v.astype(np.float64), y))
@@ -104,7 +111,7 @@ def test_threads_per_lor_needs_compensated_mode():
     with pytest.raises(yrt.YrtbError, match="tile_shift"):
         p.set_launch(256, 1, 3, order=1, tile_shift=5)
     with pytest.raises(yrt.YrtbError, match="vector_groups"):
-        p.set_launch(256, 1, 3, vector_groups=8)
+        p.set_launch(256, 1, 3, vector_groups=16)
 
 
 @pytest.mark.parametrize("shift,order,tile", [(0, 0, 1), (2, 0, 1), (5, 0, 1),
@@ -155,9 +162,9 @@ def test_autotune_keeps_fastest_and_reconstruction_matches():
         reports.append(osem.lastTuneReport)
     rep = reports[1]
     assert 0 < rep["sample_events"] <= (len(e["d1"]) + 2) // 3
-    # 3 bucket shifts x 3 orders x 4 vector-group modes, then 2 blocks x
+    # 3 bucket shifts x 3 orders x 5 vector-group modes, then 2 blocks x
     # 3 threads/LOR minus the stage-1 shape.
-    assert len(rep["tried"]) == 3 * 3 * 4 + 2 * 3 - 1
+    assert len(rep["tried"]) == 3 * 3 * 5 + 2 * 3 - 1
     best_ms = min(ms for _, ms in rep["tried"])
     assert [c for c, ms in rep["tried"] if ms == best_ms][0] == rep["best"]
     assert rel_l2(outs[1], outs[0]) < 1e-5

@@ -580,10 +580,20 @@ __device__ __forceinline__ void redV4(float* p, float4 v)
 	             :: "l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
 }
 
+// The same for an aligned pair of voxels (8-byte aligned p).
+__device__ __forceinline__ void redV2(float* p, float2 v)
+{
+	asm volatile("red.global.add.v2.f32 [%0], {%1, %2};"
+	             :: "l"(p), "f"(v.x), "f"(v.y) : "memory");
+}
+
 // VEC 1: the group is summed in registers; VEC 2: the group's four values
 // are staged in this thread's shared-memory slots (vslot[l * vstride]; a
 // single-ray walk visits each voxel once, so a slot is written at most once
-// per group) and read back only to send the group.
+// per group) and read back only to send the group; VEC 3: pairs of voxels
+// instead of groups of four, held in registers and sent as one
+// red.global.add.v2.f32 (more requests than VEC 1, fewer instructions per
+// visit).
 template <int KIND, bool TOF, bool COMP, bool FIX = false, int VEC = 0,
           bool TILE = false>
 __device__ __forceinline__ void backwardEvent(const KParams& P,
@@ -673,6 +683,33 @@ __device__ __forceinline__ void backwardEvent(const KParams& P,
 		{
 			if (gb >= 0)
 				redV4(img + gb, a4);
+			gb = -1;
+		};
+		projectEvent<KIND, TOF, COMP, TILE>(P, p1, p2, n1, n2, tofv, rid, false, visit,
+		                                    flush, part, parts);
+	}
+	else if constexpr (VEC == 3)
+	{
+		static_assert(KIND == K_SIDDON, "lanes hold one value per voxel of one ray");
+		int gb = -1;
+		float2 a2 = make_float2(0.f, 0.f);
+		auto visit = [&](int o, float w)
+		{
+			const float c = v * w;
+			const int g = o & ~1;
+			const bool nw = g != gb;
+			if (nw && gb >= 0)
+				redV2(img + gb, a2);
+			gb = g;
+			// Set, never summed, inside a pair (cleared when a new one starts).
+			const bool hi = (o & 1) != 0;
+			a2.x = hi ? (nw ? 0.f : a2.x) : c;
+			a2.y = hi ? c : (nw ? 0.f : a2.y);
+		};
+		auto flush = [&]
+		{
+			if (gb >= 0)
+				redV2(img + gb, a2);
 			gb = -1;
 		};
 		projectEvent<KIND, TOF, COMP, TILE>(P, p1, p2, n1, n2, tofv, rid, false, visit,
@@ -775,8 +812,9 @@ __global__ void __launch_bounds__(BLOCK, ((KIND == K_SIDDON && COMP) ||
 	const uint64_t gt = static_cast<uint64_t>(blockIdx.x) * BLOCK + threadIdx.x;
 	const uint64_t k = gt / TPL;
 	const int part = static_cast<int>(gt % TPL);
-	// Shared-memory slots of the staged float4 reductions (VEC bit 2).
-	constexpr int kRedMode = (VEC & 4) ? 2 : ((VEC & 2) ? 1 : 0);
+	// Shared-memory slots of the staged float4 reductions (VEC bit 2); VEC
+	// bit 3: float2 pair reductions.
+	constexpr int kRedMode = (VEC & 4) ? 2 : ((VEC & 2) ? 1 : ((VEC & 8) ? 3 : 0));
 	float* vslot = nullptr;
 	if constexpr (kRedMode == 2)
 	{
@@ -2708,14 +2746,17 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 		if constexpr (TPL == 1 || K == K_SIDDON_MR)
 		{
 			// Bit 0: float4 gathers (forward); bit 1: float4 reductions summed
-			// in registers, bit 2: staged in shared memory (back projection,
-			// bit 2 wins).  Each op instantiates only the modes it uses;
-			// multi-ray walks use the register reductions only.
+			// in registers, bit 2: staged in shared memory, bit 3: float2
+			// pair reductions (back projection; bit 2 wins over bit 1, both
+			// over bit 3).  Each op instantiates only the modes it uses;
+			// multi-ray walks use the register float4 reductions only.
 			constexpr int kUse = K == K_SIDDON_MR ? (OP == OP_FWD ? 0 : 2)
-			                                      : (OP == OP_FWD ? 1 : (OP == OP_BWD ? 6 : 7));
+			                                      : (OP == OP_FWD ? 1 : (OP == OP_BWD ? 14 : 15));
 			int vg = aligned ? (h->launch.vector_groups & kUse) : 0;
 			if (vg & 4)
 				vg &= ~2;
+			if (vg & 6)
+				vg &= ~8;
 			if (vg != 0)
 			{
 				auto vlaunch = [&](auto vc)
@@ -2731,7 +2772,9 @@ void launchTuned(const yrtb_projector* h, const Events& E, Range R,
 				case 2: vlaunch(std::integral_constant<int, 2>{}); break;
 				case 3: vlaunch(std::integral_constant<int, 3>{}); break;
 				case 4: vlaunch(std::integral_constant<int, 4>{}); break;
-				default: vlaunch(std::integral_constant<int, 5>{}); break;
+				case 5: vlaunch(std::integral_constant<int, 5>{}); break;
+				case 8: vlaunch(std::integral_constant<int, 8>{}); break;
+				default: vlaunch(std::integral_constant<int, 9>{}); break;
 				}
 				return;
 			}
@@ -3360,8 +3403,8 @@ yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
 		            "order must be YRTB_ORDER_LOR, YRTB_ORDER_SPATIAL or YRTB_ORDER_SPATIAL_FINE");
 	if (c->tile_shift < 0 || c->tile_shift > 4)
 		return fail(YRTB_ERR_ARGUMENT, "tile_shift must be in 0..4");
-	if (c->vector_groups < 0 || c->vector_groups > 7)
-		return fail(YRTB_ERR_ARGUMENT, "vector_groups must be in 0..7");
+	if (c->vector_groups < 0 || c->vector_groups > 15)
+		return fail(YRTB_ERR_ARGUMENT, "vector_groups must be in 0..15");
 	h->launch = *c;
 	return YRTB_OK;
 }
@@ -4879,9 +4922,9 @@ yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
 	                          {YRTB_ORDER_SPATIAL, 2}};
 	for (int shift : {3, 4, 5})
 		for (const auto& ot : orders)
-			for (int vec : {2, 4, 1, 0})
+			for (int vec : {2, 8, 4, 1, 0})
 			{
-				if (multiRay && (vec == 4 || vec == 1))
+				if (multiRay && (vec == 4 || vec == 1 || vec == 8))
 					continue;
 				yrtb_launch_config c = saved;
 				c.threads_per_lor = multiRay ? saved.threads_per_lor : 1;
