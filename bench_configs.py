@@ -907,6 +907,8 @@ def run_c2mr(args):
         if rays == 4:
             cfg = proj.get_launch()
             cfg["threads_per_lor"] = lanes
+            if lanes > 1 and getattr(args, "vector_groups", -1) >= 0:
+                cfg["vector_groups"] = args.vector_groups
             proj.set_launch(**cfg)
         if rays == 4 and lanes == 4:
             proj4 = proj

@@ -206,8 +206,11 @@ typedef struct
 	                         single red.global.add.v4.f32, summed in registers; bit 2: the
 	                         same with the group staged in shared memory (wins over bit 1);
 	                         bit 3: pairs of voxels sent as one red.global.add.v2.f32 (bits 1
-	                         and 2 win over it).  Images must be 16-byte aligned with a
-	                         multiple of 4 voxels per frame, else scalar accesses are used */
+	                         and 2 win over it).  Multi-ray walks use bits 1 and 3 (each ray's
+	                         group or pair sent at the end of the ray; default 8 with one
+	                         lane per ray, else 2).  Images must be
+	                         16-byte aligned with a multiple of 4 voxels per frame, else
+	                         scalar accesses are used */
 } yrtb_launch_config;
 
 yrtb_status yrtb_projector_set_launch(yrtb_projector* h,
@@ -269,14 +272,15 @@ typedef struct
  * projector over a sample of the events -- subset 0 of num_subsets
  * interleaved subsets, at most max_sample events -- in two stages: first
  * 9 event orders (bucket_shift x order x tile_shift, the sample ordered
- * with each) x 4 vector_groups modes with the current block size and one
- * thread per LOR, then every block size x threads per LOR the projector admits on
- * the fastest of those.
+ * with each) x 5 vector_groups modes (2, 8, 4, 1, 0) with the current block
+ * size and one thread per LOR (a multi-ray projector: modes 2, 8 and 0 with
+ * its lanes per event), then every block size x threads per LOR the
+ * projector admits on the fastest of those.
  * Keeps the fastest (yrtb_projector_set_launch) and reports all timings.  d_image: the image
  * the EM steps read (nx*ny*nz*nt floats; its values do not change the work).
  * Setup-time call: allocates temporaries and synchronises the stream, so it
- * must not run under stream capture.  Projectors other than single-ray
- * Siddon keep the default configuration (num_tried = 0). */
+ * must not run under stream capture.  Projectors other than Siddon
+ * (single or multi-ray) keep the default configuration (num_tried = 0). */
 yrtb_status yrtb_autotune(yrtb_projector* h, const float* d_image,
                           const yrtb_events* ev, int num_subsets,
                           uint64_t max_sample, yrtb_tune_report* report,

@@ -364,7 +364,8 @@ def test_multiray_one_lane_per_ray_matches_one_thread(tof, prec, rays):
     # the default with a table of offsets) adds the rays' forward sums in ray
     # order, as one thread walking the rays in turn does: the forward
     # projections are bit-identical; back projection and EM image equal up
-    # to the order of the FP32 atomics.  Without a table covering the call,
+    # to the order of the FP32 atomics, in each reduction mode the lanes use
+    # (scalar, float4 groups, pairs).  Without a table covering the call,
     # the projector falls back to one thread per event.
     sc, ip, p = make(num_rays=rays, tof=tof, precision=prec)
     d1, d2 = random_events(SC_ARGS, 6000, 33)
@@ -379,15 +380,18 @@ def test_multiray_one_lane_per_ray_matches_one_thread(tof, prec, rays):
     p.multiray_table(len(d1))
     cfg = p.get_launch()
     out = {}
-    for tpl in (1, lanes):
+    for tpl, vg in ((1, 0), (lanes, 0), (lanes, 2), (lanes, 8)):
         cfg["threads_per_lor"] = tpl
+        cfg["vector_groups"] = vg
         p.set_launch(**cfg)
-        out[tpl] = (p.forward(img, ev), p.backward(y, ev),
-                    p.em_step(img, torch.zeros(ip.shape, device="cuda"), ev))
-    assert torch.equal(out[1][0], v_gen)
-    assert torch.equal(out[lanes][0], out[1][0])
-    assert rel_l2(out[lanes][1].cpu().numpy(), out[1][1].cpu().numpy()) < 1e-6
-    assert rel_l2(out[lanes][2].cpu().numpy(), out[1][2].cpu().numpy()) < 1e-6
+        out[tpl, vg] = (p.forward(img, ev), p.backward(y, ev),
+                        p.em_step(img, torch.zeros(ip.shape, device="cuda"), ev))
+    base = out[1, 0]
+    assert torch.equal(base[0], v_gen)
+    for key, o in out.items():
+        assert torch.equal(o[0], base[0]), key
+        assert rel_l2(o[1].cpu().numpy(), base[1].cpu().numpy()) < 1e-6, key
+        assert rel_l2(o[2].cpu().numpy(), base[2].cpu().numpy()) < 1e-6, key
     with pytest.raises(RuntimeError):
         cfg["threads_per_lor"] = 2 * lanes
         p.set_launch(**cfg)
