@@ -216,7 +216,12 @@ struct SiddonWalker
 	// crossing equals the minimum).  Written with selects instead of
 	// branches so that the threads of a warp, whose rays step along
 	// different axes, stay converged; every value is the one the branchy
-	// formulation computes.
+	// formulation computes.  Each axis's next crossing is recomputed as
+	// (plane - p1) * inv whether it stepped or not: an axis that did not
+	// step keeps its plane, so the product has the bits it had (the first
+	// crossing is that product too), and no select of the old value is
+	// needed.  An axis the ray runs parallel to has inv = +inf and a plane
+	// above p1, so its crossing stays +inf.
 	__device__ __forceinline__ void advance()
 	{
 		const float ax = ax_next, ay = ay_next, az = az_next;
@@ -224,16 +229,12 @@ struct SiddonWalker
 		sx = ax == m;
 		sy = ay == m;
 		sz = az == m;
-		const float xn = x_cur + fdx, yn = y_cur + fdy, zn = z_cur + fdz;
-		const float axn = (xn - p1.x) * inv_x;
-		const float ayn = (yn - p1.y) * inv_y;
-		const float azn = (zn - p1.z) * inv_z;
-		x_cur = sx ? xn : x_cur;
-		y_cur = sy ? yn : y_cur;
-		z_cur = sz ? zn : z_cur;
-		ax_next = sx ? axn : ax_next;
-		ay_next = sy ? ayn : ay_next;
-		az_next = sz ? azn : az_next;
+		x_cur = sx ? x_cur + fdx : x_cur;
+		y_cur = sy ? y_cur + fdy : y_cur;
+		z_cur = sz ? z_cur + fdz : z_cur;
+		ax_next = (x_cur - p1.x) * inv_x;
+		ay_next = (y_cur - p1.y) * inv_y;
+		az_next = (z_cur - p1.z) * inv_z;
 		a_next = fminf(m, amax);
 	}
 
@@ -396,6 +397,28 @@ struct SiddonWalker
 		ax_next = flat_x ? 3.402823466e+38f : firstPlane(p1.x, p2.x, inv_x, dir_x, dx, x_cur);
 		ay_next = flat_y ? 3.402823466e+38f : firstPlane(p1.y, p2.y, inv_y, dir_y, dy, y_cur);
 		az_next = flat_z ? 3.402823466e+38f : firstPlane(p1.z, p2.z, inv_z, dir_z, dz, z_cur);
+		// Parallel axes: crossings at +inf from here on (advance), planes one
+		// voxel above p1 (their direction is +1), which no step brings back.
+		// Both compare above every crossing of the other axes and above
+		// amax <= 1, as the FLT_MAX above does.
+		{
+			const float inf = __int_as_float(0x7f800000);
+			if (flat_x)
+			{
+				inv_x = inf;
+				x_cur = p1.x + dx;
+			}
+			if (flat_y)
+			{
+				inv_y = inf;
+				y_cur = p1.y + dy;
+			}
+			if (flat_z)
+			{
+				inv_z = inf;
+				z_cur = p1.z + dz;
+			}
+		}
 
 		nx = g.nx;
 		ny = g.ny;
